@@ -1,0 +1,359 @@
+"""Benchmark of the B200 SIMPLEC outer iteration (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2] [--impl ours|reference]
+
+Metric: SIMPLEC cell-iterations/s (cells x outer iterations / device time of ``step()``).
+A "step" is one outer iteration of the hot path over the workload's mesh. Workload (default):
+the 2-D cavity on a 256 x 256 quad grid cut into 131,072 triangles along alternating
+diagonals, interior nodes jittered by +-0.2h (seed 0), Re 1000, linear-upwind convection with
+non-orthogonal correction, aggregation-AMG pressure solve, FP64 (synthetic mesh and fields).
+
+Timed region: W untimed warm-up steps (the first builds the AMG hierarchy), then exactly K
+steps, each bracketed by CUDA events on the solver's stream; L2 is flushed (a 512 MiB write)
+between timed steps, outside the events. ``value`` sums the K step times; with N > 1 every
+rank runs an independent replica (the path does not shard: replicas only), the time is the
+max over ranks and ``value`` the aggregate. ``e2e`` is the same metric through the public API
+from host data: constructing ``SimpleSolver`` from the host mesh (its host->device copies),
+W + K steps (each reads its residual report back) and the final ``fields()`` read.
+
+``--impl reference`` times the reference's CPU path on this box's cores: the oracle driver
+with the reference's own C++/OpenMP kernels (built from its sources into ``oracle/_ref``) or,
+without that library, the NumPy oracle; rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SIMPLEC cell-iters/s to 1e-6 residual vs plain FP64 GPU path; HBM % of peak"
+UNIT = "cell-iters/s"
+
+
+# ---------------------------------------------------------------------------------- workloads
+def make_workload(name):
+    import numpy as np
+
+    from gputest_b200.mesh.unstructured import box_mesh_3d, cartesian_mesh_2d
+    from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase
+
+    if name == "c1":
+        mesh = cartesian_mesh_2d(64, 64)
+        case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=[1.0, 0.0])}, viscosity=0.01,
+                                scheme="upwind", pressure_tol=1e-8, max_iter=300, tol=1e-6)
+        desc = {"workload": "cavity 64x64 quads (4,096 cells), Re 100, upwind, PCG 1e-8", "cells": mesh.n_cells}
+        return mesh, case, desc, None
+    if name == "c2":
+        mesh = cartesian_mesh_2d(256, 256, triangulate="alternating", jitter=0.2, seed=0)
+        case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=[1.0, 0.0])}, viscosity=1e-3,
+                                scheme="second-order", max_iter=100000, tol=1e-6)
+        desc = {"workload": "cavity 256x256 alternating-diagonal triangles (131,072 cells), jitter 0.2h seed 0, "
+                            "Re 1000, linear-upwind + non-orthogonal correction, SA-AMG PCG", "cells": mesh.n_cells}
+        return mesh, case, desc, None
+    if name == "c3":
+        names = ("inlet", "outlet", "wall", "wall", "wall", "wall")
+        mesh = box_mesh_3d(128, 64, 64, 4.0, 1.0, 1.0, jitter=0.1, seed=1, names=names,
+                           types=("velocity-inlet", "pressure-outlet", "wall", "wall", "wall", "wall"))
+        mu = 1.0 / 500.0
+        case = UnstructuredCase(boundaries={"inlet": BoundarySpec("inlet", velocity=[1.0, 0.0, 0.0], value=0.0),
+                                            "outlet": BoundarySpec("outlet", pressure=0.0),
+                                            "wall": BoundarySpec("wall", thermal="flux", value=5e3)},
+                                viscosity=mu, energy=True, cp=1.0, conductivity=mu / 0.71, max_iter=100000, tol=1e-6)
+
+        def inlet(solver):
+            z = mesh.zone_by_name("inlet")
+            fc = solver.fv.host.xfb[solver.fv.host.bzone == z.id]
+            u = 36.0 * fc[:, 1] * (1 - fc[:, 1]) * fc[:, 2] * (1 - fc[:, 2])
+            solver.set_boundary_velocity("inlet", np.stack([u, 0 * u, 0 * u], axis=1))
+            solver.initialize({})
+
+        desc = {"workload": "3-D duct 4x1x1, 128x64x64 hexes (524,288 cells), jitter 0.1h seed 1, parabolic inlet "
+                            "Re 500, heated walls 5e3 W/m2, Pr 0.71, FP64", "cells": mesh.n_cells}
+        return mesh, case, desc, inlet
+    raise SystemExit(f"unknown config {name!r}")
+
+
+# ---------------------------------------------------------------------------------- byte models
+def stage_bytes(solver, stage, step_info):
+    """Algorithmic DRAM bytes of one launch of a stage: every array the stage's kernels read
+    or write, counted once per pass over it (FP64 values 8 B, indices 4 B)."""
+    fv = solver.fv
+    nc, nf, nb, d, nnz = fv.nc, fv.n_if, fv.n_bf, fv.dim, fv.nnz
+    csr = nnz * 12 + (nc + 1) * 4
+    face_topo = nf * 4 * 3 + (nc + 1) * 8 + nf * 4  # fP, fN, forig, own/nei ptr, nei_face
+    if stage == "momentum_assembly":
+        faces = face_topo + nf * 8 * (2 + 3 * d) + nf * 4 * 2  # alpha, F, w, Tv, dPf, dNf, slot_PN/NP
+        cells = nc * 8 * (d + d * d + d + 1) + nc * 8 * (3 + 2 * d) + nc * 4 * 2  # U, gU, gp, vol; outputs; slot_diag, bptr
+        bnd = nb * 8 * (3 + d) + nb * 4
+        return faces + cells + bnd + csr + nnz * 8  # CSR read for the residual, values written
+    if stage == "pressure_assembly":
+        faces = face_topo + nf * 8 * (3 + 2 * d) + nf * 8 * 2 + nf * 4 * 2  # w, alpha, S, d; Fst, cf out; slots
+        cells = nc * 8 * (d + 1 + d + 1) + nc * 8 * 2 + nnz * 8
+        bnd = nb * 8 * (4 + 3 * d) + nb * 4
+        return faces + cells + bnd
+    if stage == "momentum_solve":
+        its = max(step_info["momentum_iters"])
+        k = d
+        init = csr + nc * 8 * k * 6
+        per_it = 2 * (csr + nc * 8 * k * 2) + nc * 8 * k * 14 + nc * 8 * 2
+        return init + its * per_it
+    if stage == "pressure_solve":
+        amg = solver._amg
+        its = step_info["pressure_iters"]
+        init = nc * 8 * 3
+        per_it = (csr + nc * 8 * 2) + nc * 8 * 9
+        vc = 0
+        h = amg.c
+        for l in range(h.nlevels):
+            lv = h.levels[l]
+            a = lv.nnz * 12 + (lv.n + 1) * 4
+            pr = lv.p_nnz * 12 + (lv.n + 1) * 4
+            rr = lv.p_nnz * 12 + (lv.nc + 1) * 4
+            vc += 4 * a + lv.n * 8 * (3 + 3 + 2 + 2 + 8) + pr + rr + lv.nc * 8 * 2
+        vc += amg.coarse_n * amg.coarse_n * 8 + amg.coarse_n * 16
+        return init + its * (per_it + vc) + vc
+    return None
+
+
+def sample_clocks(out_path):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        fh = open(out_path, "w")
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=fh, stderr=subprocess.DEVNULL), fh
+    except Exception:
+        return None, None
+
+
+def parse_clocks(path, dev_index):
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for line in open(path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or f[0] != str(dev_index):
+                continue
+            sm.append(float(f[1]))
+            mx = float(f[2])
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+    except Exception:
+        pass
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------- CPU reference
+def cpu_reference(mesh, case, inlet, steps, warmup, budget_s=None):
+    """Time the reference's CPU path (oracle driver + the reference's C++ kernels when built)."""
+    import numpy as np
+
+    from oracle.simplec_oracle import OracleSimple, load_native
+
+    lib = load_native()
+    threads = int(lib.ft_max_threads()) if lib is not None else 1
+    o = OracleSimple(mesh, case, native=lib)
+    if inlet is not None:
+        z = mesh.zone_by_name("inlet")
+        fc = o.fv.xfb[o.fv.bzone == z.id]
+        u = 36.0 * fc[:, 1] * (1 - fc[:, 1]) * fc[:, 2] * (1 - fc[:, 2])
+        ub = o.ub_fixed.copy()
+        ub[o.fv.bzone == z.id] = np.stack([u, 0 * u, 0 * u], axis=1)
+        o.ub_fixed = ub
+        o.initialize({})
+    case.tol = 0.0
+    for _ in range(warmup):
+        o.step()
+    t0 = time.perf_counter()
+    n = 0
+    while n < steps and (budget_s is None or time.perf_counter() - t0 < budget_s or n < 3):
+        o.step()
+        n += 1
+    dt = time.perf_counter() - t0
+    kind = "reference" if lib is not None else "port"
+    return {"value": mesh.n_cells * n / dt, "unit": UNIT, "cores": threads, "kind": kind, "iterations": n,
+            "seconds": dt, "sample": f"{n} outer iterations after {warmup} warm-up of the same workload; "
+            + ("oracle driver with the reference's own C++/OpenMP kernels built from its sources"
+               if lib is not None else "NumPy/SciPy oracle (reference C++ kernels not built)")}
+
+
+# ---------------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--converge", action="store_true", help="also run to the 1e-6 residual and report it")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        mesh, case, desc, inlet = make_workload(args.config)
+        ref = cpu_reference(mesh, case, inlet, args.steps, args.warmup)
+        line = {"metric": METRIC, "value": ref["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": ref["iterations"],
+                "warmup": args.warmup, "ms_per_step": 1e3 * ref["seconds"] / ref["iterations"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(desc, parallelism="host cores"), "impl": "reference",
+                "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": ref["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    dev = torch.cuda.current_device()
+    mesh, case, desc, inlet = make_workload(args.config)
+    nc = mesh.n_cells
+    K, W = args.steps, max(args.warmup, 1)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed run
+    run_case = __import__("copy").deepcopy(case)
+    run_case.tol = 0.0  # K steps regardless of convergence
+    s = SimpleSolver(mesh, run_case)
+    if inlet is not None:
+        inlet(s)
+    for _ in range(W):
+        s.step()
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    s.profile_stages = True
+    s.stage_times.clear()
+    launches0 = s.kernel_launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    infos = []
+    smi, smi_fh = (sample_clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
+                   if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else sample_clocks(f"/tmp/clocks_rank{rank}.csv"))
+    barrier()
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record()
+        s.step()
+        ev[k][1].record()
+        infos.append(dict(s.last_linear))
+    barrier()
+    if smi is not None:
+        smi.terminate()
+        smi.wait()
+        smi_fh.close()
+    launches = s.kernel_launches - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * nc * K / (total_ms / 1e3)
+    clocks = parse_clocks(smi_fh.name if smi_fh is not None else "", dev) if smi is not None else None
+
+    # ---- roofline of the dominant stage (stage events over the timed region)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    times = dict(s.stage_times)
+    dom = max((k for k in times if stage_bytes(s, k, infos[0]) is not None), key=lambda k: times[k])
+    byts = sum(stage_bytes(s, dom, inf) for inf in infos)
+    achieved = byts / (times[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "traffic": None, "algorithmic_bytes_per_launch": byts / K,
+                "stage_ms_per_step": {k: v / K for k, v in sorted(times.items(), key=lambda kv: -kv[1])}}
+
+    # ---- end to end through the public API, from host data
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    s2 = SimpleSolver(mesh, run_case)
+    if inlet is not None:
+        inlet(s2)
+    for _ in range(W + K):
+        s2.step()
+    f = s2.fields()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = sum(v.numel() * v.element_size() for v in s2.fv.t.values()) + sum(
+        v.numel() * v.element_size() for v in s2._bc_t.values())
+    d2h = s2.report.numel() * (W + K) + sum(v.nbytes for v in f.values())
+    e2e = {"value": world * nc * (W + K) / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d / (W + K),
+           "d2h_bytes_per_step": d2h / (W + K), "includes": "solver construction from the host mesh, W+K steps, "
+           "fields() read back"}
+
+    converge = None
+    if args.converge:
+        barrier()
+        s3 = SimpleSolver(mesh, case)
+        if inlet is not None:
+            inlet(s3)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record()
+        s3.run()
+        c1.record()
+        torch.cuda.synchronize()
+        ms = c0.elapsed_time(c1)
+        converge = {"converged": bool(s3.converged), "iterations": s3.iteration, "seconds": ms / 1e3,
+                    "value": nc * s3.iteration / (ms / 1e3), "residuals": s3.residuals()["scaled"]}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        cb_case = __import__("copy").deepcopy(case)
+        cpu = cpu_reference(mesh, cb_case, inlet, steps=1000, warmup=2, budget_s=15.0)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": dict(desc, l2="flushed between timed steps (512 MiB write)",
+                           parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "linear_iterations_last": infos[-1], "to_convergence": converge}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

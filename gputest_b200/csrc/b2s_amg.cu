@@ -1,0 +1,359 @@
+// Smoothed-aggregation AMG for the pressure-correction solve on B200.
+//
+// The reference builds its hierarchy on the host every 10 outer iterations
+// (flowtrace/linalg/amg.py:80-117, flowtrace/unstructured/simple.py:624-628). Here the
+// aggregates and the sparsity patterns of P, W = A P and A_c = P^T A P are fixed once (the
+// greedy aggregation below runs on the host at set-up), and every numeric quantity is rebuilt
+// on the device from the current matrix values:
+//   D^-1, the spectral radius of D^-1 A (15 power iterations from a fixed start vector, as
+//   amg.py:69-77), P = T - 4/(3 rho) D^-1 A T (amg.py:95-101), R = P^T, A_c = R (A P), and the
+//   inverse of the coarsest matrix (shifted by 1e-10 mean|diag| when singular, amg.py:106-112).
+// Products with a fixed output pattern are row-owned gathers: a thread accumulates one output
+// row, locating each term's slot by binary search in the row's sorted columns; no atomics.
+#include "b2s_common.cuh"
+
+namespace b2s {
+
+__device__ __forceinline__ int find_sorted(const int32_t* __restrict__ cols, int lo, int hi, int key) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cols[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void dinv_k(b2s_amg_level L) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x)
+    L.dinv[i] = 1.0 / L.val[L.diag_slot[i]];
+}
+
+// rho(D^-1 A) by 15 power iterations (amg.py:69-77): y = D^-1 A x, lam = |y|/max(|x|,1e-300),
+// x = y/max(|y|,1e-300). The normalisation of x is folded into the next product (x_j = y_j/s
+// read on the fly), so each iteration costs one grid barrier.
+__global__ void __launch_bounds__(kCoopThreads) power_coop_k(b2s_amg_level L, double* ya, double* yb, double* part0,
+                                                              double* part1) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double red[(kCoopThreads / 32 + 1) * 2];
+  __shared__ double tot[2];
+  const int n = L.n;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  double* part[2] = {part0, part1};
+  double* ybuf[2] = {ya, yb};
+  double lam = 1.0, sc = 1.0;
+  for (int it = 0; it < 15; ++it) {
+    const double* xin = it == 0 ? L.x0 : ybuf[(it - 1) & 1];
+    double* yout = ybuf[it & 1];
+    double acc[2] = {0.0, 0.0};
+    for (int i = gt; i < n; i += gs) {
+      const double di = L.dinv[i];
+      double s = 0.0;
+      for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
+        const int c = L.col[j];
+        const double xc = it == 0 ? xin[c] : xin[c] / sc;
+        s += (di * L.val[j]) * xc;
+      }
+      yout[i] = s;
+      acc[0] += s * s;
+      const double xi = it == 0 ? xin[i] : xin[i] / sc;
+      acc[1] += xi * xi;
+    }
+    block_partials<2>(acc, red, part[it & 1]);
+    grid.sync();
+    grid_totals(part[it & 1], gridDim.x, 2, tot);
+    const double ny = sqrt(tot[0]), nx = sqrt(tot[1]);
+    lam = ny / fmax(nx, 1e-300);
+    sc = fmax(ny, 1e-300);
+    __syncthreads();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *L.rho = lam;
+}
+
+// P[i,J] = T[i,J] - c sum_{k in row i, agg[k] = J} (Dinv_i A_ik) T[k,J], c = (4/3)/rho
+__global__ void pvals_k(b2s_amg_level L) {
+  const double c = (4.0 / 3.0) / *L.rho;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+    const int p0 = L.p_rowptr[i], p1 = L.p_rowptr[i + 1];
+    for (int s = p0; s < p1; ++s) L.p_val[s] = 0.0;
+    const double di = L.dinv[i];
+    for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
+      const int J = L.agg[L.col[j]];
+      const int s = find_sorted(L.p_col, p0, p1, J);
+      L.p_val[s] += (di * L.val[j]) * L.tval[J];
+    }
+    const int ai = L.agg[i];
+    for (int s = p0; s < p1; ++s) {
+      const int J = L.p_col[s];
+      const double t = (J == ai) ? L.tval[J] : 0.0;
+      L.p_val[s] = t - c * L.p_val[s];
+    }
+  }
+}
+
+__global__ void rvals_k(b2s_amg_level L) {
+  const int nnz = L.p_nnz;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x)
+    L.r_val[e] = L.p_val[L.r_from_p[e]];
+}
+
+// W = A P, row-owned
+__global__ void wvals_k(b2s_amg_level L) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+    const int w0 = L.w_rowptr[i], w1 = L.w_rowptr[i + 1];
+    for (int s = w0; s < w1; ++s) L.w_val[s] = 0.0;
+    for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
+      const double a = L.val[j];
+      const int k = L.col[j];
+      for (int e = L.p_rowptr[k]; e < L.p_rowptr[k + 1]; ++e) {
+        const int s = find_sorted(L.w_col, w0, w1, L.p_col[e]);
+        L.w_val[s] += a * L.p_val[e];
+      }
+    }
+  }
+}
+
+// A_c = R W (the next level's matrix). One warp per coarse row I: the row's sorted columns and
+// an accumulator are staged in shared memory; for each R entry (I, i) in order, the lanes split
+// W row i, whose columns are distinct, so every accumulator slot receives its terms in the
+// fixed order of the R entries (deterministic, no atomics). Rows longer than the staging
+// capacity are accumulated by lane 0 directly in global memory.
+constexpr int kRowCap = 256;
+constexpr int kGalWarps = 8;
+
+__global__ void __launch_bounds__(kGalWarps * 32) acvals_k(b2s_amg_level L, const int32_t* __restrict__ crowptr,
+                                                           const int32_t* __restrict__ ccol,
+                                                           double* __restrict__ cval) {
+  __shared__ int scol[kGalWarps][kRowCap];
+  __shared__ double sacc[kGalWarps][kRowCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (int I = blockIdx.x * kGalWarps + wib; I < L.nc; I += gridDim.x * kGalWarps) {
+    const int c0 = crowptr[I], c1 = crowptr[I + 1], m = c1 - c0;
+    const int e0 = L.r_rowptr[I], e1 = L.r_rowptr[I + 1];
+    if (m <= kRowCap) {
+      for (int t = lane; t < m; t += 32) {
+        scol[wib][t] = ccol[c0 + t];
+        sacc[wib][t] = 0.0;
+      }
+      __syncwarp();
+      for (int e = e0; e < e1; ++e) {
+        const double rv = L.r_val[e];
+        const int i = L.r_col[e];
+        const int w1 = L.w_rowptr[i + 1];
+        for (int s = L.w_rowptr[i] + lane; s < w1; s += 32) {
+          const int t = find_sorted(scol[wib], 0, m, L.w_col[s]);
+          sacc[wib][t] += rv * L.w_val[s];
+        }
+        __syncwarp();
+      }
+      for (int t = lane; t < m; t += 32) cval[c0 + t] = sacc[wib][t];
+      __syncwarp();
+    } else if (lane == 0) {
+      for (int t = c0; t < c1; ++t) cval[t] = 0.0;
+      for (int e = e0; e < e1; ++e) {
+        const double rv = L.r_val[e];
+        const int i = L.r_col[e];
+        for (int s = L.w_rowptr[i]; s < L.w_rowptr[i + 1]; ++s) {
+          const int t = find_sorted(ccol, c0, c1, L.w_col[s]);
+          cval[t] += rv * L.w_val[s];
+        }
+      }
+    }
+  }
+}
+
+// Dense coarse matrix M (n x n, row-major) with the singular shift, then its inverse by
+// Gauss-Jordan elimination in place, by one block.
+constexpr int kGJThreads = 1024;
+constexpr int kSmemCoarse = 160;  // n <= 160: the matrix lives in shared memory (<= 200 KB)
+
+__global__ void __launch_bounds__(kGJThreads) coarse_inverse_k(int n, const int32_t* __restrict__ rowptr,
+                                                              const int32_t* __restrict__ col,
+                                                              const double* __restrict__ val, int singular,
+                                                              double* __restrict__ Mg, double* __restrict__ inv) {
+  extern __shared__ double smem[];
+  __shared__ double shift_s;
+  __shared__ double rowk[1024];
+  __shared__ double colk[1024];
+  const bool in_smem = n <= kSmemCoarse;
+  double* M = in_smem ? smem : Mg;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < n * n; e += nt) M[e] = 0.0;
+  __syncthreads();
+  for (int r = tid; r < n; r += nt)
+    for (int j = rowptr[r]; j < rowptr[r + 1]; ++j) M[(int64_t)r * n + col[j]] = val[j];
+  __syncthreads();
+  if (singular) {
+    if (tid < 32) {
+      double s = 0.0;
+      for (int r = tid; r < n; r += 32) s += fabs(M[(int64_t)r * n + r]);
+      s = warp_sum(s);
+      if (tid == 0) shift_s = 1e-10 * (s / (double)n);
+    }
+    __syncthreads();
+    for (int r = tid; r < n; r += nt) M[(int64_t)r * n + r] = M[(int64_t)r * n + r] + shift_s;
+    __syncthreads();
+  }
+  // In-place Gauss-Jordan inversion. The coarse matrix is symmetric positive definite (a
+  // Galerkin product of the SPD pressure-correction matrix, shifted when singular), so no
+  // pivoting is needed. Step k copies pivot row and column, then updates every entry at once:
+  //   M[k][k] = 1/p, M[k][c] = M[k][c]/p, M[r][k] = -M[r][k]/p, M[r][c] -= M[r][k] M[k][c]/p.
+  for (int k = 0; k < n; ++k) {
+    for (int i = tid; i < n; i += nt) {
+      rowk[i] = M[(int64_t)k * n + i];
+      colk[i] = M[(int64_t)i * n + k];
+    }
+    __syncthreads();
+    const double piv = rowk[k];
+    for (int e = tid; e < n * n; e += nt) {
+      const int r = e / n, c = e - r * n;
+      double v;
+      if (r == k) v = (c == k) ? 1.0 / piv : rowk[c] / piv;
+      else if (c == k) v = -colk[r] / piv;
+      else v = M[e] - colk[r] * (rowk[c] / piv);
+      M[e] = v;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < n * n; e += nt) inv[e] = M[e];
+}
+
+__global__ void strength_changes_k(b2s_amg_level L, double theta, int32_t* __restrict__ count) {
+  int local = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+    const double di = fabs(L.val[L.diag_slot[i]]);
+    for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
+      const int c = L.col[j];
+      if (c == i) continue;
+      const double dc = fabs(L.val[L.diag_slot[c]]);
+      const int strong = fabs(L.val[j]) >= theta * sqrt(di * dc) ? 1 : 0;
+      local += strong != (int)L.strong[j];
+    }
+  }
+  if (local) atomicAdd(count, local);  // integer sum: order-independent
+}
+
+}  // namespace b2s
+
+using namespace b2s;
+
+static int power_grid(int* g) {
+  int dev = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return B2S_ERR_DEVICE;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return B2S_ERR_DEVICE;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, power_coop_k, kCoopThreads, 0) != cudaSuccess)
+    return B2S_ERR_DEVICE;
+  if (per <= 0) return B2S_ERR_DEVICE;
+  if (per > 1) per = 1;
+  *g = sms * per;
+  if (*g > kMaxCoopBlocks) *g = kMaxCoopBlocks;
+  return B2S_OK;
+}
+
+extern "C" {
+
+int64_t b2s_amg_workspace_bytes(const b2s_amg* h) {
+  if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || h->coarse_n < 1) return -1;
+  int64_t nmax = 0;
+  for (int l = 0; l < h->nlevels; ++l) nmax = h->levels[l].n > nmax ? h->levels[l].n : nmax;
+  int64_t dense = h->coarse_n > kSmemCoarse ? (int64_t)h->coarse_n * h->coarse_n : 0;
+  return (int64_t)sizeof(double) * (2 * nmax + 4 * (int64_t)kMaxCoopBlocks + dense);
+}
+
+int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s) {
+  if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || h->coarse_n < 1 || h->coarse_n > 1024 || !work ||
+      !h->coarse_inv || !h->coarse_rowptr || !h->coarse_col || !h->coarse_val)
+    return B2S_ERR_ARG;
+  if (work_bytes < b2s_amg_workspace_bytes(h)) return B2S_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)s;
+  int64_t nmax = 0;
+  for (int l = 0; l < h->nlevels; ++l) nmax = h->levels[l].n > nmax ? h->levels[l].n : nmax;
+  double* xa = (double*)work;
+  double* xb = xa + nmax;
+  double* part0 = xb + nmax;
+  double* part1 = part0 + 2 * (int64_t)kMaxCoopBlocks;
+  double* dense = part1 + 2 * (int64_t)kMaxCoopBlocks;
+  int g = 0, rc;
+  if ((rc = power_grid(&g)) != B2S_OK) return rc;
+  for (int l = 0; l < h->nlevels; ++l) {
+    b2s_amg_level L = h->levels[l];
+    if (!L.diag_slot || !L.agg || !L.tval || !L.x0 || !L.p_col || !L.p_val || !L.r_col || !L.r_from_p ||
+        !L.r_val || !L.w_rowptr || !L.w_col || !L.w_val || !L.rho)
+      return B2S_ERR_ARG;
+    dinv_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+    B2S_LAUNCH_CHECK();
+    void* args[] = {&L, &xa, &xb, &part0, &part1};  // xa, xb: the two power-iteration buffers
+    if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
+      return B2S_ERR_LAUNCH;
+    pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+    rvals_k<<<grid_for(L.p_nnz), kThreads, 0, st>>>(L);
+    wvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+    B2S_LAUNCH_CHECK();
+    const bool last = l + 1 == h->nlevels;
+    const int32_t* crow = last ? h->coarse_rowptr : h->levels[l + 1].rowptr;
+    const int32_t* ccol = last ? h->coarse_col : h->levels[l + 1].col;
+    double* cval = last ? h->coarse_val : h->levels[l + 1].val;
+    acvals_k<<<(unsigned)cdiv(L.nc, kGalWarps), kGalWarps * 32, 0, st>>>(L, crow, ccol, cval);
+    B2S_LAUNCH_CHECK();
+  }
+  const int n = h->coarse_n;
+  const size_t smem = n <= kSmemCoarse ? (size_t)n * n * sizeof(double) : 0;
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(coarse_inverse_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return B2S_ERR_LAUNCH;
+  }
+  coarse_inverse_k<<<1, kGJThreads, smem, st>>>(n, h->coarse_rowptr, h->coarse_col, h->coarse_val, h->singular,
+                                                dense, h->coarse_inv);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_amg_strength_changes_d(const b2s_amg* h, double theta, int32_t* count, b2s_stream_t s) {
+  if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || !count) return B2S_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  if (cudaMemsetAsync(count, 0, sizeof(int32_t), st) != cudaSuccess) return B2S_ERR_LAUNCH;
+  for (int l = 0; l < h->nlevels; ++l) {
+    const b2s_amg_level& L = h->levels[l];
+    if (!L.strong || !L.diag_slot) return B2S_ERR_ARG;
+    strength_changes_k<<<grid_for(L.n), kThreads, 0, st>>>(L, theta, count);
+    B2S_LAUNCH_CHECK();
+  }
+  return B2S_OK;
+}
+
+/* Greedy three-pass aggregation of flowtrace/linalg/amg.py:25-57 on the strength graph
+ * (host CSR); agg[n] receives the aggregate of every node, the return value their number. */
+int64_t b2s_host_aggregate(int64_t n, const int64_t* indptr, const int64_t* indices, int64_t* agg) {
+  if (n < 0 || !indptr || !indices || !agg) return -1;
+  for (int64_t i = 0; i < n; ++i) agg[i] = -1;
+  int64_t na = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (agg[i] >= 0) continue;
+    bool free_ = true;
+    for (int64_t k = indptr[i]; k < indptr[i + 1]; ++k)
+      if (agg[indices[k]] >= 0) {
+        free_ = false;
+        break;
+      }
+    if (free_) {
+      agg[i] = na;
+      for (int64_t k = indptr[i]; k < indptr[i + 1]; ++k) agg[indices[k]] = na;
+      ++na;
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    if (agg[i] >= 0) continue;
+    for (int64_t k = indptr[i]; k < indptr[i + 1]; ++k) {
+      const int64_t j = indices[k];
+      if (agg[j] >= 0) {
+        agg[i] = agg[j];
+        break;
+      }
+    }
+  }
+  for (int64_t i = 0; i < n; ++i)
+    if (agg[i] < 0) agg[i] = na++;
+  return na;
+}
+
+}  // extern "C"

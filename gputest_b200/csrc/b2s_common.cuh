@@ -1,0 +1,108 @@
+// Shared device helpers of the B200 SIMPLEC kernels: launch geometry, deterministic
+// reductions and the grid-wide context of the cooperative (persistent) kernels.
+//
+// Determinism: every reduction is two-pass with a fixed order (warp xor-shuffle tree, then
+// warps in index order, then blocks in index order). No floating-point atomics anywhere, so
+// results do not depend on scheduling, and in a cooperative kernel every block computes
+// bit-identical scalars, which keeps the control flow around grid.sync() uniform.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "b2simplec.h"
+
+namespace cg = cooperative_groups;
+
+namespace b2s {
+
+constexpr int kThreads = 256;        // ordinary kernels
+constexpr int kCoopThreads = 1024;   // cooperative kernels: one block per SM
+constexpr int kMaxCoopBlocks = 1184; // 148 SMs x 8
+constexpr int kWarps = kCoopThreads / 32;
+
+__host__ __device__ inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+inline unsigned grid_for(int64_t n, int threads = kThreads) {
+  int64_t g = cdiv(n > 0 ? n : 1, threads);
+  return (unsigned)(g > 2147483647 ? 2147483647 : g);
+}
+
+// Deterministic warp sum (xor tree: every lane ends with the same value).
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sum NQ per-thread values over the block; result valid in out[0..NQ) for all threads after
+// the call. smem must hold (blockDim.x/32)*NQ doubles plus NQ doubles.
+template <int NQ>
+__device__ __forceinline__ void block_sum(const double (&v)[NQ], double* smem, double (&out)[NQ]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double s = warp_sum(v[q]);
+    if (lane == 0) smem[warp * NQ + q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NQ) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += smem[w * NQ + threadIdx.x];
+    smem[nw * NQ + threadIdx.x] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) out[q] = smem[nw * NQ + q];
+  __syncthreads();
+}
+
+// Block partial sums of NQ values, quantity-major: block b writes part[q*gridDim.x + b].
+template <int NQ>
+__device__ __forceinline__ void block_partials(const double (&v)[NQ], double* smem, double* part) {
+  double out[NQ];
+  block_sum<NQ>(v, smem, out);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[(int64_t)q * gridDim.x + blockIdx.x] = out[q];
+  }
+}
+
+// Fixed-order total of quantity q over nb block partials (quantity-major layout), by one warp.
+__device__ __forceinline__ double warp_total(const double* part, int nb, int nq, int q) {
+  const int lane = threadIdx.x & 31;
+  const double* pq = part + (int64_t)q * nb;
+  double s = 0.0;
+  for (int b = lane; b < nb; b += 32) s += pq[b];
+  (void)nq;
+  return warp_sum(s);
+}
+
+// Totals of nq partial sums (nb blocks each); every thread of the block gets tot[0..nq).
+// smem must hold nq doubles.
+__device__ __forceinline__ void grid_totals(const double* part, int nb, int nq, double* smem) {
+  if (threadIdx.x < 32) {
+    for (int q = 0; q < nq; ++q) {
+      double t = warp_total(part, nb, nq, q);
+      if (threadIdx.x == 0) smem[q] = t;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool finite(double x) { return isfinite(x); }
+
+}  // namespace b2s
+
+// Checks launch errors and maps them to the ABI's status codes.
+#define B2S_LAUNCH_CHECK()                                  \
+  do {                                                      \
+    cudaError_t _e = cudaGetLastError();                    \
+    if (_e != cudaSuccess) return B2S_ERR_LAUNCH;           \
+  } while (0)

@@ -1,0 +1,795 @@
+// Finite-volume stages of the SIMPLEC outer iteration on B200: face interpolation, least-
+// squares and Green-Gauss gradients, CSR assembly, and the fused momentum, Rhie-Chow /
+// pressure-correction, correction and energy stages.
+//
+// Every kernel is cell-centric: one thread per cell walks the faces it owns (a contiguous
+// range, faces being sorted by owner), the faces it neighbours (a short index list) and its
+// boundary faces (a contiguous range). A cell writes only its own rows and its owned faces,
+// so there are no atomics and the results are deterministic. Per cell the terms are summed in
+// the order of the reference's sparse products (flowtrace/unstructured/fvmesh.py:254-309):
+// owned faces, then neighbour faces, then boundary faces, each in reference face order, and
+// the rows of Cdiff (owned and neighbour faces merged by reference face index); compiled
+// without FMA contraction, the results then match the reference's NumPy path to the bit
+// wherever the reference's own reductions are not involved.
+//
+// Bandwidth: each interior face is read by its two cells; with RCM-ordered cells the second
+// read falls inside a window that L2 (126 MB) holds, so DRAM sees each face once.
+#include "b2s_common.cuh"
+
+namespace b2s {
+
+// numpy.maximum(x, 0.0): NaN propagates, -0.0 stays -0.0.
+__device__ __forceinline__ double npmax0(double x) { return (x < 0.0) ? 0.0 : x; }
+__device__ __forceinline__ double npmin(double a, double b) { return (a <= b || a != a) ? a : b; }
+__device__ __forceinline__ double npmax(double a, double b) { return (a >= b || a != a) ? a : b; }
+
+// Visit the rows of Cdiff: the owned and neighbour faces of cell c merged by reference face
+// index; fn(face, +1/-1).
+template <class Fn>
+__device__ __forceinline__ void for_cdiff(const b2s_mesh& m, int c, Fn fn) {
+  int j = m.own_ptr[c], je = m.own_ptr[c + 1];
+  int k = m.nei_ptr[c], ke = m.nei_ptr[c + 1];
+  int kf = k < ke ? m.nei_face[k] : 0;
+  while (j < je || k < ke) {
+    bool own = (k >= ke) || (j < je && m.forig[j] < m.forig[kf]);
+    if (own) {
+      fn(j, true);
+      ++j;
+    } else {
+      fn(kf, false);
+      ++k;
+      if (k < ke) kf = m.nei_face[k];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ face interp
+__global__ void face_interp_k(b2s_mesh m, int k, const double* __restrict__ phi, double* __restrict__ out) {
+  const int64_t nf = m.nf, nc = m.nc;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nf * k; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t c = t / nf, f = t - c * nf;
+    double wf = m.w[f];
+    out[t] = wf * phi[c * nc + m.fP[f]] + (1.0 - wf) * phi[c * nc + m.fN[f]];
+  }
+}
+
+// ------------------------------------------------------------------------------ LS gradient
+// r = Cown(wl dphi d) + Cnei(wl dphi d) + Cb(wlb dphib db); grad = Ginv r
+// (flowtrace/unstructured/fvmesh.py:268-286).
+template <int DIM, int NF>
+__global__ void ls_gradient_k(b2s_mesh m, const double* __restrict__ phi, const double* __restrict__ phib,
+                              double* __restrict__ grad) {
+  const int nc = m.nc, nf = m.nf, nb = m.nb;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    double ro[NF][DIM], rn[NF][DIM], rb[NF][DIM];
+#pragma unroll
+    for (int q = 0; q < NF; ++q)
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) ro[q][a] = rn[q][a] = rb[q][a] = 0.0;
+    for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
+      const int P = m.fP[f], N = m.fN[f];
+      const double wl = m.wl[f];
+#pragma unroll
+      for (int q = 0; q < NF; ++q) {
+        const double coef = wl * (phi[(int64_t)q * nc + N] - phi[(int64_t)q * nc + P]);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) ro[q][a] += coef * m.d[(int64_t)a * nf + f];
+      }
+    }
+    for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
+      const int f = m.nei_face[k];
+      const int P = m.fP[f], N = m.fN[f];
+      const double wl = m.wl[f];
+#pragma unroll
+      for (int q = 0; q < NF; ++q) {
+        const double coef = wl * (phi[(int64_t)q * nc + N] - phi[(int64_t)q * nc + P]);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) rn[q][a] += coef * m.d[(int64_t)a * nf + f];
+      }
+    }
+    for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) {
+      const double wlb = m.wlb[f];
+#pragma unroll
+      for (int q = 0; q < NF; ++q) {
+        const double coef = wlb * (phib[(int64_t)q * nb + f] - phi[(int64_t)q * nc + c]);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) rb[q][a] += coef * m.db[(int64_t)a * nb + f];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NF; ++q) {
+      double r[DIM];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) r[a] = (ro[q][a] + rn[q][a]) + rb[q][a];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        double s = 0.0;
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) s += m.Ginv[(int64_t)(a * DIM + b) * nc + c] * r[b];
+        grad[((int64_t)q * DIM + a) * nc + c] = s;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ GG gradient
+// (1/V)(Cdiff(pf S) + Cb(phib Sb)), pf = face_interp(phi) + face_interp(grad).dxm
+// (flowtrace/unstructured/fvmesh.py:288-309).
+template <int DIM>
+__device__ __forceinline__ double gg_face_value(const b2s_mesh& m, int f, const double* phi, const double* grad) {
+  const int nc = m.nc, nf = m.nf, P = m.fP[f], N = m.fN[f];
+  const double w = m.w[f];
+  double pf = w * phi[P] + (1.0 - w) * phi[N];
+  if (grad) {
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      const double gf = w * grad[(int64_t)a * nc + P] + (1.0 - w) * grad[(int64_t)a * nc + N];
+      s = (a == 0) ? gf * m.dxm[(int64_t)a * nf + f] : s + gf * m.dxm[(int64_t)a * nf + f];
+    }
+    pf = pf + s;
+  }
+  return pf;
+}
+
+template <int DIM>
+__global__ void gg_gradient_k(b2s_mesh m, const double* __restrict__ phi, const double* __restrict__ phib,
+                              const double* __restrict__ grad, double* __restrict__ out) {
+  const int nc = m.nc, nf = m.nf, nb = m.nb;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    double si[DIM], sb[DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) si[a] = sb[a] = 0.0;
+    for_cdiff(m, c, [&](int f, bool own) {
+      const double pf = gg_face_value<DIM>(m, f, phi, grad);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        const double v = pf * m.S[(int64_t)a * nf + f];
+        si[a] += own ? v : -v;
+      }
+    });
+    for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) {
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) sb[a] += phib[f] * m.Sb[(int64_t)a * nb + f];
+    }
+    const double v = m.vol[c];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) out[(int64_t)a * nc + c] = (si[a] + sb[a]) / v;
+  }
+}
+
+// ------------------------------------------------------------------------------ assembly
+// data[slot_diag] = diag; data[slot_PN] += aPN; data[slot_NP] += aNP
+// (flowtrace/unstructured/fvmesh.py:332-348); row-owned, no atomics.
+__global__ void assemble_k(b2s_mesh m, const double* __restrict__ diag, const double* __restrict__ aPN,
+                           const double* __restrict__ aNP, double* __restrict__ val) {
+  const int nc = m.nc;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    for (int s = m.rowptr[c]; s < m.rowptr[c + 1]; ++s) val[s] = 0.0;
+    for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) val[m.slot_PN[f]] += aPN[f];
+    for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
+      const int f = m.nei_face[k];
+      val[m.slot_NP[f]] += aNP[f];
+    }
+    val[m.slot_diag[c]] = diag[c];
+  }
+}
+
+// ------------------------------------------------------------------------------ boundary values
+// ub = (m_wall + m_inlet) ub_fixed + m_sym (UP - (UP.n) n) + m_pres UP, UP = U_P (+ gU_P . dbt);
+// pb = m_pres pb_fixed + (1 - m_pres)(p_P (+ gp_P . db))   (simple.py:305-325)
+template <int DIM>
+__global__ void flow_bvals_k(b2s_mesh m, b2s_bc bc, const double* __restrict__ Up, const double* __restrict__ gUp,
+                             const double* __restrict__ gpf, double* __restrict__ bUp) {
+  const int nc = m.nc, nb = m.nb;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nb; f += gridDim.x * blockDim.x) {
+    const int P = m.bP[f];
+    double UP[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      UP[k] = Up[(int64_t)(1 + k) * nc + P];
+      if (gUp) {
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          const double t = gUp[((int64_t)(1 + k) * DIM + a) * nc + P] * m.dbt[(int64_t)a * nb + f];
+          s = (a == 0) ? t : s + t;
+        }
+        UP[k] = UP[k] + s;
+      }
+    }
+    double un = 0.0;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      const double t = UP[k] * m.nbv[(int64_t)k * nb + f];
+      un = (k == 0) ? t : un + t;
+    }
+    const double fixed = bc.m_wall[f] + bc.m_inlet[f], msym = bc.m_sym[f], mp = bc.m_pres[f];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      const double sym = UP[k] - un * m.nbv[(int64_t)k * nb + f];
+      bUp[(int64_t)(1 + k) * nb + f] = (fixed * bc.ub_fixed[(int64_t)k * nb + f] + msym * sym) + mp * UP[k];
+    }
+    double pP = Up[P];
+    if (gpf) {
+      double s = 0.0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        const double t = gpf[(int64_t)a * nc + P] * m.db[(int64_t)a * nb + f];
+        s = (a == 0) ? t : s + t;
+      }
+      pP = pP + s;
+    }
+    bUp[f] = mp * bc.pb_fixed[f] + (1.0 - mp) * pP;
+  }
+}
+
+// ------------------------------------------------------------------------------ transport rows
+// One row of a convection-diffusion system (simple.py:340-374): coefficients, the CSR row,
+// and the right-hand side of NQ scalar fields that share the matrix.
+//   diag = (Cown(D + max(F,0)) + Cnei(D + max(-F,0))) + Cb(Db + max(Fb,0)),  D = gamma alpha
+//   aPN = -(D + max(-F,0)), aNP = -(D + max(F,0)),  Db = gamma alpha_b dirichlet
+//   rhs = Cb((Db + max(-Fb,0)) phib) + Cdiff(gamma gf.T) [- Cdiff(F (ho - up))] + extra
+template <int DIM, int NQ>
+struct RowOut {
+  double diag;     // a_P (before relaxation and extra diagonal terms)
+  double sumnb;    // scatter(-aPN, -aNP)
+  double rhs[NQ];  // without the extra source
+};
+
+template <int DIM, int NQ>
+__device__ __forceinline__ RowOut<DIM, NQ> transport_row(const b2s_mesh& m, int c, double gamma,
+                                                         const double* dirichlet, const double* F, const double* Fb,
+                                                         const double* phi, int64_t phi_stride,
+                                                         const double* grad, int64_t grad_stride,
+                                                         const double* phib, int64_t phib_stride, bool second,
+                                                         double* val, bool write_offdiag) {
+  const int nc = m.nc, nf = m.nf, nb = m.nb;
+  RowOut<DIM, NQ> o;
+  double s_own = 0.0, s_nei = 0.0, s_b = 0.0, nb_own = 0.0, nb_nei = 0.0;
+  for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
+    const double D = gamma * m.alpha[f], Ff = F[f];
+    s_own += D + npmax0(Ff);
+    const double aPN = -(D + npmax0(-Ff));
+    nb_own += -aPN;
+    if (write_offdiag) val[m.slot_PN[f]] = aPN;
+  }
+  for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
+    const int f = m.nei_face[k];
+    const double D = gamma * m.alpha[f], Ff = F[f];
+    s_nei += D + npmax0(-Ff);
+    const double aNP = -(D + npmax0(Ff));
+    nb_nei += -aNP;
+    if (write_offdiag) val[m.slot_NP[f]] = aNP;
+  }
+  double rb[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) rb[q] = 0.0;
+  for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) {
+    const double Db = gamma * m.alpha_b[f] * dirichlet[f];
+    const double Fbf = Fb[f];
+    s_b += Db + npmax0(Fbf);
+    const double coef = Db + npmax0(-Fbf);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) rb[q] += coef * phib[q * phib_stride + f];
+  }
+  o.diag = (s_own + s_nei) + s_b;
+  o.sumnb = nb_own + nb_nei;
+  // explicit non-orthogonal diffusion and deferred second-order correction over Cdiff rows
+  double rn[NQ], rh[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) rn[q] = rh[q] = 0.0;
+  for_cdiff(m, c, [&](int f, bool own) {
+    const int P = m.fP[f], N = m.fN[f];
+    const double w = m.w[f], w1 = 1.0 - w, Ff = F[f];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const double* g = grad + q * grad_stride;
+      double s = 0.0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        const double gf = w * g[(int64_t)a * nc + P] + w1 * g[(int64_t)a * nc + N];
+        const double t = gf * m.Tv[(int64_t)a * nf + f];
+        s = (a == 0) ? t : s + t;
+      }
+      const double v = gamma * s;
+      rn[q] += own ? v : -v;
+      if (second) {
+        const double* ph = phi + q * phi_stride;
+        const double phP = ph[P], phN = ph[N];
+        double hoP = 0.0, hoN = 0.0;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          const double tP = g[(int64_t)a * nc + P] * m.dPf[(int64_t)a * nf + f];
+          const double tN = g[(int64_t)a * nc + N] * m.dNf[(int64_t)a * nf + f];
+          hoP = (a == 0) ? tP : hoP + tP;
+          hoN = (a == 0) ? tN : hoN + tN;
+        }
+        hoP = phP + hoP;
+        hoN = phN + hoN;
+        const bool up = Ff >= 0.0;
+        const double lo = npmin(phP, phN), hi = npmax(phP, phN);
+        const double ho = npmin(npmax(up ? hoP : hoN, lo), hi);
+        const double dc = Ff * (ho - (up ? phP : phN));
+        rh[q] += own ? dc : -dc;
+      }
+    }
+  });
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double r = rb[q] + rn[q];
+    if (second) r = r - rh[q];
+    o.rhs[q] = r;
+  }
+  return o;
+}
+
+// (A x)_c over the CSR row in stored order with a_cc = dval (scipy's csr_matvec order).
+__device__ __forceinline__ double row_apply(const b2s_mesh& m, const double* val, int c, double dval,
+                                            const double* x) {
+  const int sd = m.slot_diag[c];
+  double s = 0.0;
+  for (int j = m.rowptr[c]; j < m.rowptr[c + 1]; ++j) s += (j == sd ? dval : val[j]) * x[m.col[j]];
+  return s;
+}
+
+// ------------------------------------------------------------------------------ momentum
+template <int DIM>
+__global__ void momentum_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Up,
+                                    const double* __restrict__ gUp, const double* __restrict__ gp,
+                                    const double* __restrict__ bUp, const double* __restrict__ F,
+                                    const double* __restrict__ Fb, const double* __restrict__ por,
+                                    const double* __restrict__ msrc, double* __restrict__ val,
+                                    double* __restrict__ diag_out, double* __restrict__ inv_out,
+                                    double* __restrict__ dP_out, double* __restrict__ b_out,
+                                    double* __restrict__ br_out, double* __restrict__ part) {
+  __shared__ double red[(kThreads / 32 + 1) * 2 * DIM];
+  const int nc = m.nc, nb = m.nb;
+  const double au = prm.relax_u;
+  double acc[2 * DIM];
+#pragma unroll
+  for (int q = 0; q < 2 * DIM; ++q) acc[q] = 0.0;
+  const bool drive = prm.body[0] != 0.0 || prm.body[1] != 0.0 || (DIM == 3 && prm.body[2] != 0.0);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
+                                                 (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
+    double diag = o.diag;
+    const double V = m.vol[c];
+    if (por) diag = diag + por[c] * V;
+    const double diag_r = diag / au;
+    val[m.slot_diag[c]] = diag_r;
+    inv_out[c] = 1.0 / diag_r;
+    diag_out[c] = diag;
+    double denom = diag_r;
+    if (prm.simplec) {
+      denom = diag_r - o.sumnb;
+      denom = (denom > 1e-12 * diag_r) ? denom : diag_r;
+    }
+    dP_out[c] = V / denom;
+    const double cr = (1.0 - au) / au;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      double src = -gp[(int64_t)k * nc + c] * V;
+      if (drive) src = src + V * prm.body[k];
+      if (msrc) src = src + msrc[(int64_t)k * nc + c];
+      const double rhs = o.rhs[k] + src;
+      const double* u = Up + (int64_t)(1 + k) * nc;
+      const double Au = row_apply(m, val, c, diag, u);
+      acc[k] += fabs(rhs - Au);
+      acc[DIM + k] += fabs(diag * u[c]);
+      b_out[(int64_t)k * nc + c] = rhs;
+      br_out[(int64_t)k * nc + c] = rhs + (cr * diag) * u[c];
+    }
+  }
+  block_partials<2 * DIM>(acc, red, part);
+}
+
+// ------------------------------------------------------------------------------ pressure correction
+// Rhie-Chow predictor fluxes and the p' system (simple.py:583-623). Face values are computed
+// identically from both sides of a face, so owner and neighbour see the same bits.
+template <int DIM>
+__device__ __forceinline__ void rc_face(const b2s_mesh& m, const b2s_flow_params& prm, int f, const double* Ustar,
+                                        const double* p, const double* gp, const double* dP, double& Fst,
+                                        double& cf) {
+  const int nc = m.nc, nf = m.nf, P = m.fP[f], N = m.fN[f];
+  const double w = m.w[f], w1 = 1.0 - w;
+  const double dF = w * dP[P] + w1 * dP[N];
+  double us = 0.0, gd = 0.0;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    const double uf = w * Ustar[(int64_t)a * nc + P] + w1 * Ustar[(int64_t)a * nc + N];
+    const double gf = w * gp[(int64_t)a * nc + P] + w1 * gp[(int64_t)a * nc + N];
+    const double t1 = uf * m.S[(int64_t)a * nf + f], t2 = gf * m.d[(int64_t)a * nf + f];
+    us = (a == 0) ? t1 : us + t1;
+    gd = (a == 0) ? t2 : gd + t2;
+  }
+  const double al = m.alpha[f];
+  Fst = prm.rho * (us - dF * al * (p[N] - p[P] - gd));
+  cf = prm.rho * dF * al;
+}
+
+template <int DIM>
+__device__ __forceinline__ void rc_bface(const b2s_mesh& m, const b2s_bc& bc, const b2s_flow_params& prm, int f,
+                                         int P, const double* Ustar, const double* p, const double* gp,
+                                         const double* dP, double& Fbst, double& cb) {
+  const int nc = m.nc, nb = m.nb;
+  double ui = 0.0, us = 0.0, gd = 0.0;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    const double sb = m.Sb[(int64_t)a * nb + f];
+    const double t0 = bc.ub_fixed[(int64_t)a * nb + f] * sb;
+    const double t1 = Ustar[(int64_t)a * nc + P] * sb;
+    const double t2 = gp[(int64_t)a * nc + P] * m.db[(int64_t)a * nb + f];
+    ui = (a == 0) ? t0 : ui + t0;
+    us = (a == 0) ? t1 : us + t1;
+    gd = (a == 0) ? t2 : gd + t2;
+  }
+  const double mp = bc.m_pres[f];
+  const double fb_in = prm.rho * ui * bc.m_inlet[f];
+  const double fb_pr = prm.rho * (us - dP[P] * m.alpha_b[f] * (bc.pb_fixed[f] - p[P] - gd));
+  Fbst = fb_in + fb_pr * mp;
+  cb = prm.rho * dP[P] * m.alpha_b[f] * mp;
+}
+
+template <int DIM>
+__global__ void pressure_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Ustar,
+                                    const double* __restrict__ p, const double* __restrict__ gp,
+                                    const double* __restrict__ dP, double* __restrict__ Fst_out,
+                                    double* __restrict__ cf_out, double* __restrict__ Fbst_out,
+                                    double* __restrict__ cb_out, double* __restrict__ val, double* __restrict__ rhs,
+                                    double* __restrict__ part) {
+  __shared__ double red[(kThreads / 32 + 1) * 1];
+  const int nc = m.nc;
+  double acc[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    double d_own = 0.0, d_nei = 0.0, d_b = 0.0, m_int = 0.0, m_b = 0.0;
+    for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
+      double Fst, cf;
+      rc_face<DIM>(m, prm, f, Ustar, p, gp, dP, Fst, cf);
+      Fst_out[f] = Fst;
+      cf_out[f] = cf;
+      d_own += cf;
+      val[m.slot_PN[f]] = -cf;
+    }
+    for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
+      const int f = m.nei_face[k];
+      double Fst, cf;
+      rc_face<DIM>(m, prm, f, Ustar, p, gp, dP, Fst, cf);
+      d_nei += cf;
+      val[m.slot_NP[f]] = -cf;
+    }
+    for_cdiff(m, c, [&](int f, bool own) {
+      double Fst, cf;
+      rc_face<DIM>(m, prm, f, Ustar, p, gp, dP, Fst, cf);
+      m_int += own ? Fst : -Fst;
+    });
+    for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) {
+      double Fbst, cb;
+      rc_bface<DIM>(m, bc, prm, f, c, Ustar, p, gp, dP, Fbst, cb);
+      Fbst_out[f] = Fbst;
+      cb_out[f] = cb;
+      d_b += cb;
+      m_b += Fbst;
+    }
+    val[m.slot_diag[c]] = (d_own + d_nei) + d_b;
+    const double mass = m_int + m_b;
+    rhs[c] = -mass;
+    acc[0] += fabs(mass);
+  }
+  block_partials<1>(acc, red, part);
+}
+
+// ------------------------------------------------------------------------------ corrections
+template <int DIM>
+__global__ void correct_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Fst,
+                          const double* __restrict__ cf, const double* __restrict__ Fbst,
+                          const double* __restrict__ cb, const double* __restrict__ pp, const double* __restrict__ p,
+                          const double* __restrict__ Ustar, const double* __restrict__ dP, double* __restrict__ F,
+                          double* __restrict__ Fb, double* __restrict__ Up_new, double* __restrict__ part) {
+  __shared__ double red[(kThreads / 32 + 1) * 3];
+  const int nc = m.nc, nf = m.nf, nb = m.nb;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    double ro[DIM], rn[DIM], rb[DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) ro[a] = rn[a] = rb[a] = 0.0;
+    const double ppc = pp[c];
+    for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
+      const int N = m.fN[f];
+      const double ppN = pp[N];
+      const double Fn = Fst[f] + cf[f] * (ppc - ppN);
+      F[f] = Fn;
+      acc[1] += fabs(Fn);
+      const double coef = m.wl[f] * (ppN - ppc);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) ro[a] += coef * m.d[(int64_t)a * nf + f];
+    }
+    for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
+      const int f = m.nei_face[k];
+      const double coef = m.wl[f] * (ppc - pp[m.fP[f]]);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) rn[a] += coef * m.d[(int64_t)a * nf + f];
+    }
+    for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) {
+      const double fbn = Fbst[f] + cb[f] * ppc;
+      Fb[f] = fbn;
+      acc[2] += fabs(fbn);
+      const double ppb = (1.0 - bc.m_pres[f]) * ppc;
+      const double coef = m.wlb[f] * (ppb - ppc);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) rb[a] += coef * m.db[(int64_t)a * nb + f];
+    }
+    const double pn = p[c] + prm.relax_p * ppc;
+    Up_new[c] = pn;
+    acc[0] += pn;
+    double r[DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) r[a] = (ro[a] + rn[a]) + rb[a];
+    const double dp = dP[c];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      double s = 0.0;
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) s += m.Ginv[(int64_t)(a * DIM + b) * nc + c] * r[b];
+      Up_new[(int64_t)(1 + a) * nc + c] = Ustar[(int64_t)a * nc + c] - dp * s;
+    }
+  }
+  block_partials<3>(acc, red, part);
+}
+
+__global__ void remove_mean_k(int n, double* __restrict__ x, const double* __restrict__ part, int nblk, int nq,
+                              int q) {
+  __shared__ double tot[1];
+  grid_totals(part + (int64_t)q * nblk, nblk, 1, tot);
+  const double mean = tot[0] / (double)n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = x[i] - mean;
+}
+
+__global__ void sum_partials_k(const double* __restrict__ part, int nblk, int nq, int npairs,
+                               const int32_t* __restrict__ q_of, double* __restrict__ out) {
+  for (int j = blockIdx.x; j < npairs; j += gridDim.x) {
+    const double t = warp_total(part, nblk, nq, q_of[j]);
+    if (threadIdx.x == 0) out[j] = t;
+  }
+}
+
+// ------------------------------------------------------------------------------ energy
+// Tb = fixed ? tval : T_P (+ gT_P . dbt); outlet backflow (Fb < 0) takes tval (simple.py:783-791)
+template <int DIM>
+__global__ void energy_bvals_k(b2s_mesh m, b2s_bc bc, const double* __restrict__ T, const double* __restrict__ gT,
+                               const double* __restrict__ Fb, double* __restrict__ Tb) {
+  const int nc = m.nc, nb = m.nb;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nb; f += gridDim.x * blockDim.x) {
+    const int P = m.bP[f];
+    double TP = T[P];
+    if (gT) {
+      double s = 0.0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        const double t = gT[(int64_t)a * nc + P] * m.dbt[(int64_t)a * nb + f];
+        s = (a == 0) ? t : s + t;
+      }
+      TP = TP + s;
+    }
+    double v = bc.m_tfix[f] != 0.0 ? bc.tval[f] : TP;
+    if (bc.m_out[f] != 0.0 && Fb[f] < 0.0) v = bc.tval[f];
+    Tb[f] = v;
+  }
+}
+
+template <int DIM>
+__global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, double gamma, double cp, double aT, int second,
+                                  const double* __restrict__ T, const double* __restrict__ gT,
+                                  const double* __restrict__ Tb, const double* __restrict__ F,
+                                  const double* __restrict__ Fb, const double* __restrict__ esrc,
+                                  double* __restrict__ val, double* __restrict__ diag_out, double* __restrict__ inv_out,
+                                  double* __restrict__ b_out, double* __restrict__ br_out, double* __restrict__ part) {
+  __shared__ double red[(kThreads / 32 + 1) * 2];
+  const int nc = m.nc, nb = m.nb;
+  double acc[2] = {0.0, 0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    RowOut<DIM, 1> o = transport_row<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
+                                             second != 0, val, true);
+    // q_in = Cb(flux tval |Sb| / cp) (+ source)
+    double q = 0.0;
+    for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) q += bc.m_tflux[f] * bc.tval[f] * m.Sb_mag[f] / cp;
+    if (esrc) q = q + esrc[c];
+    const double rhs = o.rhs[0] + q;
+    const double diag = o.diag;
+    const double Au = row_apply(m, val, c, diag, T);
+    acc[0] += fabs(rhs - Au);
+    acc[1] += fabs(diag * T[c]);
+    const double dr = diag / aT;
+    val[m.slot_diag[c]] = dr;
+    inv_out[c] = 1.0 / dr;
+    diag_out[c] = diag;
+    b_out[c] = rhs;
+    br_out[c] = rhs + (((1.0 - aT) / aT) * diag) * T[c];
+  }
+  block_partials<2>(acc, red, part);
+}
+
+}  // namespace b2s
+
+using namespace b2s;
+
+static unsigned part_grid(int64_t n) {
+  int64_t g = cdiv(n > 0 ? n : 1, kThreads);
+  return (unsigned)(g < kMaxCoopBlocks ? g : kMaxCoopBlocks);
+}
+
+template <int DIM>
+static void launch_ls(const b2s_mesh* m, int nfield, const double* phi, const double* phib, double* grad,
+                      cudaStream_t st) {
+  unsigned g = grid_for(m->nc);
+  switch (nfield) {
+    case 1: ls_gradient_k<DIM, 1><<<g, kThreads, 0, st>>>(*m, phi, phib, grad); break;
+    case 2: ls_gradient_k<DIM, 2><<<g, kThreads, 0, st>>>(*m, phi, phib, grad); break;
+    case 3: ls_gradient_k<DIM, 3><<<g, kThreads, 0, st>>>(*m, phi, phib, grad); break;
+    default: ls_gradient_k<DIM, 4><<<g, kThreads, 0, st>>>(*m, phi, phib, grad); break;
+  }
+}
+
+extern "C" {
+
+int b2s_abi_version(void) { return B2S_ABI_VERSION; }
+
+int b2s_device_sm_count(void) {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  return n;
+}
+
+int b2s_part_blocks(int32_t n) { return (int)part_grid(n); }
+
+static bool mesh_ok(const b2s_mesh* m) {
+  return m && m->nc > 0 && m->nf >= 0 && m->nb >= 0 && (m->dim == 2 || m->dim == 3) && m->own_ptr && m->fP &&
+         m->fN && m->bptr;
+}
+
+int b2s_face_interp_d(const b2s_mesh* m, int k, const double* phi, double* out, b2s_stream_t s) {
+  if (!mesh_ok(m) || k < 1 || !phi || !out) return B2S_ERR_ARG;
+  if (m->nf == 0) return B2S_OK;
+  face_interp_k<<<grid_for((int64_t)m->nf * k), kThreads, 0, (cudaStream_t)s>>>(*m, k, phi, out);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_ls_gradient_d(const b2s_mesh* m, int nfield, const double* phi, const double* phib, double* grad,
+                      b2s_stream_t s) {
+  if (!mesh_ok(m) || nfield < 1 || nfield > 4 || !phi || (!phib && m->nb) || !grad) return B2S_ERR_ARG;
+  if (m->dim == 2) launch_ls<2>(m, nfield, phi, phib, grad, (cudaStream_t)s);
+  else launch_ls<3>(m, nfield, phi, phib, grad, (cudaStream_t)s);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_gg_gradient_d(const b2s_mesh* m, const double* phi, const double* phib, const double* grad, double* out,
+                      b2s_stream_t s) {
+  if (!mesh_ok(m) || !phi || (!phib && m->nb) || !out) return B2S_ERR_ARG;
+  unsigned g = grid_for(m->nc);
+  if (m->dim == 2) gg_gradient_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, phi, phib, grad, out);
+  else gg_gradient_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, phi, phib, grad, out);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_assemble_d(const b2s_mesh* m, const double* diag, const double* aPN, const double* aNP, double* val,
+                   b2s_stream_t s) {
+  if (!mesh_ok(m) || !diag || (!aPN && m->nf) || (!aNP && m->nf) || !val || !m->rowptr) return B2S_ERR_ARG;
+  assemble_k<<<grid_for(m->nc), kThreads, 0, (cudaStream_t)s>>>(*m, diag, aPN, aNP, val);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_flow_bvals_d(const b2s_mesh* m, const b2s_bc* bc, const double* Up, const double* gUp, const double* gpf,
+                     double* bUp, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !Up || !bUp) return B2S_ERR_ARG;
+  if (m->nb == 0) return B2S_OK;
+  unsigned g = grid_for(m->nb);
+  if (m->dim == 2) flow_bvals_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, Up, gUp, gpf, bUp);
+  else flow_bvals_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, Up, gUp, gpf, bUp);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_momentum_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Up,
+                            const double* gUp, const double* gp, const double* bUp, const double* F,
+                            const double* Fb, const double* porosity, const double* msrc, double* val,
+                            double* diag, double* inv, double* dP, double* b, double* br, double* part,
+                            b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !diag || !inv || !dP || !b ||
+      !br || !part || !(prm->relax_u > 0.0))
+    return B2S_ERR_ARG;
+  unsigned g = part_grid(m->nc);
+  if (m->dim == 2)
+    momentum_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb, porosity,
+                                                                 msrc, val, diag, inv, dP, b, br, part);
+  else
+    momentum_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb, porosity,
+                                                                 msrc, val, diag, inv, dP, b, br, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_pressure_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Ustar,
+                            const double* p, const double* gp, const double* dP, double* Fst, double* cf,
+                            double* Fbst, double* cb, double* val, double* rhs, double* part, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !prm || !Ustar || !p || !gp || !dP || !Fst || !cf || !Fbst || !cb || !val || !rhs ||
+      !part)
+    return B2S_ERR_ARG;
+  unsigned g = part_grid(m->nc);
+  if (m->dim == 2)
+    pressure_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Ustar, p, gp, dP, Fst, cf, Fbst, cb,
+                                                                 val, rhs, part);
+  else
+    pressure_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Ustar, p, gp, dP, Fst, cf, Fbst, cb,
+                                                                 val, rhs, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_correct_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Fst,
+                  const double* cf, const double* Fbst, const double* cb, const double* pp, const double* p,
+                  const double* Ustar, const double* dP, double* F, double* Fb, double* Up_new, double* part,
+                  b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !prm || !Fst || !cf || !Fbst || !cb || !pp || !p || !Ustar || !dP || !F || !Fb ||
+      !Up_new || !part)
+    return B2S_ERR_ARG;
+  unsigned g = part_grid(m->nc);
+  if (m->dim == 2)
+    correct_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Fst, cf, Fbst, cb, pp, p, Ustar, dP, F, Fb,
+                                                       Up_new, part);
+  else
+    correct_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Fst, cf, Fbst, cb, pp, p, Ustar, dP, F, Fb,
+                                                       Up_new, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_remove_mean_d(int32_t n, double* x, const double* part, int nblk, int nq, int q, b2s_stream_t s) {
+  if (n <= 0 || !x || !part || nblk <= 0 || nq <= 0 || q < 0 || q >= nq) return B2S_ERR_ARG;
+  remove_mean_k<<<part_grid(n), kThreads, 0, (cudaStream_t)s>>>(n, x, part, nblk, nq, q);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_sum_partials_d(const double* part, int nblk, int nq, int npairs, const int32_t* q_of, double* out,
+                       b2s_stream_t s) {
+  if (!part || nblk <= 0 || nq <= 0 || npairs <= 0 || !q_of || !out) return B2S_ERR_ARG;
+  sum_partials_k<<<(unsigned)npairs, 32, 0, (cudaStream_t)s>>>(part, nblk, nq, npairs, q_of, out);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_energy_bvals_d(const b2s_mesh* m, const b2s_bc* bc, const double* T, const double* gT, const double* Fb,
+                       double* Tb, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !T || !Fb || !Tb) return B2S_ERR_ARG;
+  if (m->nb == 0) return B2S_OK;
+  unsigned g = grid_for(m->nb);
+  if (m->dim == 2) energy_bvals_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, T, gT, Fb, Tb);
+  else energy_bvals_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, T, gT, Fb, Tb);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp, double relax_T,
+                          int second_order, const double* T, const double* gT, const double* Tb, const double* F,
+                          const double* Fb, const double* esrc, double* val, double* diag, double* inv, double* b,
+                          double* br, double* part, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !T || !gT || (!Tb && m->nb) || !F || !Fb || !val || !diag || !inv || !b || !br ||
+      !part || !(relax_T > 0.0) || !(cp != 0.0))
+    return B2S_ERR_ARG;
+  unsigned g = part_grid(m->nc);
+  if (m->dim == 2)
+    energy_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT, Tb,
+                                                               F, Fb, esrc, val, diag, inv, b, br, part);
+  else
+    energy_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT, Tb,
+                                                               F, Fb, esrc, val, diag, inv, b, br, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+}  // extern "C"

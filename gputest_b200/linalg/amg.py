@@ -1,0 +1,248 @@
+"""Smoothed-aggregation AMG hierarchy for the pressure-correction solve on B200.
+
+Set-up follows ``flowtrace/linalg/amg.py:80-117`` once, on the host, on the first matrix it
+is given: strength of connection (theta = 0.08), greedy three-pass aggregation (the C++ helper
+``b2s_host_aggregate``), and the resulting sparsity patterns of P = (I - w D^-1 A) T,
+W = A P and A_c = P^T W, level by level. From then on the aggregates and patterns are fixed
+and every numeric quantity is rebuilt on the device by ``rebuild()`` (``b2s_amg_rebuild_d``):
+D^-1, the spectral radius by 15 power iterations from the reference's start vector
+(``default_rng(0)``, ``amg.py:69-77``), P, R = P^T, the Galerkin products and the inverse of
+the coarsest matrix. The V-cycle (2+2 damped-Jacobi sweeps, w = 0.8) runs inside the PCG
+kernel.
+
+Difference from the reference, by design: the reference re-aggregates at every rebuild. Here
+the aggregates of the first build are kept; the strength graph they come from is recomputed
+by ``strength_changed()`` so a caller can detect when it would differ. ``max_coarse``
+defaults to 150 (the reference's 300) so that the coarsest matrix is inverted in one block's
+shared memory; 300 reproduces the reference's hierarchy exactly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import scipy.sparse as sp
+
+from .. import _lib
+
+
+def strength(A: sp.csr_matrix, theta: float) -> sp.csr_matrix:
+    """|a_ij| >= theta sqrt(|a_ii a_jj|), i != j (``flowtrace/linalg/amg.py:60-66``)."""
+    A = A.tocoo()
+    d = np.abs(A.diagonal())
+    mask = (A.row != A.col) & (np.abs(A.data) >= theta * np.sqrt(d[A.row] * d[A.col]))
+    S = sp.csr_matrix((np.ones(int(mask.sum())), (A.row[mask], A.col[mask])), shape=A.shape)
+    S.sort_indices()
+    return S
+
+
+def aggregate(S: sp.csr_matrix):
+    """Greedy aggregation of the strength graph (``flowtrace/linalg/amg.py:25-57``), in C++."""
+    n = S.shape[0]
+    indptr = np.ascontiguousarray(S.indptr, dtype=np.int64)
+    indices = np.ascontiguousarray(S.indices, dtype=np.int64)
+    agg = np.empty(n, dtype=np.int64)
+    na = _lib.lib().b2s_host_aggregate(n, indptr.ctypes.data, indices.ctypes.data, agg.ctypes.data)
+    if na < 0:
+        raise RuntimeError("b2s_host_aggregate failed")
+    return agg, int(na)
+
+
+def spectral_radius(M, iters=15, seed=0) -> float:
+    """Power iteration of ``flowtrace/linalg/amg.py:69-77`` (host, set-up only)."""
+    x = np.random.default_rng(seed).standard_normal(M.shape[0])
+    lam = 1.0
+    for _ in range(iters):
+        y = M @ x
+        lam = np.linalg.norm(y) / max(np.linalg.norm(x), 1e-300)
+        x = y / max(np.linalg.norm(y), 1e-300)
+    return lam
+
+
+def strong_mask(A: sp.csr_matrix, theta: float) -> np.ndarray:
+    """Per stored entry of A (CSR order): True where the connection is strong (amg.py:60-66)."""
+    A = sp.csr_matrix(A)
+    rows = np.repeat(np.arange(A.shape[0]), np.diff(A.indptr))
+    d = np.abs(A.diagonal())
+    return (rows != A.indices) & (np.abs(A.data) >= theta * np.sqrt(d[rows] * d[A.indices]))
+
+
+def _pattern(M) -> sp.csr_matrix:
+    M = sp.csr_matrix(M)
+    M = sp.csr_matrix((np.ones(M.nnz, dtype=np.float64), M.indices, M.indptr), shape=M.shape)
+    M.sum_duplicates()
+    M.sort_indices()
+    return M
+
+
+class AMGHierarchy:
+    """Fixed-pattern SA-AMG hierarchy whose numeric part lives on the device.
+
+    ``A_host`` is the first matrix in the reference's numbering (SciPy CSR); ``perm`` maps
+    device rows to reference rows for level 0, whose device pattern is ``(rowptr, col)`` with
+    ``diag_slot``; ``val`` is the device tensor of level-0 values that the solver rewrites
+    before every rebuild.
+    """
+
+    def __init__(self, A_host, perm, rowptr, col, diag_slot, val, slot_ref, singular=False, theta=0.08,
+                 max_coarse=150, max_levels=20, sweeps=2, omega=0.8):
+        import torch
+
+        dev = val.device
+        self.singular, self.sweeps, self.omega, self.theta = bool(singular), int(sweeps), float(omega), theta
+        A = sp.csr_matrix(A_host, dtype=np.float64)
+        perm = np.asarray(perm, dtype=np.int64)
+        n0 = A.shape[0]
+        # ---- host set-up on the reference numbering (values drive the coarse strength graphs)
+        aggs, counts, mats = [], [], []
+        while A.shape[0] > max_coarse and len(aggs) < max_levels - 1:
+            S = strength(A, theta)
+            agg, na = aggregate(S)
+            if na >= A.shape[0] * 0.9:
+                break
+            T = sp.csr_matrix((np.ones(A.shape[0]), (np.arange(A.shape[0]), agg)), shape=(A.shape[0], na))
+            cnt = np.asarray(T.sum(axis=0)).ravel()
+            T = T @ sp.diags(1.0 / np.sqrt(cnt))
+            Dinv = 1.0 / A.diagonal()
+            DA = sp.diags(Dinv) @ A
+            rho = spectral_radius(DA)
+            P = (T - (4.0 / 3.0 / rho) * (DA @ T)).tocsr()
+            aggs.append(agg)
+            counts.append(cnt)
+            mats.append(A)
+            A = (P.T @ A @ P).tocsr()
+        # no aggregation (at most max_coarse rows, or too weakly connected): the preconditioner is
+        # the coarse solve of the matrix itself, as in the reference
+        self.n_levels = len(aggs) + 1
+        # ---- structural patterns and device buffers, level 0 in device numbering
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
+        self._keep = []
+        self.sizes = []
+        h = self.c = _lib.Amg()
+        h.nlevels = len(aggs)
+        h.singular = int(self.singular)
+        h.sweeps = self.sweeps
+        h.omega = self.omega
+        rp = np.asarray(rowptr.cpu().numpy(), dtype=np.int64)
+        cl = np.asarray(col.cpu().numpy(), dtype=np.int64)
+        Apat = sp.csr_matrix((np.ones(cl.size), cl, rp), shape=(n0, n0))
+        # the hierarchy's own copy of the level-0 values: like the reference's preconditioner
+        # object, the V-cycle keeps the matrix of the last rebuild until the next one
+        self.src_val = val
+        self.val0 = torch.empty_like(val)
+        self.val0.copy_(val)
+        level_val = self.val0
+        level_rowptr, level_col, level_diag = rowptr, col, diag_slot
+        self.rowptr0, self.col0, self.n0 = rowptr, col, n0
+        for l, (agg, cnt) in enumerate(zip(aggs, counts)):
+            n = Apat.shape[0]
+            na = cnt.size
+            if l == 0:
+                agg_l = agg[perm]
+                x0 = np.random.default_rng(0).standard_normal(n)[perm]
+            else:
+                agg_l = agg
+                x0 = np.random.default_rng(0).standard_normal(n)
+            T = sp.csr_matrix((np.ones(n), (np.arange(n), agg_l)), shape=(n, na))
+            Pp = _pattern(_pattern(Apat) @ T)
+            Wp = _pattern(_pattern(Apat) @ Pp)
+            Cp = _pattern(Pp.T.tocsr() @ Wp)
+            # R = P^T with the map from R entries to P entries
+            prow = np.repeat(np.arange(n), np.diff(Pp.indptr))
+            order = np.lexsort((prow, Pp.indices))
+            r_col = prow[order]
+            r_rowptr = np.concatenate([[0], np.cumsum(np.bincount(Pp.indices, minlength=na))])
+            # strength flags of the set-up on this level's device pattern
+            if l == 0:
+                flags = strong_mask(mats[0], theta)[slot_ref]
+            else:
+                Sh = mats[l]
+                rows_h = np.repeat(np.arange(n), np.diff(Sh.indptr))
+                keys_s = (rows_h * n + Sh.indices)[strong_mask(Sh, theta)]
+                rows_p = np.repeat(np.arange(n), np.diff(Apat.indptr))
+                flags = np.isin(rows_p.astype(np.int64) * n + Apat.indices, keys_s)
+            L = h.levels[l]
+            L.n, L.nnz, L.nc, L.p_nnz, L.w_nnz = n, Apat.nnz, na, Pp.nnz, Wp.nnz
+            bufs = {
+                "rowptr": level_rowptr, "col": level_col, "val": level_val, "diag_slot": level_diag,
+                "dinv": torch.empty(n, dtype=torch.float64, device=dev), "agg": i32(agg_l),
+                "tval": f64(1.0 / np.sqrt(cnt)), "x0": f64(x0), "p_rowptr": i32(Pp.indptr), "p_col": i32(Pp.indices),
+                "p_val": torch.empty(Pp.nnz, dtype=torch.float64, device=dev), "r_rowptr": i32(r_rowptr),
+                "r_col": i32(r_col), "r_from_p": i32(order), "r_val": torch.empty(Pp.nnz, dtype=torch.float64, device=dev),
+                "w_rowptr": i32(Wp.indptr), "w_col": i32(Wp.indices),
+                "w_val": torch.empty(Wp.nnz, dtype=torch.float64, device=dev),
+                "rho": torch.zeros(1, dtype=torch.float64, device=dev),
+                "strong": torch.as_tensor(np.ascontiguousarray(flags, dtype=np.uint8), device=dev),
+            }
+            for k, v in bufs.items():
+                setattr(L, k, v.data_ptr())
+            self._keep.append(bufs)
+            self.sizes.append(n)
+            # next level: pattern Cp in aggregate numbering
+            Apat = Cp
+            level_rowptr, level_col = i32(Cp.indptr), i32(Cp.indices)
+            level_val = torch.empty(Cp.nnz, dtype=torch.float64, device=dev)
+            rows = np.repeat(np.arange(Cp.shape[0]), np.diff(Cp.indptr))
+            dpos = np.flatnonzero(Cp.indices == rows)
+            if dpos.size != Cp.shape[0]:
+                raise RuntimeError("a coarse matrix lacks a diagonal entry")
+            level_diag = i32(dpos)
+            self._keep.append({"rowptr": level_rowptr, "col": level_col, "val": level_val, "diag": level_diag})
+        nc = Apat.shape[0]
+        self.coarse_n = nc
+        self.sizes.append(nc)
+        self.coarse_val = level_val
+        self.coarse_inv = torch.empty((nc, nc), dtype=torch.float64, device=dev)
+        h.coarse_n = nc
+        h.coarse_rowptr, h.coarse_col = level_rowptr.data_ptr(), level_col.data_ptr()
+        h.coarse_val, h.coarse_inv = level_val.data_ptr(), self.coarse_inv.data_ptr()
+        self.cref = ctypes.byref(h)
+        L = _lib.lib()
+        wb = L.b2s_amg_workspace_bytes(self.cref)
+        pb = L.b2s_pcg_workspace_bytes(self.cref)
+        if wb < 0 or pb < 0:
+            raise RuntimeError("invalid AMG hierarchy")
+        self.work_rebuild = torch.empty(max(wb, 8) // 8 + 1, dtype=torch.float64, device=dev)
+        self.work_pcg = torch.empty(max(pb, 8) // 8 + 1, dtype=torch.float64, device=dev)
+        self._count = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._count_host = torch.zeros(1, dtype=torch.int32)
+        if dev.type == "cuda":
+            self._count_host = self._count_host.pin_memory()
+
+    def strength_changed(self, stream=None) -> bool:
+        """True when, with the current level matrices, some level's strength graph differs from the
+        set-up's: the reference would then build different aggregates (it re-aggregates at every
+        rebuild). Synchronises the stream."""
+        import torch
+
+        _lib.check(_lib.lib().b2s_amg_strength_changes_d(self.cref, self.theta, self._count.data_ptr(),
+                                                         _lib.stream_ptr(stream)), "b2s_amg_strength_changes_d")
+        self._count_host.copy_(self._count, non_blocking=True)
+        (stream or torch.cuda.current_stream()).synchronize()
+        return int(self._count_host[0]) != 0
+
+    def rebuild(self, stream=None):
+        """Copy the current level-0 values and recompute every numeric quantity (device)."""
+        self.val0.copy_(self.src_val)
+        _lib.check(_lib.lib().b2s_amg_rebuild_d(self.cref, self.work_rebuild.data_ptr(),
+                                                self.work_rebuild.numel() * 8, _lib.stream_ptr(stream)),
+                   "b2s_amg_rebuild_d")
+
+    def vcycle(self, b, stream=None):
+        import torch
+
+        x = torch.empty_like(b)
+        _lib.check(_lib.lib().b2s_amg_vcycle_d(self.cref, b.contiguous().data_ptr(), x.data_ptr(),
+                                               self.work_pcg.data_ptr(), self.work_pcg.numel() * 8,
+                                               _lib.stream_ptr(stream)), "b2s_amg_vcycle_d")
+        return x
+
+    def pcg(self, b, x, tol, maxiter, project, info, stream=None):
+        """Solve A x = b by AMG-PCG, A the current level-0 matrix (``src_val``); info is the device
+        address of a b2s_solve_info record."""
+        _lib.check(_lib.lib().b2s_pcg_amg_d(self.cref, self.n0, self.rowptr0.data_ptr(), self.col0.data_ptr(),
+                                            self.src_val.data_ptr(), b.data_ptr(), x.data_ptr(), float(tol), int(maxiter),
+                                            int(bool(project)), self.work_pcg.data_ptr(), self.work_pcg.numel() * 8,
+                                            info, _lib.stream_ptr(stream)), "b2s_pcg_amg_d")

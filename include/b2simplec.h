@@ -1,0 +1,291 @@
+/* b2simplec — the SIMPLEC outer iteration of an unstructured finite-volume solver, as
+ * hand-written CUDA for NVIDIA B200 (sm_100a), behind a plain C ABI.
+ *
+ * Counterpart of FlowTrace's native kernel ABI (flowtrace/native/fvm_kernels.h:27-72, ABI 2)
+ * and of the array code of flowtrace/unstructured/simple.py:500-703 that calls it. Differences
+ * from the reference's ABI, all deliberate:
+ *   - every pointer is a DEVICE pointer; each call takes the stream it is ordered on and
+ *     never synchronises it (results that the host needs are written to device memory);
+ *   - cell/face indices are int32 (the reference passes int64 face/cell indices);
+ *   - every function returns an int status: B2S_OK, or a negative B2S_ERR_* code;
+ *   - the library never allocates: callers pass work space, sized by the *_workspace_bytes
+ *     queries (the reference's ft_bicgstab_jacobi takes its 7n-double work array the same way);
+ *   - vector fields are component-major ("SoA"): a field with k components over n entities is
+ *     k contiguous arrays of n values, component c at offset c*n.
+ *
+ * Entity order: cells in the mesh's device order (a reverse Cuthill-McKee permutation of the
+ * reference's order), interior faces sorted by (owner, reference face index), boundary faces
+ * sorted by (owner, reference boundary-face index). The host layer keeps the permutations
+ * and converts to and from the reference's order.
+ */
+#ifndef B2SIMPLEC_H
+#define B2SIMPLEC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2S_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define B2S_API __attribute__((visibility("default")))
+#else
+#define B2S_API
+#endif
+
+#define B2S_OK 0
+#define B2S_ERR_ARG (-1)        /* invalid size, null pointer or unsupported option */
+#define B2S_ERR_LAUNCH (-2)     /* a kernel launch failed (cudaGetLastError) */
+#define B2S_ERR_WORKSPACE (-3)  /* work space smaller than the *_workspace_bytes query */
+#define B2S_ERR_DEVICE (-4)     /* no usable device, or a device query failed */
+
+typedef struct CUstream_st* b2s_stream_t; /* a cudaStream_t; NULL is the legacy default stream */
+
+/* Finite-volume description of one mesh (device arrays). Counterpart of the arrays that
+ * flowtrace/unstructured/fvmesh.py:61-230 precomputes. */
+typedef struct b2s_mesh {
+  int32_t nc, nf, nb, dim, nnz;
+  /* interior faces: owner, neighbour, reference interior-face index */
+  const int32_t* fP;
+  const int32_t* fN;
+  const int32_t* forig;
+  const int32_t* own_ptr;  /* [nc+1]: the faces a cell owns are own_ptr[c] .. own_ptr[c+1]-1 */
+  const int32_t* nei_ptr;  /* [nc+1] */
+  const int32_t* nei_face; /* [nf]: faces whose neighbour is the cell, by reference face index */
+  const int32_t* bP;       /* [nb] boundary-face owner */
+  const int32_t* bptr;     /* [nc+1]: boundary faces of a cell */
+  const double* w;         /* [nf] owner interpolation weight */
+  const double* alpha;     /* [nf] S.S / S.d */
+  const double* wl;        /* [nf] least-squares weight 1/|d|^2 */
+  const double* S;         /* [dim][nf] area vector, owner -> neighbour */
+  const double* d;         /* [dim][nf] x_N - x_P */
+  const double* Tv;        /* [dim][nf] non-orthogonal part S - alpha d */
+  const double* dxm;       /* [dim][nf] face centre minus its point on the P-N line */
+  const double* dPf;       /* [dim][nf] owner centre -> face centre */
+  const double* dNf;       /* [dim][nf] neighbour centre -> face centre */
+  const double* alpha_b;   /* [nb] */
+  const double* wlb;       /* [nb] */
+  const double* Sb_mag;    /* [nb] */
+  const double* Sb;        /* [dim][nb] outward area vector */
+  const double* db;        /* [dim][nb] face centre minus owner centre */
+  const double* nbv;       /* [dim][nb] unit outward normal */
+  const double* dbt;       /* [dim][nb] tangential part of db */
+  const double* vol;       /* [nc] */
+  const double* Ginv;      /* [dim][dim][nc] inverse least-squares matrices */
+  const int32_t* rowptr;   /* [nc+1] CSR pattern of cell-cell operators */
+  const int32_t* col;      /* [nnz] (each row in the reference's column order) */
+  const int32_t* slot_diag;/* [nc] */
+  const int32_t* slot_PN;  /* [nf] CSR slot of (P, N) */
+  const int32_t* slot_NP;  /* [nf] CSR slot of (N, P) */
+} b2s_mesh;
+
+/* Boundary conditions as face masks (0/1 doubles, as flowtrace/unstructured/simple.py:228-240). */
+typedef struct b2s_bc {
+  const double* m_wall;
+  const double* m_inlet;
+  const double* m_pres;    /* outlet or pressure opening */
+  const double* m_sym;
+  const double* m_dirvel;  /* wall, inlet or symmetry: Dirichlet velocity */
+  const double* ub_fixed;  /* [dim][nb] */
+  const double* pb_fixed;  /* [nb] */
+  const double* m_tfix;    /* [nb] fixed temperature */
+  const double* m_tflux;   /* [nb] given heat flux */
+  const double* m_out;     /* [nb] outlet (backflow takes tval) */
+  const double* tval;      /* [nb] */
+} b2s_bc;
+
+/* ----------------------------------------------------------------------------------------- */
+B2S_API int b2s_abi_version(void);
+/* Number of multiprocessors of the current device (0 without a device). */
+B2S_API int b2s_device_sm_count(void);
+
+/* out[c][f] = w[f] phi[c][P] + (1 - w[f]) phi[c][N] for k components.
+ * Replaces ft_face_interp (flowtrace/native/fvm_kernels.h:34-36). */
+B2S_API int b2s_face_interp_d(const b2s_mesh* m, int k, const double* phi, double* out, b2s_stream_t s);
+
+/* Least-squares cell gradients of nfield fields at once: phi [nfield][nc], phib [nfield][nb],
+ * grad [nfield][dim][nc]. Replaces ft_ls_gradient (fvm_kernels.h:38-44). */
+B2S_API int b2s_ls_gradient_d(const b2s_mesh* m, int nfield, const double* phi, const double* phib, double* grad,
+                      b2s_stream_t s);
+
+/* Green-Gauss gradient with the skewness correction from grad (NULL: none); out [dim][nc].
+ * Replaces ft_gg_gradient (fvm_kernels.h:46-53). */
+B2S_API int b2s_gg_gradient_d(const b2s_mesh* m, const double* phi, const double* phib, const double* grad, double* out,
+                      b2s_stream_t s);
+
+/* CSR values of a cell-cell operator from its diagonal and face coefficients (faces sharing a
+ * cell pair are summed). Replaces ft_assemble (fvm_kernels.h:55-58). */
+B2S_API int b2s_assemble_d(const b2s_mesh* m, const double* diag, const double* aPN, const double* aNP, double* val,
+                   b2s_stream_t s);
+
+/* y[c][i] = sum_j A[i,j] x[c][j] for k right-hand sides. Replaces ft_csr_spmm (fvm_kernels.h:30-32). */
+B2S_API int b2s_spmv_d(int32_t n, int k, const int32_t* rowptr, const int32_t* col, const double* val, const double* x,
+               double* y, b2s_stream_t s);
+
+/* Outcome of a Krylov solve, per system, written to device memory. */
+typedef struct b2s_solve_info {
+  int32_t iterations;
+  int32_t converged;
+  double residual; /* final relative residual; NaN after a breakdown with a non-finite residual */
+} b2s_solve_info;
+
+/* Jacobi-preconditioned BiCGSTAB on nrhs (1..3) independent systems that share one matrix:
+ * b, x, inv_diag are [nrhs][n] ([n] for inv_diag); x holds x0 on entry. Same algorithm and
+ * stopping rules as flowtrace/linalg/krylov.py:68-121 with relative_to_initial, per system.
+ * Replaces ft_bicgstab_jacobi (fvm_kernels.h:60-66); info is [nrhs] device structs. */
+B2S_API int64_t b2s_bicgstab_workspace_bytes(int32_t n, int nrhs);
+B2S_API int b2s_bicgstab_jacobi_d(int32_t n, int nrhs, const int32_t* rowptr, const int32_t* col, const double* val,
+                          const double* b, const double* inv_diag, double* x, double tol, int maxiter,
+                          int relative_to_initial, void* work, int64_t work_bytes, b2s_solve_info* info,
+                          b2s_stream_t s);
+
+/* ----------------------------------------------------------------------------------------- */
+/* Fused stages of one SIMPLEC outer iteration (flowtrace/unstructured/simple.py:500-703).    */
+
+typedef struct b2s_flow_params {
+  double rho, mu, relax_u, relax_p;
+  double body[3];          /* uniform body force per unit volume */
+  int32_t simplec;         /* 1: SIMPLEC d-coefficients, 0: SIMPLE */
+  int32_t second_order;    /* bounded second-order deferred correction in momentum */
+  int32_t singular_p;      /* no pressure boundary: the pressure is fixed by its mean */
+  int32_t pad;
+} b2s_flow_params;
+
+/* Boundary values of p and U (simple.py:305-325) with lagged gradients: Up is [1+dim][nc]
+ * (p, then the velocity components), gUp [1+dim][dim][nc] or NULL, gpf [dim][nc] (the
+ * pressure gradient used by the reconstruction) or NULL; out [1+dim][nb]. */
+B2S_API int b2s_flow_bvals_d(const b2s_mesh* m, const b2s_bc* bc, const double* Up, const double* gUp, const double* gpf,
+                     double* bUp, b2s_stream_t s);
+
+/* Momentum system (simple.py:526-590): coefficients, right-hand sides, CSR values of the
+ * under-relaxed matrix, Jacobi inverse, SIMPLEC d = V/(a_P/alpha_u - sum a_nb), the Fluent-
+ * scaled residual partial sums, and b_r = b + (1-alpha_u)/alpha_u a_P u.
+ *   in:  Up [1+dim][nc], gUp [1+dim][dim][nc], gp [dim][nc] (pressure force gradient),
+ *        bUp [1+dim][nb], F [nf], Fb [nb], porosity [nc] or NULL (Brinkman alpha, adds
+ *        alpha V to a_P), msrc [dim][nc] or NULL (momentum source already times V)
+ *   out: val [nnz] (relaxed), diag [nc] (unrelaxed a_P), inv [nc], dP [nc], b [dim][nc],
+ *        br [dim][nc], part [nblk][2*dim] block partials of sum|b - A u| and sum|a_P u|;
+ *        *nblk receives the number of blocks used (at most b2s_part_blocks(nc)). */
+B2S_API int b2s_part_blocks(int32_t n);
+B2S_API int b2s_momentum_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Up,
+                            const double* gUp, const double* gp, const double* bUp, const double* F,
+                            const double* Fb, const double* porosity, const double* msrc, double* val,
+                            double* diag, double* inv, double* dP, double* b, double* br, double* part,
+                            b2s_stream_t s);
+
+/* Rhie-Chow predictor fluxes and the pressure-correction system (simple.py:583-623):
+ *   in:  Ustar [dim][nc], p [nc], gp [dim][nc], dP [nc]
+ *   out: Fst [nf], cf [nf], Fbst [nb], cb [nb], val [nnz] (A_p), rhs [nc] (= -m*),
+ *        part [nblk] block partials of sum|m*|. */
+B2S_API int b2s_pressure_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Ustar,
+                            const double* p, const double* gp, const double* dP, double* Fst, double* cf,
+                            double* Fbst, double* cb, double* val, double* rhs, double* part, b2s_stream_t s);
+
+/* Corrections (simple.py:638-646): F = F* + c_f (p'_P - p'_N), Fb = Fb* + c_b p'_P,
+ * p_new = p + relax_p p', U_new = U* - d grad_LS(p'). Up_new is [1+dim][nc] (p, U).
+ * part [nblk][3]: sum p_new, sum|F| (owned faces), sum|Fb|. The mean of p_new is removed by
+ * b2s_remove_mean_d when the pressure is singular. */
+B2S_API int b2s_correct_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Fst,
+                  const double* cf, const double* Fbst, const double* cb, const double* pp, const double* p,
+                  const double* Ustar, const double* dP, double* F, double* Fb, double* Up_new, double* part,
+                  b2s_stream_t s);
+
+/* x -= (sum of nblk partials at part[q], stride nq) / n. */
+B2S_API int b2s_remove_mean_d(int32_t n, double* x, const double* part, int nblk, int nq, int q, b2s_stream_t s);
+
+/* Sums column q of nblk x nq block partials into out[j] for the (q, j) pairs listed. */
+B2S_API int b2s_sum_partials_d(const double* part, int nblk, int nq, int npairs, const int32_t* q_of, double* out,
+                       b2s_stream_t s);
+
+/* Energy (simple.py:778-813): boundary temperatures, gradient, assembly and the scaled
+ * residual; T_b uses the lagged gradient gT (NULL on the first iteration).
+ *   out: Tb [nb] */
+B2S_API int b2s_energy_bvals_d(const b2s_mesh* m, const b2s_bc* bc, const double* T, const double* gT, const double* Fb,
+                       double* Tb, b2s_stream_t s);
+/*   in:  T [nc], gT [dim][nc], Tb [nb], F, Fb, esrc [nc] or NULL (already times V/cp)
+ *   out: val [nnz] (relaxed by relax_T), diag, inv, b, br [nc], part [nblk][2] */
+B2S_API int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp, double relax_T,
+                          int second_order, const double* T, const double* gT, const double* Tb, const double* F,
+                          const double* Fb, const double* esrc, double* val, double* diag, double* inv, double* b,
+                          double* br, double* part, b2s_stream_t s);
+
+/* ----------------------------------------------------------------------------------------- */
+/* Smoothed-aggregation AMG (flowtrace/linalg/amg.py:80-146) with aggregates and sparsity
+ * patterns fixed at set-up; every numeric quantity is rebuilt on the device. */
+
+#define B2S_AMG_MAX_LEVELS 20
+
+typedef struct b2s_amg_level {
+  int32_t n, nnz;              /* rows and entries of A */
+  int32_t nc;                  /* rows of the next level */
+  int32_t p_nnz, w_nnz;
+  const int32_t* rowptr;       /* A (level 0: the pressure-correction matrix) */
+  const int32_t* col;
+  double* val;                 /* level 0: the caller's matrix values; coarser: rebuilt */
+  const int32_t* diag_slot;    /* [n] */
+  double* dinv;                /* [n] */
+  const int32_t* agg;          /* [n] aggregate of each row */
+  const double* tval;          /* [nc] 1/sqrt(aggregate size) */
+  const double* x0;            /* [n] start vector of the spectral-radius power iteration */
+  const int32_t* p_rowptr;     /* P = (I - 4/(3 rho) D^-1 A) T, [n x nc], sorted columns */
+  const int32_t* p_col;
+  double* p_val;
+  const int32_t* r_rowptr;     /* R = P^T, [nc x n] */
+  const int32_t* r_col;
+  const int32_t* r_from_p;     /* R entry -> P entry */
+  double* r_val;
+  const int32_t* w_rowptr;     /* W = A P, [n x nc], sorted columns */
+  const int32_t* w_col;
+  double* w_val;
+  double* rho;                 /* [1] spectral radius estimate (device) */
+  const uint8_t* strong;       /* [nnz] strength of each entry at set-up (1: strong), or NULL */
+} b2s_amg_level;
+
+typedef struct b2s_amg {
+  int32_t nlevels;             /* levels with smoothing; the coarse level follows */
+  int32_t coarse_n;
+  int32_t singular;            /* shift the coarse matrix by 1e-10 mean|diag| */
+  int32_t sweeps;              /* Jacobi sweeps before and after the coarse correction */
+  double omega;                /* Jacobi damping */
+  const int32_t* coarse_rowptr;/* coarse CSR (values are level nlevels-1's Galerkin product) */
+  const int32_t* coarse_col;
+  double* coarse_val;
+  double* coarse_inv;          /* [coarse_n][coarse_n] */
+  b2s_amg_level levels[B2S_AMG_MAX_LEVELS];
+} b2s_amg;
+
+/* Rebuild every numeric quantity of the hierarchy from level 0's matrix values. */
+B2S_API int64_t b2s_amg_workspace_bytes(const b2s_amg* h);
+B2S_API int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s);
+
+/* Preconditioned CG with one V-cycle per iteration (flowtrace/linalg/krylov.py:25-65 with
+ * M = SmoothedAggregationAMG) on the operator A = (rowptr, col, val) of n rows; the hierarchy
+ * keeps the matrices of its last rebuild, as the reference's preconditioner object does between
+ * rebuilds. project != 0 removes the mean from the residual and the preconditioned residual
+ * (singular pure-Neumann systems). x starts at zero. */
+B2S_API int64_t b2s_pcg_workspace_bytes(const b2s_amg* h);
+B2S_API int b2s_pcg_amg_d(const b2s_amg* h, int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,
+                          const double* b, double* x, double tol, int maxiter, int project, void* work,
+                          int64_t work_bytes, b2s_solve_info* info, b2s_stream_t s);
+
+/* Number of matrix entries, over all levels with smoothing, whose strength of connection
+ * |a_ij| >= theta sqrt(|a_ii a_jj|) differs from the set-up's (the levels' strong flags); the
+ * reference re-aggregates at every rebuild, so a non-zero count means its aggregates changed.
+ * *count (device int) is overwritten. */
+B2S_API int b2s_amg_strength_changes_d(const b2s_amg* h, double theta, int32_t* count, b2s_stream_t s);
+
+/* Apply one V-cycle: x = M b (for tests of the preconditioner). */
+B2S_API int b2s_amg_vcycle_d(const b2s_amg* h, const double* b, double* x, void* work, int64_t work_bytes, b2s_stream_t s);
+
+/* Host set-up helper: the greedy three-pass aggregation of flowtrace/linalg/amg.py:25-57 on a
+ * strength graph given as HOST CSR arrays; agg[n] (host) receives each node's aggregate and
+ * the return value is the number of aggregates (-1 on invalid arguments). */
+B2S_API int64_t b2s_host_aggregate(int64_t n, const int64_t* indptr, const int64_t* indices, int64_t* agg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
