@@ -16,7 +16,8 @@ LIB_PATH = os.path.join(HERE, "csrc", "libb2simplec.so")
 ABI_VERSION = 1
 
 B2S_OK = 0
-_ERRORS = {-1: "invalid argument", -2: "kernel launch failed", -3: "work space too small", -4: "no usable CUDA device"}
+_ERRORS = {-1: "invalid argument", -2: "kernel launch failed", -3: "work space too small", -4: "no usable CUDA device",
+           -5: "problem larger than the fixed capacity"}
 
 P = ctypes.c_void_p
 I32, I64, F64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
@@ -86,6 +87,8 @@ _SIGS = {
     "b2s_amg_vcycle_d": ([P, P, P, P, I64, P], ctypes.c_int),
     "b2s_host_aggregate": ([I64, P, P, P], I64),
     "b2s_amg_strength_changes_d": ([P, F64, P, P], ctypes.c_int),
+    "b2s_bicgstab_jacobi_noalloc_d": ([I32, ctypes.c_int, P, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, P, P],
+                                      ctypes.c_int),
 }
 
 _lib: Optional[ctypes.CDLL] = None

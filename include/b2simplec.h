@@ -40,6 +40,7 @@ extern "C" {
 #define B2S_ERR_LAUNCH (-2)     /* a kernel launch failed (cudaGetLastError) */
 #define B2S_ERR_WORKSPACE (-3)  /* work space smaller than the *_workspace_bytes query */
 #define B2S_ERR_DEVICE (-4)     /* no usable device, or a device query failed */
+#define B2S_ERR_TOO_LARGE (-5)  /* the problem exceeds a fixed capacity (b2s_bicgstab_jacobi_noalloc_d) */
 
 typedef struct CUstream_st* b2s_stream_t; /* a cudaStream_t; NULL is the legacy default stream */
 
@@ -140,6 +141,20 @@ B2S_API int b2s_bicgstab_jacobi_d(int32_t n, int nrhs, const int32_t* rowptr, co
                           const double* b, const double* inv_diag, double* x, double tol, int maxiter,
                           int relative_to_initial, void* work, int64_t work_bytes, b2s_solve_info* info,
                           b2s_stream_t s);
+
+/* The same Jacobi-BiCGSTAB for callers that cannot allocate device memory (a host code that
+ * reaches the solver only through this C ABI and owns no CUDA allocator, or one whose device
+ * memory is fully handed out before the solve): no work argument; the work space is a static
+ * device array inside the library, sized for n * nrhs <= B2S_NOALLOC_MAX_UNKNOWNS (larger
+ * problems return B2S_ERR_TOO_LARGE), held by every GPU that loads the library until exit. The
+ * first call on a device looks the array's device address up (make it before any stream
+ * capture); calls that overlap on the GPU share the array and race. No counterpart in the
+ * reference, whose ft_bicgstab_jacobi always takes its work array from the caller. */
+#define B2S_NOALLOC_MAX_UNKNOWNS 131072
+B2S_API int b2s_bicgstab_jacobi_noalloc_d(int32_t n, int nrhs, const int32_t* rowptr, const int32_t* col,
+                                          const double* val, const double* b, const double* inv_diag, double* x,
+                                          double tol, int maxiter, int relative_to_initial, b2s_solve_info* info,
+                                          b2s_stream_t s);
 
 /* ----------------------------------------------------------------------------------------- */
 /* Fused stages of one SIMPLEC outer iteration (flowtrace/unstructured/simple.py:500-703).    */
