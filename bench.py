@@ -188,6 +188,20 @@ def cpu_reference(mesh, case, inlet, steps, warmup, budget_s=None):
                if lib is not None else "NumPy/SciPy oracle (reference C++ kernels not built)")}
 
 
+# ---------------------------------------------------------------------------------- replicas
+def max_over_ranks(ms: float, world: int, device=None) -> float:
+    """The slowest rank's time: every rank runs an independent replica, so the job takes as long
+    as its slowest replica (all-reduce MAX; NCCL on CUDA tensors, gloo on CPU ones)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -270,11 +284,7 @@ def main():
         smi_fh.close()
     launches = s.kernel_launches - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), world, "cuda")
     value = world * nc * K / (total_ms / 1e3)
     clocks = parse_clocks(smi_fh.name if smi_fh is not None else "", dev) if smi is not None else None
 
@@ -306,11 +316,7 @@ def main():
     f = s2.fields()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
     h2d = sum(v.numel() * v.element_size() for v in s2.fv.t.values()) + sum(
         v.numel() * v.element_size() for v in s2._bc_t.values())
     d2h = s2.report.numel() * (W + K) + sum(v.nbytes for v in f.values())

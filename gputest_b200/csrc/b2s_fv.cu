@@ -609,6 +609,46 @@ __global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, double gamma, double cp
   block_partials<2>(acc, red, part);
 }
 
+// ------------------------------------------------------------------------------ diagnostics
+// r = b - A x, s = |b| + |A| |x| per row over the CSR in stored order; dval (when given)
+// replaces the diagonal values (the unrelaxed a_P of a system stored relaxed)
+// (flowtrace/unstructured/diagnostics.py:146-151).
+__global__ void row_residuals_k(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                const double* __restrict__ val, const int32_t* __restrict__ slot_diag,
+                                const double* __restrict__ dval, const double* __restrict__ b,
+                                const double* __restrict__ x, double* __restrict__ r, double* __restrict__ sc) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int sd = dval ? slot_diag[i] : -1;
+    double ax = 0.0, as = 0.0;
+    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j) {
+      const double a = (j == sd) ? dval[i] : val[j];
+      const double xj = x[col[j]];
+      ax += a * xj;
+      as += fabs(a) * fabs(xj);
+    }
+    r[i] = b[i] - ax;
+    sc[i] = fabs(b[i]) + as;
+  }
+}
+
+// Cell mass imbalance m = Cdiff F + Cb Fb and throughflow t = Cown|F| + Cnei|F| + Cb|Fb|
+// (diagnostics.py:253-257).
+__global__ void flux_balance_k(b2s_mesh m, const double* __restrict__ F, const double* __restrict__ Fb,
+                               double* __restrict__ mout, double* __restrict__ tout) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < m.nc; c += gridDim.x * blockDim.x) {
+    double mi = 0.0, mb = 0.0, to = 0.0, tn = 0.0, tb = 0.0;
+    for_cdiff(m, c, [&](int f, bool own) { mi += own ? F[f] : -F[f]; });
+    for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) to += fabs(F[f]);
+    for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) tn += fabs(F[m.nei_face[k]]);
+    for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) {
+      mb += Fb[f];
+      tb += fabs(Fb[f]);
+    }
+    mout[c] = mi + mb;
+    tout[c] = (to + tn) + tb;
+  }
+}
+
 }  // namespace b2s
 
 using namespace b2s;
@@ -788,6 +828,23 @@ int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, dou
   else
     energy_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT, Tb,
                                                                F, Fb, esrc, val, diag, inv, b, br, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_row_residuals_d(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,
+                        const int32_t* slot_diag, const double* dval, const double* b, const double* x, double* r,
+                        double* s_out, b2s_stream_t s) {
+  if (n <= 0 || !rowptr || !col || !val || !b || !x || !r || !s_out || (dval && !slot_diag)) return B2S_ERR_ARG;
+  row_residuals_k<<<grid_for(n), kThreads, 0, (cudaStream_t)s>>>(n, rowptr, col, val, slot_diag, dval, b, x, r, s_out);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_flux_balance_d(const b2s_mesh* m, const double* F, const double* Fb, double* mass, double* through,
+                       b2s_stream_t s) {
+  if (!mesh_ok(m) || !F || !Fb || !mass || !through) return B2S_ERR_ARG;
+  flux_balance_k<<<grid_for(m->nc), kThreads, 0, (cudaStream_t)s>>>(*m, F, Fb, mass, through);
   B2S_LAUNCH_CHECK();
   return B2S_OK;
 }

@@ -226,6 +226,15 @@ B2S_API int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double ga
                           const double* Fb, const double* esrc, double* val, double* diag, double* inv, double* b,
                           double* br, double* part, b2s_stream_t s);
 
+/* Row residuals and scales of a system (flowtrace/unstructured/diagnostics.py:146-151):
+ * r = b - A x, s = |b| + |A| |x|; with dval, row i's diagonal entry (slot_diag[i]) is dval[i]. */
+B2S_API int b2s_row_residuals_d(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,
+                                const int32_t* slot_diag, const double* dval, const double* b, const double* x,
+                                double* r, double* s_out, b2s_stream_t s);
+/* Cell mass imbalance (net outflow) and throughflow sum |F| of face fluxes (diagnostics.py:253-257). */
+B2S_API int b2s_flux_balance_d(const b2s_mesh* m, const double* F, const double* Fb, double* mass, double* through,
+                               b2s_stream_t s);
+
 /* ----------------------------------------------------------------------------------------- */
 /* Smoothed-aggregation AMG (flowtrace/linalg/amg.py:80-146) with aggregates and sparsity
  * patterns fixed at set-up; every numeric quantity is rebuilt on the device. */

@@ -1,0 +1,149 @@
+"""Host-side logic on CPU: the C ABI library loads and exports what the header declares, the
+device layout maps back to the reference's numbering, the AMG host set-up reproduces the
+reference's hierarchy, and the case objects validate like the reference's."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+from gputest_b200.mesh.unstructured import box_mesh_3d, cartesian_mesh_2d, compute_geometry, extrude_to_3d
+from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase, default_boundaries
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from gputest_b200 import _lib
+
+    L = _lib.lib()
+    assert L.b2s_abi_version() == _lib.ABI_VERSION
+    header = open(os.path.join(ROOT, "include", "b2simplec.h")).read()
+    declared = re.findall(r"^B2S_API\s+\w+\s+(b2s_\w+)\s*\(", header, flags=re.M)
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(L, name), name
+        assert name in _lib._SIGS, f"{name} is declared in the header but not bound"
+
+
+def test_host_aggregation_is_the_reference_greedy_algorithm():
+    import scipy.sparse as sp
+
+    from gputest_b200.linalg.amg import aggregate, strength
+    from oracle.simplec_oracle import _aggregate_py
+
+    rng = np.random.default_rng(4)
+    A = sp.random(300, 300, density=0.02, random_state=5, format="csr")
+    A = A + A.T + sp.eye(300) * 5
+    S = strength(A.tocsr(), 0.08)
+    a1, n1 = aggregate(S)
+    a2, n2 = _aggregate_py(S.indptr, S.indices, 300)
+    assert n1 == n2 and np.array_equal(a1, a2)
+    assert rng is not None
+
+
+@pytest.mark.parametrize("mesh", [cartesian_mesh_2d(20, 16, triangulate=True, warp=0.05),
+                                  cartesian_mesh_2d(30, 20, triangulate="alternating", jitter=0.2),
+                                  box_mesh_3d(6, 5, 4, 4, 1, 1, jitter=0.1, seed=1),
+                                  extrude_to_3d(cartesian_mesh_2d(6, 5, warp=0.05), 4, 0.5)],
+                         ids=["tri", "alt", "box", "extruded"])
+def test_device_layout_maps_back_to_the_reference_numbering(mesh):
+    from gputest_b200.unstructured.fvmesh import FVMesh
+    from oracle.simplec_oracle import OracleFV
+
+    fv = FVMesh(mesh, device="cpu")
+    o = OracleFV(mesh)
+    t = {k: v.numpy() for k, v in fv.t.items()}
+    perm, nc = fv.perm, fv.nc
+    assert np.array_equal(perm[t["fP"]], o.P[fv.face_ref]) and np.array_equal(perm[t["fN"]], o.N[fv.face_ref])
+    assert np.array_equal(perm[t["bP"]], o.Pb[fv.bface_ref])
+    assert np.array_equal(np.diff(t["own_ptr"]), np.bincount(t["fP"], minlength=nc))
+    assert np.all(t["fP"][np.repeat(np.arange(fv.n_if), 1)] == np.repeat(np.arange(nc), np.diff(t["own_ptr"])))
+    assert np.array_equal(t["fN"][t["nei_face"]], np.repeat(np.arange(nc), np.diff(t["nei_ptr"])))
+    rows = np.repeat(np.arange(nc), np.diff(t["rowptr"]))
+    assert np.array_equal(rows[t["slot_PN"]], t["fP"]) and np.array_equal(t["col"][t["slot_PN"]], t["fN"])
+    assert np.array_equal(rows[t["slot_NP"]], t["fN"]) and np.array_equal(t["col"][t["slot_NP"]], t["fP"])
+    assert np.array_equal(t["col"][t["slot_diag"]], np.arange(nc))
+    # every device CSR row holds its reference row's columns in the reference's order
+    ref_cols = [o.indices[o.indptr[perm[c]]:o.indptr[perm[c] + 1]] for c in range(nc)]
+    dev_cols = [perm[t["col"][t["rowptr"][c]:t["rowptr"][c + 1]]] for c in range(nc)]
+    assert all(np.array_equal(a, b) for a, b in zip(ref_cols, dev_cols))
+    assert np.array_equal(t["S"].T, o.S[fv.face_ref])
+    assert np.array_equal(t["Ginv"].T.reshape(nc, fv.dim, fv.dim), o.Ginv[perm])
+    # matrix_to_host inverts the slot permutation exactly
+    vals = np.arange(fv.nnz, dtype=np.float64)
+    import torch
+
+    A = fv.matrix_to_host(torch.as_tensor(vals))
+    assert np.array_equal(A.indptr, o.indptr) and np.array_equal(A.indices, o.indices)
+    assert np.array_equal(A.data[fv.slot_ref], vals)
+    # reverse Cuthill-McKee does not widen the cell bandwidth
+    assert np.abs(t["fP"] - t["fN"]).max() <= np.abs(o.P - o.N).max()
+
+
+def test_amg_host_setup_reproduces_the_reference_hierarchy():
+    import torch
+
+    from gputest_b200.linalg.amg import AMGHierarchy
+    from gputest_b200.unstructured.fvmesh import FVMesh
+    from oracle.simplec_oracle import OracleSimple, SmoothedAggregationAMG
+
+    mesh = cartesian_mesh_2d(48, 48, triangulate="alternating", jitter=0.2)
+    case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=[1.0, 0.0])}, viscosity=0.01)
+    o = OracleSimple(mesh, case)
+    for _ in range(3):
+        o.step()
+    Ap = o._capture["Ap"]
+    fv = FVMesh(mesh, device="cpu")
+    h = AMGHierarchy(Ap, fv.perm, fv.rowptr, fv.col, fv.t["slot_diag"], torch.as_tensor(Ap.data[fv.slot_ref]),
+                     fv.slot_ref, singular=True, max_coarse=300)
+    ref = SmoothedAggregationAMG(Ap, singular=True)
+    assert h.sizes == [lv[0].shape[0] for lv in ref.levels] + [ref.coarse_inv.shape[0]]
+    agg0 = h._keep[0]["agg"].numpy()
+    assert np.array_equal(agg0, ref.aggregates[0][fv.perm])  # device rows carry the reference aggregates
+
+
+def test_generated_meshes_are_valid():
+    for m, vol in ((cartesian_mesh_2d(16, 12, triangulate="alternating", jitter=0.2), 1.0),
+                   (box_mesh_3d(8, 4, 4, 4.0, 1.0, 1.0, jitter=0.1, seed=1), 4.0)):
+        g = compute_geometry(m)
+        assert g.flipped_faces == 0 and np.all(g.cell_volume > 0)
+        assert g.total_volume == pytest.approx(vol, rel=1e-12)
+    alt = cartesian_mesh_2d(4, 4, triangulate="alternating")
+    assert alt.n_cells == 32 and int((alt.neighbour >= 0).sum()) == 16 + 12 + 12
+
+
+def test_case_validation_matches_the_reference():
+    with pytest.raises(ValueError):
+        BoundarySpec(kind="nonsense")
+    with pytest.raises(ValueError):
+        UnstructuredCase(algorithm="PISO")
+    assert UnstructuredCase(algorithm="simple").relax_p == 0.3
+    with pytest.raises(ValueError):
+        UnstructuredCase(radiation="p1")
+    m = cartesian_mesh_2d(7, 3, 4.0, 1.0, names=("inlet", "outlet", "bottom", "top"),
+                          types=("velocity-inlet", "pressure-outlet", "wall", "wall"))
+    b = default_boundaries(m)
+    assert b["inlet"].kind == "inlet" and b["inlet"].normal_speed == 1.0 and b["outlet"].kind == "outlet"
+
+
+def test_solver_refuses_unsupported_models_without_a_device():
+    from gputest_b200.unstructured.simple import _check_scope
+
+    with pytest.raises(NotImplementedError):
+        _check_scope(UnstructuredCase(turbulence="k-omega-sst"))
+    with pytest.raises(NotImplementedError):
+        _check_scope(UnstructuredCase(unsteady=True))
+    _check_scope(UnstructuredCase())
+
+
+def test_product_path_raises_without_a_cuda_device():
+    import torch
+
+    from gputest_b200 import _lib
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(RuntimeError, match="CUDA device"):
+        _lib.require_device()
