@@ -69,6 +69,40 @@ __global__ void __launch_bounds__(kCoopThreads) power_coop_k(b2s_amg_level L, do
   if (blockIdx.x == 0 && threadIdx.x == 0) *L.rho = lam;
 }
 
+// The same power iteration by one block (levels of at most kPowerBlockRows rows, where a grid
+// barrier per iteration costs more than the work).
+constexpr int kPowerBlockRows = 2048;
+
+__global__ void __launch_bounds__(kCoopThreads) power_block_k(b2s_amg_level L, double* ya, double* yb) {
+  __shared__ double red[(kCoopThreads / 32 + 1) * 2];
+  double* ybuf[2] = {ya, yb};
+  double lam = 1.0, sc = 1.0;
+  for (int it = 0; it < 15; ++it) {
+    const double* xin = it == 0 ? L.x0 : ybuf[(it - 1) & 1];
+    double* yout = ybuf[it & 1];
+    double acc[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+      const double di = L.dinv[i];
+      double s = 0.0;
+      for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
+        const int c = L.col[j];
+        const double xc = it == 0 ? xin[c] : xin[c] / sc;
+        s += (di * L.val[j]) * xc;
+      }
+      yout[i] = s;
+      acc[0] += s * s;
+      const double xi = it == 0 ? xin[i] : xin[i] / sc;
+      acc[1] += xi * xi;
+    }
+    double tot[2];
+    block_sum<2>(acc, red, tot);
+    const double ny = sqrt(tot[0]), nx = sqrt(tot[1]);
+    lam = ny / fmax(nx, 1e-300);
+    sc = fmax(ny, 1e-300);
+  }
+  if (threadIdx.x == 0) *L.rho = lam;
+}
+
 // P[i,J] = T[i,J] - c sum_{k in row i, agg[k] = J} (Dinv_i A_ik) T[k,J], c = (4/3)/rho
 __global__ void pvals_k(b2s_amg_level L) {
   const double c = (4.0 / 3.0) / *L.rho;
@@ -204,13 +238,16 @@ __global__ void __launch_bounds__(kGJThreads) coarse_inverse_k(int n, const int3
     }
     __syncthreads();
     const double piv = rowk[k];
-    for (int e = tid; e < n * n; e += nt) {
-      const int r = e / n, c = e - r * n;
-      double v;
-      if (r == k) v = (c == k) ? 1.0 / piv : rowk[c] / piv;
-      else if (c == k) v = -colk[r] / piv;
-      else v = M[e] - colk[r] * (rowk[c] / piv);
-      M[e] = v;
+    for (int r = tid >> 5; r < n; r += nt >> 5) {  // rows over warps, columns over lanes
+      double* Mr = M + (int64_t)r * n;
+      const double cr = colk[r];
+      for (int c = tid & 31; c < n; c += 32) {
+        double v;
+        if (r == k) v = (c == k) ? 1.0 / piv : rowk[c] / piv;
+        else if (c == k) v = -cr / piv;
+        else v = Mr[c] - cr * (rowk[c] / piv);
+        Mr[c] = v;
+      }
     }
     __syncthreads();
   }
@@ -281,9 +318,13 @@ int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stre
       return B2S_ERR_ARG;
     dinv_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
     B2S_LAUNCH_CHECK();
-    void* args[] = {&L, &xa, &xb, &part0, &part1};  // xa, xb: the two power-iteration buffers
-    if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
-      return B2S_ERR_LAUNCH;
+    if (L.n <= kPowerBlockRows) {
+      power_block_k<<<1, kCoopThreads, 0, st>>>(L, xa, xb);
+    } else {
+      void* args[] = {&L, &xa, &xb, &part0, &part1};  // xa, xb: the two power-iteration buffers
+      if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
+        return B2S_ERR_LAUNCH;
+    }
     pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
     rvals_k<<<grid_for(L.p_nnz), kThreads, 0, st>>>(L);
     wvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);

@@ -154,6 +154,8 @@ class SimpleSolver:
         self.stage_times = defaultdict(float)  # device milliseconds per stage when profile_stages is on
         self.profile_stages = False
         self._events = []
+        self.use_graphs = True  # replay the stage sequence as a CUDA graph when no AMG rebuild is due
+        self._graphs = {}
         self._lag = False  # lagged gradients available for the boundary reconstruction
         self._lagT = False
         self.porosity = None
@@ -438,8 +440,10 @@ class SimpleSolver:
             self.stage_times[name] += a.elapsed_time(b)
         self._events = []
 
-    def _launch(self):
-        """Enqueue one outer iteration's stages on the current stream (no synchronisation)."""
+    def _launch(self, amg_ready=False):
+        """Enqueue one outer iteration's stages on the current stream (no synchronisation).
+        With ``amg_ready`` the AMG hierarchy is current and no host work is done: the sequence
+        can be captured into a CUDA graph."""
         L, fv = _lib.lib(), self.fv
         self._mark("start")
         s = _lib.stream_ptr()
@@ -488,7 +492,8 @@ class SimpleSolver:
                                              self.rhs_p.data_ptr(), pt(self.Q_CONT), s), "b2s_pressure_assemble_d")
         self.kernel_launches += 3  # momentum assembly, BiCGSTAB, pressure assembly
         self._mark("pressure_assembly")
-        self._ensure_amg(s)
+        if not amg_ready:
+            self._ensure_amg(s)
         self._mark("amg_rebuild")
         self._amg.pcg(self.rhs_p, self.pp, self.case.pressure_tol, 200, self.singular_p, self.info_p)
         self.kernel_launches += 1
@@ -550,13 +555,49 @@ class SimpleSolver:
         infos = read_info(raw[self.NQ * 8:])
         return scal, infos
 
+    def _graph_key(self):
+        return (self._cur, self._lag, self._lagT, self.relax_u, self.relax_p, self.algo,
+                None if self.porosity is None else self.porosity.data_ptr(),
+                None if self.mom_source is None else self.mom_source.data_ptr(),
+                None if self.energy_source is None else self.energy_source.data_ptr(), id(self._amg))
+
+    def _launch_graph(self):
+        """Replay (capturing on first use) the CUDA graph of an outer iteration that needs no
+        AMG rebuild: the ~15 launches of the stage sequence become one graph launch."""
+        import torch
+
+        key = self._graph_key()
+        ent = self._graphs.get(key)
+        if ent is None:
+            g = torch.cuda.CUDAGraph()
+            k0 = self.kernel_launches
+            with torch.cuda.graph(g):
+                old, new = self._launch(amg_ready=True)
+            ent = (g, old, new, self.kernel_launches - k0)
+            self.kernel_launches = k0
+            self._graphs[key] = ent
+        g, old, new, nk = ent
+        g.replay()
+        self.kernel_launches += nk
+        self._amg_age += 1
+        return old, new
+
     def step(self) -> float:
         """One outer iteration (``flowtrace/unstructured/simple.py:500-703``)."""
         if self.finished:
             return 0.0
         self._capture = None
         c, dim = self.case, self.dim
-        old, new = self._launch()
+        rebuild_due = self._amg is None or self._amg_age >= self.amg_rebuild
+        if self.use_graphs and not rebuild_due and self._lag and not self.profile_stages:
+            try:
+                old, new = self._launch_graph()
+            except RuntimeError:
+                self.use_graphs = False  # capture unsupported here: enqueue the stages one by one
+                self._graphs.clear()
+                old, new = self._launch()
+        else:
+            old, new = self._launch()
         scal, infos = self._read_report()
         self._cur = new
         mom_info, p_info = infos[:dim], infos[dim]
