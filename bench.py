@@ -50,14 +50,14 @@ def make_workload(name):
         case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=[1.0, 0.0])}, viscosity=0.01,
                                 scheme="upwind", pressure_tol=1e-8, max_iter=300, tol=1e-6)
         desc = {"workload": "cavity 64x64 quads (4,096 cells), Re 100, upwind, PCG 1e-8", "cells": mesh.n_cells}
-        return mesh, case, desc, None
+        return mesh, case, desc, None, {}
     if name == "c2":
         mesh = cartesian_mesh_2d(256, 256, triangulate="alternating", jitter=0.2, seed=0)
         case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=[1.0, 0.0])}, viscosity=1e-3,
                                 scheme="second-order", max_iter=100000, tol=1e-6)
         desc = {"workload": "cavity 256x256 alternating-diagonal triangles (131,072 cells), jitter 0.2h seed 0, "
                             "Re 1000, linear-upwind + non-orthogonal correction, SA-AMG PCG", "cells": mesh.n_cells}
-        return mesh, case, desc, None
+        return mesh, case, desc, None, {}
     if name == "c3":
         names = ("inlet", "outlet", "wall", "wall", "wall", "wall")
         mesh = box_mesh_3d(128, 64, 64, 4.0, 1.0, 1.0, jitter=0.1, seed=1, names=names,
@@ -75,9 +75,12 @@ def make_workload(name):
             solver.set_boundary_velocity("inlet", np.stack([u, 0 * u, 0 * u], axis=1))
             solver.initialize({})
 
+        # smoothed aggregation with the strength rule of pyamg's defaults (theta 0): the reference's
+        # own theta 0.08 needs ~150 CG iterations per solve on this anisotropic mesh already at 65k
+        # cells (operator complexity 6.5); theta 0 needs 4 (complexity 1.5)
         desc = {"workload": "3-D duct 4x1x1, 128x64x64 hexes (524,288 cells), jitter 0.1h seed 1, parabolic inlet "
-                            "Re 500, heated walls 5e3 W/m2, Pr 0.71, FP64", "cells": mesh.n_cells}
-        return mesh, case, desc, inlet
+                            "Re 500, heated walls 5e3 W/m2, Pr 0.71; SA-AMG strength theta 0", "cells": mesh.n_cells}
+        return mesh, case, desc, inlet, {"amg_theta": 0.0}
     raise SystemExit(f"unknown config {name!r}")
 
 
@@ -155,7 +158,7 @@ def parse_clocks(path, dev_index):
 
 
 # ---------------------------------------------------------------------------------- CPU reference
-def cpu_reference(mesh, case, inlet, steps, warmup, budget_s=None):
+def cpu_reference(mesh, case, inlet, steps, warmup, budget_s=None, amg_theta=0.08):
     """Time the reference's CPU path (oracle driver + the reference's C++ kernels when built)."""
     import numpy as np
 
@@ -163,7 +166,7 @@ def cpu_reference(mesh, case, inlet, steps, warmup, budget_s=None):
 
     lib = load_native()
     threads = int(lib.ft_max_threads()) if lib is not None else 1
-    o = OracleSimple(mesh, case, native=lib)
+    o = OracleSimple(mesh, case, native=lib, amg_theta=amg_theta)
     if inlet is not None:
         z = mesh.zone_by_name("inlet")
         fc = o.fv.xfb[o.fv.bzone == z.id]
@@ -209,6 +212,8 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--config", default="c2")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="fp64: the drop-in SimpleSolver; mixed: MixedSimpleSolver (float systems, double residuals)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--converge", action="store_true", help="also run to the 1e-6 residual and report it")
@@ -221,8 +226,8 @@ def main():
         if rank != 0:
             return
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-        mesh, case, desc, inlet = make_workload(args.config)
-        ref = cpu_reference(mesh, case, inlet, args.steps, args.warmup)
+        mesh, case, desc, inlet, skw = make_workload(args.config)
+        ref = cpu_reference(mesh, case, inlet, args.steps, args.warmup, amg_theta=skw.get("amg_theta", 0.08))
         line = {"metric": METRIC, "value": ref["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": ref["iterations"],
                 "warmup": args.warmup, "ms_per_step": 1e3 * ref["seconds"] / ref["iterations"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -242,10 +247,13 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     else:
         torch.cuda.set_device(0)
+    from gputest_b200.unstructured.mixed import MixedSimpleSolver
     from gputest_b200.unstructured.simple import SimpleSolver
 
     dev = torch.cuda.current_device()
-    mesh, case, desc, inlet = make_workload(args.config)
+    mesh, case, desc, inlet, skw = make_workload(args.config)
+    Solver = MixedSimpleSolver if args.precision == "mixed" else SimpleSolver
+    mk = lambda c: Solver(mesh, c, **skw)  # noqa: E731
     nc = mesh.n_cells
     K, W = args.steps, max(args.warmup, 1)
 
@@ -257,7 +265,7 @@ def main():
     # ---- device-timed run
     run_case = __import__("copy").deepcopy(case)
     run_case.tol = 0.0  # K steps regardless of convergence
-    s = SimpleSolver(mesh, run_case)
+    s = mk(run_case)
     if inlet is not None:
         inlet(s)
     for _ in range(W):
@@ -323,7 +331,7 @@ def main():
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    s2 = SimpleSolver(mesh, run_case)
+    s2 = mk(run_case)
     if inlet is not None:
         inlet(s2)
     for _ in range(W + K):
@@ -342,7 +350,7 @@ def main():
     converge = None
     if args.converge:
         barrier()
-        s3 = SimpleSolver(mesh, case)
+        s3 = mk(case)
         if inlet is not None:
             inlet(s3)
         c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -358,7 +366,8 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         cb_case = __import__("copy").deepcopy(case)
-        cpu = cpu_reference(mesh, cb_case, inlet, steps=1000, warmup=2, budget_s=15.0)
+        cpu = cpu_reference(mesh, cb_case, inlet, steps=1000, warmup=2, budget_s=15.0,
+                            amg_theta=skw.get("amg_theta", 0.08))
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if world > 1:
@@ -368,8 +377,8 @@ def main():
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": dict(desc, l2="flushed between timed steps (512 MiB write)",
+            "dtype": "f64" if args.precision == "fp64" else "f32 systems, f64 residuals", "data": "synthetic",
+            "config": dict(desc, precision=args.precision, l2="flushed between timed steps (512 MiB write)",
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "linear_iterations_last": infos[K - 1], "cuda_graphs": graphs, "to_convergence": converge}

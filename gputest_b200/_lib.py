@@ -13,7 +13,7 @@ from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "csrc", "libb2simplec.so")
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 B2S_OK = 0
 _ERRORS = {-1: "invalid argument", -2: "kernel launch failed", -3: "work space too small", -4: "no usable CUDA device",
@@ -27,7 +27,8 @@ class Mesh(ctypes.Structure):
     _fields_ = [("nc", I32), ("nf", I32), ("nb", I32), ("dim", I32), ("nnz", I32)] + [
         (name, P) for name in ("fP", "fN", "forig", "own_ptr", "nei_ptr", "nei_face", "bP", "bptr", "w", "alpha", "wl",
                                "S", "d", "Tv", "dxm", "dPf", "dNf", "alpha_b", "wlb", "Sb_mag", "Sb", "db", "nbv",
-                               "dbt", "vol", "Ginv", "rowptr", "col", "slot_diag", "slot_PN", "slot_NP")]
+                               "dbt", "vol", "Ginv", "rowptr", "col", "slot_diag", "slot_PN", "slot_NP")] + [
+        ("tiles", P), ("ntiles", I32), ("pad_", I32)]
 
 
 class BC(ctypes.Structure):
@@ -51,12 +52,18 @@ class AmgLevel(ctypes.Structure):
     _fields_ = [("n", I32), ("nnz", I32), ("nc", I32), ("p_nnz", I32), ("w_nnz", I32)] + [
         (name, P) for name in ("rowptr", "col", "val", "diag_slot", "dinv", "agg", "tval", "x0", "p_rowptr", "p_col",
                                "p_val", "r_rowptr", "r_col", "r_from_p", "r_val", "w_rowptr", "w_col", "w_val", "rho",
-                               "strong")]
+                               "strong", "group_ptr")]
+
+
+class Amg32(ctypes.Structure):
+    """Float copies of the hierarchy's per-level values (``b2s_amg_f32``)."""
+    _fields_ = [(name, P * MAX_LEVELS) for name in ("val", "dinv", "p_val", "r_val")]
 
 
 class Amg(ctypes.Structure):
     _fields_ = [("nlevels", I32), ("coarse_n", I32), ("singular", I32), ("sweeps", I32), ("omega", F64),
                 ("coarse_rowptr", P), ("coarse_col", P), ("coarse_val", P), ("coarse_inv", P),
+                ("ngroups", I32), ("pad_", I32), ("coarse_group_ptr", P), ("coarse_inv_off", P), ("group_singular", P),
                 ("levels", AmgLevel * MAX_LEVELS)]
 
 
@@ -91,6 +98,17 @@ _SIGS = {
     "b2s_flux_balance_d": ([P, P, P, P, P, P], ctypes.c_int),
     "b2s_bicgstab_jacobi_noalloc_d": ([I32, ctypes.c_int, P, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, P, P],
                                       ctypes.c_int),
+    # mixed precision
+    "b2s_momentum_assemble_mixed_d": ([P] * 16 + [P], ctypes.c_int),
+    "b2s_pressure_assemble_mixed_d": ([P] * 14 + [P], ctypes.c_int),
+    "b2s_energy_assemble_mixed_d": ([P, P, F64, F64, F64, ctypes.c_int] + [P] * 10 + [P], ctypes.c_int),
+    "b2s_bicgstab_f32_workspace_bytes": ([I32, ctypes.c_int], I64),
+    "b2s_bicgstab_jacobi_f32_d": ([I32, ctypes.c_int, P, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   P, P, P, I64, P, P], ctypes.c_int),
+    "b2s_amg_to_f32_d": ([P, P, P], ctypes.c_int),
+    "b2s_pcg_mixed_workspace_bytes": ([P], I64),
+    "b2s_pcg_amg_mixed_d": ([P, P, P, P, P, I32, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, ctypes.c_int, F64, P,
+                             I64, P, P], ctypes.c_int),
 }
 
 _lib: Optional[ctypes.CDLL] = None

@@ -150,7 +150,7 @@ __global__ void wvals_k(b2s_amg_level L) {
 // an accumulator are staged in shared memory; for each R entry (I, i) in order, the lanes split
 // W row i, whose columns are distinct, so every accumulator slot receives its terms in the
 // fixed order of the R entries (deterministic, no atomics). Rows longer than the staging
-// capacity are accumulated by lane 0 directly in global memory.
+// capacity are processed in windows of kRowCap consecutive columns.
 constexpr int kRowCap = 256;
 constexpr int kGalWarps = 8;
 
@@ -181,15 +181,32 @@ __global__ void __launch_bounds__(kGalWarps * 32) acvals_k(b2s_amg_level L, cons
       }
       for (int t = lane; t < m; t += 32) cval[c0 + t] = sacc[wib][t];
       __syncwarp();
-    } else if (lane == 0) {
-      for (int t = c0; t < c1; ++t) cval[t] = 0.0;
-      for (int e = e0; e < e1; ++e) {
-        const double rv = L.r_val[e];
-        const int i = L.r_col[e];
-        for (int s = L.w_rowptr[i]; s < L.w_rowptr[i + 1]; ++s) {
-          const int t = find_sorted(ccol, c0, c1, L.w_col[s]);
-          cval[t] += rv * L.w_val[s];
+    } else {
+      // a long row: windows of kRowCap columns, each staged and accumulated as above; W entries
+      // outside the window's column range are skipped (every slot still receives its terms in
+      // the order of the R entries)
+      for (int t0 = 0; t0 < m; t0 += kRowCap) {
+        const int mw = (m - t0) < kRowCap ? (m - t0) : kRowCap;
+        for (int t = lane; t < mw; t += 32) {
+          scol[wib][t] = ccol[c0 + t0 + t];
+          sacc[wib][t] = 0.0;
         }
+        __syncwarp();
+        const int lo = scol[wib][0], hi = scol[wib][mw - 1];
+        for (int e = e0; e < e1; ++e) {
+          const double rv = L.r_val[e];
+          const int i = L.r_col[e];
+          const int w1 = L.w_rowptr[i + 1];
+          for (int s = L.w_rowptr[i] + lane; s < w1; s += 32) {
+            const int c = L.w_col[s];
+            if (c < lo || c > hi) continue;
+            const int t = find_sorted(scol[wib], 0, mw, c);
+            if (t < mw && scol[wib][t] == c) sacc[wib][t] += rv * L.w_val[s];
+          }
+          __syncwarp();
+        }
+        for (int t = lane; t < mw; t += 32) cval[c0 + t0 + t] = sacc[wib][t];
+        __syncwarp();
       }
     }
   }
@@ -285,6 +302,25 @@ static int power_grid(int* g) {
   if (*g > kMaxCoopBlocks) *g = kMaxCoopBlocks;
   return B2S_OK;
 }
+
+namespace b2s {
+// ---------------------------------------------------------------------------------- float copies
+struct F32Segs {
+  int n;
+  const double* src[4 * B2S_AMG_MAX_LEVELS];
+  float* dst[4 * B2S_AMG_MAX_LEVELS];
+  int64_t len[4 * B2S_AMG_MAX_LEVELS];
+};
+
+__global__ void to_f32_k(F32Segs s) {
+  const int k = blockIdx.y;
+  if (k >= s.n) return;
+  const double* src = s.src[k];
+  float* dst = s.dst[k];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < s.len[k]; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+}  // namespace b2s
 
 extern "C" {
 
@@ -395,6 +431,33 @@ int64_t b2s_host_aggregate(int64_t n, const int64_t* indptr, const int64_t* indi
   for (int64_t i = 0; i < n; ++i)
     if (agg[i] < 0) agg[i] = na++;
   return na;
+}
+
+int b2s_amg_to_f32_d(const b2s_amg* h, const b2s_amg_f32* h32, b2s_stream_t s) {
+  if (!h || !h32 || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS) return B2S_ERR_ARG;
+  F32Segs g;
+  g.n = 0;
+  int64_t longest = 1;
+  for (int l = 0; l < h->nlevels; ++l) {
+    const b2s_amg_level& L = h->levels[l];
+    const double* src[4] = {L.val, L.dinv, L.p_val, L.r_val};
+    float* dst[4] = {h32->val[l], h32->dinv[l], h32->p_val[l], h32->r_val[l]};
+    const int64_t len[4] = {L.nnz, L.n, L.p_nnz, L.p_nnz};
+    for (int q = 0; q < 4; ++q) {
+      if (!src[q] || !dst[q]) return B2S_ERR_ARG;
+      g.src[g.n] = src[q];
+      g.dst[g.n] = dst[q];
+      g.len[g.n] = len[q];
+      if (len[q] > longest) longest = len[q];
+      ++g.n;
+    }
+  }
+  if (g.n == 0) return B2S_OK;
+  int64_t gx = cdiv(longest, kThreads);
+  if (gx > 4 * kMaxCoopBlocks) gx = 4 * kMaxCoopBlocks;
+  to_f32_k<<<dim3((unsigned)gx, (unsigned)g.n), kThreads, 0, (cudaStream_t)s>>>(g);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
 }
 
 }  // extern "C"

@@ -237,13 +237,13 @@ struct RowOut {
   double rhs[NQ];  // without the extra source
 };
 
-template <int DIM, int NQ>
+template <int DIM, int NQ, class VT>
 __device__ __forceinline__ RowOut<DIM, NQ> transport_row(const b2s_mesh& m, int c, double gamma,
                                                          const double* dirichlet, const double* F, const double* Fb,
                                                          const double* phi, int64_t phi_stride,
                                                          const double* grad, int64_t grad_stride,
                                                          const double* phib, int64_t phib_stride, bool second,
-                                                         double* val, bool write_offdiag) {
+                                                         VT* val, bool write_offdiag) {
   const int nc = m.nc, nf = m.nf, nb = m.nb;
   RowOut<DIM, NQ> o;
   double s_own = 0.0, s_nei = 0.0, s_b = 0.0, nb_own = 0.0, nb_nei = 0.0;
@@ -431,12 +431,12 @@ __device__ __forceinline__ void rc_bface(const b2s_mesh& m, const b2s_bc& bc, co
   cb = prm.rho * dP[P] * m.alpha_b[f] * mp;
 }
 
-template <int DIM>
+template <int DIM, class VT>
 __global__ void pressure_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Ustar,
                                     const double* __restrict__ p, const double* __restrict__ gp,
                                     const double* __restrict__ dP, double* __restrict__ Fst_out,
                                     double* __restrict__ cf_out, double* __restrict__ Fbst_out,
-                                    double* __restrict__ cb_out, double* __restrict__ val, double* __restrict__ rhs,
+                                    double* __restrict__ cb_out, VT* __restrict__ val, double* __restrict__ rhs,
                                     double* __restrict__ part) {
   __shared__ double red[(kThreads / 32 + 1) * 1];
   const int nc = m.nc;
@@ -605,6 +605,115 @@ __global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, double gamma, double cp
     diag_out[c] = diag;
     b_out[c] = rhs;
     br_out[c] = rhs + (((1.0 - aT) / aT) * diag) * T[c];
+  }
+  block_partials<2>(acc, red, part);
+}
+
+// ------------------------------------------------------------------------------ mixed precision
+// The mixed-precision iteration solves every linear system in correction form: the residual
+// r = b - A phi of the unrelaxed system is evaluated in double from the coefficients in
+// registers (the nonlinear residual, whose zero is the converged solution), and the relaxed
+// system A_r dphi = r (A_r: diagonal a_P / alpha; the same iterates as A_r phi = b_r from
+// x0 = phi) is stored in float for the Krylov solve; phi + dphi is formed in double.
+
+// sum_nb a_nb phi_nb of row c for NQ fields: upwind + diffusion off-diagonals recomputed from
+// the face data the row assembly has just read (simple.py:340-353).
+template <int NQ>
+__device__ __forceinline__ void offdiag_apply(const b2s_mesh& m, int c, double gamma, const double* F,
+                                              const double* phi, int64_t phi_stride, double (&out)[NQ]) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) out[q] = 0.0;
+  for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
+    const double aPN = -(gamma * m.alpha[f] + npmax0(-F[f]));
+    const int N = m.fN[f];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) out[q] += aPN * phi[q * phi_stride + N];
+  }
+  for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
+    const int f = m.nei_face[k];
+    const double aNP = -(gamma * m.alpha[f] + npmax0(F[f]));
+    const int P = m.fP[f];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) out[q] += aNP * phi[q * phi_stride + P];
+  }
+}
+
+template <int DIM>
+__global__ void momentum_assemble_mixed_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Up,
+                                          const double* __restrict__ gUp, const double* __restrict__ gp,
+                                          const double* __restrict__ bUp, const double* __restrict__ F,
+                                          const double* __restrict__ Fb, const double* __restrict__ por,
+                                          const double* __restrict__ msrc, float* __restrict__ val,
+                                          float* __restrict__ inv_out, double* __restrict__ dP_out,
+                                          float* __restrict__ r_out, double* __restrict__ part) {
+  __shared__ double red[(kThreads / 32 + 1) * 2 * DIM];
+  const int nc = m.nc, nb = m.nb;
+  const double au = prm.relax_u;
+  double acc[2 * DIM];
+#pragma unroll
+  for (int q = 0; q < 2 * DIM; ++q) acc[q] = 0.0;
+  const bool drive = prm.body[0] != 0.0 || prm.body[1] != 0.0 || (DIM == 3 && prm.body[2] != 0.0);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
+                                                 (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
+    double diag = o.diag;
+    const double V = m.vol[c];
+    if (por) diag = diag + por[c] * V;
+    const double diag_r = diag / au;
+    val[m.slot_diag[c]] = (float)diag_r;
+    inv_out[c] = (float)(1.0 / diag_r);
+    double denom = diag_r;
+    if (prm.simplec) {
+      denom = diag_r - o.sumnb;
+      denom = (denom > 1e-12 * diag_r) ? denom : diag_r;
+    }
+    dP_out[c] = V / denom;
+    double anb[DIM];
+    offdiag_apply<DIM>(m, c, prm.mu, F, Up + nc, nc, anb);
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      double src = -gp[(int64_t)k * nc + c] * V;
+      if (drive) src = src + V * prm.body[k];
+      if (msrc) src = src + msrc[(int64_t)k * nc + c];
+      const double rhs = o.rhs[k] + src;
+      const double uc = Up[(int64_t)(1 + k) * nc + c];
+      const double r = rhs - (diag * uc + anb[k]);
+      acc[k] += fabs(r);
+      acc[DIM + k] += fabs(diag * uc);
+      r_out[(int64_t)k * nc + c] = (float)r;
+    }
+  }
+  block_partials<2 * DIM>(acc, red, part);
+}
+
+template <int DIM>
+__global__ void energy_assemble_mixed_k(b2s_mesh m, b2s_bc bc, double gamma, double cp, double aT, int second,
+                                        const double* __restrict__ T, const double* __restrict__ gT,
+                                        const double* __restrict__ Tb, const double* __restrict__ F,
+                                        const double* __restrict__ Fb, const double* __restrict__ esrc,
+                                        float* __restrict__ val, float* __restrict__ inv_out, float* __restrict__ r_out,
+                                        double* __restrict__ part) {
+  __shared__ double red[(kThreads / 32 + 1) * 2];
+  const int nc = m.nc, nb = m.nb;
+  double acc[2] = {0.0, 0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    RowOut<DIM, 1> o = transport_row<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
+                                             second != 0, val, true);
+    double q = 0.0;
+    for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) q += bc.m_tflux[f] * bc.tval[f] * m.Sb_mag[f] / cp;
+    if (esrc) q = q + esrc[c];
+    const double rhs = o.rhs[0] + q;
+    const double diag = o.diag;
+    double anb[1];
+    offdiag_apply<1>(m, c, gamma, F, T, nc, anb);
+    const double Tc = T[c];
+    const double r = rhs - (diag * Tc + anb[0]);
+    acc[0] += fabs(r);
+    acc[1] += fabs(diag * Tc);
+    const double dr = diag / aT;
+    val[m.slot_diag[c]] = (float)dr;
+    inv_out[c] = (float)(1.0 / dr);
+    r_out[c] = (float)r;
   }
   block_partials<2>(acc, red, part);
 }
@@ -828,6 +937,60 @@ int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, dou
   else
     energy_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT, Tb,
                                                                F, Fb, esrc, val, diag, inv, b, br, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_momentum_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                  const double* Up, const double* gUp, const double* gp, const double* bUp,
+                                  const double* F, const double* Fb, const double* porosity, const double* msrc,
+                                  float* val, float* inv, double* dP, float* r, double* part, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !inv || !dP || !r || !part ||
+      !(prm->relax_u > 0.0))
+    return B2S_ERR_ARG;
+  unsigned g = part_grid(m->nc);
+  if (m->dim == 2)
+    momentum_assemble_mixed_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb,
+                                                                       porosity, msrc, val, inv, dP, r, part);
+  else
+    momentum_assemble_mixed_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb,
+                                                                       porosity, msrc, val, inv, dP, r, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_pressure_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                  const double* Ustar, const double* p, const double* gp, const double* dP,
+                                  double* Fst, double* cf, double* Fbst, double* cb, float* val, double* rhs,
+                                  double* part, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !prm || !Ustar || !p || !gp || !dP || !Fst || !cf || !Fbst || !cb || !val || !rhs ||
+      !part)
+    return B2S_ERR_ARG;
+  unsigned g = part_grid(m->nc);
+  if (m->dim == 2)
+    pressure_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Ustar, p, gp, dP, Fst, cf, Fbst, cb,
+                                                                 val, rhs, part);
+  else
+    pressure_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Ustar, p, gp, dP, Fst, cf, Fbst, cb,
+                                                                 val, rhs, part);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_energy_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp, double relax_T,
+                                int second_order, const double* T, const double* gT, const double* Tb,
+                                const double* F, const double* Fb, const double* esrc, float* val, float* inv,
+                                float* r, double* part, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !T || !gT || (!Tb && m->nb) || !F || !Fb || !val || !inv || !r || !part ||
+      !(relax_T > 0.0) || !(cp != 0.0))
+    return B2S_ERR_ARG;
+  unsigned g = part_grid(m->nc);
+  if (m->dim == 2)
+    energy_assemble_mixed_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T,
+                                                                     gT, Tb, F, Fb, esrc, val, inv, r, part);
+  else
+    energy_assemble_mixed_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T,
+                                                                     gT, Tb, F, Fb, esrc, val, inv, r, part);
   B2S_LAUNCH_CHECK();
   return B2S_OK;
 }

@@ -45,21 +45,28 @@ __device__ __forceinline__ void grid_reduce(cg::grid_group& grid, const double (
 }
 
 // ---------------------------------------------------------------------------------- BiCGSTAB
-struct BicgArgs {
+// T is the storage type of the matrix values and the vectors (double, or float for the
+// mixed-precision path); scalars and every reduction are accumulated in double.
+template <class T>
+struct BicgArgsT {
   int n, nr;
   const int32_t* rowptr;
   const int32_t* col;
-  const double* val;
-  const double* b;
-  const double* inv;
-  double* x;
+  const T* val;
+  const T* b;
+  const T* inv;
+  T* x;
   double tol;
   int maxiter, rel;
-  double* work;
+  int zero_x0;           // start from x = 0 (x is not read)
+  T* work;
   double* part0;
   double* part1;
   b2s_solve_info* info;
+  double* out64;         // when set: out64 = base64 + x at the end (a correction added in double)
+  const double* base64;
 };
+using BicgArgs = BicgArgsT<double>;
 
 enum { ACTIVE = 0, CONVERGED = 1, STOPPED = 2 };
 
@@ -71,8 +78,8 @@ enum { ACTIVE = 0, CONVERGED = 1, STOPPED = 2 };
 //   3. r = s - omega t, r.r, r_hat.r.
 // p and v alternate between two buffers so that neighbours read the previous iteration's values.
 // x gets alpha h + omega hs one phase later (after the breakdown test), as the reference does.
-template <int NR>
-__global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
+template <int NR, class T>
+__global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double red[(kCoopThreads / 32 + 1) * 3 * NR];
   __shared__ double tot[3 * NR];
@@ -80,11 +87,11 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   double* part[2] = {a.part0, a.part1};
   int pb = 0;
-  double *r[NR], *rh[NR], *pp[2][NR], *vv[2][NR], *h[NR], *s[NR], *hs[NR], *t[NR], *x[NR];
-  const double* b[NR];
+  T *r[NR], *rh[NR], *pp[2][NR], *vv[2][NR], *h[NR], *s[NR], *hs[NR], *t[NR], *x[NR];
+  const T* b[NR];
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
-    double* w = a.work + (int64_t)10 * k * n;
+    T* w = a.work + (int64_t)10 * k * n;
     r[k] = w;
     rh[k] = w + n;
     pp[0][k] = w + 2 * (int64_t)n;
@@ -98,7 +105,7 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
     x[k] = a.x + (int64_t)k * n;
     b[k] = a.b + (int64_t)k * n;
   }
-  const double* inv = a.inv;
+  const T* inv = a.inv;
   int cur = 0;  // p, v of the previous iteration are pp[cur], vv[cur]
   // ---- r = b - A x, r_hat = r, p = v = 0
   {
@@ -110,15 +117,18 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
       double ax[NR];
 #pragma unroll
       for (int k = 0; k < NR; ++k) ax[k] = 0.0;
-      for (int j = j0; j < j1; ++j) {
-        const double av = a.val[j];
-        const int c = a.col[j];
+      if (!a.zero_x0) {
+        for (int j = j0; j < j1; ++j) {
+          const double av = a.val[j];
+          const int c = a.col[j];
 #pragma unroll
-        for (int k = 0; k < NR; ++k) ax[k] += av * x[k][c];
+          for (int k = 0; k < NR; ++k) ax[k] += av * x[k][c];
+        }
       }
 #pragma unroll
       for (int k = 0; k < NR; ++k) {
         const double bi = b[k][i], ri = bi - ax[k];
+        if (a.zero_x0) x[k][i] = 0.0;
         r[k][i] = ri;
         rh[k][i] = ri;
         pp[0][k][i] = 0.0;
@@ -171,10 +181,10 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
       double acc[3 * NR];
 #pragma unroll
       for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
-      double* po[NR];
-      double* vo[NR];
-      double* pn[NR];
-      double* vn[NR];
+      T* po[NR];
+      T* vo[NR];
+      T* pn[NR];
+      T* vn[NR];
 #pragma unroll
       for (int k = 0; k < NR; ++k) {
         po[k] = pp[cur][k];
@@ -238,7 +248,7 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
       double acc[3 * NR];
 #pragma unroll
       for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
-      double* v[NR];
+      T* v[NR];
 #pragma unroll
       for (int k = 0; k < NR; ++k) v[k] = vv[cur][k];
       for (int i = gt; i < n; i += gs) {
@@ -340,6 +350,7 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
     for (int k = 0; k < NR; ++k) {
       if (pend_a[k]) x[k][i] = x[k][i] + alpha[k] * h[k][i];
       if (pend[k]) x[k][i] = (x[k][i] + alpha[k] * h[k][i]) + omega[k] * hs[k][i];
+      if (a.out64) a.out64[(int64_t)k * n + i] = a.base64[(int64_t)k * n + i] + (double)x[k][i];
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -357,67 +368,86 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgs a) {
 }
 
 // ---------------------------------------------------------------------------------- AMG-PCG
-struct VBuf {  // per-level V-cycle vectors
-  double* b;
-  double* x;
-  double* y;
-  double* r;
+// T is the storage type of the level matrices and the V-cycle/CG vectors: double, or float on
+// the mixed-precision path. Scalars, reductions and the coarse solve's arithmetic stay double.
+template <class T>
+struct VBufT {  // per-level V-cycle vectors
+  T* b;
+  T* x;
+  T* y;
+  T* r;
 };
 
-struct PcgArgs {
+template <class T>
+struct LvVals {  // per-level values in the storage type
+  const T* val;
+  const T* dinv;
+  const T* p_val;
+  const T* r_val;
+};
+
+template <class T>
+struct PcgArgsT {
   b2s_amg h;
+  LvVals<T> lvv[B2S_AMG_MAX_LEVELS];
   int n;                 // the operator A (the current matrix)
   const int32_t* rowptr;
   const int32_t* col;
-  const double* val;
-  const double* b;
-  double* x;
+  const T* val;
+  const T* b;
+  T* x;
   double tol;
   int maxiter, project;
-  double* r;
-  double* p;
-  double* p2;
-  double* q;
-  double* cb;   // coarse right-hand side
-  double* cx;   // coarse solution
+  T* r;
+  T* p;
+  T* p2;
+  T* q;
+  T* cb;   // coarse right-hand side
+  T* cx;   // coarse solution
   double* part0;
   double* part1;
-  VBuf lv[B2S_AMG_MAX_LEVELS];
+  VBufT<T> lv[B2S_AMG_MAX_LEVELS];
   b2s_solve_info* info;
 };
+using PcgArgs = PcgArgsT<double>;
+
+// Rows of a V-cycle phase. Levels whose rows average at least kWideRow entries (the dense
+// coarse levels of 3-D hierarchies) are walked one warp per row, lanes striding the row and a
+// shuffle sum at the end; the others one thread per row in stored order.
+constexpr int kWideRow = 24;
+
+struct Rows {
+  int first, stride, lane, step;
+  bool wide;
+  __device__ __forceinline__ Rows(bool w, int t, int n)
+      : first(w ? t >> 5 : t), stride(w ? n >> 5 : n), lane(w ? (t & 31) : 0), step(w ? 32 : 1), wide(w) {}
+  __device__ __forceinline__ double total(double s) const { return wide ? warp_sum(s) : s; }
+  __device__ __forceinline__ bool writer() const { return lane == 0; }
+};
+
+__device__ __forceinline__ bool wide_level(int n, int64_t nnz) { return nnz >= (int64_t)kWideRow * n; }
 
 // One damped-Jacobi step y = x + (w Dinv)(b - A x); x == NULL means x = w Dinv b (fused).
-__device__ __forceinline__ void jacobi_step(const b2s_amg_level& L, double w, const double* b, const double* x,
-                                            double* y, int gt, int gs) {
-  for (int i = gt; i < L.n; i += gs) {
+template <class T>
+__device__ __forceinline__ void jacobi_step(const b2s_amg_level& L, const LvVals<T>& V, double w, const T* b,
+                                            const T* x, T* y, int gt, int gs) {
+  const Rows R(wide_level(L.n, L.nnz), gt, gs);
+  for (int i = R.first; i < L.n; i += R.stride) {
     double s = 0.0, xi;
-    const double wd = w * L.dinv[i];
+    const double wd = w * V.dinv[i];
     if (x) {
-      for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) s += L.val[j] * x[L.col[j]];
+      for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.step) s += V.val[j] * x[L.col[j]];
       xi = x[i];
     } else {
-      for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
+      for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.step) {
         const int c = L.col[j];
-        s += L.val[j] * ((w * L.dinv[c]) * b[c]);
+        s += V.val[j] * ((w * V.dinv[c]) * b[c]);
       }
       xi = wd * b[i];
     }
-    y[i] = xi + wd * (b[i] - s);
+    s = R.total(s);
+    if (R.writer()) y[i] = xi + wd * (b[i] - s);
   }
-}
-
-struct Mat0 {
-  int n;
-  const int32_t* rowptr;
-  const int32_t* col;
-  const double* val;
-};
-
-// Level-0 matrix: the finest smoothing level, or the coarse matrix itself when the hierarchy
-// has no smoothing level (a matrix at or below max_coarse rows, amg.py:90 with no iteration).
-__device__ __forceinline__ Mat0 level0(const b2s_amg& h) {
-  if (h.nlevels > 0) return {h.levels[0].n, h.levels[0].rowptr, h.levels[0].col, h.levels[0].val};
-  return {h.coarse_n, h.coarse_rowptr, h.coarse_col, h.coarse_val};
 }
 
 // Barrier of a V-cycle phase: the whole grid for the large levels, block 0 alone for the tail.
@@ -433,40 +463,50 @@ struct Phase {
 
 // Down-leg of level l (amg.py:135-139): pre-smoothing (the first two sweeps fused: the first
 // sweep's x = w D^-1 b is evaluated on the fly), residual, restriction to the next level.
-__device__ __forceinline__ double* vdown(const PcgArgs& a, int l, const double* b, const Phase& ph) {
+template <class T>
+__device__ __forceinline__ T* vdown(const PcgArgsT<T>& a, int l, const T* b, const Phase& ph) {
   const b2s_amg& h = a.h;
   const b2s_amg_level& lv = h.levels[l];
+  const LvVals<T>& V = a.lvv[l];
   const int L = h.nlevels;
   const double w = h.omega;
-  double* X = a.lv[l].x;
-  double* Y = a.lv[l].y;
-  double* c = X;
+  T* X = a.lv[l].x;
+  T* Y = a.lv[l].y;
+  T* c = X;
   if (h.sweeps <= 1) {
-    for (int i = ph.t; i < lv.n; i += ph.n) X[i] = (w * lv.dinv[i]) * b[i];
+    for (int i = ph.t; i < lv.n; i += ph.n) X[i] = (w * V.dinv[i]) * b[i];
   } else {
-    jacobi_step(lv, w, b, nullptr, X, ph.t, ph.n);
-    double* o = Y;
+    jacobi_step(lv, V, w, b, (const T*)nullptr, X, ph.t, ph.n);
+    T* o = Y;
     for (int sw = 2; sw < h.sweeps; ++sw) {
       ph.sync();
-      jacobi_step(lv, w, b, c, o, ph.t, ph.n);
-      double* tmp = c;
+      jacobi_step(lv, V, w, b, (const T*)c, o, ph.t, ph.n);
+      T* tmp = c;
       c = o;
       o = tmp;
     }
   }
   ph.sync();
-  double* R = a.lv[l].r;
-  for (int i = ph.t; i < lv.n; i += ph.n) {
-    double s = 0.0;
-    for (int j = lv.rowptr[i]; j < lv.rowptr[i + 1]; ++j) s += lv.val[j] * c[lv.col[j]];
-    R[i] = b[i] - s;
+  T* Rv = a.lv[l].r;
+  {
+    const Rows R(wide_level(lv.n, lv.nnz), ph.t, ph.n);
+    for (int i = R.first; i < lv.n; i += R.stride) {
+      double s = 0.0;
+      for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.step) s += V.val[j] * c[lv.col[j]];
+      s = R.total(s);
+      if (R.writer()) Rv[i] = b[i] - s;
+    }
   }
   ph.sync();
-  double* bn = (l + 1 < L) ? a.lv[l + 1].b : a.cb;
-  for (int I = ph.t; I < lv.nc; I += ph.n) {
-    double s = 0.0;
-    for (int j = lv.r_rowptr[I]; j < lv.r_rowptr[I + 1]; ++j) s += lv.r_val[j] * R[lv.r_col[j]];
-    bn[I] = s;
+  T* bn = (l + 1 < L) ? a.lv[l + 1].b : a.cb;
+  {
+    const Rows R(wide_level(lv.nc, lv.p_nnz), ph.t, ph.n);
+    for (int I = R.first; I < lv.nc; I += R.stride) {
+      double s = 0.0;
+      for (int j = lv.r_rowptr[I] + R.lane; j < lv.r_rowptr[I + 1]; j += R.step) s += V.r_val[j] * Rv[lv.r_col[j]];
+      s = R.total(s);
+      if (R.writer()) bn[I] = s;
+    }
   }
   ph.sync();
   return c;
@@ -475,40 +515,52 @@ __device__ __forceinline__ double* vdown(const PcgArgs& a, int l, const double* 
 // Up-leg of level l (amg.py:139-142): x += P xc, then the post-smoothing sweeps. With stats
 // (level 0 on the grid) the last sweep also accumulates sum z, sum r z and sum r for the PCG
 // and ends with their grid-wide reduction into stats.
-__device__ __forceinline__ double* vup(const PcgArgs& a, int l, const double* b, double* c, const double* xc,
-                                       const Phase& ph, const double* rr, double* red, double* stats, int pb) {
+template <class T>
+__device__ __forceinline__ T* vup(const PcgArgsT<T>& a, int l, const T* b, T* c, const T* xc, const Phase& ph,
+                                  const T* rr, double* red, double* stats, int pb) {
   const b2s_amg& h = a.h;
   const b2s_amg_level& lv = h.levels[l];
+  const LvVals<T>& V = a.lvv[l];
   const double w = h.omega;
-  double* o = (c == a.lv[l].x) ? a.lv[l].y : a.lv[l].x;
+  T* o = (c == a.lv[l].x) ? a.lv[l].y : a.lv[l].x;
   const bool want = stats != nullptr;
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int i = ph.t; i < lv.n; i += ph.n) {
-    double s = 0.0;
-    for (int j = lv.p_rowptr[i]; j < lv.p_rowptr[i + 1]; ++j) s += lv.p_val[j] * xc[lv.p_col[j]];
-    const double zi = c[i] + s;
-    c[i] = zi;
-    if (want && h.sweeps == 0) {
-      acc[0] += zi;
-      acc[1] += rr[i] * zi;
-      acc[2] += rr[i];
+  {
+    const Rows R(wide_level(lv.n, lv.p_nnz), ph.t, ph.n);
+    for (int i = R.first; i < lv.n; i += R.stride) {
+      double s = 0.0;
+      for (int j = lv.p_rowptr[i] + R.lane; j < lv.p_rowptr[i + 1]; j += R.step) s += V.p_val[j] * xc[lv.p_col[j]];
+      s = R.total(s);
+      const double zi = c[i] + s;
+      if (R.writer()) {
+        c[i] = zi;
+        if (want && h.sweeps == 0) {
+          acc[0] += zi;
+          acc[1] += rr[i] * zi;
+          acc[2] += rr[i];
+        }
+      }
     }
   }
+  const Rows R(wide_level(lv.n, lv.nnz), ph.t, ph.n);
   for (int sw = 0; sw < h.sweeps; ++sw) {
     ph.sync();
     const bool last = sw + 1 == h.sweeps;
-    for (int i = ph.t; i < lv.n; i += ph.n) {
+    for (int i = R.first; i < lv.n; i += R.stride) {
       double s = 0.0;
-      for (int j = lv.rowptr[i]; j < lv.rowptr[i + 1]; ++j) s += lv.val[j] * c[lv.col[j]];
-      const double zi = c[i] + (w * lv.dinv[i]) * (b[i] - s);
-      o[i] = zi;
-      if (want && last) {
-        acc[0] += zi;
-        acc[1] += rr[i] * zi;
-        acc[2] += rr[i];
+      for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.step) s += V.val[j] * c[lv.col[j]];
+      s = R.total(s);
+      const double zi = c[i] + (w * V.dinv[i]) * (b[i] - s);
+      if (R.writer()) {
+        o[i] = zi;
+        if (want && last) {
+          acc[0] += zi;
+          acc[1] += rr[i] * zi;
+          acc[2] += rr[i];
+        }
       }
     }
-    double* tmp = c;
+    T* tmp = c;
     c = o;
     o = tmp;
   }
@@ -522,8 +574,9 @@ __device__ __forceinline__ double* vup(const PcgArgs& a, int l, const double* b,
   return c;
 }
 
-// Coarse solve cx = inv(Ac) cb, one warp per row.
-__device__ __forceinline__ void vcoarse(const PcgArgs& a, const double* cb, const Phase& ph) {
+// Coarse solve cx = inv(Ac) cb, one warp per row; the inverse and the arithmetic are double.
+template <class T>
+__device__ __forceinline__ void vcoarse(const PcgArgsT<T>& a, const T* cb, const Phase& ph) {
   const int nc = a.h.coarse_n, lane = threadIdx.x & 31;
   for (int I = ph.t >> 5; I < nc; I += ph.n >> 5) {
     const double* row = a.h.coarse_inv + (int64_t)I * nc;
@@ -538,45 +591,51 @@ __device__ __forceinline__ void vcoarse(const PcgArgs& a, const double* cb, cons
 // Buffer holding level l's solution after its up-leg: the down-leg ends in x after sweeps-2
 // ping-pong swaps (x alone for one sweep), the up-leg swaps once per sweep. Every block can thus
 // name the buffer without having run the level.
-__device__ __forceinline__ double* tail_result(const PcgArgs& a, int l) {
+template <class T>
+__device__ __forceinline__ T* tail_result(const PcgArgsT<T>& a, int l) {
   const int sw = a.h.sweeps;
   const int down = sw <= 1 ? 0 : sw - 2;
   return ((down + sw) & 1) ? a.lv[l].y : a.lv[l].x;
 }
 
-// Levels of at most kTailRows rows (no more rows than one block has threads), and the coarse
-// solve, run in block 0 with block barriers while the other blocks wait at the next grid
-// barrier: below that size a level is latency-bound and a grid barrier costs more than it saves.
+// Levels of at most kTailRows rows (no more rows than one block has threads) and kTailNnz
+// entries, and the coarse solve, run in block 0 with block barriers while the other blocks wait
+// at the next grid barrier: below that size a level is latency-bound and a grid barrier costs
+// more than it saves.
 constexpr int kTailRows = kCoopThreads;
+constexpr int kTailNnz = 16384;
 
 // z = M r: the V-cycle of flowtrace/linalg/amg.py:130-142. Returns the buffer holding z. With
 // stats != nullptr, when level 0 runs on the whole grid, stats[0..2] receive sum z, sum r z and
 // sum r (r = rhs0) and *have_stats is set; otherwise the caller reduces them itself.
-__device__ double* vcycle(cg::grid_group& grid, const PcgArgs& a, const double* rhs0, int gt, int gs,
-                          double* red = nullptr, double* stats = nullptr, int pb = 0, bool* have_stats = nullptr) {
+template <class T>
+__device__ T* vcycle(cg::grid_group& grid, const PcgArgsT<T>& a, const T* rhs0, int gt, int gs,
+                     double* red = nullptr, double* stats = nullptr, int pb = 0, bool* have_stats = nullptr) {
   const b2s_amg& h = a.h;
   const int L = h.nlevels;
-  double* cur[B2S_AMG_MAX_LEVELS];
-  const double* cb = (L == 0) ? rhs0 : a.cb;
-  int Lg = 0;  // levels with more than kTailRows rows run on the whole grid
-  while (Lg < L && h.levels[Lg].n > kTailRows) ++Lg;
+  T* cur[B2S_AMG_MAX_LEVELS];
+  const T* cb = (L == 0) ? rhs0 : a.cb;
+  int Lg = L;  // levels from Lg on (all small) run in block 0; the others on the whole grid
+  while (Lg > 0 && h.levels[Lg - 1].n <= kTailRows && h.levels[Lg - 1].nnz <= kTailNnz &&
+         h.levels[Lg - 1].p_nnz <= kTailNnz)
+    --Lg;
   const Phase gph = {&grid, false, gt, gs};
   const Phase tph = {&grid, true, (int)threadIdx.x, (int)blockDim.x};
-  for (int l = 0; l < Lg; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : a.lv[l].b, gph);
+  for (int l = 0; l < Lg; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, gph);
   if (Lg == L && h.coarse_n > kTailRows) {
     vcoarse(a, cb, gph);
   } else {
     if (blockIdx.x == 0) {
-      for (int l = Lg; l < L; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : a.lv[l].b, tph);
+      for (int l = Lg; l < L; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, tph);
       vcoarse(a, cb, tph);
       for (int l = L - 1; l >= Lg; --l)
-        cur[l] = vup(a, l, (l == 0) ? rhs0 : a.lv[l].b, cur[l], (l + 1 < L) ? cur[l + 1] : a.cx, tph, nullptr,
-                     nullptr, nullptr, 0);
+        cur[l] = vup(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, cur[l], (const T*)((l + 1 < L) ? cur[l + 1] : a.cx),
+                     tph, (const T*)nullptr, nullptr, nullptr, 0);
     }
     grid.sync();
   }
   for (int l = Lg - 1; l >= 0; --l) {
-    const double* xc;
+    const T* xc;
     if (l + 1 < L) {
       // the next level's solution: every block tracks it on the grid levels; for the first tail
       // level (run by block 0 alone) every block names it from the sweep parity
@@ -586,8 +645,8 @@ __device__ double* vcycle(cg::grid_group& grid, const PcgArgs& a, const double* 
       xc = a.cx;
     }
     const bool st = (l == 0) && stats != nullptr;
-    cur[l] = vup(a, l, (l == 0) ? rhs0 : a.lv[l].b, cur[l], xc, gph, rhs0, st ? red : nullptr, st ? stats : nullptr,
-                 pb);
+    cur[l] = vup(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, cur[l], xc, gph, rhs0, st ? red : nullptr,
+                 st ? stats : nullptr, pb);
     if (st && have_stats) *have_stats = true;
   }
   if (L == 0) return a.cx;
@@ -595,32 +654,33 @@ __device__ double* vcycle(cg::grid_group& grid, const PcgArgs& a, const double* 
   return cur[0];
 }
 
-// Preconditioned CG (flowtrace/linalg/krylov.py:25-65). Per iteration: one phase computes
-// p = z' + beta p_old into a second buffer and q = A p with the neighbours' p evaluated on the
-// fly (same arithmetic), one phase updates x and r, then the V-cycle, whose last sweep also
-// reduces sum z, sum r z and sum r; z' = z - mean(z) (the projection) is applied lazily and
-// r.z' = sum r z - mean(z) sum r.
-__global__ void __launch_bounds__(kCoopThreads) pcg_amg_coop_k(PcgArgs a) {
-  cg::grid_group grid = cg::this_grid();
-  __shared__ double red[(kCoopThreads / 32 + 1) * 3];
-  __shared__ double tot[3];
-  __shared__ double stats[3];
-  const Mat0 A = {a.n, a.rowptr, a.col, a.val};
-  const int n = A.n;
+struct CgOutcome {
+  int its, conv;
+  double res;
+};
+
+// Preconditioned CG (flowtrace/linalg/krylov.py:25-65) of A x = b from x = 0, with a.r, a.p,
+// a.p2, a.q as work vectors. Per iteration: one phase computes p = z' + beta p_old into a
+// second buffer and q = A p with the neighbours' p evaluated on the fly (same arithmetic), one
+// phase updates x and r, then the V-cycle, whose last sweep also reduces sum z, sum r z and
+// sum r; z' = z - mean(z) (the projection) is applied lazily and r.z' = sum r z - mean(z) sum r.
+// pb is the partial buffer to use next (updated).
+template <class T>
+__device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const T* bvec, T* x, double tol,
+                              int maxiter, double* red, double* tot, double* stats, int& pb) {
+  const int n = a.n;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   double* part[2] = {a.part0, a.part1};
-  int pb = 0;
-  double* r = a.r;
-  double* q = a.q;
-  double* x = a.x;
-  double* pbuf[2] = {a.p, a.p2};
+  T* r = a.r;
+  T* q = a.q;
+  T* pbuf[2] = {a.p, a.p2};
   int pc = 0;
   const double nd = (double)n;
   double bb, rr;
   {
     double acc[2] = {0.0, 0.0};
     for (int i = gt; i < n; i += gs) {
-      const double bi = a.b[i];
+      const double bi = bvec[i];
       x[i] = 0.0;
       r[i] = bi;
       acc[0] += bi * bi;
@@ -650,17 +710,17 @@ __global__ void __launch_bounds__(kCoopThreads) pcg_amg_coop_k(PcgArgs a) {
   int its = 0, conv = 0;
   double res = rnorm / bnorm;
   bool done = false;
-  if (rnorm / bnorm < a.tol) {
+  if (rnorm / bnorm < tol) {
     conv = 1;
     done = true;
   }
   // z = M r with the statistics of its projection
   double rz = 0.0, zm = 0.0;
-  double* z = nullptr;
+  T* z = nullptr;
   auto precondition = [&]() {
     __syncthreads();
     bool have = false;
-    z = vcycle(grid, a, r, gt, gs, red, stats, pb, &have);
+    z = vcycle(grid, a, (const T*)r, gt, gs, red, stats, pb, &have);
     double sz, srz, sr;
     if (have) {
       pb ^= 1;
@@ -688,18 +748,18 @@ __global__ void __launch_bounds__(kCoopThreads) pcg_amg_coop_k(PcgArgs a) {
   if (!done) rz = precondition();
   double beta = 0.0;
   bool first = true;
-  for (int k = 1; k <= a.maxiter && !done; ++k) {
+  for (int k = 1; k <= maxiter && !done; ++k) {
     // p = z' + beta p_old (z' on the first iteration); q = A p; p.q
-    double* pn = pbuf[pc];
-    const double* po = pbuf[pc ^ 1];
+    T* pn = pbuf[pc];
+    const T* po = pbuf[pc ^ 1];
     {
       double acc[2] = {0.0, 0.0};
       for (int i = gt; i < n; i += gs) {
         double s = 0.0;
-        for (int j = A.rowptr[i]; j < A.rowptr[i + 1]; ++j) {
-          const int c = A.col[j];
+        for (int j = a.rowptr[i]; j < a.rowptr[i + 1]; ++j) {
+          const int c = a.col[j];
           const double pj = first ? z[c] - zm : (z[c] - zm) + beta * po[c];
-          s += A.val[j] * pj;
+          s += a.val[j] * pj;
         }
         const double pi = first ? z[i] - zm : (z[i] - zm) + beta * po[i];
         pn[i] = pi;
@@ -733,7 +793,7 @@ __global__ void __launch_bounds__(kCoopThreads) pcg_amg_coop_k(PcgArgs a) {
     }
     rnorm = sqrt(tot[0]);
     __syncthreads();
-    if (rnorm / bnorm < a.tol) {
+    if (rnorm / bnorm < tol) {
       its = k;
       res = rnorm / bnorm;
       conv = 1;
@@ -751,6 +811,133 @@ __global__ void __launch_bounds__(kCoopThreads) pcg_amg_coop_k(PcgArgs a) {
     rz = rz_new;
     its = k;
     res = rnorm / bnorm;
+  }
+  return {its, conv, res};
+}
+
+__global__ void __launch_bounds__(kCoopThreads) pcg_amg_coop_k(PcgArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double red[(kCoopThreads / 32 + 1) * 3];
+  __shared__ double tot[3];
+  __shared__ double stats[3];
+  int pb = 0;
+  const CgOutcome o = pcg_core(grid, a, a.b, a.x, a.tol, a.maxiter, red, tot, stats, pb);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.info->iterations = o.its;
+    a.info->converged = o.conv;
+    a.info->residual = o.res;
+  }
+}
+
+// ---------------------------------------------------------------------------------- mixed PCG
+// Mixed-precision pressure-correction solve: the AMG-PCG above in float (level matrices, the
+// operator and the vectors in float; reductions and the coarse solve in double) inside an
+// iterative-refinement loop kept in double: x64 += the float correction, then the true residual
+// r64 = b - A x64 is evaluated in double from the double face coefficients (A x)_c =
+// sum_f cf_f (x_c - x_nb) + sum_b cb_b x_c, the operator the pressure assembly defines
+// (diag = sum cf + sum cb, off-diagonals -cf). The stopping test is the reference's,
+// |r| / |b| < tol with r projected when the system is singular, on r64.
+struct PcgMixedArgs {
+  PcgArgsT<float> a;     // the float solver; a.b is the float right-hand side of each pass
+  b2s_mesh m;            // cell/face topology of the operator
+  const double* cf;      // [nf] interior face coefficients
+  const double* cbf;     // [nb] boundary face coefficients
+  const double* b64;     // [n] right-hand side
+  double* x64;           // [n] solution
+  double* r64;           // [n] work: the double residual
+  float* rb32;           // [n] work: the float right-hand side of a pass
+  float* d32;            // [n] work: the float correction of a pass
+  double tol;
+  int maxiter, maxpass;
+  double min_inner_tol;  // floor of a pass's relative tolerance (the float solver's reach)
+};
+
+__global__ void __launch_bounds__(kCoopThreads) pcg_mixed_coop_k(PcgMixedArgs M) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double red[(kCoopThreads / 32 + 1) * 3];
+  __shared__ double tot[3];
+  __shared__ double stats[3];
+  const PcgArgsT<float>& a = M.a;
+  const b2s_mesh& m = M.m;
+  const int n = a.n;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  double* part[2] = {a.part0, a.part1};
+  int pb = 0;
+  const double nd = (double)n;
+  double bb, sb;
+  {
+    double acc[2] = {0.0, 0.0};
+    for (int i = gt; i < n; i += gs) {
+      const double bi = M.b64[i];
+      M.x64[i] = 0.0;
+      acc[0] += bi * bi;
+      acc[1] += bi;
+    }
+    grid_reduce<2>(grid, acc, red, part[pb], tot);
+    pb ^= 1;
+    bb = tot[0];
+    sb = tot[1];
+  }
+  double bnorm = sqrt(bb);
+  if (bnorm == 0.0) bnorm = 1.0;
+  // pass 0 residual: r = b (projected)
+  double mean = a.project ? sb / nd : 0.0;
+  double rr;
+  {
+    double acc[2] = {0.0, 0.0};
+    for (int i = gt; i < n; i += gs) {
+      const double ri = M.b64[i] - mean;
+      M.r64[i] = ri;
+      M.rb32[i] = (float)ri;
+      acc[0] += ri * ri;
+    }
+    __syncthreads();
+    grid_reduce<2>(grid, acc, red, part[pb], tot);
+    pb ^= 1;
+    rr = tot[0];
+  }
+  double res = sqrt(rr) / bnorm;
+  int its = 0, conv = res < M.tol ? 1 : 0;
+  for (int pass = 0; pass < M.maxpass && !conv && its < M.maxiter; ++pass) {
+    double tin = M.tol / res;
+    if (tin < M.min_inner_tol) tin = M.min_inner_tol;
+    __syncthreads();
+    const CgOutcome o = pcg_core(grid, a, (const float*)M.rb32, M.d32, tin, M.maxiter - its, red, tot, stats, pb);
+    its += o.its;
+    // x64 += d; then r64 = b - A x64 in double, its sum and sum of squares
+    for (int i = gt; i < n; i += gs) M.x64[i] = M.x64[i] + (double)M.d32[i];
+    grid.sync();
+    double acc[2] = {0.0, 0.0};
+    for (int c = gt; c < n; c += gs) {
+      const double xc = M.x64[c];
+      double ax = 0.0;
+      for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) ax += M.cf[f] * (xc - M.x64[m.fN[f]]);
+      for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
+        const int f = m.nei_face[k];
+        ax += M.cf[f] * (xc - M.x64[m.fP[f]]);
+      }
+      for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) ax += M.cbf[f] * xc;
+      const double ri = M.b64[c] - ax;
+      M.r64[c] = ri;
+      acc[0] += ri * ri;
+      acc[1] += ri;
+    }
+    __syncthreads();
+    grid_reduce<2>(grid, acc, red, part[pb], tot);
+    pb ^= 1;
+    mean = a.project ? tot[1] / nd : 0.0;
+    rr = a.project ? tot[0] - tot[1] * mean : tot[0];
+    if (rr < 0.0) rr = 0.0;
+    res = sqrt(rr) / bnorm;
+    __syncthreads();
+    if (!(res == res)) break;
+    if (res < M.tol) {
+      conv = 1;
+      break;
+    }
+    if (o.its == 0 && !o.conv) break;  // the float solver made no progress
+    for (int i = gt; i < n; i += gs) M.rb32[i] = (float)(M.r64[i] - mean);
+    grid.sync();
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.info->iterations = its;
@@ -776,6 +963,49 @@ static int coop_grid(K kernel, int* grid_out) {
   (void)cached_grid;
   *grid_out = g;
   return B2S_OK;
+}
+
+template <class T>
+static T* pcg_layout(const b2s_amg* h, T* w, PcgArgsT<T>& a) {
+  const int64_t n = h->nlevels ? h->levels[0].n : h->coarse_n;
+  a.r = w;
+  a.p = w + n;
+  a.p2 = w + 2 * n;
+  a.q = w + 3 * n;
+  T* c = w + 4 * n;
+  a.cb = c;
+  a.cx = c + h->coarse_n;
+  c += 2 * (int64_t)h->coarse_n;
+  for (int l = 0; l < h->nlevels; ++l) {
+    const int64_t m = h->levels[l].n;
+    a.lv[l].b = c;
+    a.lv[l].x = c + m;
+    a.lv[l].y = c + 2 * m;
+    a.lv[l].r = c + 3 * m;
+    c += 4 * m;
+  }
+  return c;
+}
+
+template <class T, int NR>
+static int launch_bicgstab_nr(BicgArgsT<T>& a, b2s_stream_t s) {
+  void* args[] = {&a};
+  int g = 0, rc;
+  if ((rc = coop_grid(bicgstab_coop_k<NR, T>, &g)) != B2S_OK) return rc;
+  if (cudaLaunchCooperativeKernel((void*)bicgstab_coop_k<NR, T>, g, kCoopThreads, args, 0, (cudaStream_t)s) !=
+      cudaSuccess)
+    return B2S_ERR_LAUNCH;
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+template <class T>
+static int launch_bicgstab(BicgArgsT<T>& a, int nrhs, b2s_stream_t s) {
+  switch (nrhs) {
+    case 1: return launch_bicgstab_nr<T, 1>(a, s);
+    case 2: return launch_bicgstab_nr<T, 2>(a, s);
+    default: return launch_bicgstab_nr<T, 3>(a, s);
+  }
 }
 
 }  // namespace b2s
@@ -817,34 +1047,49 @@ int b2s_bicgstab_jacobi_d(int32_t n, int nrhs, const int32_t* rowptr, const int3
   a.tol = tol;
   a.maxiter = maxiter;
   a.rel = relative_to_initial ? 1 : 0;
+  a.zero_x0 = 0;
   a.work = (double*)work;
   a.part0 = a.work + (int64_t)10 * nrhs * n;
   a.part1 = a.part0 + (int64_t)kMaxCoopBlocks * 3 * nrhs;
   a.info = info;
-  void* args[] = {&a};
-  int g = 0, rc;
-  switch (nrhs) {
-    case 1:
-      if ((rc = coop_grid(bicgstab_coop_k<1>, &g)) != B2S_OK) return rc;
-      if (cudaLaunchCooperativeKernel((void*)bicgstab_coop_k<1>, g, kCoopThreads, args, 0, (cudaStream_t)s) !=
-          cudaSuccess)
-        return B2S_ERR_LAUNCH;
-      break;
-    case 2:
-      if ((rc = coop_grid(bicgstab_coop_k<2>, &g)) != B2S_OK) return rc;
-      if (cudaLaunchCooperativeKernel((void*)bicgstab_coop_k<2>, g, kCoopThreads, args, 0, (cudaStream_t)s) !=
-          cudaSuccess)
-        return B2S_ERR_LAUNCH;
-      break;
-    default:
-      if ((rc = coop_grid(bicgstab_coop_k<3>, &g)) != B2S_OK) return rc;
-      if (cudaLaunchCooperativeKernel((void*)bicgstab_coop_k<3>, g, kCoopThreads, args, 0, (cudaStream_t)s) !=
-          cudaSuccess)
-        return B2S_ERR_LAUNCH;
-      break;
-  }
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  a.out64 = nullptr;
+  a.base64 = nullptr;
+  return launch_bicgstab(a, nrhs, s);
+}
+
+int64_t b2s_bicgstab_f32_workspace_bytes(int32_t n, int nrhs) {
+  if (n <= 0 || nrhs < 1 || nrhs > 3) return -1;
+  return (int64_t)sizeof(float) * ((int64_t)10 * nrhs * n) + (int64_t)sizeof(double) * 2 * kMaxCoopBlocks * 3 * nrhs;
+}
+
+int b2s_bicgstab_jacobi_f32_d(int32_t n, int nrhs, const int32_t* rowptr, const int32_t* col, const float* val,
+                              const float* b, const float* inv_diag, float* x, double tol, int maxiter,
+                              int relative_to_initial, int zero_x0, double* out64, const double* base64, void* work,
+                              int64_t work_bytes, b2s_solve_info* info, b2s_stream_t s) {
+  if (n <= 0 || nrhs < 1 || nrhs > 3 || !rowptr || !col || !val || !b || !inv_diag || !x || !work || !info ||
+      maxiter < 0 || ((out64 == nullptr) != (base64 == nullptr)))
+    return B2S_ERR_ARG;
+  if (work_bytes < b2s_bicgstab_f32_workspace_bytes(n, nrhs)) return B2S_ERR_WORKSPACE;
+  BicgArgsT<float> a;
+  a.n = n;
+  a.nr = nrhs;
+  a.rowptr = rowptr;
+  a.col = col;
+  a.val = val;
+  a.b = b;
+  a.inv = inv_diag;
+  a.x = x;
+  a.tol = tol;
+  a.maxiter = maxiter;
+  a.rel = relative_to_initial ? 1 : 0;
+  a.zero_x0 = zero_x0 ? 1 : 0;
+  a.work = (float*)work;
+  a.part0 = (double*)((char*)work + sizeof(float) * (int64_t)10 * nrhs * n);
+  a.part1 = a.part0 + (int64_t)kMaxCoopBlocks * 3 * nrhs;
+  a.info = info;
+  a.out64 = out64;
+  a.base64 = base64;
+  return launch_bicgstab(a, nrhs, s);
 }
 
 static bool amg_ok(const b2s_amg* h) {
@@ -868,25 +1113,11 @@ int64_t b2s_pcg_workspace_bytes(const b2s_amg* h) {
 }
 
 static void pcg_layout(const b2s_amg* h, double* w, PcgArgs& a) {
-  const int64_t n = h->nlevels ? h->levels[0].n : h->coarse_n;
-  a.r = w;
-  a.p = w + n;
-  a.p2 = w + 2 * n;
-  a.q = w + 3 * n;
-  double* c = w + 4 * n;
-  a.cb = c;
-  a.cx = c + h->coarse_n;
-  c += 2 * (int64_t)h->coarse_n;
-  for (int l = 0; l < h->nlevels; ++l) {
-    const int64_t m = h->levels[l].n;
-    a.lv[l].b = c;
-    a.lv[l].x = c + m;
-    a.lv[l].y = c + 2 * m;
-    a.lv[l].r = c + 3 * m;
-    c += 4 * m;
-  }
+  double* c = pcg_layout<double>(h, w, a);
   a.part0 = c;
   a.part1 = c + (int64_t)kMaxCoopBlocks * 3;
+  for (int l = 0; l < h->nlevels; ++l)
+    a.lvv[l] = {h->levels[l].val, h->levels[l].dinv, h->levels[l].p_val, h->levels[l].r_val};
 }
 
 int b2s_pcg_amg_d(const b2s_amg* h, int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,
@@ -912,6 +1143,72 @@ int b2s_pcg_amg_d(const b2s_amg* h, int32_t n, const int32_t* rowptr, const int3
   int g = 0, rc;
   if ((rc = coop_grid(pcg_amg_coop_k, &g)) != B2S_OK) return rc;
   if (cudaLaunchCooperativeKernel((void*)pcg_amg_coop_k, g, kCoopThreads, args, 0, (cudaStream_t)s) != cudaSuccess)
+    return B2S_ERR_LAUNCH;
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+static bool amg32_ok(const b2s_amg* h, const b2s_amg_f32* h32) {
+  if (!h32) return false;
+  for (int l = 0; l < h->nlevels; ++l)
+    if (!h32->val[l] || !h32->dinv[l] || !h32->p_val[l] || !h32->r_val[l]) return false;
+  return true;
+}
+
+int64_t b2s_pcg_mixed_workspace_bytes(const b2s_amg* h) {
+  if (!amg_ok(h)) return -1;
+  const int64_t n = h->nlevels ? h->levels[0].n : h->coarse_n;
+  int64_t f = 4 * n + 2 * (int64_t)h->coarse_n + 2 * n;  // float vectors
+  for (int l = 0; l < h->nlevels; ++l) f += 4 * (int64_t)h->levels[l].n;
+  const int64_t d = n + 2 * (int64_t)kMaxCoopBlocks * 3;  // r64 and the partial sums
+  return d * (int64_t)sizeof(double) + f * (int64_t)sizeof(float) + 16;
+}
+
+int b2s_pcg_amg_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const b2s_mesh* m, const double* cf,
+                        const double* cb, int32_t n, const int32_t* rowptr, const int32_t* col, const float* val,
+                        const double* b, double* x, double tol, int maxiter, int project, int maxpass,
+                        double min_inner_tol, void* work, int64_t work_bytes, b2s_solve_info* info, b2s_stream_t s) {
+  if (!amg_ok(h) || !amg32_ok(h, h32) || !m || !cf || (!cb && m->nb) || !rowptr || !col || !val || !b || !x ||
+      !work || !info || maxiter < 0 || maxpass < 1 || !(min_inner_tol > 0.0))
+    return B2S_ERR_ARG;
+  if (n != (h->nlevels ? h->levels[0].n : h->coarse_n) || n != m->nc) return B2S_ERR_ARG;
+  if (!m->own_ptr || !m->nei_ptr || !m->nei_face || !m->fN || !m->fP || !m->bptr) return B2S_ERR_ARG;
+  if (work_bytes < b2s_pcg_mixed_workspace_bytes(h)) return B2S_ERR_WORKSPACE;
+  PcgMixedArgs M;
+  PcgArgsT<float>& a = M.a;
+  a.h = *h;
+  for (int l = 0; l < h->nlevels; ++l) a.lvv[l] = {h32->val[l], h32->dinv[l], h32->p_val[l], h32->r_val[l]};
+  a.n = n;
+  a.rowptr = rowptr;
+  a.col = col;
+  a.val = val;
+  a.x = nullptr;
+  a.tol = tol;
+  a.maxiter = maxiter;
+  a.project = project ? 1 : 0;
+  a.info = info;
+  double* dw = (double*)work;
+  M.r64 = dw;
+  a.part0 = dw + n;
+  a.part1 = a.part0 + (int64_t)kMaxCoopBlocks * 3;
+  float* fw = (float*)(a.part1 + (int64_t)kMaxCoopBlocks * 3);
+  float* rest = pcg_layout<float>(h, fw, a);
+  M.rb32 = rest;
+  M.d32 = rest + n;
+  a.b = M.rb32;
+  M.m = *m;
+  M.cf = cf;
+  M.cbf = cb;
+  M.b64 = b;
+  M.x64 = x;
+  M.tol = tol;
+  M.maxiter = maxiter;
+  M.maxpass = maxpass;
+  M.min_inner_tol = min_inner_tol;
+  void* args[] = {&M};
+  int g = 0, rc;
+  if ((rc = coop_grid(pcg_mixed_coop_k, &g)) != B2S_OK) return rc;
+  if (cudaLaunchCooperativeKernel((void*)pcg_mixed_coop_k, g, kCoopThreads, args, 0, (cudaStream_t)s) != cudaSuccess)
     return B2S_ERR_LAUNCH;
   B2S_LAUNCH_CHECK();
   return B2S_OK;

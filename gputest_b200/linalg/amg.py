@@ -131,6 +131,7 @@ class AMGHierarchy:
         # the hierarchy's own copy of the level-0 values: like the reference's preconditioner
         # object, the V-cycle keeps the matrix of the last rebuild until the next one
         self.src_val = val
+        self.src_val32 = None
         self.val0 = torch.empty_like(val)
         self.val0.copy_(val)
         level_val = self.val0
@@ -224,11 +225,54 @@ class AMGHierarchy:
         return int(self._count_host[0]) != 0
 
     def rebuild(self, stream=None):
-        """Copy the current level-0 values and recompute every numeric quantity (device)."""
+        """Copy the current level-0 values and recompute every numeric quantity (device). With a
+        float source (``enable_mixed``) the values are widened first and the float copies of the
+        level values are refreshed after the rebuild."""
+        if self.src_val32 is not None:
+            self.src_val.copy_(self.src_val32)
         self.val0.copy_(self.src_val)
         _lib.check(_lib.lib().b2s_amg_rebuild_d(self.cref, self.work_rebuild.data_ptr(),
                                                 self.work_rebuild.numel() * 8, _lib.stream_ptr(stream)),
                    "b2s_amg_rebuild_d")
+        if self.src_val32 is not None:
+            _lib.check(_lib.lib().b2s_amg_to_f32_d(self.cref, self.c32ref, _lib.stream_ptr(stream)), "b2s_amg_to_f32_d")
+
+    def enable_mixed(self, val32):
+        """Prepare the float solve: float copies of every level's values (refreshed by ``rebuild``)
+        and the workspace of ``pcg_mixed``; val32 is the float level-0 operator, whose values
+        ``rebuild`` widens into ``src_val`` before rebuilding."""
+        import torch
+
+        dev = val32.device
+        self.src_val32 = val32
+        h = self.c
+        h32 = self.c32 = _lib.Amg32()
+        self._keep32 = []
+        for l in range(h.nlevels):
+            L = h.levels[l]
+            bufs = {"val": torch.empty(L.nnz, dtype=torch.float32, device=dev),
+                    "dinv": torch.empty(L.n, dtype=torch.float32, device=dev),
+                    "p_val": torch.empty(L.p_nnz, dtype=torch.float32, device=dev),
+                    "r_val": torch.empty(L.p_nnz, dtype=torch.float32, device=dev)}
+            for k, v in bufs.items():
+                getattr(h32, k)[l] = v.data_ptr()
+            self._keep32.append(bufs)
+        self.c32ref = ctypes.byref(h32)
+        mb = _lib.lib().b2s_pcg_mixed_workspace_bytes(self.cref)
+        if mb < 0:
+            raise RuntimeError("invalid AMG hierarchy")
+        self.work_mixed = torch.empty(mb // 8 + 1, dtype=torch.float64, device=dev)
+
+    def pcg_mixed(self, mesh_ref, cf, cb, b, x, tol, maxiter, project, info, maxpass=8, min_inner_tol=1e-5,
+                  stream=None):
+        """Solve A x = b (double b, x) by float AMG-PCG passes with double iterative refinement,
+        A applied in double from the face coefficients cf, cb of the mesh (``b2s_pcg_amg_mixed_d``)."""
+        _lib.check(_lib.lib().b2s_pcg_amg_mixed_d(self.cref, self.c32ref, mesh_ref, cf.data_ptr(), cb.data_ptr(),
+                                                  self.n0, self.rowptr0.data_ptr(), self.col0.data_ptr(),
+                                                  self.src_val32.data_ptr(), b.data_ptr(), x.data_ptr(), float(tol),
+                                                  int(maxiter), int(bool(project)), int(maxpass), float(min_inner_tol),
+                                                  self.work_mixed.data_ptr(), self.work_mixed.numel() * 8, info,
+                                                  _lib.stream_ptr(stream)), "b2s_pcg_amg_mixed_d")
 
     def vcycle(self, b, stream=None):
         import torch

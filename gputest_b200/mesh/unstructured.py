@@ -492,3 +492,57 @@ def sort_faces_by_zone(mesh: UnstructuredMesh) -> UnstructuredMesh:
                             owner=mesh.owner[perm], neighbour=mesh.neighbour[perm], face_zone=fz,
                             n_cells=mesh.n_cells, cell_zone=mesh.cell_zone, zones=zones, name=mesh.name,
                             periodic=periodic)
+
+
+def union_mesh(meshes: List[UnstructuredMesh], prefixes: Optional[List[str]] = None,
+               name: str = "batch") -> UnstructuredMesh:
+    """Disjoint union of meshes of one dimension: the block-diagonal batch of independent cases.
+
+    Cells, faces and nodes of mesh i follow those of meshes 0..i-1; every zone is kept, renamed
+    ``prefixes[i] + name`` (default ``"c{i}/"``) with a fresh id, and the faces are then sorted by
+    zone (interior zones first). ``union_groups`` gives the mesh each union cell came from."""
+    if not meshes:
+        raise ValueError("no meshes")
+    dim = meshes[0].dim
+    if any(m.dim != dim for m in meshes):
+        raise ValueError("meshes of different dimensions")
+    if any(m.periodic for m in meshes):
+        raise NotImplementedError("periodic meshes cannot be batched")
+    prefixes = prefixes or [f"c{i}/" for i in range(len(meshes))]
+    nodes, fptr, fnodes, own, nei, fz, cz, zones = [], [np.zeros(1, dtype=np.int64)], [], [], [], [], [], {}
+    n_off = c_off = fn_off = 0
+    zid = 1
+    for m, pre in zip(meshes, prefixes):
+        remap = {}
+        for z in sorted(m.zones.values(), key=lambda z: z.id):
+            remap[z.id] = zid
+            zones[zid] = Zone(zid, pre + z.name, z.type, z.kind)
+            zid += 1
+        lut = np.zeros(max(m.zones) + 1, dtype=np.int64)
+        for old, new in remap.items():
+            lut[old] = new
+        nodes.append(m.nodes)
+        fptr.append(m.face_ptr[1:] + fn_off)
+        fnodes.append(m.face_nodes + n_off)
+        own.append(m.owner + c_off)
+        nei.append(np.where(m.neighbour >= 0, m.neighbour + c_off, -1))
+        fz.append(lut[m.face_zone])
+        cz.append(lut[m.cell_zone])
+        n_off += m.n_nodes
+        c_off += m.n_cells
+        fn_off += int(m.face_ptr[-1])
+    cell_zone = np.concatenate(cz)
+    for z in zones.values():
+        if z.kind == "cell":
+            where = np.flatnonzero(cell_zone == z.id)
+            if where.size:
+                z.first, z.last = int(where[0]), int(where[-1])
+    u = UnstructuredMesh(dim=dim, nodes=np.concatenate(nodes), face_ptr=np.concatenate(fptr).astype(np.int64),
+                         face_nodes=np.concatenate(fnodes), owner=np.concatenate(own), neighbour=np.concatenate(nei),
+                         face_zone=np.concatenate(fz), n_cells=c_off, cell_zone=cell_zone, zones=zones, name=name)
+    return sort_faces_by_zone(u)
+
+
+def union_groups(meshes: List[UnstructuredMesh]) -> np.ndarray:
+    """Index of the source mesh of every cell of ``union_mesh(meshes)``."""
+    return np.repeat(np.arange(len(meshes)), [m.n_cells for m in meshes])

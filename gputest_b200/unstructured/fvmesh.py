@@ -124,7 +124,10 @@ class FVMesh:
     """Device layout of a mesh (see the module docstring). ``device`` defaults to the current
     CUDA device; there is no CPU variant."""
 
-    def __init__(self, mesh: UnstructuredMesh, device=None, reorder: bool = True):
+    def __init__(self, mesh: UnstructuredMesh, device=None, reorder: bool = True, groups=None):
+        """``groups`` (one label per cell, optional): cells of one group are kept contiguous in the
+        device order, groups in increasing label order (the reverse Cuthill-McKee order within
+        each) - the layout of a block-diagonal batch of independent cases."""
         import torch
 
         self.device = device if device is not None else _lib.require_device()
@@ -143,6 +146,9 @@ class FVMesh:
             perm = np.asarray(reverse_cuthill_mckee(adj, symmetric_mode=True), dtype=np.int64)
         else:
             perm = np.arange(nc, dtype=np.int64)
+        if groups is not None:
+            groups = np.asarray(groups)
+            perm = perm[np.argsort(groups[perm], kind="stable")]
         iperm = np.empty(nc, dtype=np.int64)
         iperm[perm] = np.arange(nc)
         self.perm, self.iperm = perm, iperm  # device -> reference, reference -> device

@@ -85,7 +85,7 @@ class DeviceBackend:
         torch.cuda.synchronize(self.torch_device)
 
 
-def _check_scope(case: UnstructuredCase):
+def _check_scope(case: UnstructuredCase, precisions=("fp64",)):
     unsupported = []
     if case.turbulence != "laminar":
         unsupported.append(f"turbulence={case.turbulence!r}")
@@ -103,7 +103,7 @@ def _check_scope(case: UnstructuredCase):
         unsupported.append("transient runs")
     if any(case.buoyancy[:3]):
         unsupported.append("buoyancy")
-    if case.precision not in ("fp64",):
+    if case.precision not in precisions:
         unsupported.append(f"precision={case.precision!r} in SimpleSolver (use MixedSimpleSolver)")
     if unsupported:
         raise NotImplementedError("the B200 SIMPLEC path does not implement: " + ", ".join(unsupported))
@@ -117,11 +117,19 @@ class SimpleSolver:
     GUARD_MIN_RELAX = 0.1
     GUARD_FALLBACK = True
     GUARD_MIN_RELAX_U = 0.2
+    PRECISIONS = ("fp64",)
 
-    def __init__(self, mesh: UnstructuredMesh, case: UnstructuredCase, backend=None, max_coarse: int = 150):
+    def __init__(self, mesh: UnstructuredMesh, case: UnstructuredCase, backend=None, max_coarse: int = 150,
+                 amg_theta: float = 0.08):
+        """``max_coarse``: rows at which the AMG hierarchy stops coarsening (the reference uses 300;
+        150 keeps the coarse inverse in shared memory). ``amg_theta``: strength-of-connection
+        threshold of the aggregation; 0.08 is the reference's own smoothed aggregation
+        (``flowtrace/linalg/amg.py:80-101``, its preconditioner on GPU backends), 0.0 the strength
+        rule of pyamg's ``smoothed_aggregation_solver`` defaults that its CPU backend calls
+        (``amg.py:149-168``), far better conditioned on anisotropic 3-D meshes."""
         import torch
 
-        _check_scope(case)
+        _check_scope(case, self.PRECISIONS)
         self.case, self.mesh = case, mesh
         self.torch_device = _lib.require_device()
         self.be = DeviceBackend(self.torch_device)
@@ -147,6 +155,7 @@ class SimpleSolver:
         # round trip of the pressure matrix per rebuild.
         self.reaggregate = False
         self.max_coarse = int(max_coarse)
+        self.amg_theta = float(amg_theta)
         self.last_linear = {}
         self.external_energy = False
         self.relax_p = float(case.relax_p) if case.relax_p is not None else auto_relax_p(fv.non_orthogonality_deg)
@@ -403,7 +412,8 @@ class SimpleSolver:
         torch.cuda.current_stream().synchronize()
         A_host = self.fv.matrix_to_host(self.val_P)
         self._amg = AMGHierarchy(A_host, self.fv.perm, self.fv.rowptr, self.fv.col, self.fv.t["slot_diag"],
-                                 self.val_P, self.fv.slot_ref, singular=self.singular_p, max_coarse=self.max_coarse)
+                                 self.val_P, self.fv.slot_ref, singular=self.singular_p, max_coarse=self.max_coarse,
+                                 theta=self.amg_theta)
         self.amg_setups += 1
 
     def _ensure_amg(self, s):

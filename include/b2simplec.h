@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define B2S_ABI_VERSION 1
+#define B2S_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define B2S_API __attribute__((visibility("default")))
@@ -80,6 +80,13 @@ typedef struct b2s_mesh {
   const int32_t* slot_diag;/* [nc] */
   const int32_t* slot_PN;  /* [nf] CSR slot of (P, N) */
   const int32_t* slot_NP;  /* [nf] CSR slot of (N, P) */
+  /* Optional tiling of the cells (NULL: none), for block-diagonal batches of independent cases:
+   * tile t is cells tiles[t] .. tiles[t+1]-1, at most 256 cells, never two cases. With a tiling,
+   * the stages that write per-block partial sums (momentum, pressure, correction and energy
+   * assembly) give one partial per tile (b2s_mesh_part_blocks), so sums per case follow. */
+  const int32_t* tiles;
+  int32_t ntiles;
+  int32_t pad_;
 } b2s_mesh;
 
 /* Boundary conditions as face masks (0/1 doubles, as flowtrace/unstructured/simple.py:228-240). */
@@ -265,6 +272,7 @@ typedef struct b2s_amg_level {
   double* w_val;
   double* rho;                 /* [1] spectral radius estimate (device) */
   const uint8_t* strong;       /* [nnz] strength of each entry at set-up (1: strong), or NULL */
+  const int32_t* group_ptr;    /* batches: [ngroups+1] rows of each case on this level, or NULL */
 } b2s_amg_level;
 
 typedef struct b2s_amg {
@@ -276,7 +284,16 @@ typedef struct b2s_amg {
   const int32_t* coarse_rowptr;/* coarse CSR (values are level nlevels-1's Galerkin product) */
   const int32_t* coarse_col;
   double* coarse_val;
-  double* coarse_inv;          /* [coarse_n][coarse_n] */
+  double* coarse_inv;          /* [coarse_n][coarse_n]; batches: one dense block per case */
+  /* Batches of independent cases (ngroups > 0): every level is block diagonal with the rows of a
+   * case contiguous (levels[l].group_ptr), the coarse inverse is stored per case (block g of
+   * size n_g = coarse_group_ptr[g+1]-coarse_group_ptr[g] at coarse_inv + coarse_inv_off[g]) and
+   * the singular shift applies per case (group_singular[g]). */
+  int32_t ngroups;
+  int32_t pad_;
+  const int32_t* coarse_group_ptr;
+  const int64_t* coarse_inv_off;
+  const int32_t* group_singular;
   b2s_amg_level levels[B2S_AMG_MAX_LEVELS];
 } b2s_amg;
 
@@ -307,6 +324,68 @@ B2S_API int b2s_amg_vcycle_d(const b2s_amg* h, const double* b, double* x, void*
  * strength graph given as HOST CSR arrays; agg[n] (host) receives each node's aggregate and
  * the return value is the number of aggregates (-1 on invalid arguments). */
 B2S_API int64_t b2s_host_aggregate(int64_t n, const int64_t* indptr, const int64_t* indices, int64_t* agg);
+
+/* ----------------------------------------------------------------------------------------- */
+/* Mixed precision. No counterpart in the reference (its path is FP64 throughout): the linear    */
+/* systems are stored and solved in float, while the nonlinear residuals, the continuity and     */
+/* norm reductions, the iterative refinement of the pressure-correction solve and the AMG        */
+/* coarsest-level solve stay double. Every linear system is solved in correction form           */
+/* A_r dphi = b - A phi from dphi = 0, so a converged iteration is the double one's fixed point. */
+
+/* Momentum assembly of b2s_momentum_assemble_d with the relaxed matrix values and the Jacobi
+ * inverse written in float, and, instead of b / b_r, the double residual r = b - A U of the
+ * unrelaxed system ([dim][nc], stored in float). part receives the same scaled-residual sums. */
+B2S_API int b2s_momentum_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                          const double* Up, const double* gUp, const double* gp, const double* bUp,
+                                          const double* F, const double* Fb, const double* porosity,
+                                          const double* msrc, float* val, float* inv, double* dP, float* r,
+                                          double* part, b2s_stream_t s);
+
+/* Pressure-correction assembly of b2s_pressure_assemble_d with the matrix values in float. */
+B2S_API int b2s_pressure_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                          const double* Ustar, const double* p, const double* gp, const double* dP,
+                                          double* Fst, double* cf, double* Fbst, double* cb, float* val, double* rhs,
+                                          double* part, b2s_stream_t s);
+
+/* Energy assembly of b2s_energy_assemble_d in the form of b2s_momentum_assemble_mixed_d. */
+B2S_API int b2s_energy_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp,
+                                        double relax_T, int second_order, const double* T, const double* gT,
+                                        const double* Tb, const double* F, const double* Fb, const double* esrc,
+                                        float* val, float* inv, float* r, double* part, b2s_stream_t s);
+
+/* Jacobi-BiCGSTAB of b2s_bicgstab_jacobi_d with float matrix values and vectors (reductions in
+ * double). zero_x0 starts from x = 0 without reading x; out64/base64 (both or neither, [nrhs][n])
+ * receive out64 = base64 + x in double at the end. */
+B2S_API int64_t b2s_bicgstab_f32_workspace_bytes(int32_t n, int nrhs);
+B2S_API int b2s_bicgstab_jacobi_f32_d(int32_t n, int nrhs, const int32_t* rowptr, const int32_t* col,
+                                      const float* val, const float* b, const float* inv_diag, float* x, double tol,
+                                      int maxiter, int relative_to_initial, int zero_x0, double* out64,
+                                      const double* base64, void* work, int64_t work_bytes, b2s_solve_info* info,
+                                      b2s_stream_t s);
+
+/* Float copies of the hierarchy's per-level values (the V-cycle of the mixed solve reads these;
+ * the coarse inverse stays double). Arrays are caller-allocated with the level sizes. */
+typedef struct b2s_amg_f32 {
+  float* val[B2S_AMG_MAX_LEVELS];
+  float* dinv[B2S_AMG_MAX_LEVELS];
+  float* p_val[B2S_AMG_MAX_LEVELS];
+  float* r_val[B2S_AMG_MAX_LEVELS];
+} b2s_amg_f32;
+B2S_API int b2s_amg_to_f32_d(const b2s_amg* h, const b2s_amg_f32* h32, b2s_stream_t s);
+
+/* Pressure-correction solve with iterative refinement: passes of the AMG-PCG in float (tolerance
+ * tol / current relative residual, floored at min_inner_tol), each followed by x += correction
+ * and the true residual r = b - A x in double, A applied from the double face coefficients
+ * (A x)_c = sum_f cf_f (x_c - x_nb) + sum_b cb_b x_c of the mesh m. Stops when |r| / |b| < tol
+ * (r projected when project != 0), after maxpass passes or maxiter float iterations in total.
+ * (rowptr, col, val) is the float operator of the inner solve; x ([n], double) is overwritten.
+ * info->iterations counts the float iterations, info->residual is the double one. */
+B2S_API int64_t b2s_pcg_mixed_workspace_bytes(const b2s_amg* h);
+B2S_API int b2s_pcg_amg_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const b2s_mesh* m, const double* cf,
+                                const double* cb, int32_t n, const int32_t* rowptr, const int32_t* col,
+                                const float* val, const double* b, double* x, double tol, int maxiter, int project,
+                                int maxpass, double min_inner_tol, void* work, int64_t work_bytes,
+                                b2s_solve_info* info, b2s_stream_t s);
 
 #ifdef __cplusplus
 }

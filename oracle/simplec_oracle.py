@@ -570,13 +570,14 @@ class OracleSimple:
     GUARD_GROWTH, GUARD_ROUNDOFF, GUARD_EVERY = 20.0, 1e-6, 20                      # simple.py:706-712
     GUARD_FACTOR, GUARD_MIN_RELAX, GUARD_FALLBACK, GUARD_MIN_RELAX_U = 0.6, 0.1, True, 0.2
 
-    def __init__(self, mesh, case, native=None, porosity=None):
+    def __init__(self, mesh, case, native=None, porosity=None, amg_theta=0.08):
         for attr, off in (("turbulence", "laminar"), ("radiation", "off")):
             if getattr(case, attr) != off:
                 raise NotImplementedError(f"{attr}={getattr(case, attr)!r} is outside the oracle's scope")
         if case.unsteady or case.species or case.mrf or case.solids or case.periodic:
             raise NotImplementedError("transient, species, MRF, solids and periodic cases are outside the oracle's scope")
         self.case, self.mesh = case, mesh
+        self.amg_theta = float(amg_theta)
         self.native = native
         self.fv = fv = OracleFV(mesh, native)
         self.dim = dim = mesh.dim
@@ -814,7 +815,7 @@ class OracleSimple:
         res["continuity"] = float(np.sum(np.abs(mass)))
         if self._amg is None or self._amg_age >= self.amg_rebuild:                     # simple.py:624-628
             Ah = Ap.csr if hasattr(Ap, "csr") else Ap
-            self._amg = SmoothedAggregationAMG(Ah, singular=self.singular_p)
+            self._amg = SmoothedAggregationAMG(Ah, theta=self.amg_theta, singular=self.singular_p)
             self._amg_age = 0
         self._amg_age += 1
         project = (lambda v: v - v.mean()) if self.singular_p else None

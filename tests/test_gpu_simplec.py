@@ -23,11 +23,11 @@ def _rel(a, b):
     return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
 
 
-def _pair(mesh, case, n, max_coarse=300):
+def _pair(mesh, case, n, max_coarse=300, amg_theta=0.08):
     from gputest_b200.unstructured.simple import SimpleSolver
 
-    o = OracleSimple(mesh, case)
-    s = SimpleSolver(mesh, case, max_coarse=max_coarse)
+    o = OracleSimple(mesh, case, amg_theta=amg_theta)
+    s = SimpleSolver(mesh, case, max_coarse=max_coarse, amg_theta=amg_theta)
     s.reaggregate = True  # the reference re-aggregates at every rebuild
     for _ in range(n):
         o.step()
@@ -170,3 +170,20 @@ def test_assembly_per_entry_from_the_same_state():
              "Fst": (cs["Fst"], co["Fst"]), "Fbst": (cs["Fbst"], co["Fbst"])}
     for k, (ours, ref) in pairs.items():
         assert np.abs(ours - ref).max() <= 1e-12 * np.abs(ref).max(), k
+
+
+def test_simplec_iterates_equal_oracle_with_pyamg_strength_rule():
+    """The AMG with strength threshold 0 (pyamg's default rule) on a jittered 3-D duct with an
+    outlet: iterates against the oracle configured the same way."""
+    names = ("inlet", "outlet", "wall", "wall", "wall", "wall")
+    mesh = box_mesh_3d(12, 6, 6, 4.0, 1.0, 1.0, jitter=0.1, seed=1, names=names,
+                       types=("velocity-inlet", "pressure-outlet", "wall", "wall", "wall", "wall"))
+    case = UnstructuredCase(boundaries={"inlet": BoundarySpec("inlet", velocity=[1.0, 0.0, 0.0]),
+                                        "outlet": BoundarySpec("outlet", pressure=0.0),
+                                        "wall": BoundarySpec("wall")},
+                            viscosity=0.02, max_iter=30, tol=0.0, pressure_tol=TIGHT)
+    o, s = _pair(mesh, case, 15, amg_theta=0.0)
+    fo, fs = o.fields(), s.fields()
+    for k in fo:
+        assert _rel(fs[k], fo[k]) < 1e-9, k
+    assert s._amg.sizes == [lv[0].shape[0] for lv in o._amg.levels] + [o._amg.coarse_inv.shape[0]]
