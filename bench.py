@@ -84,6 +84,38 @@ def make_workload(name):
     raise SystemExit(f"unknown config {name!r}")
 
 
+def make_batch_workload(ncase=256, seed=2, lo=1e3, hi=6.4e4):
+    """The batched sweep: ncase independent 2-D cases from ``default_rng(seed)``; per case a fair
+    coin picks a lid-driven cavity (unit square) or a 4 x 1 channel, the cell count is log-uniform
+    in [lo, hi] (nearest grid), interior nodes jittered by +-0.15h, Re uniform in [100, 2000],
+    lid/inlet speed U uniform in [0.5, 2], viscosity U L / Re (L = 1)."""
+    import numpy as np
+
+    from gputest_b200.mesh.unstructured import cartesian_mesh_2d
+    from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase
+
+    rng = np.random.default_rng(seed)
+    meshes, cases, kinds = [], [], []
+    for i in range(ncase):
+        cavity = rng.random() < 0.5
+        nc = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        re = float(rng.uniform(100.0, 2000.0))
+        u = float(rng.uniform(0.5, 2.0))
+        if cavity:
+            n = max(4, int(round(np.sqrt(nc))))
+            m = cartesian_mesh_2d(n, n, jitter=0.15, seed=i)
+            b = {"top": BoundarySpec("wall", velocity=[u, 0.0])}
+        else:
+            ny = max(2, int(round(np.sqrt(nc / 4.0))))
+            m = cartesian_mesh_2d(4 * ny, ny, 4.0, 1.0, names=("in", "out", "bottom", "top"), jitter=0.15, seed=i)
+            b = {"in": BoundarySpec("inlet", velocity=[u, 0.0]), "out": BoundarySpec("outlet"),
+                 "bottom": BoundarySpec("wall"), "top": BoundarySpec("wall")}
+        meshes.append(m)
+        cases.append(UnstructuredCase(boundaries=b, viscosity=u / re, tol=1e-6, max_iter=100000))
+        kinds.append("cavity" if cavity else "channel")
+    return meshes, cases, kinds
+
+
 # ---------------------------------------------------------------------------------- byte models
 def stage_bytes(solver, stage, step_info):
     """Algorithmic DRAM bytes of one launch of a stage: every array the stage's kernels read
@@ -103,14 +135,18 @@ def stage_bytes(solver, stage, step_info):
         bnd = nb * 8 * (4 + 3 * d) + nb * 4
         return faces + cells + bnd
     if stage == "momentum_solve":
-        its = max(step_info["momentum_iters"])
+        import numpy as np
+
+        its = int(np.max(step_info["momentum_iters"]))
         k = d
         init = csr + nc * 8 * k * 6
         per_it = 2 * (csr + nc * 8 * k * 2) + nc * 8 * k * 14 + nc * 8 * 2
         return init + its * per_it
     if stage == "pressure_solve":
+        import numpy as np
+
         amg = solver._amg
-        its = step_info["pressure_iters"]
+        its = int(np.max(step_info["pressure_iters"]))
         init = nc * 8 * 3
         per_it = (csr + nc * 8 * 2) + nc * 8 * 9
         vc = 0
@@ -205,6 +241,201 @@ def max_over_ranks(ms: float, world: int, device=None) -> float:
     return float(t.item())
 
 
+# ---------------------------------------------------------------------------------- batched sweep
+def run_batch(args, rank, world):
+    """The batched sweep (``--config c4``): all cases as one ``BatchSimpleSolver`` (the timed arm)
+    against the same cases solved one at a time by ``MixedSimpleSolver`` (same arithmetic), on a
+    stratified sample of cases whose per-step times are interpolated over the cell count. With
+    N > 1 ranks the cases are dealt to ranks by cell count (replicas of the batch mechanism,
+    no collective in the data path)."""
+    import numpy as np
+    import torch
+
+    from gputest_b200.unstructured.batch import BatchSimpleSolver
+    from gputest_b200.unstructured.mixed import MixedSimpleSolver
+
+    meshes, cases, kinds = make_batch_workload(args.batch_cases)
+    order = np.argsort([-m.n_cells for m in meshes], kind="stable")
+    load = np.zeros(world)
+    mine = []
+    for i in order:  # greedy cells-balanced deal
+        r = int(np.argmin(load))
+        load[r] += meshes[i].n_cells
+        if r == rank:
+            mine.append(int(i))
+    mine.sort()
+    meshes, cases, kinds = [meshes[i] for i in mine], [cases[i] for i in mine], [kinds[i] for i in mine]
+    ncell = int(sum(m.n_cells for m in meshes))
+    K, W = args.steps, max(args.warmup, 3)
+    t0 = time.perf_counter()
+    bs = BatchSimpleSolver(meshes, [__import__("copy").deepcopy(c) for c in cases])
+    for c in bs.cases + [bs.case]:
+        c.tol = 0.0
+    setup_s = time.perf_counter() - t0
+    for _ in range(W):
+        bs.step()
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    l0 = bs.kernel_launches
+    torch.cuda.synchronize()
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record()
+        bs.step()
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    launches = bs.kernel_launches - l0
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    bs.profile_stages = True
+    bs.stage_times.clear()
+    infos = []
+    for _ in range(K):
+        flush.zero_()
+        bs.step()
+        infos.append(dict(bs.last_linear))
+    bs.profile_stages = False
+    torch.cuda.synchronize()
+    times = dict(bs.stage_times)
+    # one case at a time, same arithmetic: a stratified sample by cell count
+    idx = np.argsort([m.n_cells for m in meshes], kind="stable")
+    sample = sorted(set(int(idx[int(j)]) for j in np.linspace(0, len(idx) - 1, min(args.batch_sample, len(idx))).round()))
+    samp = []
+    for i in sample:
+        c = __import__("copy").deepcopy(cases[i])
+        c.tol = 0.0
+        s1 = MixedSimpleSolver(meshes[i], c)
+        for _ in range(W):
+            s1.step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(K):
+            s1.step()
+        e1.record()
+        torch.cuda.synchronize()
+        samp.append((meshes[i].n_cells, e0.elapsed_time(e1) / K))
+        del s1
+    xs = np.log([a for a, _ in samp])
+    ys = np.array([b for _, b in samp])
+    seq_ms = float(sum(np.interp(np.log(m.n_cells), xs, ys) for m in meshes))
+    one = ncell / (seq_ms / 1e3)
+    ms_max = max_over_ranks(ms, world, "cuda")
+    tot = torch.tensor([float(ncell) * K], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(tot)
+    value = float(tot.item()) / (ms_max / 1e3)
+    conv = None
+    if args.converge:
+        bc = BatchSimpleSolver(meshes, cases)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record()
+        bc.run()
+        c1.record()
+        torch.cuda.synchronize()
+        cms = c0.elapsed_time(c1)
+        conv = {"all_converged": bool(bc.converged), "iterations": bc.iteration, "seconds": cms / 1e3,
+                "case_iterations": {"min": int(bc.case_converged_at.min()), "median": float(np.median(bc.case_converged_at)),
+                                    "max": int(bc.case_converged_at.max())},
+                "useful_cell_iters_per_s": float(np.dot(bs.case_cells, np.maximum(bc.case_converged_at, 0)) / (cms / 1e3)),
+                "value": ncell * bc.iteration / (cms / 1e3)}
+    return {"value": value, "ms": ms_max, "ncell": ncell, "ncase": len(meshes), "setup_s": setup_s,
+            "launches": launches, "times": times, "infos": infos, "one_at_a_time": one, "seq_ms": seq_ms,
+            "sample": samp, "solver": bs, "converge": conv,
+            "kinds": {"cavity": kinds.count("cavity"), "channel": kinds.count("channel")}}
+
+
+def batch_cpu_reference(args):
+    """The reference's CPU path on the batched sweep: the cases run one after another (as the
+    reference's batch runner does), timed on a stratified sample of 8 cases for a bounded time
+    each and extrapolated over the cell count of all cases."""
+    import numpy as np
+
+    meshes, cases, kinds = make_batch_workload(args.batch_cases)
+    idx = np.argsort([m.n_cells for m in meshes], kind="stable")
+    sample = sorted(set(int(idx[int(j)]) for j in np.linspace(0, len(idx) - 1, 8).round()))
+    pts, cores, kind = [], 1, "port"
+    for i in sample:
+        r = cpu_reference(meshes[i], __import__("copy").deepcopy(cases[i]), None, steps=1000, warmup=1, budget_s=3.0)
+        pts.append((meshes[i].n_cells, 1e3 * r["seconds"] / r["iterations"]))
+        cores, kind = r["cores"], r["kind"]
+    xs, ys = np.log([a for a, _ in pts]), np.array([b for _, b in pts])
+    ncell = sum(m.n_cells for m in meshes)
+    seq_ms = float(sum(np.interp(np.log(m.n_cells), xs, ys) for m in meshes))
+    value = ncell / (seq_ms / 1e3)
+    ref = {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "iterations": 1, "seconds": seq_ms / 1e3,
+           "sample": f"{len(sample)} of {len(meshes)} cases, one after another, >= 3 s each after 1 warm-up "
+                     "iteration; per-iteration time interpolated over the cell count of every case"}
+    desc = {"workload": f"batched sweep: {len(meshes)} 2-D cavity/channel cases, 1k-64k cells log-uniform, jitter "
+                        f"0.15h, Re 100-2000, seed 2 ({ncell:,} cells)", "cells": ncell}
+    return ref, desc
+
+
+def main_batch(args, rank, world, dev):
+    import torch
+
+    smi, smi_fh = (sample_clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
+                   if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else sample_clocks(f"/tmp/clocks_rank{rank}.csv"))
+    t_e2e = time.perf_counter()
+    r = run_batch(args, rank, world)
+    if smi is not None:
+        smi.terminate()
+        smi.wait()
+        smi_fh.close()
+    clocks = parse_clocks(smi_fh.name, dev) if smi is not None else None
+    bs, K = r["solver"], args.steps
+    torch.cuda.synchronize()
+    f = bs.fields()
+    e2e_s = time.perf_counter() - t_e2e
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    times = r["times"]
+    dom = max((k for k in ("momentum_assembly", "pressure_assembly") if k in times), key=lambda k: times[k])
+    byts = sum(stage_bytes(bs, dom, inf) for inf in r["infos"])
+    achieved = byts / (times[dom] / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        ref, _ = batch_cpu_reference(args)
+        cpu = {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    W = max(args.warmup, 3)
+    nall = r["ncell"] * world
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": r["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 systems, f64 residuals", "data": "synthetic",
+            "config": {"workload": f"batched sweep: {r['ncase']} 2-D cavity/channel cases, 1k-64k cells log-uniform, "
+                                   f"jitter 0.15h, Re 100-2000, seed 2 ({r['ncell']:,} cells on rank 0)",
+                       "cases": r["kinds"], "precision": "mixed", "l2": "flushed between timed steps (512 MiB write)",
+                       "parallelism": f"cases dealt to {world} ranks" if world > 1 else "single GPU"},
+            "one_at_a_time": {"value": r["one_at_a_time"], "unit": UNIT, "ratio": r["value"] / world / r["one_at_a_time"],
+                              "sample": f"{len(r['sample'])} cases timed alone with MixedSimpleSolver "
+                                        f"({K} steps each), per-step time interpolated over the cell count"},
+            "e2e": {"value": nall * (W + 2 * K) / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": sum(v.numel() * v.element_size() for v in bs.fv.t.values()) / (W + 2 * K),
+                    "d2h_bytes_per_step": (bs.report_g.numel() * (W + 2 * K) + sum(v.nbytes for v in f.values()))
+                    / (W + 2 * K),
+                    "includes": "host set-up of the batch (union mesh, device mesh, AMG), W+2K steps, fields()"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                         "traffic": None, "algorithmic_bytes_per_launch": byts / K,
+                         "stage_ms_per_step": {k: v / K for k, v in sorted(times.items(), key=lambda kv: -kv[1])}},
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": r["launches"], "setup_seconds": r["setup_s"],
+            "to_convergence": r["converge"]}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -217,6 +448,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--converge", action="store_true", help="also run to the 1e-6 residual and report it")
+    ap.add_argument("--batch-cases", type=int, default=256, help="c4: cases in the sweep")
+    ap.add_argument("--batch-sample", type=int, default=24, help="c4: cases timed one at a time")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -226,8 +459,11 @@ def main():
         if rank != 0:
             return
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-        mesh, case, desc, inlet, skw = make_workload(args.config)
-        ref = cpu_reference(mesh, case, inlet, args.steps, args.warmup, amg_theta=skw.get("amg_theta", 0.08))
+        if args.config == "c4":
+            ref, desc = batch_cpu_reference(args)
+        else:
+            mesh, case, desc, inlet, skw = make_workload(args.config)
+            ref = cpu_reference(mesh, case, inlet, args.steps, args.warmup, amg_theta=skw.get("amg_theta", 0.08))
         line = {"metric": METRIC, "value": ref["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": ref["iterations"],
                 "warmup": args.warmup, "ms_per_step": 1e3 * ref["seconds"] / ref["iterations"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -251,6 +487,8 @@ def main():
     from gputest_b200.unstructured.simple import SimpleSolver
 
     dev = torch.cuda.current_device()
+    if args.config == "c4":
+        return main_batch(args, rank, world, dev)
     mesh, case, desc, inlet, skw = make_workload(args.config)
     Solver = MixedSimpleSolver if args.precision == "mixed" else SimpleSolver
     mk = lambda c: Solver(mesh, c, **skw)  # noqa: E731

@@ -109,6 +109,16 @@ _SIGS = {
     "b2s_pcg_mixed_workspace_bytes": ([P], I64),
     "b2s_pcg_amg_mixed_d": ([P, P, P, P, P, I32, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, ctypes.c_int, F64, P,
                              I64, P, P], ctypes.c_int),
+    # batches
+    "b2s_mesh_part_blocks": ([P], ctypes.c_int),
+    "b2s_group_sums_d": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P], ctypes.c_int),
+    "b2s_remove_group_means_d": ([P, P, P, ctypes.c_int, ctypes.c_int, P, P, P, P, P], ctypes.c_int),
+    "b2s_bicgstab_groups_workspace_bytes": ([I32, ctypes.c_int, ctypes.c_int], I64),
+    "b2s_bicgstab_groups_f32_d": ([ctypes.c_int, P, P, I32, ctypes.c_int, P, P, P, P, P, P, F64, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, P, P, P, I64, P, P], ctypes.c_int),
+    "b2s_pcg_groups_workspace_bytes": ([P], I64),
+    "b2s_pcg_groups_mixed_d": ([P, P, P, P, P, P, P, I32, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, F64, P, I64,
+                                P, P], ctypes.c_int),
 }
 
 _lib: Optional[ctypes.CDLL] = None

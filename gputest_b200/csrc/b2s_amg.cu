@@ -217,31 +217,27 @@ __global__ void __launch_bounds__(kGalWarps * 32) acvals_k(b2s_amg_level L, cons
 constexpr int kGJThreads = 1024;
 constexpr int kSmemCoarse = 160;  // n <= 160: the matrix lives in shared memory (<= 200 KB)
 
-__global__ void __launch_bounds__(kGJThreads) coarse_inverse_k(int n, const int32_t* __restrict__ rowptr,
-                                                              const int32_t* __restrict__ col,
-                                                              const double* __restrict__ val, int singular,
-                                                              double* __restrict__ Mg, double* __restrict__ inv) {
-  extern __shared__ double smem[];
-  __shared__ double shift_s;
-  __shared__ double rowk[1024];
-  __shared__ double colk[1024];
-  const bool in_smem = n <= kSmemCoarse;
-  double* M = in_smem ? smem : Mg;
+// Dense inverse of the n x n matrix whose CSR rows are rows r0 .. r0+n-1 (columns r0 ..
+// r0+n-1) of (rowptr, col, val), by the calling block; M is the n x n work matrix.
+__device__ __forceinline__ void gj_inverse(int n, int r0, const int32_t* __restrict__ rowptr,
+                                           const int32_t* __restrict__ col, const double* __restrict__ val,
+                                           int singular, double* M, double* __restrict__ inv, double* rowk,
+                                           double* colk, double* shift_s) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int e = tid; e < n * n; e += nt) M[e] = 0.0;
   __syncthreads();
   for (int r = tid; r < n; r += nt)
-    for (int j = rowptr[r]; j < rowptr[r + 1]; ++j) M[(int64_t)r * n + col[j]] = val[j];
+    for (int j = rowptr[r0 + r]; j < rowptr[r0 + r + 1]; ++j) M[(int64_t)r * n + (col[j] - r0)] = val[j];
   __syncthreads();
   if (singular) {
     if (tid < 32) {
       double s = 0.0;
       for (int r = tid; r < n; r += 32) s += fabs(M[(int64_t)r * n + r]);
       s = warp_sum(s);
-      if (tid == 0) shift_s = 1e-10 * (s / (double)n);
+      if (tid == 0) *shift_s = 1e-10 * (s / (double)n);
     }
     __syncthreads();
-    for (int r = tid; r < n; r += nt) M[(int64_t)r * n + r] = M[(int64_t)r * n + r] + shift_s;
+    for (int r = tid; r < n; r += nt) M[(int64_t)r * n + r] = M[(int64_t)r * n + r] + *shift_s;
     __syncthreads();
   }
   // In-place Gauss-Jordan inversion. The coarse matrix is symmetric positive definite (a
@@ -269,6 +265,35 @@ __global__ void __launch_bounds__(kGJThreads) coarse_inverse_k(int n, const int3
     __syncthreads();
   }
   for (int e = tid; e < n * n; e += nt) inv[e] = M[e];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kGJThreads) coarse_inverse_k(int n, const int32_t* __restrict__ rowptr,
+                                                              const int32_t* __restrict__ col,
+                                                              const double* __restrict__ val, int singular,
+                                                              double* __restrict__ Mg, double* __restrict__ inv) {
+  extern __shared__ double smem[];
+  __shared__ double shift_s;
+  __shared__ double rowk[1024];
+  __shared__ double colk[1024];
+  double* M = n <= kSmemCoarse ? smem : Mg;
+  gj_inverse(n, 0, rowptr, col, val, singular, M, inv, rowk, colk, &shift_s);
+}
+
+// Batches: the dense inverse of every case's coarse block, one block per case (n_g <= kSmemCoarse).
+__global__ void __launch_bounds__(kGJThreads) coarse_inverse_groups_k(const int32_t* __restrict__ gptr,
+                                                                     const int64_t* __restrict__ off,
+                                                                     const int32_t* __restrict__ gsing,
+                                                                     const int32_t* __restrict__ rowptr,
+                                                                     const int32_t* __restrict__ col,
+                                                                     const double* __restrict__ val,
+                                                                     double* __restrict__ inv) {
+  extern __shared__ double smem[];
+  __shared__ double shift_s;
+  __shared__ double rowk[kSmemCoarse];
+  __shared__ double colk[kSmemCoarse];
+  const int g = blockIdx.x, r0 = gptr[g], n = gptr[g + 1] - r0;
+  gj_inverse(n, r0, rowptr, col, val, gsing[g], smem, inv + off[g], rowk, colk, &shift_s);
 }
 
 __global__ void strength_changes_k(b2s_amg_level L, double theta, int32_t* __restrict__ count) {
@@ -328,13 +353,14 @@ int64_t b2s_amg_workspace_bytes(const b2s_amg* h) {
   if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || h->coarse_n < 1) return -1;
   int64_t nmax = 0;
   for (int l = 0; l < h->nlevels; ++l) nmax = h->levels[l].n > nmax ? h->levels[l].n : nmax;
-  int64_t dense = h->coarse_n > kSmemCoarse ? (int64_t)h->coarse_n * h->coarse_n : 0;
+  int64_t dense = (h->ngroups == 0 && h->coarse_n > kSmemCoarse) ? (int64_t)h->coarse_n * h->coarse_n : 0;
   return (int64_t)sizeof(double) * (2 * nmax + 4 * (int64_t)kMaxCoopBlocks + dense);
 }
 
 int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s) {
-  if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || h->coarse_n < 1 || h->coarse_n > 1024 || !work ||
-      !h->coarse_inv || !h->coarse_rowptr || !h->coarse_col || !h->coarse_val)
+  if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || h->coarse_n < 1 ||
+      (h->ngroups == 0 && h->coarse_n > 1024) || !work || !h->coarse_inv || !h->coarse_rowptr || !h->coarse_col ||
+      !h->coarse_val || (h->ngroups > 0 && (!h->coarse_group_ptr || !h->coarse_inv_off || !h->group_singular)))
     return B2S_ERR_ARG;
   if (work_bytes < b2s_amg_workspace_bytes(h)) return B2S_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)s;
@@ -372,13 +398,23 @@ int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stre
     acvals_k<<<(unsigned)cdiv(L.nc, kGalWarps), kGalWarps * 32, 0, st>>>(L, crow, ccol, cval);
     B2S_LAUNCH_CHECK();
   }
-  const int n = h->coarse_n;
-  const size_t smem = n <= kSmemCoarse ? (size_t)n * n * sizeof(double) : 0;
-  if (smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(coarse_inverse_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+  if (h->ngroups > 0) {  // one dense block per case, each at most kSmemCoarse rows (checked at set-up)
+    const size_t gsm = (size_t)kSmemCoarse * kSmemCoarse * sizeof(double);
+    if (cudaFuncSetAttribute(coarse_inverse_groups_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm) !=
         cudaSuccess)
       return B2S_ERR_LAUNCH;
+    coarse_inverse_groups_k<<<(unsigned)h->ngroups, kGJThreads, gsm, st>>>(
+        h->coarse_group_ptr, h->coarse_inv_off, h->group_singular, h->coarse_rowptr, h->coarse_col, h->coarse_val,
+        h->coarse_inv);
+    B2S_LAUNCH_CHECK();
+    return B2S_OK;
   }
+  const int n = h->coarse_n;
+  const size_t smem = n <= kSmemCoarse ? (size_t)n * n * sizeof(double) : 0;
+  // the dynamic share above 48 KB minus the kernel's static 16 KB needs the opt-in
+  if (smem > 0 && cudaFuncSetAttribute(coarse_inverse_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                      cudaSuccess)
+    return B2S_ERR_LAUNCH;
   coarse_inverse_k<<<1, kGJThreads, smem, st>>>(n, h->coarse_rowptr, h->coarse_col, h->coarse_val, h->singular,
                                                 dense, h->coarse_inv);
   B2S_LAUNCH_CHECK();

@@ -43,6 +43,16 @@ __device__ __forceinline__ void for_cdiff(const b2s_mesh& m, int c, Fn fn) {
   }
 }
 
+// Cells of this block in a stage that writes one partial sum per block: a grid-stride range
+// of cells, or, on a tiled mesh (block-diagonal batches), exactly the cells of tile blockIdx.x.
+struct CellRange {
+  int c, end, step;
+};
+__device__ __forceinline__ CellRange cell_range(const b2s_mesh& m) {
+  if (m.tiles) return {m.tiles[blockIdx.x] + (int)threadIdx.x, m.tiles[blockIdx.x + 1], (int)blockDim.x};
+  return {(int)(blockIdx.x * blockDim.x + threadIdx.x), m.nc, (int)(gridDim.x * blockDim.x)};
+}
+
 // ------------------------------------------------------------------------------ face interp
 __global__ void face_interp_k(b2s_mesh m, int k, const double* __restrict__ phi, double* __restrict__ out) {
   const int64_t nf = m.nf, nc = m.nc;
@@ -350,7 +360,8 @@ __global__ void momentum_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, 
 #pragma unroll
   for (int q = 0; q < 2 * DIM; ++q) acc[q] = 0.0;
   const bool drive = prm.body[0] != 0.0 || prm.body[1] != 0.0 || (DIM == 3 && prm.body[2] != 0.0);
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+  for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
+    const int c = r_.c;
     RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
                                                  (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
     double diag = o.diag;
@@ -439,9 +450,9 @@ __global__ void pressure_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, 
                                     double* __restrict__ cb_out, VT* __restrict__ val, double* __restrict__ rhs,
                                     double* __restrict__ part) {
   __shared__ double red[(kThreads / 32 + 1) * 1];
-  const int nc = m.nc;
   double acc[1] = {0.0};
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+  for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
+    const int c = r_.c;
     double d_own = 0.0, d_nei = 0.0, d_b = 0.0, m_int = 0.0, m_b = 0.0;
     for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
       double Fst, cf;
@@ -489,7 +500,8 @@ __global__ void correct_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const doub
   __shared__ double red[(kThreads / 32 + 1) * 3];
   const int nc = m.nc, nf = m.nf, nb = m.nb;
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+  for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
+    const int c = r_.c;
     double ro[DIM], rn[DIM], rb[DIM];
 #pragma unroll
     for (int a = 0; a < DIM; ++a) ro[a] = rn[a] = rb[a] = 0.0;
@@ -587,7 +599,8 @@ __global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, double gamma, double cp
   __shared__ double red[(kThreads / 32 + 1) * 2];
   const int nc = m.nc, nb = m.nb;
   double acc[2] = {0.0, 0.0};
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+  for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
+    const int c = r_.c;
     RowOut<DIM, 1> o = transport_row<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
                                              second != 0, val, true);
     // q_in = Cb(flux tval |Sb| / cp) (+ source)
@@ -653,7 +666,8 @@ __global__ void momentum_assemble_mixed_k(b2s_mesh m, b2s_bc bc, b2s_flow_params
 #pragma unroll
   for (int q = 0; q < 2 * DIM; ++q) acc[q] = 0.0;
   const bool drive = prm.body[0] != 0.0 || prm.body[1] != 0.0 || (DIM == 3 && prm.body[2] != 0.0);
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+  for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
+    const int c = r_.c;
     RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
                                                  (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
     double diag = o.diag;
@@ -696,7 +710,8 @@ __global__ void energy_assemble_mixed_k(b2s_mesh m, b2s_bc bc, double gamma, dou
   __shared__ double red[(kThreads / 32 + 1) * 2];
   const int nc = m.nc, nb = m.nb;
   double acc[2] = {0.0, 0.0};
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+  for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
+    const int c = r_.c;
     RowOut<DIM, 1> o = transport_row<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
                                              second != 0, val, true);
     double q = 0.0;
@@ -762,6 +777,8 @@ __global__ void flux_balance_k(b2s_mesh m, const double* __restrict__ F, const d
 
 using namespace b2s;
 
+static unsigned part_grid(int64_t n);
+static unsigned part_grid_m(const b2s_mesh& m) { return m.tiles ? (unsigned)m.ntiles : part_grid(m.nc); }
 static unsigned part_grid(int64_t n) {
   int64_t g = cdiv(n > 0 ? n : 1, kThreads);
   return (unsigned)(g < kMaxCoopBlocks ? g : kMaxCoopBlocks);
@@ -851,7 +868,7 @@ int b2s_momentum_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_
   if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !diag || !inv || !dP || !b ||
       !br || !part || !(prm->relax_u > 0.0))
     return B2S_ERR_ARG;
-  unsigned g = part_grid(m->nc);
+  unsigned g = part_grid_m(*m);
   if (m->dim == 2)
     momentum_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb, porosity,
                                                                  msrc, val, diag, inv, dP, b, br, part);
@@ -868,7 +885,7 @@ int b2s_pressure_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_
   if (!mesh_ok(m) || !bc || !prm || !Ustar || !p || !gp || !dP || !Fst || !cf || !Fbst || !cb || !val || !rhs ||
       !part)
     return B2S_ERR_ARG;
-  unsigned g = part_grid(m->nc);
+  unsigned g = part_grid_m(*m);
   if (m->dim == 2)
     pressure_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Ustar, p, gp, dP, Fst, cf, Fbst, cb,
                                                                  val, rhs, part);
@@ -886,7 +903,7 @@ int b2s_correct_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* pr
   if (!mesh_ok(m) || !bc || !prm || !Fst || !cf || !Fbst || !cb || !pp || !p || !Ustar || !dP || !F || !Fb ||
       !Up_new || !part)
     return B2S_ERR_ARG;
-  unsigned g = part_grid(m->nc);
+  unsigned g = part_grid_m(*m);
   if (m->dim == 2)
     correct_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Fst, cf, Fbst, cb, pp, p, Ustar, dP, F, Fb,
                                                        Up_new, part);
@@ -930,7 +947,7 @@ int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, dou
   if (!mesh_ok(m) || !bc || !T || !gT || (!Tb && m->nb) || !F || !Fb || !val || !diag || !inv || !b || !br ||
       !part || !(relax_T > 0.0) || !(cp != 0.0))
     return B2S_ERR_ARG;
-  unsigned g = part_grid(m->nc);
+  unsigned g = part_grid_m(*m);
   if (m->dim == 2)
     energy_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT, Tb,
                                                                F, Fb, esrc, val, diag, inv, b, br, part);
@@ -948,7 +965,7 @@ int b2s_momentum_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s
   if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !inv || !dP || !r || !part ||
       !(prm->relax_u > 0.0))
     return B2S_ERR_ARG;
-  unsigned g = part_grid(m->nc);
+  unsigned g = part_grid_m(*m);
   if (m->dim == 2)
     momentum_assemble_mixed_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb,
                                                                        porosity, msrc, val, inv, dP, r, part);
@@ -966,7 +983,7 @@ int b2s_pressure_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s
   if (!mesh_ok(m) || !bc || !prm || !Ustar || !p || !gp || !dP || !Fst || !cf || !Fbst || !cb || !val || !rhs ||
       !part)
     return B2S_ERR_ARG;
-  unsigned g = part_grid(m->nc);
+  unsigned g = part_grid_m(*m);
   if (m->dim == 2)
     pressure_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Ustar, p, gp, dP, Fst, cf, Fbst, cb,
                                                                  val, rhs, part);
@@ -984,7 +1001,7 @@ int b2s_energy_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, double gamm
   if (!mesh_ok(m) || !bc || !T || !gT || (!Tb && m->nb) || !F || !Fb || !val || !inv || !r || !part ||
       !(relax_T > 0.0) || !(cp != 0.0))
     return B2S_ERR_ARG;
-  unsigned g = part_grid(m->nc);
+  unsigned g = part_grid_m(*m);
   if (m->dim == 2)
     energy_assemble_mixed_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T,
                                                                      gT, Tb, F, Fb, esrc, val, inv, r, part);

@@ -86,7 +86,12 @@ class AMGHierarchy:
     """
 
     def __init__(self, A_host, perm, rowptr, col, diag_slot, val, slot_ref, singular=False, theta=0.08,
-                 max_coarse=150, max_levels=20, sweeps=2, omega=0.8):
+                 max_coarse=150, max_levels=20, sweeps=2, omega=0.8, groups=None, group_singular=None):
+        """``groups`` (batches of independent cases, optional): the case of every row of A_host
+        (reference numbering; A_host block diagonal by case, each case's rows contiguous in the
+        device order). Aggregates are then numbered case by case, coarsening goes on until every
+        case has at most ``max_coarse`` rows, and the coarsest level keeps one dense inverse per
+        case (shifted where ``group_singular``)."""
         import torch
 
         dev = val.device
@@ -94,13 +99,32 @@ class AMGHierarchy:
         A = sp.csr_matrix(A_host, dtype=np.float64)
         perm = np.asarray(perm, dtype=np.int64)
         n0 = A.shape[0]
+        batched = groups is not None
+        if batched:
+            gl = np.asarray(groups, dtype=np.int64)
+            ngroups = int(gl.max()) + 1
+            level_groups = [gl]
+
+        def too_big(A):
+            if not batched:
+                return A.shape[0] > max_coarse
+            return np.bincount(level_groups[-1], minlength=ngroups).max() > max_coarse
+
         # ---- host set-up on the reference numbering (values drive the coarse strength graphs)
         aggs, counts, mats = [], [], []
-        while A.shape[0] > max_coarse and len(aggs) < max_levels - 1:
+        while too_big(A) and len(aggs) < max_levels - 1:
             S = strength(A, theta)
             agg, na = aggregate(S)
             if na >= A.shape[0] * 0.9:
                 break
+            if batched:  # number the aggregates case by case (aggregates never cross cases)
+                g_of = np.empty(na, dtype=np.int64)
+                g_of[agg] = level_groups[-1]
+                order = np.argsort(g_of, kind="stable")
+                new_id = np.empty(na, dtype=np.int64)
+                new_id[order] = np.arange(na)
+                agg = new_id[agg]
+                level_groups.append(g_of[order])
             T = sp.csr_matrix((np.ones(A.shape[0]), (np.arange(A.shape[0]), agg)), shape=(A.shape[0], na))
             cnt = np.asarray(T.sum(axis=0)).ravel()
             T = T @ sp.diags(1.0 / np.sqrt(cnt))
@@ -177,6 +201,9 @@ class AMGHierarchy:
                 "rho": torch.zeros(1, dtype=torch.float64, device=dev),
                 "strong": torch.as_tensor(np.ascontiguousarray(flags, dtype=np.uint8), device=dev),
             }
+            if batched:
+                bufs["group_ptr"] = i32(np.concatenate([[0], np.cumsum(np.bincount(level_groups[l],
+                                                                                    minlength=ngroups))]))
             for k, v in bufs.items():
                 setattr(L, k, v.data_ptr())
             self._keep.append(bufs)
@@ -195,7 +222,23 @@ class AMGHierarchy:
         self.coarse_n = nc
         self.sizes.append(nc)
         self.coarse_val = level_val
-        self.coarse_inv = torch.empty((nc, nc), dtype=torch.float64, device=dev)
+        if batched:
+            sizes_g = np.bincount(level_groups[-1], minlength=ngroups)
+            if sizes_g.max() > 160:
+                raise RuntimeError("a case's coarsest AMG level has more than 160 rows")
+            off = np.concatenate([[0], np.cumsum(sizes_g.astype(np.int64) ** 2)])
+            self.coarse_inv = torch.empty(int(off[-1]), dtype=torch.float64, device=dev)
+            gs = np.zeros(ngroups, dtype=np.int32) if group_singular is None else np.asarray(group_singular)
+            self._keep.append({"cgp": i32(np.concatenate([[0], np.cumsum(sizes_g)])),
+                               "off": torch.as_tensor(off[:-1].astype(np.int64), device=dev), "gs": i32(gs)})
+            h.ngroups = ngroups
+            h.coarse_group_ptr = self._keep[-1]["cgp"].data_ptr()
+            h.coarse_inv_off = self._keep[-1]["off"].data_ptr()
+            h.group_singular = self._keep[-1]["gs"].data_ptr()
+            self.ngroups = ngroups
+        else:
+            self.coarse_inv = torch.empty((nc, nc), dtype=torch.float64, device=dev)
+            self.ngroups = 0
         h.coarse_n = nc
         h.coarse_rowptr, h.coarse_col = level_rowptr.data_ptr(), level_col.data_ptr()
         h.coarse_val, h.coarse_inv = level_val.data_ptr(), self.coarse_inv.data_ptr()
@@ -258,7 +301,8 @@ class AMGHierarchy:
                 getattr(h32, k)[l] = v.data_ptr()
             self._keep32.append(bufs)
         self.c32ref = ctypes.byref(h32)
-        mb = _lib.lib().b2s_pcg_mixed_workspace_bytes(self.cref)
+        mb = (_lib.lib().b2s_pcg_groups_workspace_bytes(self.cref) if self.ngroups
+              else _lib.lib().b2s_pcg_mixed_workspace_bytes(self.cref))
         if mb < 0:
             raise RuntimeError("invalid AMG hierarchy")
         self.work_mixed = torch.empty(mb // 8 + 1, dtype=torch.float64, device=dev)
@@ -290,3 +334,15 @@ class AMGHierarchy:
                                             self.src_val.data_ptr(), b.data_ptr(), x.data_ptr(), float(tol), int(maxiter),
                                             int(bool(project)), self.work_pcg.data_ptr(), self.work_pcg.numel() * 8,
                                             info, _lib.stream_ptr(stream)), "b2s_pcg_amg_d")
+
+    def pcg_groups_mixed(self, mesh_ref, order, project, cf, cb, b, x, tol, maxiter, info, maxpass=8,
+                         min_inner_tol=1e-5, stream=None):
+        """Per-case refined solves of a batch hierarchy (``b2s_pcg_groups_mixed_d``): order and
+        project are device int32 tensors [ngroups]; info the device address of ngroups records."""
+        _lib.check(_lib.lib().b2s_pcg_groups_mixed_d(self.cref, self.c32ref, order.data_ptr(), project.data_ptr(),
+                                                     mesh_ref, cf.data_ptr(), cb.data_ptr(), self.n0,
+                                                     self.rowptr0.data_ptr(), self.col0.data_ptr(),
+                                                     self.src_val32.data_ptr(), b.data_ptr(), x.data_ptr(), float(tol),
+                                                     int(maxiter), int(maxpass), float(min_inner_tol),
+                                                     self.work_mixed.data_ptr(), self.work_mixed.numel() * 8, info,
+                                                     _lib.stream_ptr(stream)), "b2s_pcg_groups_mixed_d")

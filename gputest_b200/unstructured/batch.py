@@ -1,0 +1,314 @@
+"""Batches of independent SIMPLEC cases on one device: ``BatchSimpleSolver``.
+
+The reference runs a sweep of cases one after another, each through its own solver
+(``flowtrace/runtime/batch.py:142-222`` calling ``SimpleSolver.step``). Here the cases of a batch
+are one block-diagonal problem: their meshes are joined into a disjoint union
+(``union_mesh``, each case's cells contiguous on the device), every finite-volume stage is one
+launch for all of them, and the linear solves are per case inside persistent launches that
+deal whole cases to blocks (``b2s_bicgstab_groups_f32_d``, ``b2s_pcg_groups_mixed_d``). Every
+case keeps its own Krylov scalars and stopping tests, its own residual normalisation and
+convergence test (``simple.py:675-703``), its own pressure level when it is closed, and its own
+viscosity (the diffusion coefficients of the momentum assembly are scaled per face). The
+arithmetic is the mixed-precision iteration of ``MixedSimpleSolver``; with no AMG rebuild due,
+a whole outer iteration of all cases is one CUDA graph replay.
+
+Differences from running the cases one by one: the AMG hierarchy is set up for the union
+(aggregates never cross cases; coarsening stops when every case has at most ``max_coarse``
+rows, and each case's coarsest block gets its own dense inverse), and the spectral-radius
+estimate of each level's prolongation smoother is taken over all cases of the level. These
+change the preconditioner, not the converged fields. The stability guard of the single-case
+solver is off. Cases keep iterating until every case has converged (a converged case's
+residuals keep falling), and ``case_converged_at`` records when each one first passed.
+"""
+
+from __future__ import annotations
+
+import copy
+import ctypes
+from typing import List, Sequence
+
+import numpy as np
+
+from .. import _lib
+from ..linalg.amg import AMGHierarchy
+from ..linalg.krylov import INFO_DTYPE, read_info
+from ..mesh.unstructured import UnstructuredMesh, union_groups, union_mesh
+from .case import UnstructuredCase
+from .mixed import MixedSimpleSolver
+from .simple import COMPONENTS
+
+_SHARED = ("density", "scheme", "relax_u", "relax_p", "pressure_tol", "algorithm", "pressure_gradient",
+           "init_velocity", "body_force", "tol", "max_iter")
+
+
+def _union_case(cases: Sequence[UnstructuredCase], meshes: Sequence[UnstructuredMesh]) -> UnstructuredCase:
+    base = cases[0]
+    for c in cases[1:]:
+        for k in _SHARED:
+            if getattr(c, k) != getattr(base, k):
+                raise ValueError(f"cases of a batch must share {k!r}")
+    if any(c.energy for c in cases):
+        raise NotImplementedError("batches without the energy equation only")
+    u = copy.deepcopy(base)
+    u.boundaries = {}
+    for i, (c, m) in enumerate(zip(cases, meshes)):
+        for z in m.boundary_zones():
+            if z.name in c.boundaries:
+                u.boundaries[f"c{i}/{z.name}"] = copy.deepcopy(c.boundaries[z.name])
+    u.viscosity = 1.0  # the per-case viscosity scales the momentum diffusion coefficients
+    return u
+
+
+class BatchSimpleSolver(MixedSimpleSolver):
+    """Many independent cases (list of meshes and cases of one dimension) solved together."""
+
+    def __init__(self, meshes: List[UnstructuredMesh], cases: List[UnstructuredCase], max_coarse: int = 150,
+                 amg_theta: float = 0.08):
+        if len(meshes) != len(cases) or not meshes:
+            raise ValueError("one case per mesh")
+        self.meshes, self.cases = list(meshes), list(cases)
+        self.ncase = len(meshes)
+        self.case_cells = np.array([m.n_cells for m in meshes], dtype=np.int64)
+        self.case_offsets = np.concatenate([[0], np.cumsum(self.case_cells)])
+        self._cell_groups = union_groups(meshes)  # reference (union) numbering
+        self.mu_case = np.array([float(c.viscosity) for c in cases])
+        super().__init__(union_mesh(self.meshes), _union_case(cases, meshes), max_coarse=max_coarse,
+                         amg_theta=amg_theta)
+        self.guard_enabled = False
+        self.case_iteration = 0
+        self.case_converged_at = np.full(self.ncase, -1, dtype=np.int64)
+        self._res_max5_case = np.zeros(self.ncase)
+
+    # ------------------------------------------------------------------ set-up
+    def _prepare_mesh(self):
+        import torch
+
+        fv = self.fv
+        dev = self.torch_device
+        g_dev = self._cell_groups[fv.perm]  # case of every device cell
+        if np.any(np.diff(g_dev) < 0):
+            raise RuntimeError("cases are not contiguous on the device")
+        cells = np.concatenate([[0], np.cumsum(np.bincount(g_dev, minlength=self.ncase))])
+        # tiles of at most 256 cells inside each case
+        tiles, tile_group = [0], []
+        for g in range(self.ncase):
+            a, b = int(cells[g]), int(cells[g + 1])
+            cuts = list(range(a + 256, b, 256)) + [b]
+            tiles += cuts
+            tile_group += [g] * len(cuts)
+        fv.set_tiling(np.array(tiles))
+        group_tiles = np.concatenate([[0], np.cumsum(np.bincount(tile_group, minlength=self.ncase))])
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
+        self.g_cells, self.g_tiles, self.g_tile_group = i32(cells), i32(group_tiles), i32(tile_group)
+        self.g_cells_h = cells
+        self.g_order = i32(np.argsort(-np.diff(cells), kind="stable"))  # largest case first
+        # momentum diffusion scaled by each case's viscosity (owner's case for faces)
+        t = fv.t
+        mu_f = self.mu_case[g_dev[t["fP"].cpu().numpy()]] if fv.n_if else np.zeros(0)
+        mu_b = self.mu_case[g_dev[t["bP"].cpu().numpy()]] if fv.n_bf else np.zeros(0)
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
+        self._mom_t = {
+            "alpha": f64(mu_f * t["alpha"].cpu().numpy()) if fv.n_if else t["alpha"],
+            "alpha_b": f64(mu_b * t["alpha_b"].cpu().numpy()) if fv.n_bf else t["alpha_b"],
+            "Tv": f64(mu_f[None, :] * t["Tv"].cpu().numpy().reshape(fv.dim, -1)) if fv.n_if else t["Tv"],
+        }
+        mm = _lib.Mesh()
+        ctypes.memmove(ctypes.byref(mm), ctypes.byref(fv.cmesh), ctypes.sizeof(mm))
+        mm.alpha, mm.alpha_b, mm.Tv = (self._mom_t[k].data_ptr() for k in ("alpha", "alpha_b", "Tv"))
+        self._mesh_mom = mm
+        self._m_mom = ctypes.byref(mm)
+
+    def _build_boundaries(self):
+        import torch
+
+        super()._build_boundaries()
+        fv = self.fv
+        g_dev = self._cell_groups[fv.perm]
+        bP = fv.t["bP"].cpu().numpy() if fv.n_bf else np.zeros(0, dtype=np.int64)
+        m_pres_dev = self._bc_t["m_pres"].cpu().numpy()[: fv.n_bf]  # device boundary-face order
+        open_ = np.zeros(self.ncase, dtype=bool)
+        if fv.n_bf:
+            np.logical_or.at(open_, g_dev[bP], m_pres_dev > 0)
+        self.case_singular = ~open_
+        self.g_singular = torch.as_tensor(self.case_singular.astype(np.int32), device=self.torch_device)
+
+    def _allocate(self):
+        import torch
+
+        super()._allocate()
+        dev, nc, dim, ng = self.torch_device, self.nc, self.dim, self.ncase
+        L = _lib.lib()
+        wb = L.b2s_bicgstab_groups_workspace_bytes(nc, dim, 1)
+        self.work_bicg_g = torch.empty(wb // 8 + 1, dtype=torch.float64, device=dev)
+        nrec = ng * (dim + 1)
+        self.report_g = torch.zeros(ng * self.NQ * 8 + nrec * INFO_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        self.report_g_host = torch.zeros_like(self.report_g, device="cpu").pin_memory()
+        self.gscal = self.report_g[: ng * self.NQ * 8].view(torch.float64)
+        base = self.report_g.data_ptr() + ng * self.NQ * 8
+        self.info_mom_g = base
+        self.info_p_g = base + ng * dim * INFO_DTYPE.itemsize
+
+    def _setup_amg(self):
+        import torch
+
+        torch.cuda.current_stream().synchronize()
+        self.val_P.copy_(self.val_P32)
+        A_host = self.fv.matrix_to_host(self.val_P)
+        self._amg = AMGHierarchy(A_host, self.fv.perm, self.fv.rowptr, self.fv.col, self.fv.t["slot_diag"],
+                                 self.val_P, self.fv.slot_ref, singular=False, max_coarse=self.max_coarse,
+                                 theta=self.amg_theta, groups=self._cell_groups,
+                                 group_singular=self.case_singular.astype(np.int32))
+        self.amg_setups += 1
+        self._amg.enable_mixed(self.val_P32)
+
+    # ------------------------------------------------------------------ iteration
+    def _launch(self, amg_ready=False):
+        L, fv = _lib.lib(), self.fv
+        self._mark("start")
+        s = _lib.stream_ptr()
+        m, bc = fv.cmesh_ref, ctypes.byref(self.cbc)
+        prm = self._params()
+        pr = ctypes.byref(prm)
+        dim, nc, ng = self.dim, self.nc, self.ncase
+        old = self._cur
+        new = next(i for i in range(3) if i != old)
+        Up, F, Fb = self._Up[old], self._F[old], self._Fb[old]
+        lag = self._lag
+        gg = self.case.pressure_gradient == "green-gauss"
+        gp_force_prev = self.gpf if gg else self.gUp[0]
+        _lib.check(L.b2s_flow_bvals_d(m, bc, Up.data_ptr(), self.gUp.data_ptr() if lag else None,
+                                      gp_force_prev.data_ptr() if lag else None, self.bUp.data_ptr(), s),
+                   "b2s_flow_bvals_d")
+        _lib.check(L.b2s_ls_gradient_d(m, 1 + dim, Up.data_ptr(), self.bUp.data_ptr(), self.gUp.data_ptr(), s),
+                   "b2s_ls_gradient_d")
+        if gg:
+            _lib.check(L.b2s_gg_gradient_d(m, Up.data_ptr(), self.bUp.data_ptr(), self.gUp.data_ptr(),
+                                           self.gpf.data_ptr(), s), "b2s_gg_gradient_d")
+            gp = self.gpf
+        else:
+            gp = self.gUp[0]
+        self._lag = True
+        self.kernel_launches += 3 if gg else 2
+        self._mark("gradients")
+        part = self.part
+        pt = lambda q: part.data_ptr() + 8 * q * self.nblk  # noqa: E731
+        _lib.check(L.b2s_momentum_assemble_mixed_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(),
+                                                   gp.data_ptr(), self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
+                                                   None, None, self.val_A32.data_ptr(), self.inv32.data_ptr(),
+                                                   self.dP.data_ptr(), self.r32.data_ptr(), pt(self.Q_MOM), s),
+                   "b2s_momentum_assemble_mixed_d")
+        self._mark("momentum_assembly")
+        _lib.check(L.b2s_bicgstab_groups_f32_d(ng, self.g_cells.data_ptr(), self.g_order.data_ptr(), nc, dim,
+                                               fv.rowptr.data_ptr(), fv.col.data_ptr(), self.val_A32.data_ptr(),
+                                               self.r32.data_ptr(), self.inv32.data_ptr(), self.dU32.data_ptr(), 0.1,
+                                               30, 1, 1, self.Ustar.data_ptr(), Up[1:].data_ptr(),
+                                               self.work_bicg_g.data_ptr(), self.work_bicg_g.numel() * 8,
+                                               self.info_mom_g, s), "b2s_bicgstab_groups_f32_d")
+        self._mark("momentum_solve")
+        _lib.check(L.b2s_pressure_assemble_mixed_d(m, bc, pr, self.Ustar.data_ptr(), Up.data_ptr(), gp.data_ptr(),
+                                                   self.dP.data_ptr(), self.Fst.data_ptr(), self.cf.data_ptr(),
+                                                   self.Fbst.data_ptr(), self.cb.data_ptr(), self.val_P32.data_ptr(),
+                                                   self.rhs_p.data_ptr(), pt(self.Q_CONT), s),
+                   "b2s_pressure_assemble_mixed_d")
+        self.kernel_launches += 3
+        self._mark("pressure_assembly")
+        if not amg_ready:
+            self._ensure_amg(s)
+        self._mark("amg_rebuild")
+        self._amg.pcg_groups_mixed(m, self.g_order, self.g_singular, self.cf, self.cb, self.rhs_p, self.pp,
+                                   self.case.pressure_tol, 200, self.info_p_g, maxpass=self.REFINE_PASSES,
+                                   min_inner_tol=self.INNER_TOL_FLOOR)
+        self.kernel_launches += 1
+        self._mark("pressure_solve")
+        Upn, Fn, Fbn = self._Up[new], self._F[new], self._Fb[new]
+        _lib.check(L.b2s_correct_d(m, bc, pr, self.Fst.data_ptr(), self.cf.data_ptr(), self.Fbst.data_ptr(),
+                                   self.cb.data_ptr(), self.pp.data_ptr(), Up.data_ptr(), self.Ustar.data_ptr(),
+                                   self.dP.data_ptr(), Fn.data_ptr(), Fbn.data_ptr(), Upn.data_ptr(),
+                                   pt(self.Q_SUMP), s), "b2s_correct_d")
+        self.kernel_launches += 1
+        if self.case_singular.any():
+            _lib.check(L.b2s_remove_group_means_d(m, Upn.data_ptr(), part.data_ptr(), self.nblk, self.Q_SUMP,
+                                                  self.g_tiles.data_ptr(), self.g_tile_group.data_ptr(),
+                                                  self.g_cells.data_ptr(), self.g_singular.data_ptr(), s),
+                       "b2s_remove_group_means_d")
+            self.kernel_launches += 1
+        self._mark("corrections")
+        _lib.check(L.b2s_group_sums_d(part.data_ptr(), self.nblk, self.NQ, ng, self.g_tiles.data_ptr(),
+                                      self.gscal.data_ptr(), s), "b2s_group_sums_d")
+        self.kernel_launches += 1
+        self._mark("residuals")
+        return old, new
+
+    def _read_report(self):
+        import torch
+
+        self.report_g_host.copy_(self.report_g, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        if self._events:
+            self._resolve_stage_events()
+        raw = self.report_g_host.numpy()
+        ng = self.ncase
+        scal = raw[: ng * self.NQ * 8].view(np.float64).reshape(ng, self.NQ).copy()
+        infos = read_info(raw[ng * self.NQ * 8:])
+        return scal, infos
+
+    def step(self) -> float:
+        """One outer iteration of every case (``simple.py:500-703`` per case)."""
+        if self.finished:
+            return 0.0
+        self._capture = None
+        c, dim, ng = self.case, self.dim, self.ncase
+        rebuild_due = self._amg is None or self._amg_age >= self.amg_rebuild
+        if self.use_graphs and not rebuild_due and self._lag and not self.profile_stages:
+            try:
+                old, new = self._launch_graph()
+            except RuntimeError:
+                self.use_graphs = False
+                self._graphs.clear()
+                old, new = self._launch()
+        else:
+            old, new = self._launch()
+        scal, infos = self._read_report()
+        self._cur = new
+        self.iteration += 1
+        self.step_count = self.iteration
+        num = scal[:, self.Q_MOM:self.Q_MOM + dim]
+        den = scal[:, self.Q_MOM + dim:self.Q_MOM + 2 * dim]
+        floor = 1e-3 * np.maximum(den.max(axis=1), 1e-300)
+        res = {name: num[:, k] / np.maximum(den[:, k], floor) for k, name in enumerate(COMPONENTS[:dim])}
+        cont = scal[:, self.Q_CONT].copy()
+        if self.iteration <= 5:
+            self._res_max5_case = np.maximum(self._res_max5_case, np.maximum(cont, 1e-300))
+        flux = scal[:, self.Q_SUMF] + scal[:, self.Q_SUMFB]
+        res["continuity"] = cont / np.maximum(self._res_max5_case, 1e-3 * flux)
+        self._case_res = res
+        mom = infos[: ng * dim]
+        self.last_linear = {"momentum_iters": np.array([i.iterations for i in mom]).reshape(ng, dim),
+                            "pressure_iters": np.array([i.iterations for i in infos[ng * dim: ng * (dim + 1)]]),
+                            "pressure_residual": np.array([i.residual for i in infos[ng * dim: ng * (dim + 1)]])}
+        worst = np.max(np.stack(list(res.values())), axis=0)
+        done = (worst < c.tol) & (self.iteration > 5)
+        newly = done & (self.case_converged_at < 0)
+        self.case_converged_at[newly] = self.iteration
+        self.converged = bool(np.all(self.case_converged_at >= 0))
+        return 1.0
+
+    @property
+    def finished(self) -> bool:
+        return self.converged or self.iteration >= self.case.max_iter
+
+    def case_residuals(self, i: int) -> dict:
+        """Scaled residuals of case i after the last iteration (``simple.py:675-703``)."""
+        return {k: float(v[i]) for k, v in self._case_res.items()}
+
+    def case_fields(self, i: int) -> dict:
+        """``fields()`` of case i (host arrays in its own cell numbering)."""
+        f = self.fields()
+        a, b = int(self.case_offsets[i]), int(self.case_offsets[i + 1])
+        return {k: v[a:b] for k, v in f.items()}
+
+    def residuals(self) -> dict:
+        return {"scaled": {k: float(np.max(v)) for k, v in self._case_res.items()}}
+
+    def diagnostics(self) -> dict:
+        raise NotImplementedError("diagnostics() is per case: solve the case with SimpleSolver")

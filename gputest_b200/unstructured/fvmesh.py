@@ -215,6 +215,19 @@ class FVMesh:
         a = np.asarray(a, dtype=np.float64)[self.perm]
         return torch.as_tensor(np.ascontiguousarray(a.T if a.ndim > 1 else a), device=self.device)
 
+    def set_tiling(self, tiles) -> None:
+        """Tile the cells (``b2s_mesh.tiles``): tiles[t] .. tiles[t+1]-1 are the cells of tile t,
+        at most 256 each, in device numbering; the partial-sum stages then give one partial per
+        tile."""
+        import torch
+
+        tiles = np.asarray(tiles, dtype=np.int64)
+        if tiles[0] != 0 or tiles[-1] != self.nc or np.any(np.diff(tiles) <= 0) or np.any(np.diff(tiles) > 256):
+            raise ValueError("invalid tiling")
+        self.t["tiles"] = torch.as_tensor(tiles.astype(np.int32), device=self.device)
+        self.cmesh.tiles = self.t["tiles"].data_ptr()
+        self.cmesh.ntiles = int(tiles.size - 1)
+
     def cells_to_host(self, t):
         """Device SoA tensor [...][nc] -> (nc, ...) host array in reference order."""
         a = t.detach().double().cpu().numpy()

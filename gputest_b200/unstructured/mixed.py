@@ -91,8 +91,8 @@ class MixedSimpleSolver(SimpleSolver):
         self._mark("gradients")
         part = self.part
         pt = lambda q: part.data_ptr() + 8 * q * self.nblk  # noqa: E731
-        _lib.check(L.b2s_momentum_assemble_mixed_d(m, bc, pr, Up.data_ptr(), self.gUp.data_ptr(), gp.data_ptr(),
-                                                   self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
+        _lib.check(L.b2s_momentum_assemble_mixed_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(),
+                                                   gp.data_ptr(), self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
                                                    None if self.porosity is None else self.porosity.data_ptr(),
                                                    None if self.mom_source is None else self.mom_source.data_ptr(),
                                                    self.val_A32.data_ptr(), self.inv32.data_ptr(), self.dP.data_ptr(),

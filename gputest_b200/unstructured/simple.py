@@ -135,7 +135,8 @@ class SimpleSolver:
         self.be = DeviceBackend(self.torch_device)
         self.dtype = np.dtype(np.float64)
         t0 = time.perf_counter()
-        self.fv = fv = FVMesh(mesh, self.torch_device)
+        self.fv = fv = FVMesh(mesh, self.torch_device, groups=getattr(self, "_cell_groups", None))
+        self._prepare_mesh()
         self.dim = dim = mesh.dim
         self.nc = nc = mesh.n_cells
         self.energy = bool(case.energy)
@@ -183,6 +184,9 @@ class SimpleSolver:
         self.setup_seconds = time.perf_counter() - t0
 
     # ------------------------------------------------------------------ set-up
+    def _prepare_mesh(self):
+        """Hook run right after the device mesh is built (batches tile it here)."""
+        self._m_mom = self.fv.cmesh_ref  # mesh of the momentum assembly (batches scale its diffusion)
     def _build_boundaries(self):
         """Boundary kinds, fixed values and masks (``flowtrace/unstructured/simple.py:185-240``)."""
         fv, case, dim = self.fv, self.case, self.dim
@@ -269,7 +273,7 @@ class SimpleSolver:
             self.Tb, self.gT = z(nb), z(dim, nc)
             self.val_T, self.diagT, self.invT, self.bT, self.brT = z(nnz), z(nc), z(nc), z(nc), z(nc)
         L = _lib.lib()
-        self.nblk = L.b2s_part_blocks(nc)
+        self.nblk = L.b2s_mesh_part_blocks(fv.cmesh_ref)
         self.Q_MOM, self.Q_CONT, self.Q_SUMP = 0, 2 * dim, 2 * dim + 1
         self.Q_SUMF, self.Q_SUMFB, self.Q_ENUM, self.Q_EDEN = 2 * dim + 2, 2 * dim + 3, 2 * dim + 4, 2 * dim + 5
         self.NQ = 2 * dim + 6
@@ -482,7 +486,7 @@ class SimpleSolver:
         self._mark("gradients")
         part = self.part
         pt = lambda q: part.data_ptr() + 8 * q * self.nblk  # noqa: E731
-        _lib.check(L.b2s_momentum_assemble_d(m, bc, pr, Up.data_ptr(), self.gUp.data_ptr(), gp.data_ptr(),
+        _lib.check(L.b2s_momentum_assemble_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(), gp.data_ptr(),
                                              self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
                                              None if self.porosity is None else self.porosity.data_ptr(),
                                              None if self.mom_source is None else self.mom_source.data_ptr(),

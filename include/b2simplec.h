@@ -387,6 +387,45 @@ B2S_API int b2s_pcg_amg_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const 
                                 int maxpass, double min_inner_tol, void* work, int64_t work_bytes,
                                 b2s_solve_info* info, b2s_stream_t s);
 
+/* ----------------------------------------------------------------------------------------- */
+/* Batches of independent cases. No counterpart in the reference, which runs the cases of a     */
+/* sweep one after another (flowtrace/runtime/batch.py:142-222): here they share one device      */
+/* mesh, the disjoint union of their meshes with each case's cells contiguous, every stage runs */
+/* once for all of them, and each Krylov solve keeps per-case scalars and stopping tests.        */
+
+/* Partial-sum blocks of the stages of a mesh: its tile count when tiled, else b2s_part_blocks. */
+B2S_API int b2s_mesh_part_blocks(const b2s_mesh* m);
+
+/* out[g][q] = sum of part[q][t] over the tiles t = group_tiles[g] .. group_tiles[g+1]-1. */
+B2S_API int b2s_group_sums_d(const double* part, int nblk, int nq, int ngroups, const int32_t* group_tiles,
+                             double* out, b2s_stream_t s);
+
+/* x -= the mean of x over every case g with singular[g] != 0, the sums taken from part[q][tiles
+ * of the case] (as written by b2s_correct_d on the tiled mesh m); group_cells [ngroups+1]. */
+B2S_API int b2s_remove_group_means_d(const b2s_mesh* m, double* x, const double* part, int nblk, int q,
+                                     const int32_t* group_tiles, const int32_t* tile_group,
+                                     const int32_t* group_cells, const int32_t* singular, b2s_stream_t s);
+
+/* Jacobi-BiCGSTAB in float of every case's rows (group_ptr [ngroups+1]) as separate systems,
+ * with the semantics of b2s_bicgstab_jacobi_f32_d per case; order [ngroups] is the processing
+ * order (largest first); info is [ngroups][nrhs]. */
+B2S_API int64_t b2s_bicgstab_groups_workspace_bytes(int32_t n, int nrhs, int single);
+B2S_API int b2s_bicgstab_groups_f32_d(int ngroups, const int32_t* group_ptr, const int32_t* order, int32_t n, int nrhs,
+                                      const int32_t* rowptr, const int32_t* col, const float* val, const float* b,
+                                      const float* inv_diag, float* x, double tol, int maxiter,
+                                      int relative_to_initial, int zero_x0, double* out64, const double* base64,
+                                      void* work, int64_t work_bytes, b2s_solve_info* info, b2s_stream_t s);
+
+/* The refined pressure-correction solve of b2s_pcg_amg_mixed_d per case, on a batch hierarchy
+ * (h->ngroups > 0); project [ngroups] marks the singular cases, info is [ngroups]. */
+B2S_API int64_t b2s_pcg_groups_workspace_bytes(const b2s_amg* h);
+B2S_API int b2s_pcg_groups_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const int32_t* order,
+                                   const int32_t* project, const b2s_mesh* m, const double* cf, const double* cb,
+                                   int32_t n, const int32_t* rowptr, const int32_t* col, const float* val,
+                                   const double* b, double* x, double tol, int maxiter, int maxpass,
+                                   double min_inner_tol, void* work, int64_t work_bytes, b2s_solve_info* info,
+                                   b2s_stream_t s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -187,3 +187,14 @@ def test_simplec_iterates_equal_oracle_with_pyamg_strength_rule():
     for k in fo:
         assert _rel(fs[k], fo[k]) < 1e-9, k
     assert s._amg.sizes == [lv[0].shape[0] for lv in o._amg.levels] + [o._amg.coarse_inv.shape[0]]
+
+
+def test_coarse_inverse_of_every_shared_memory_size():
+    """Coarse levels of 70 rows (a 20 x 20 jittered cavity with max_coarse 150): the dense
+    inverse's shared memory plus the kernel's static buffers exceed the default 48 KB."""
+    o, s = _pair(cartesian_mesh_2d(20, 20, jitter=0.15, seed=0),
+                 _cavity_case(viscosity=0.01, max_iter=10, tol=0.0, pressure_tol=TIGHT), 5, max_coarse=150)
+    assert s._amg.sizes[-1] > 64
+    fo, fs = o.fields(), s.fields()
+    for k in ("x-velocity", "y-velocity", "pressure"):
+        assert _rel(fs[k], fo[k]) < 1e-9, k

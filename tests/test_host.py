@@ -147,3 +147,32 @@ def test_product_path_raises_without_a_cuda_device():
         pytest.skip("a device is present")
     with pytest.raises(RuntimeError, match="CUDA device"):
         _lib.require_device()
+
+
+def test_union_mesh_keeps_every_case_and_its_geometry():
+    """The disjoint union of a batch: each case's cells contiguous (reference and device order),
+    zones renamed per case, geometry identical to the case's own."""
+    from gputest_b200.mesh.unstructured import cartesian_mesh_2d, compute_geometry, union_groups, union_mesh
+    from gputest_b200.unstructured.fvmesh import FVMesh
+
+    meshes = [cartesian_mesh_2d(5, 4, jitter=0.1, seed=1),
+              cartesian_mesh_2d(8, 3, 4.0, 1.0, names=("in", "out", "bottom", "top"), jitter=0.1, seed=2),
+              cartesian_mesh_2d(3, 3, triangulate=True)]
+    u = union_mesh(meshes)
+    g = union_groups(meshes)
+    assert u.n_cells == sum(m.n_cells for m in meshes)
+    gu = compute_geometry(u)
+    off = 0
+    for i, m in enumerate(meshes):
+        gm = compute_geometry(m)
+        assert np.allclose(gu.cell_volume[off:off + m.n_cells], gm.cell_volume, rtol=0, atol=1e-15)
+        assert np.allclose(gu.cell_centre[off:off + m.n_cells], gm.cell_centre, rtol=0, atol=1e-15)
+        for z in m.boundary_zones():
+            zu = u.zone_by_name(f"c{i}/{z.name}")
+            assert zu is not None and zu.count == z.count and zu.type == z.type
+        off += m.n_cells
+    fv = FVMesh(u, device="cpu", groups=g)
+    gd = g[fv.perm]
+    assert np.all(np.diff(gd) >= 0)
+    # no interior face joins two cases
+    assert np.all(g[fv.host.P] == g[fv.host.N])
