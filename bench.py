@@ -328,7 +328,10 @@ def run_batch(args, rank, world):
     value = float(tot.item()) / (ms_max / 1e3)
     conv = None
     if args.converge:
-        bc = BatchSimpleSolver(meshes, cases)
+        cc = [__import__("copy").deepcopy(c) for c in cases]
+        for c in cc:
+            c.max_iter = args.converge_max_iter
+        bc = BatchSimpleSolver(meshes, cc)
         c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         c0.record()
         bc.run()
@@ -450,6 +453,7 @@ def main():
     ap.add_argument("--converge", action="store_true", help="also run to the 1e-6 residual and report it")
     ap.add_argument("--batch-cases", type=int, default=256, help="c4: cases in the sweep")
     ap.add_argument("--batch-sample", type=int, default=24, help="c4: cases timed one at a time")
+    ap.add_argument("--converge-max-iter", type=int, default=6000, help="c4: outer-iteration cap of --converge")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

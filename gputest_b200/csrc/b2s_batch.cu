@@ -6,9 +6,10 @@
 // the cells in which no tile straddles two cases, so that their per-tile partial sums add up to
 // per-case sums here. The Krylov solves are per case: each case keeps its own scalars (alpha,
 // beta, omega, convergence), as if it were solved alone. They are persistent launches in which
-// a block takes whole cases from a fixed work list (largest first, dealt round-robin over the
-// blocks) and runs each one's solve with block-level barriers only: no grid barrier, no atomics,
-// every reduction in a fixed order.
+// a team - the blocks of one thread-block cluster - takes whole cases from a fixed work list
+// (largest first, dealt round-robin over the teams) and runs each one's solve with cluster
+// barriers and distributed-shared-memory sums only: no grid barrier, no atomics, every
+// reduction in a fixed order.
 //
 // The AMG hierarchy of a batch is block diagonal too (aggregates never cross cases, and are
 // numbered case by case), so a case's V-cycle touches only its own rows on every level, and its
@@ -53,25 +54,63 @@ __global__ void remove_group_means_k(b2s_mesh m, double* __restrict__ x, const d
   if (c < m.tiles[t + 1]) x[c] = x[c] - mean;
 }
 
-// ---------------------------------------------------------------------------------- block helpers
-// Sum of NQ values over the block, every thread receives the totals (red: (32+1)*NQ doubles).
-template <int NQ>
-__device__ __forceinline__ void bsum(double (&v)[NQ], double* red) {
-  double out[NQ];
-  block_sum<NQ>(v, red, out);
+// ---------------------------------------------------------------------------------- case teams
+// A case is solved by a team: the blocks of one thread-block cluster (kClusterBlocks blocks,
+// each on its own SM). Rows are dealt over all the team's threads; a team barrier is the
+// cluster barrier (which also orders the team's global-memory accesses), and a team sum adds
+// the block sums of the team's blocks read from their shared memory (distributed shared
+// memory), in rank order, so that every thread of the team gets the same bits.
+constexpr int kClusterBlocks = 4;
+
+struct Team {
+  int t, n;      // this thread's index in the team and the team's size
+  int rank, nb;  // this block's rank in the cluster and the cluster's blocks
+  int pb;        // which of the two exchange buffers the next sum writes
+  double* xbuf;  // [2][8] block sums exchanged between the cluster's blocks
+  __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+  template <int NQ>
+  __device__ __forceinline__ void sum(double (&v)[NQ], double* red) {
+    static_assert(NQ <= 8, "team sums of at most 8 values");
+    double out[NQ];
+    block_sum<NQ>(v, red, out);
+    double* mine = xbuf + pb * 8;
+    if (threadIdx.x == 0)
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) v[q] = out[q];
+      for (int q = 0; q < NQ; ++q) mine[q] = out[q];
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = 0.0;
+    for (int r = 0; r < nb; ++r) {
+      const double* other = cl.map_shared_rank(mine, r);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) v[q] += other[q];
+    }
+    pb ^= 1;  // the next sum writes the other buffer: a block still reading this one is safe
+  }
+};
+
+__device__ __forceinline__ Team make_team(double* xbuf) {
+  cg::cluster_group cl = cg::this_cluster();
+  Team tm;
+  tm.rank = (int)cl.block_rank();
+  tm.nb = (int)cl.num_blocks();
+  tm.t = tm.rank * (int)blockDim.x + (int)threadIdx.x;
+  tm.n = tm.nb * (int)blockDim.x;
+  tm.pb = 0;
+  tm.xbuf = xbuf;
+  return tm;
 }
 
-// Rows [lo, hi) of a block: one thread per row, or one warp per row for long rows.
+// Rows [lo, hi) of a team: one thread per row, or one warp per row for long rows.
 struct BRows {
   int first, stride, lane, step;
   bool wide;
-  __device__ __forceinline__ BRows(bool w, int lo) {
+  __device__ __forceinline__ BRows(bool w, int lo, const Team& tm) {
     wide = w;
-    first = lo + (w ? (int)(threadIdx.x >> 5) : (int)threadIdx.x);
-    stride = w ? (int)(blockDim.x >> 5) : (int)blockDim.x;
-    lane = w ? (int)(threadIdx.x & 31) : 0;
+    first = lo + (w ? (tm.t >> 5) : tm.t);
+    stride = w ? (tm.n >> 5) : tm.n;
+    lane = w ? (tm.t & 31) : 0;
     step = w ? 32 : 1;
   }
   __device__ __forceinline__ double total(double s) const { return wide ? warp_sum(s) : s; }
@@ -103,7 +142,8 @@ struct BicgGroupArgs {
 // Jacobi-BiCGSTAB of one case's rows (flowtrace/linalg/krylov.py:68-121 with
 // relative_to_initial), NR systems sharing the matrix, each with its own scalars.
 template <int NR, class T>
-__device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double* red, b2s_solve_info* info) {
+__device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double* red, b2s_solve_info* info,
+                               Team& tm) {
   const int n = a.n;
   const int64_t nnz = a.rowptr[hi] - a.rowptr[lo];
   T *x[NR], *r[NR], *rh[NR], *p[NR], *v[NR], *h[NR], *s[NR], *t[NR];
@@ -128,7 +168,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
 #pragma unroll
   for (int q = 0; q < 2 * NR; ++q) acc[q] = 0.0;
   {
-    const BRows R(wide, lo);
+    const BRows R(wide, lo, tm);
     for (int i = R.first; i < hi; i += R.stride) {
 #pragma unroll
       for (int k = 0; k < NR; ++k) {
@@ -149,7 +189,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
       }
     }
   }
-  bsum<2 * NR>(acc, red);
+  tm.sum<2 * NR>(acc, red);
   bool act[NR];
   int its[NR], conv[NR];
   double rho[NR], alpha[NR], omega[NR], bnorm[NR], babs[NR], rnorm[NR], res[NR];
@@ -174,11 +214,11 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
     double d1[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) d1[k] = 0.0;
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+    for (int i = lo + tm.t; i < hi; i += tm.n)
 #pragma unroll
       for (int k = 0; k < NR; ++k)
         if (act[k]) d1[k] += (double)rh[k][i] * (double)r[k][i];
-    bsum<NR>(d1, red);
+    tm.sum<NR>(d1, red);
     double beta[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
@@ -194,7 +234,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
       rho[k] = d1[k];
     }
     // p = r + beta (p - omega v), h = inv p
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+    for (int i = lo + tm.t; i < hi; i += tm.n)
 #pragma unroll
       for (int k = 0; k < NR; ++k)
         if (act[k]) {
@@ -202,13 +242,13 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
           p[k][i] = pi;
           h[k][i] = (double)inv[i] * pi;
         }
-    __syncthreads();
+    tm.sync();
     // v = A h, r_hat . v
     double d2[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) d2[k] = 0.0;
     {
-      const BRows R(wide, lo);
+      const BRows R(wide, lo, tm);
       for (int i = R.first; i < hi; i += R.stride)
 #pragma unroll
         for (int k = 0; k < NR; ++k)
@@ -223,7 +263,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
             }
           }
     }
-    bsum<NR>(d2, red);
+    tm.sum<NR>(d2, red);
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
       if (!act[k]) continue;
@@ -239,7 +279,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
     double d3[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) d3[k] = 0.0;
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+    for (int i = lo + tm.t; i < hi; i += tm.n)
 #pragma unroll
       for (int k = 0; k < NR; ++k)
         if (act[k]) {
@@ -247,7 +287,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
           s[k][i] = si;
           d3[k] += si * si;
         }
-    bsum<NR>(d3, red);
+    tm.sum<NR>(d3, red);
     bool sdone[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
@@ -262,20 +302,20 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
       }
     }
     // systems converged on |s|: x += alpha h (hs = inv s is evaluated on the fly below)
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+    for (int i = lo + tm.t; i < hi; i += tm.n)
 #pragma unroll
       for (int k = 0; k < NR; ++k)
         if (sdone[k]) x[k][i] = (double)x[k][i] + alpha[k] * (double)h[k][i];
 #pragma unroll
     for (int k = 0; k < NR; ++k)
       if (sdone[k]) act[k] = false;
-    __syncthreads();
+    tm.sync();
     // t = A (inv s); t.t, t.s
     double d4[2 * NR];
 #pragma unroll
     for (int q = 0; q < 2 * NR; ++q) d4[q] = 0.0;
     {
-      const BRows R(wide, lo);
+      const BRows R(wide, lo, tm);
       for (int i = R.first; i < hi; i += R.stride)
 #pragma unroll
         for (int k = 0; k < NR; ++k)
@@ -293,7 +333,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
             }
           }
     }
-    bsum<2 * NR>(d4, red);
+    tm.sum<2 * NR>(d4, red);
 #pragma unroll
     for (int k = 0; k < NR; ++k)
       if (act[k]) omega[k] = d4[k] > 0.0 ? d4[NR + k] / d4[k] : 0.0;
@@ -301,14 +341,14 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
     double d5[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) d5[k] = 0.0;
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+    for (int i = lo + tm.t; i < hi; i += tm.n)
 #pragma unroll
       for (int k = 0; k < NR; ++k)
         if (act[k]) {
           const double ri = (double)s[k][i] - omega[k] * (double)t[k][i];
           d5[k] += ri * ri;
         }
-    bsum<NR>(d5, red);
+    tm.sum<NR>(d5, red);
     bool upd[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
@@ -337,7 +377,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
         res[k] = rn / bnorm[k];
       }
     }
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+    for (int i = lo + tm.t; i < hi; i += tm.n)
 #pragma unroll
       for (int k = 0; k < NR; ++k)
         if (upd[k]) {
@@ -345,29 +385,34 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
           x[k][i] = ((double)x[k][i] + alpha[k] * (double)h[k][i]) + omega[k] * ((double)inv[i] * si);
           r[k][i] = si - omega[k] * (double)t[k][i];
         }
-    __syncthreads();
+    tm.sync();
   }
   if (a.out64)
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+    for (int i = lo + tm.t; i < hi; i += tm.n)
 #pragma unroll
       for (int k = 0; k < NR; ++k) a.out64[(int64_t)k * n + i] = a.base64[(int64_t)k * n + i] + (double)x[k][i];
-  if (threadIdx.x == 0)
+  if (tm.t == 0)
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
       info[k].iterations = its[k] ? its[k] : (conv[k] ? 0 : a.maxiter);
       info[k].converged = conv[k];
       info[k].residual = res[k];
     }
-  __syncthreads();
+  tm.sync();
 }
 
+// Cluster c of the launch takes cases order[c], order[c + nclusters], ...
 template <int NR, class T>
 __global__ void __launch_bounds__(kBatchThreads) bicgstab_groups_k(BicgGroupArgs<T> a) {
   __shared__ double red[(kBatchWarps + 1) * 2 * NR];
-  for (int k = blockIdx.x; k < a.ngroups; k += gridDim.x) {
+  __shared__ double xbuf[16];
+  Team tm = make_team(xbuf);
+  const int cid = (int)blockIdx.x / tm.nb, ncl = (int)gridDim.x / tm.nb;
+  for (int k = cid; k < a.ngroups; k += ncl) {
     const int g = a.order[k];
-    bicgstab_group<NR, T>(a, a.group_ptr[g], a.group_ptr[g + 1], red, a.info + (int64_t)g * NR);
+    bicgstab_group<NR, T>(a, a.group_ptr[g], a.group_ptr[g + 1], red, a.info + (int64_t)g * NR, tm);
   }
+  tm.sync();  // no block leaves while another may still read its shared memory
 }
 
 // ---------------------------------------------------------------------------------- AMG-PCG
@@ -412,7 +457,7 @@ struct PcgGroupArgs {
 // residual, restriction on every level, the case's dense coarse inverse, then prolongation and
 // post-smoothing; returns the buffer holding z (rows of case g on level 0).
 template <class T>
-__device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, double* red) {
+__device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, double* red, Team& tm) {
   const b2s_amg& h = a.h;
   const int L = h.nlevels;
   const double w = h.omega;
@@ -429,9 +474,9 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
     T* c = X;
     // first sweep fused: x = w D^-1 b; then y = x + w D^-1 (b - A x) with x on the fly
     if (h.sweeps <= 1) {
-      for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) X[i] = (w * (double)dinv[i]) * (double)b[i];
+      for (int i = lo + tm.t; i < hi; i += tm.n) X[i] = (w * (double)dinv[i]) * (double)b[i];
     } else {
-      const BRows R(wide, lo);
+      const BRows R(wide, lo, tm);
       for (int i = R.first; i < hi; i += R.stride) {
         double s = 0.0;
         for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.step) {
@@ -444,8 +489,8 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
       }
       T* o = Y;
       for (int sw = 2; sw < h.sweeps; ++sw) {
-        __syncthreads();
-        const BRows R2(wide, lo);
+        tm.sync();
+        const BRows R2(wide, lo, tm);
         for (int i = R2.first; i < hi; i += R2.stride) {
           double s = 0.0;
           for (int j = lv.rowptr[i] + R2.lane; j < lv.rowptr[i + 1]; j += R2.step) s += (double)val[j] * (double)c[lv.col[j]];
@@ -457,10 +502,10 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
         o = tmp;
       }
     }
-    __syncthreads();
+    tm.sync();
     T* Rv = a.lr[l];
     {
-      const BRows R(wide, lo);
+      const BRows R(wide, lo, tm);
       for (int i = R.first; i < hi; i += R.stride) {
         double s = 0.0;
         for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.step) s += (double)val[j] * (double)c[lv.col[j]];
@@ -468,12 +513,12 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
         if (R.writer()) Rv[i] = (double)b[i] - s;
       }
     }
-    __syncthreads();
+    tm.sync();
     const int clo = (l + 1 < L) ? h.levels[l + 1].group_ptr[g] : h.coarse_group_ptr[g];
     const int chi = (l + 1 < L) ? h.levels[l + 1].group_ptr[g + 1] : h.coarse_group_ptr[g + 1];
     T* bn = (l + 1 < L) ? a.lb[l + 1] : a.cb;
     {
-      const BRows R(lv.p_nnz >= (int64_t)kBatchWideRow * lv.nc, clo);
+      const BRows R(lv.p_nnz >= (int64_t)kBatchWideRow * lv.nc, clo, tm);
       for (int I = R.first; I < chi; I += R.stride) {
         double s = 0.0;
         for (int j = lv.r_rowptr[I] + R.lane; j < lv.r_rowptr[I + 1]; j += R.step) s += (double)a.lrval[l][j] * (double)Rv[lv.r_col[j]];
@@ -481,7 +526,7 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
         if (R.writer()) bn[I] = s;
       }
     }
-    __syncthreads();
+    tm.sync();
     cur[l] = c;
   }
   // coarse: cx = inv_g cb (double inverse), one warp per row
@@ -489,15 +534,15 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
   {
     const int clo = h.coarse_group_ptr[g], nn = h.coarse_group_ptr[g + 1] - clo;
     const double* inv = h.coarse_inv + h.coarse_inv_off[g];
-    const int lane = threadIdx.x & 31;
-    for (int I = (int)(threadIdx.x >> 5); I < nn; I += (int)(blockDim.x >> 5)) {
+    const int lane = tm.t & 31;
+    for (int I = tm.t >> 5; I < nn; I += tm.n >> 5) {
       double s = 0.0;
       for (int J = lane; J < nn; J += 32) s += inv[(int64_t)I * nn + J] * (double)cb[clo + J];
       s = warp_sum(s);
       if (lane == 0) a.cx[clo + I] = s;
     }
   }
-  __syncthreads();
+  tm.sync();
   for (int l = L - 1; l >= 0; --l) {
     const b2s_amg_level& lv = h.levels[l];
     const int lo = lv.group_ptr[g], hi = lv.group_ptr[g + 1];
@@ -509,7 +554,7 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
     T* c = cur[l];
     T* o = (c == a.lx[l]) ? a.ly[l] : a.lx[l];
     {
-      const BRows R(lv.p_nnz >= (int64_t)kBatchWideRow * lv.n, lo);
+      const BRows R(lv.p_nnz >= (int64_t)kBatchWideRow * lv.n, lo, tm);
       for (int i = R.first; i < hi; i += R.stride) {
         double s = 0.0;
         for (int j = lv.p_rowptr[i] + R.lane; j < lv.p_rowptr[i + 1]; j += R.step) s += (double)a.lpval[l][j] * (double)xc[lv.p_col[j]];
@@ -518,8 +563,8 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
       }
     }
     for (int sw = 0; sw < h.sweeps; ++sw) {
-      __syncthreads();
-      const BRows R(wide, lo);
+      tm.sync();
+      const BRows R(wide, lo, tm);
       for (int i = R.first; i < hi; i += R.stride) {
         double s = 0.0;
         for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.step) s += (double)val[j] * (double)c[lv.col[j]];
@@ -530,7 +575,7 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
       c = o;
       o = tmp;
     }
-    __syncthreads();
+    tm.sync();
     cur[l] = c;
   }
   (void)red;
@@ -545,7 +590,7 @@ struct GroupOutcome {
 // Preconditioned CG (flowtrace/linalg/krylov.py:25-65) of case g's rows, x = 0 at the start;
 // with project the residual and the preconditioned residual are kept mean-free.
 template <class T>
-__device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec, T* x, double tol, int maxiter,
+__device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec, T* x, double tol, int maxiter, Team& tm,
                                   bool project, double* red) {
   const int lo = a.h.nlevels ? a.h.levels[0].group_ptr[g] : a.h.coarse_group_ptr[g];
   const int hi = a.h.nlevels ? a.h.levels[0].group_ptr[g + 1] : a.h.coarse_group_ptr[g + 1];
@@ -554,21 +599,21 @@ __device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec
   T* p = a.p;
   T* q = a.q;
   double v2[2] = {0.0, 0.0};
-  for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) {
+  for (int i = lo + tm.t; i < hi; i += tm.n) {
     const double bi = bvec[i];
     x[i] = 0.0;
     v2[0] += bi * bi;
     v2[1] += bi;
   }
-  bsum<2>(v2, red);
+  tm.sum<2>(v2, red);
   const double bb = v2[0], mb = project ? v2[1] / nd : 0.0;
   double v1[1] = {0.0};
-  for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) {
+  for (int i = lo + tm.t; i < hi; i += tm.n) {
     const double ri = (double)bvec[i] - mb;
     r[i] = ri;
     v1[0] += ri * ri;
   }
-  bsum<1>(v1, red);
+  tm.sum<1>(v1, red);
   double bnorm = sqrt(bb);
   if (bnorm == 0.0) bnorm = 1.0;
   double rnorm = sqrt(v1[0]);
@@ -578,30 +623,30 @@ __device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec
     return o;
   }
   auto precondition = [&](double& rz) -> T* {
-    T* z = vcycle_group(a, g, (const T*)r, red);
+    T* z = vcycle_group(a, g, (const T*)r, red, tm);
     double s3[3] = {0.0, 0.0, 0.0};
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) {
+    for (int i = lo + tm.t; i < hi; i += tm.n) {
       const double zi = z[i], ri = r[i];
       s3[0] += zi;
       s3[1] += ri * zi;
       s3[2] += ri;
     }
-    bsum<3>(s3, red);
+    tm.sum<3>(s3, red);
     const double zm = project ? s3[0] / nd : 0.0;
     if (project)
-      for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) z[i] = (double)z[i] - zm;
+      for (int i = lo + tm.t; i < hi; i += tm.n) z[i] = (double)z[i] - zm;
     rz = project ? s3[1] - zm * s3[2] : s3[1];
-    __syncthreads();
+    tm.sync();
     return z;
   };
   double rz;
   T* z = precondition(rz);
-  for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) p[i] = z[i];
-  __syncthreads();
+  for (int i = lo + tm.t; i < hi; i += tm.n) p[i] = z[i];
+  tm.sync();
   for (int k = 1; k <= maxiter; ++k) {
     double pq[1] = {0.0};
     {
-      const BRows R(false, lo);
+      const BRows R(false, lo, tm);
       for (int i = R.first; i < hi; i += R.stride) {
         double s = 0.0;
         for (int j = a.rowptr[i]; j < a.rowptr[i + 1]; ++j) s += (double)a.val[j] * (double)p[a.col[j]];
@@ -609,7 +654,7 @@ __device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec
         pq[0] += (double)p[i] * s;
       }
     }
-    bsum<1>(pq, red);
+    tm.sum<1>(pq, red);
     if (pq[0] <= 0.0) {
       o.its = k;
       o.res = rnorm / bnorm;
@@ -617,13 +662,13 @@ __device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec
     }
     const double alpha = rz / pq[0];
     double rr[1] = {0.0};
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) {
+    for (int i = lo + tm.t; i < hi; i += tm.n) {
       x[i] = (double)x[i] + alpha * (double)p[i];
       const double ri = (double)r[i] - alpha * (double)q[i];
       r[i] = ri;
       rr[0] += ri * ri;
     }
-    bsum<1>(rr, red);
+    tm.sum<1>(rr, red);
     rnorm = sqrt(rr[0]);
     o.its = k;
     o.res = rnorm / bnorm;
@@ -636,8 +681,8 @@ __device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec
     if (rz == 0.0) return o;
     const double beta = rz_new / rz;
     rz = rz_new;
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) p[i] = (double)z[i] + beta * (double)p[i];
-    __syncthreads();
+    for (int i = lo + tm.t; i < hi; i += tm.n) p[i] = (double)z[i] + beta * (double)p[i];
+    tm.sync();
   }
   return o;
 }
@@ -645,42 +690,42 @@ __device__ GroupOutcome pcg_group(const PcgGroupArgs<T>& a, int g, const T* bvec
 // Refined solve of case g: float PCG passes, double x += d and double residual from the face
 // coefficients, the reference's stopping test on it (as b2s_pcg_amg_mixed_d, per case).
 template <class T>
-__device__ void pcg_refined_group(const PcgGroupArgs<T>& a, int g, double* red) {
+__device__ void pcg_refined_group(const PcgGroupArgs<T>& a, int g, double* red, Team& tm) {
   const b2s_mesh& m = a.m;
   const int lo = a.h.nlevels ? a.h.levels[0].group_ptr[g] : a.h.coarse_group_ptr[g];
   const int hi = a.h.nlevels ? a.h.levels[0].group_ptr[g + 1] : a.h.coarse_group_ptr[g + 1];
   const bool project = a.project[g] != 0;
   const double nd = (double)(hi - lo);
   double v2[2] = {0.0, 0.0};
-  for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) {
+  for (int i = lo + tm.t; i < hi; i += tm.n) {
     const double bi = a.b64[i];
     a.x64[i] = 0.0;
     v2[0] += bi * bi;
     v2[1] += bi;
   }
-  bsum<2>(v2, red);
+  tm.sum<2>(v2, red);
   double bnorm = sqrt(v2[0]);
   if (bnorm == 0.0) bnorm = 1.0;
   double mean = project ? v2[1] / nd : 0.0;
   double v1[1] = {0.0};
-  for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) {
+  for (int i = lo + tm.t; i < hi; i += tm.n) {
     const double ri = a.b64[i] - mean;
     a.r64[i] = ri;
     a.rb[i] = ri;
     v1[0] += ri * ri;
   }
-  bsum<1>(v1, red);
+  tm.sum<1>(v1, red);
   double res = sqrt(v1[0]) / bnorm;
   int its = 0, conv = res < a.tol ? 1 : 0;
   for (int pass = 0; pass < a.maxpass && !conv && its < a.maxiter; ++pass) {
     double tin = a.tol / res;
     if (tin < a.min_inner_tol) tin = a.min_inner_tol;
-    const GroupOutcome o = pcg_group(a, g, (const T*)a.rb, a.d, tin, a.maxiter - its, project, red);
+    const GroupOutcome o = pcg_group(a, g, (const T*)a.rb, a.d, tin, a.maxiter - its, tm, project, red);
     its += o.its;
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) a.x64[i] = a.x64[i] + (double)a.d[i];
-    __syncthreads();
+    for (int i = lo + tm.t; i < hi; i += tm.n) a.x64[i] = a.x64[i] + (double)a.d[i];
+    tm.sync();
     double s2[2] = {0.0, 0.0};
-    for (int c = lo + (int)threadIdx.x; c < hi; c += blockDim.x) {
+    for (int c = lo + tm.t; c < hi; c += tm.n) {
       const double xc = a.x64[c];
       double ax = 0.0;
       for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) ax += a.cf[f] * (xc - a.x64[m.fN[f]]);
@@ -694,7 +739,7 @@ __device__ void pcg_refined_group(const PcgGroupArgs<T>& a, int g, double* red) 
       s2[0] += ri * ri;
       s2[1] += ri;
     }
-    bsum<2>(s2, red);
+    tm.sum<2>(s2, red);
     mean = project ? s2[1] / nd : 0.0;
     double rr = project ? s2[0] - s2[1] * mean : s2[0];
     if (rr < 0.0) rr = 0.0;
@@ -705,36 +750,52 @@ __device__ void pcg_refined_group(const PcgGroupArgs<T>& a, int g, double* red) 
       break;
     }
     if (o.its == 0 && !o.conv) break;
-    for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) a.rb[i] = a.r64[i] - mean;
-    __syncthreads();
+    for (int i = lo + tm.t; i < hi; i += tm.n) a.rb[i] = a.r64[i] - mean;
+    tm.sync();
   }
-  if (threadIdx.x == 0) {
+  if (tm.t == 0) {
     a.info[g].iterations = its;
     a.info[g].converged = conv;
     a.info[g].residual = res;
   }
-  __syncthreads();
+  tm.sync();
 }
 
 template <class T>
 __global__ void __launch_bounds__(kBatchThreads) pcg_groups_k(PcgGroupArgs<T> a) {
   __shared__ double red[(kBatchWarps + 1) * 3];
-  for (int k = blockIdx.x; k < a.h.ngroups; k += gridDim.x) pcg_refined_group<T>(a, a.order[k], red);
+  __shared__ double xbuf[16];
+  Team tm = make_team(xbuf);
+  const int cid = (int)blockIdx.x / tm.nb, ncl = (int)gridDim.x / tm.nb;
+  for (int k = cid; k < a.h.ngroups; k += ncl) pcg_refined_group<T>(a, a.order[k], red, tm);
+  tm.sync();  // no block leaves while another may still read its shared memory
 }
 
 }  // namespace b2s
 
 using namespace b2s;
 
-static int batch_grid(const void* kernel, int ngroups, int* g) {
-  int dev = 0, sms = 0, per = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return B2S_ERR_DEVICE;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return B2S_ERR_DEVICE;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBatchThreads, 0) != cudaSuccess)
-    return B2S_ERR_DEVICE;
-  if (per < 1) per = 1;
-  const int64_t cap = (int64_t)sms * per;
-  *g = (int)(ngroups < cap ? ngroups : cap);
+// Launch one team (a cluster of kClusterBlocks blocks) per case up to the number of clusters that
+// fit on the device at once; the teams then walk the case list.
+static int launch_teams(const void* kernel, int ngroups, void** args, b2s_stream_t s) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kClusterBlocks;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kClusterBlocks, 1, 1);
+  cfg.blockDim = dim3(kBatchThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = (cudaStream_t)s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, kernel, &cfg) != cudaSuccess || ncl < 1) return B2S_ERR_DEVICE;
+  if (ncl > ngroups) ncl = ngroups;
+  cfg.gridDim = dim3((unsigned)(ncl * kClusterBlocks), 1, 1);
+  if (cudaLaunchKernelExC(&cfg, kernel, args) != cudaSuccess) return B2S_ERR_LAUNCH;
+  B2S_LAUNCH_CHECK();
   return B2S_OK;
 }
 
@@ -743,11 +804,7 @@ static int launch_bicg_groups(BicgGroupArgs<T>& a, b2s_stream_t s) {
   void* args[] = {&a};
   const void* k = a.nr == 1 ? (const void*)bicgstab_groups_k<1, T>
                   : a.nr == 2 ? (const void*)bicgstab_groups_k<2, T> : (const void*)bicgstab_groups_k<3, T>;
-  int g = 0, rc;
-  if ((rc = batch_grid(k, a.ngroups, &g)) != B2S_OK) return rc;
-  if (cudaLaunchKernel(k, g, kBatchThreads, args, 0, (cudaStream_t)s) != cudaSuccess) return B2S_ERR_LAUNCH;
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  return launch_teams(k, a.ngroups, args, s);
 }
 
 extern "C" {
@@ -889,12 +946,7 @@ int b2s_pcg_groups_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const int32
   a.min_inner_tol = min_inner_tol;
   a.info = info;
   void* args[] = {&a};
-  int g = 0, rc;
-  if ((rc = batch_grid((const void*)pcg_groups_k<float>, h->ngroups, &g)) != B2S_OK) return rc;
-  if (cudaLaunchKernel((const void*)pcg_groups_k<float>, g, kBatchThreads, args, 0, (cudaStream_t)s) != cudaSuccess)
-    return B2S_ERR_LAUNCH;
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  return launch_teams((const void*)pcg_groups_k<float>, h->ngroups, args, s);
 }
 
 }  // extern "C"

@@ -114,8 +114,22 @@ class AMGHierarchy:
         aggs, counts, mats = [], [], []
         while too_big(A) and len(aggs) < max_levels - 1:
             S = strength(A, theta)
+            if batched:
+                # cases already at most max_coarse rows keep their size: no strong connections, so
+                # every row of theirs is an aggregate of its own (a case coarsened to a handful of
+                # rows would make a singular case's coarse block numerically zero)
+                gsz = np.bincount(level_groups[-1], minlength=ngroups)
+                big_row = gsz[level_groups[-1]] > max_coarse
+                S = S.tocoo()
+                keep = big_row[S.row]
+                S = sp.csr_matrix((S.data[keep], (S.row[keep], S.col[keep])), shape=S.shape)
             agg, na = aggregate(S)
-            if na >= A.shape[0] * 0.9:
+            if batched:
+                n_big = int(big_row.sum())
+                na_big = na - int((~big_row).sum())
+                if na_big >= n_big * 0.9:
+                    break
+            elif na >= A.shape[0] * 0.9:
                 break
             if batched:  # number the aggregates case by case (aggregates never cross cases)
                 g_of = np.empty(na, dtype=np.int64)
