@@ -38,7 +38,8 @@ class BC(ctypes.Structure):
 
 class FlowParams(ctypes.Structure):
     _fields_ = [("rho", F64), ("mu", F64), ("relax_u", F64), ("relax_p", F64), ("body", F64 * 3),
-                ("simplec", I32), ("second_order", I32), ("singular_p", I32), ("pad", I32)]
+                ("simplec", I32), ("second_order", I32), ("singular_p", I32), ("pad", I32),
+                ("relax_u_cell", P), ("relax_p_cell", P), ("simplec_cell", P)]
 
 
 class SolveInfo(ctypes.Structure):

@@ -73,6 +73,46 @@ __global__ void __launch_bounds__(kCoopThreads) power_coop_k(b2s_amg_level L, do
 // barrier per iteration costs more than the work).
 constexpr int kPowerBlockRows = 2048;
 
+// Batches: the power iteration of power_block_k per case (one block per case on its rows). A
+// case that this level does not coarsen (every row its own aggregate, next_ptr giving the same
+// row count) gets rho = infinity, so that its prolongation is the plain injection P = T and its
+// coarse block the same matrix.
+__global__ void __launch_bounds__(kCoopThreads) power_groups_k(b2s_amg_level L, const int32_t* __restrict__ next_ptr,
+                                                              double* ya, double* yb) {
+  __shared__ double red[(kCoopThreads / 32 + 1) * 2];
+  const int g = blockIdx.x, lo = L.group_ptr[g], hi = L.group_ptr[g + 1];
+  if (next_ptr[g + 1] - next_ptr[g] == hi - lo) {
+    if (threadIdx.x == 0) L.rho[g] = INFINITY;
+    return;
+  }
+  double* ybuf[2] = {ya, yb};
+  double lam = 1.0, sc = 1.0;
+  for (int it = 0; it < 15; ++it) {
+    const double* xin = it == 0 ? L.x0 : ybuf[(it - 1) & 1];
+    double* yout = ybuf[it & 1];
+    double acc[2] = {0.0, 0.0};
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      const double di = L.dinv[i];
+      double s = 0.0;
+      for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
+        const int c = L.col[j];
+        const double xc = it == 0 ? xin[c] : xin[c] / sc;
+        s += (di * L.val[j]) * xc;
+      }
+      yout[i] = s;
+      acc[0] += s * s;
+      const double xi = it == 0 ? xin[i] : xin[i] / sc;
+      acc[1] += xi * xi;
+    }
+    double tot[2];
+    block_sum<2>(acc, red, tot);
+    const double ny = sqrt(tot[0]), nx = sqrt(tot[1]);
+    lam = ny / fmax(nx, 1e-300);
+    sc = fmax(ny, 1e-300);
+  }
+  if (threadIdx.x == 0) L.rho[g] = lam;
+}
+
 __global__ void __launch_bounds__(kCoopThreads) power_block_k(b2s_amg_level L, double* ya, double* yb) {
   __shared__ double red[(kCoopThreads / 32 + 1) * 2];
   double* ybuf[2] = {ya, yb};
@@ -104,9 +144,20 @@ __global__ void __launch_bounds__(kCoopThreads) power_block_k(b2s_amg_level L, d
 }
 
 // P[i,J] = T[i,J] - c sum_{k in row i, agg[k] = J} (Dinv_i A_ik) T[k,J], c = (4/3)/rho
-__global__ void pvals_k(b2s_amg_level L) {
-  const double c = (4.0 / 3.0) / *L.rho;
+// With ngroups > 0 (batches) the spectral radius is per case: rho[g] for the rows of case g.
+__global__ void pvals_k(b2s_amg_level L, int ngroups) {
+  const double c0 = ngroups > 0 ? 0.0 : (4.0 / 3.0) / *L.rho;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+    double c = c0;
+    if (ngroups > 0) {
+      int lo = 0, hi = ngroups;  // the case g with group_ptr[g] <= i < group_ptr[g+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (L.group_ptr[mid] <= i) lo = mid;
+        else hi = mid;
+      }
+      c = (4.0 / 3.0) / L.rho[lo];
+    }
     const int p0 = L.p_rowptr[i], p1 = L.p_rowptr[i + 1];
     for (int s = p0; s < p1; ++s) L.p_val[s] = 0.0;
     const double di = L.dinv[i];
@@ -380,14 +431,18 @@ int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stre
       return B2S_ERR_ARG;
     dinv_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
     B2S_LAUNCH_CHECK();
-    if (L.n <= kPowerBlockRows) {
+    if (h->ngroups > 0) {
+      if (!L.group_ptr) return B2S_ERR_ARG;
+      const int32_t* next = (l + 1 < h->nlevels) ? h->levels[l + 1].group_ptr : h->coarse_group_ptr;
+      power_groups_k<<<(unsigned)h->ngroups, kCoopThreads, 0, st>>>(L, next, xa, xb);
+    } else if (L.n <= kPowerBlockRows) {
       power_block_k<<<1, kCoopThreads, 0, st>>>(L, xa, xb);
     } else {
       void* args[] = {&L, &xa, &xb, &part0, &part1};  // xa, xb: the two power-iteration buffers
       if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
         return B2S_ERR_LAUNCH;
     }
-    pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+    pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L, h->ngroups);
     rvals_k<<<grid_for(L.p_nnz), kThreads, 0, st>>>(L);
     wvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
     B2S_LAUNCH_CHECK();

@@ -355,13 +355,14 @@ __global__ void momentum_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, 
                                     double* __restrict__ br_out, double* __restrict__ part) {
   __shared__ double red[(kThreads / 32 + 1) * 2 * DIM];
   const int nc = m.nc, nb = m.nb;
-  const double au = prm.relax_u;
   double acc[2 * DIM];
 #pragma unroll
   for (int q = 0; q < 2 * DIM; ++q) acc[q] = 0.0;
   const bool drive = prm.body[0] != 0.0 || prm.body[1] != 0.0 || (DIM == 3 && prm.body[2] != 0.0);
   for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
     const int c = r_.c;
+    const double au = prm.relax_u_cell ? prm.relax_u_cell[c] : prm.relax_u;
+    const bool simplec = prm.simplec_cell ? prm.simplec_cell[c] != 0 : prm.simplec != 0;
     RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
                                                  (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
     double diag = o.diag;
@@ -372,7 +373,7 @@ __global__ void momentum_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, 
     inv_out[c] = 1.0 / diag_r;
     diag_out[c] = diag;
     double denom = diag_r;
-    if (prm.simplec) {
+    if (simplec) {
       denom = diag_r - o.sumnb;
       denom = (denom > 1e-12 * diag_r) ? denom : diag_r;
     }
@@ -531,7 +532,7 @@ __global__ void correct_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const doub
 #pragma unroll
       for (int a = 0; a < DIM; ++a) rb[a] += coef * m.db[(int64_t)a * nb + f];
     }
-    const double pn = p[c] + prm.relax_p * ppc;
+    const double pn = p[c] + (prm.relax_p_cell ? prm.relax_p_cell[c] : prm.relax_p) * ppc;
     Up_new[c] = pn;
     acc[0] += pn;
     double r[DIM];
@@ -661,13 +662,14 @@ __global__ void momentum_assemble_mixed_k(b2s_mesh m, b2s_bc bc, b2s_flow_params
                                           float* __restrict__ r_out, double* __restrict__ part) {
   __shared__ double red[(kThreads / 32 + 1) * 2 * DIM];
   const int nc = m.nc, nb = m.nb;
-  const double au = prm.relax_u;
   double acc[2 * DIM];
 #pragma unroll
   for (int q = 0; q < 2 * DIM; ++q) acc[q] = 0.0;
   const bool drive = prm.body[0] != 0.0 || prm.body[1] != 0.0 || (DIM == 3 && prm.body[2] != 0.0);
   for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
     const int c = r_.c;
+    const double au = prm.relax_u_cell ? prm.relax_u_cell[c] : prm.relax_u;
+    const bool simplec = prm.simplec_cell ? prm.simplec_cell[c] != 0 : prm.simplec != 0;
     RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
                                                  (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
     double diag = o.diag;
@@ -677,7 +679,7 @@ __global__ void momentum_assemble_mixed_k(b2s_mesh m, b2s_bc bc, b2s_flow_params
     val[m.slot_diag[c]] = (float)diag_r;
     inv_out[c] = (float)(1.0 / diag_r);
     double denom = diag_r;
-    if (prm.simplec) {
+    if (simplec) {
       denom = diag_r - o.sumnb;
       denom = (denom > 1e-12 * diag_r) ? denom : diag_r;
     }

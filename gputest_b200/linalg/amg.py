@@ -212,7 +212,7 @@ class AMGHierarchy:
                 "r_col": i32(r_col), "r_from_p": i32(order), "r_val": torch.empty(Pp.nnz, dtype=torch.float64, device=dev),
                 "w_rowptr": i32(Wp.indptr), "w_col": i32(Wp.indices),
                 "w_val": torch.empty(Wp.nnz, dtype=torch.float64, device=dev),
-                "rho": torch.zeros(1, dtype=torch.float64, device=dev),
+                "rho": torch.zeros(ngroups if batched else 1, dtype=torch.float64, device=dev),
                 "strong": torch.as_tensor(np.ascontiguousarray(flags, dtype=np.uint8), device=dev),
             }
             if batched:

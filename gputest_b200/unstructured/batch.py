@@ -14,11 +14,12 @@ a whole outer iteration of all cases is one CUDA graph replay.
 
 Differences from running the cases one by one: the AMG hierarchy is set up for the union
 (aggregates never cross cases; coarsening stops when every case has at most ``max_coarse``
-rows, and each case's coarsest block gets its own dense inverse), and the spectral-radius
-estimate of each level's prolongation smoother is taken over all cases of the level. These
-change the preconditioner, not the converged fields. The stability guard of the single-case
-solver is off. Cases keep iterating until every case has converged (a converged case's
-residuals keep falling), and ``case_converged_at`` records when each one first passed.
+rows - a case already that small is carried to the next level unchanged - and each case's
+coarsest block gets its own dense inverse). This changes the preconditioner, not the converged
+fields. The stability guard of the single-case
+solver runs per case (its rollback and relaxation ladder, with per-case relaxation factors).
+Cases keep iterating until every case has converged (a converged case's residuals keep
+falling), and ``case_converged_at`` records when each one first passed.
 """
 
 from __future__ import annotations
@@ -74,7 +75,6 @@ class BatchSimpleSolver(MixedSimpleSolver):
         self.mu_case = np.array([float(c.viscosity) for c in cases])
         super().__init__(union_mesh(self.meshes), _union_case(cases, meshes), max_coarse=max_coarse,
                          amg_theta=amg_theta)
-        self.guard_enabled = False
         self.case_iteration = 0
         self.case_converged_at = np.full(self.ncase, -1, dtype=np.int64)
         self._res_max5_case = np.zeros(self.ncase)
@@ -147,6 +147,15 @@ class BatchSimpleSolver(MixedSimpleSolver):
         base = self.report_g.data_ptr() + ng * self.NQ * 8
         self.info_mom_g = base
         self.info_p_g = base + ng * dim * INFO_DTYPE.itemsize
+        # per-case relaxation (lowered per case by the stability guard), expanded per cell
+        self.case_relax_u = np.full(ng, float(self.case.relax_u))
+        self.case_relax_p = np.full(ng, float(self.relax_p))
+        self.case_algo = [self.case.algorithm] * ng
+        self.relax_u_c = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.relax_p_c = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.simplec_c = torch.empty(nc, dtype=torch.int32, device=dev)
+        for g in range(ng):
+            self._set_case_relax(g)
 
     def _setup_amg(self):
         import torch
@@ -160,6 +169,96 @@ class BatchSimpleSolver(MixedSimpleSolver):
                                  group_singular=self.case_singular.astype(np.int32))
         self.amg_setups += 1
         self._amg.enable_mixed(self.val_P32)
+
+    def _params(self):
+        prm = super()._params()
+        prm.relax_u_cell = self.relax_u_c.data_ptr()
+        prm.relax_p_cell = self.relax_p_c.data_ptr()
+        prm.simplec_cell = self.simplec_c.data_ptr()
+        return prm
+
+    def _set_case_relax(self, g):
+        a, b = int(self.g_cells_h[g]), int(self.g_cells_h[g + 1])
+        self.relax_u_c[a:b] = float(self.case_relax_u[g])
+        self.relax_p_c[a:b] = float(self.case_relax_p[g])
+        self.simplec_c[a:b] = int(self.case_algo[g] == "SIMPLEC")
+
+    # ------------------------------------------------------------------ stability guard per case
+    def _case_slices(self, g):
+        """Device index ranges of case g: cells, owned interior faces, boundary faces."""
+        a, b = int(self.g_cells_h[g]), int(self.g_cells_h[g + 1])
+        return (a, b), (int(self._own_ptr_h[a]), int(self._own_ptr_h[b])), (int(self._bptr_h[a]), int(self._bptr_h[b]))
+
+    def _snapshot_cases(self, cases):
+        c = self._cur
+        for g in cases:
+            (a, b), (fa, fb), (ba, bb) = self._case_slices(g)
+            self._snap_Up[:, a:b] = self._Up[c][:, a:b]
+            self._snap_F[fa:fb] = self._F[c][fa:fb]
+            self._snap_Fb[ba:bb] = self._Fb[c][ba:bb]
+            self._snap_it[g] = self.iteration
+
+    def _restore_case(self, g):
+        c = self._cur
+        (a, b), (fa, fb), (ba, bb) = self._case_slices(g)
+        self._Up[c][:, a:b] = self._snap_Up[:, a:b]
+        self._F[c][fa:fb] = self._snap_F[fa:fb]
+        self._Fb[c][ba:bb] = self._snap_Fb[ba:bb]
+        # no lagged gradients for the restored case (the single-case rollback drops them too)
+        self.gUp[:, :, a:b] = 0.0
+        self.gpf[:, a:b] = 0.0
+
+    def _reset_guard(self):
+        super()._reset_guard()
+        if not hasattr(self, "g_cells_h"):
+            return
+        ng = self.ncase
+        self._own_ptr_h = self.fv.t["own_ptr"].cpu().numpy()
+        self._bptr_h = self.fv.t["bptr"].cpu().numpy()
+        c = self._cur
+        self._snap_Up, self._snap_F, self._snap_Fb = self._Up[c].clone(), self._F[c].clone(), self._Fb[c].clone()
+        self._snap_it = np.zeros(ng, dtype=np.int64)
+        self._snap_r = np.full(ng, np.inf)
+        self._case_guard_min = np.full(ng, np.inf)
+        self.case_guard_events = [[] for _ in range(ng)]
+
+    def _case_guard(self, r, flux):
+        """``SimpleSolver._stability_guard`` per case (``simple.py:722-776``): a case whose raw
+        continuity residual is not finite or grew GUARD_GROWTH-fold over its best goes back to
+        its last snapshot with lower relaxation (pressure first, then SIMPLE with 0.3 / 0.3)."""
+        rolled = np.zeros(self.ncase, dtype=bool)
+        if not self.guard_enabled:
+            return rolled
+        ref = np.maximum(self._case_guard_min, self.GUARD_ROUNDOFF * flux)
+        bad = ~np.isfinite(r) | ((self.iteration > 10) & (r > self.GUARD_GROWTH * ref))
+        for g in np.flatnonzero(bad):
+            if self.case_relax_p[g] * self.GUARD_FACTOR >= self.GUARD_MIN_RELAX:
+                self.case_relax_p[g] *= self.GUARD_FACTOR
+            elif self.case_algo[g] == "SIMPLEC" or self.case_relax_u[g] * 0.7 >= self.GUARD_MIN_RELAX_U - 1e-12:
+                if self.case_algo[g] == "SIMPLEC":
+                    self.case_algo[g] = "SIMPLE"
+                    self.case_relax_u[g], self.case_relax_p[g] = min(self.case_relax_u[g], 0.3), 0.3
+                else:
+                    self.case_relax_u[g] *= 0.7
+            else:
+                continue
+            self._restore_case(int(g))
+            self._set_case_relax(int(g))
+            self._case_guard_min[g] = self._snap_r[g]
+            self.case_guard_events[g].append({"detected_at": self.iteration, "restored_to": int(self._snap_it[g]),
+                                              "relax_p": round(float(self.case_relax_p[g]), 4),
+                                              "relax_u": round(float(self.case_relax_u[g]), 4),
+                                              "algorithm": self.case_algo[g], "continuity": float(r[g])})
+            rolled[g] = True
+        if rolled.any():
+            self._amg_age = 10 ** 9  # a new preconditioner, as after the single-case rollback
+        ok = np.isfinite(r) & ~rolled & (self.iteration > 5)
+        self._case_guard_min[ok] = np.minimum(self._case_guard_min[ok], r[ok])
+        if self.iteration % self.GUARD_EVERY == 0:
+            snap = np.flatnonzero(ok & (r <= 2.0 * self._case_guard_min))
+            self._snapshot_cases(snap)
+            self._snap_r[snap] = r[snap]
+        return rolled
 
     # ------------------------------------------------------------------ iteration
     def _launch(self, amg_ready=False):
@@ -282,12 +381,13 @@ class BatchSimpleSolver(MixedSimpleSolver):
         flux = scal[:, self.Q_SUMF] + scal[:, self.Q_SUMFB]
         res["continuity"] = cont / np.maximum(self._res_max5_case, 1e-3 * flux)
         self._case_res = res
+        rolled = self._case_guard(cont, flux)
         mom = infos[: ng * dim]
         self.last_linear = {"momentum_iters": np.array([i.iterations for i in mom]).reshape(ng, dim),
                             "pressure_iters": np.array([i.iterations for i in infos[ng * dim: ng * (dim + 1)]]),
                             "pressure_residual": np.array([i.residual for i in infos[ng * dim: ng * (dim + 1)]])}
         worst = np.max(np.stack(list(res.values())), axis=0)
-        done = (worst < c.tol) & (self.iteration > 5)
+        done = (worst < c.tol) & (self.iteration > 5) & ~rolled
         newly = done & (self.case_converged_at < 0)
         self.case_converged_at[newly] = self.iteration
         self.converged = bool(np.all(self.case_converged_at >= 0))

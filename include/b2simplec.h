@@ -173,6 +173,11 @@ typedef struct b2s_flow_params {
   int32_t second_order;    /* bounded second-order deferred correction in momentum */
   int32_t singular_p;      /* no pressure boundary: the pressure is fixed by its mean */
   int32_t pad;
+  /* Batches (optional, NULL: the scalars above): per-cell under-relaxation and SIMPLEC flag, so
+   * that each case of a batch keeps its own (its stability guard lowers them per case). */
+  const double* relax_u_cell;
+  const double* relax_p_cell;
+  const int32_t* simplec_cell;
 } b2s_flow_params;
 
 /* Boundary values of p and U (simple.py:305-325) with lagged gradients: Up is [1+dim][nc]
@@ -270,7 +275,7 @@ typedef struct b2s_amg_level {
   const int32_t* w_rowptr;     /* W = A P, [n x nc], sorted columns */
   const int32_t* w_col;
   double* w_val;
-  double* rho;                 /* [1] spectral radius estimate (device) */
+  double* rho;                 /* [1] spectral radius estimate (device); batches: [ngroups] */
   const uint8_t* strong;       /* [nnz] strength of each entry at set-up (1: strong), or NULL */
   const int32_t* group_ptr;    /* batches: [ngroups+1] rows of each case on this level, or NULL */
 } b2s_amg_level;

@@ -87,3 +87,29 @@ def test_batch_rejects_cases_that_differ_in_shared_settings():
     cases[1].scheme = "upwind"
     with pytest.raises(ValueError):
         BatchSimpleSolver(meshes, cases)
+
+
+def test_batch_stability_guard_rolls_back_one_case_only():
+    """A case driven to divergence (planted in its state on the host side: its fluxes scaled up)
+    is rolled back and relaxed by its own guard; the other cases are untouched by it."""
+    import torch
+
+    from gputest_b200.unstructured.batch import BatchSimpleSolver
+
+    meshes, cases = _cases(tol=0.0, max_iter=100)
+    bs = BatchSimpleSolver(meshes, cases)
+    ref = BatchSimpleSolver(meshes, cases)
+    for _ in range(25):
+        bs.step()
+        ref.step()
+    (a, b), (fa, fb), _ = bs._case_slices(1)
+    bs._F[bs._cur][fa:fb] *= 1e6  # wreck case 1's mass fluxes
+    bs.step()
+    ref.step()
+    assert bs.case_guard_events[1] and not any(bs.case_guard_events[g] for g in (0, 2, 3))
+    assert bs.case_relax_p[1] < ref.case_relax_p[1]
+    for g in (0, 2, 3):
+        assert bs.case_residuals(g) == ref.case_residuals(g)
+    for _ in range(5):
+        bs.step()
+    assert np.isfinite(bs.case_residuals(1)["continuity"])
