@@ -118,6 +118,7 @@ _SIGS = {
     "b2s_bicgstab_groups_f32_d": ([ctypes.c_int, P, P, I32, ctypes.c_int, P, P, P, P, P, P, F64, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, P, P, P, I64, P, P], ctypes.c_int),
     "b2s_pcg_groups_workspace_bytes": ([P], I64),
+    "b2s_residual_vjp_d": ([P, P, F64, F64, F64, ctypes.c_int] + [P] * 18 + [P], ctypes.c_int),
     "b2s_pcg_groups_mixed_d": ([P, P, P, P, P, P, P, I32, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, F64, P, I64,
                                 P, P], ctypes.c_int),
 }

@@ -1,0 +1,512 @@
+"""Discrete adjoint of the steady SIMPLEC solution: dJ/d(Brinkman porosity, inlet velocity).
+
+The converged state of the outer iteration (``flowtrace/unstructured/simple.py:500-703``) is the
+zero of a residual R(x; theta). It is written here with the lagged and derived quantities of the
+iteration as unknowns of their own, so that every block is an explicit local function:
+
+    x = (U [nc, dim], p [nc], g [nc, dim], F [nf], Fb [nb]),  theta = (alpha [nc], ub [nb, dim])
+
+    R_m  = b - A U                   momentum (upwind + diffusion, ``simple.py:340-374``, with
+                                     the Brinkman drag alpha V on the diagonal and the pressure
+                                     force -g V, g the Green-Gauss gradient)
+    R_c  = Cdiff F + Cb Fb           continuity
+    R_g  = g - GG(p, p_b(p, g))      the pressure gradient, with the boundary pressure
+                                     reconstructed from it (``simple.py:315-325``)
+    R_F  = F - RC(U, p, g, dP)       Rhie-Chow face fluxes (``simple.py:583-613``), dP the SIMPLEC
+    R_Fb = Fb - RCb(U, p, g, dP, ub) coefficient V / (a_P / alpha_u - sum a_nb) of the momentum
+                                     matrix (which depends on F, Fb and alpha)
+
+At a converged SIMPLEC state R = 0 (the pressure correction vanishes, the lagged gradient is the
+current one). Scope: upwind convection (no deferred second-order correction) on meshes whose
+non-orthogonal terms vanish (Cartesian quads: S parallel to d, face centres on the P-N line,
+boundary offsets normal to the face), laminar, no energy; the objective is the pressure drop
+between the inlet and the outlet (area-weighted boundary pressures) plus the viscous
+dissipation sum 2 mu V |sym grad U|^2 with the least-squares velocity gradient.
+
+``TorchResidual`` is the plain-PyTorch transcription of R and J (autograd gives their exact
+derivatives; it is the check of the CUDA vector-Jacobian product ``b2s_residual_vjp_d``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Dict
+
+import numpy as np
+
+WALL, INLET = "wall", "inlet"
+
+
+def _check_scope(h, tol=1e-9):
+    scale = np.sqrt(np.abs(h.vol).max()) if h.nc else 1.0
+    if h.n_if and np.abs(h.Tvec).max() > tol * max(np.abs(h.S).max(), 1e-300):
+        raise NotImplementedError("the adjoint needs a mesh without non-orthogonal correction")
+    if h.n_if and np.abs(h.dxm).max() > tol * scale:
+        raise NotImplementedError("the adjoint needs face centres on the owner-neighbour line")
+    if h.n_bf and np.abs(h.db_t).max() > tol * scale:
+        raise NotImplementedError("the adjoint needs boundary offsets normal to the faces")
+
+
+class TorchResidual:
+    """R(x; theta) and J(x) in plain PyTorch on the reference numbering of a mesh.
+
+    ``bc`` holds the solver's boundary data on the reference boundary-face order: the masks
+    ``m_wall``, ``m_inlet``, ``m_pres``, ``m_dirvel`` and the fixed pressures ``pb_fixed``.
+    ``case`` gives density, viscosity and relax_u (the SIMPLEC coefficient uses the momentum
+    diagonal divided by it)."""
+
+    def __init__(self, host, bc: Dict[str, np.ndarray], case, relax_u=None, simplec=True, device="cpu", dtype=None,
+                 inlet_mask=None, outlet_mask=None):
+        """``relax_u`` and ``simplec`` are the solver's at convergence (its stability guard may have
+        lowered the relaxation or switched to SIMPLE); they enter through the coefficient dP."""
+        import torch
+
+        _check_scope(host)
+        if case.scheme != "upwind":
+            raise NotImplementedError("the adjoint covers scheme='upwind'")
+        if case.pressure_gradient != "green-gauss":
+            raise NotImplementedError("the adjoint covers the Green-Gauss pressure gradient")
+        dt = dtype or torch.float64
+        T = lambda a: torch.as_tensor(np.asarray(a), dtype=dt, device=device)  # noqa: E731
+        I = lambda a: torch.as_tensor(np.asarray(a, dtype=np.int64), device=device)  # noqa: E731
+        h = host
+        self.h, self.nc, self.nf, self.nb, self.dim = h, h.nc, h.n_if, h.n_bf, h.dim
+        self.P, self.N, self.Pb = I(h.P), I(h.N), I(h.Pb)
+        self.S, self.Sb, self.d, self.db = T(h.S), T(h.Sb), T(h.d), T(h.db)
+        self.w, self.alpha, self.alpha_b = T(h.w), T(h.alpha), T(h.alpha_b)
+        self.vol, self.wl, self.wlb, self.Ginv = T(h.vol), T(h.wl), T(h.wlb), T(h.Ginv)
+        self.m_wall, self.m_inlet = T(bc["m_wall"]), T(bc["m_inlet"])
+        self.m_pres, self.m_dirvel, self.pb_fixed = T(bc["m_pres"]), T(bc["m_dirvel"]), T(bc["pb_fixed"])
+        self.rho, self.mu = float(case.density), float(case.viscosity)
+        self.au = float(case.relax_u if relax_u is None else relax_u)
+        self.simplec = bool(simplec)
+        self.Sbm = T(h.Sb_mag)
+        self.inlet = T(bc["m_inlet"] if inlet_mask is None else inlet_mask)
+        self.outlet = T(bc["m_pres"] if outlet_mask is None else outlet_mask)
+        self.dt, self.device = dt, device
+
+    # ---------------------------------------------------------------- packing
+    def sizes(self):
+        nc, d = self.nc, self.dim
+        return [nc * d, nc, nc * d, self.nf, self.nb]
+
+    def split(self, v):
+        nc, d = self.nc, self.dim
+        a = np.cumsum([0] + self.sizes())
+        return (v[a[0]:a[1]].reshape(nc, d), v[a[1]:a[2]], v[a[2]:a[3]].reshape(nc, d), v[a[3]:a[4]], v[a[4]:a[5]])
+
+    def pack(self, U, p, g, F, Fb):
+        import torch
+
+        return torch.cat([U.reshape(-1), p.reshape(-1), g.reshape(-1), F.reshape(-1), Fb.reshape(-1)])
+
+    # ---------------------------------------------------------------- pieces
+    def _scatter(self, own, nei, bnd=None):
+        import torch
+
+        out = torch.zeros(self.nc, dtype=self.dt, device=self.device)
+        out = out.index_add(0, self.P, own).index_add(0, self.N, nei)
+        if bnd is not None:
+            out = out.index_add(0, self.Pb, bnd)
+        return out
+
+    def boundary_pressure(self, p, g):
+        """p_b: the fixed value on pressure faces, else p_P + g_P . d_b (``simple.py:315-325``)."""
+        pP = p[self.Pb] + (g[self.Pb] * self.db).sum(1)
+        return self.m_pres * self.pb_fixed + (1.0 - self.m_pres) * pP
+
+    def boundary_velocity(self, U, ub):
+        """u_b: the fixed value on walls and inlets, U_P on pressure faces (no tangential offset)."""
+        fixed = (self.m_wall + self.m_inlet)[:, None]
+        return fixed * ub + self.m_pres[:, None] * U[self.Pb]
+
+    def green_gauss(self, p, pb):
+        """(1/V)(Cown(pf S) - Cnei(pf S) + Cb(pb Sb)), pf the face interpolate (``fvmesh.py:288-309``)."""
+        pf = self.w * p[self.P] + (1.0 - self.w) * p[self.N]
+        v = pf[:, None] * self.S
+        out = []
+        for a in range(self.dim):
+            out.append(self._scatter(v[:, a], -v[:, a], pb * self.Sb[:, a]) / self.vol)
+        import torch
+
+        return torch.stack(out, dim=1)
+
+    def ls_gradient(self, phi, phib):
+        """Least-squares gradient (``fvmesh.py:268-286``)."""
+        import torch
+
+        dphi = (phi[self.N] - phi[self.P]) * self.wl
+        dphib = (phib - phi[self.Pb]) * self.wlb
+        r = torch.stack([self._scatter(dphi * self.d[:, a], dphi * self.d[:, a], dphib * self.db[:, a])
+                         for a in range(self.dim)], dim=1)
+        return torch.einsum("cab,cb->ca", self.Ginv, r)
+
+    def coefficients(self, F, Fb, alpha_por):
+        import torch
+
+        D = self.mu * self.alpha
+        relu = torch.relu
+        Db = self.mu * self.alpha_b * self.m_dirvel
+        diag = self._scatter(D + relu(F), D + relu(-F), Db + relu(Fb)) + alpha_por * self.vol
+        aPN, aNP = -(D + relu(-F)), -(D + relu(F))
+        sum_nb = self._scatter(-aPN, -aNP)
+        return diag, aPN, aNP, Db, sum_nb
+
+    # ---------------------------------------------------------------- R and J
+    def residual(self, x, alpha_por, ub):
+        """R(x; theta) as one vector in the block order of ``split``."""
+        import torch
+
+        U, p, g, F, Fb = self.split(x)
+        rho = self.rho
+        diag, aPN, aNP, Db, sum_nb = self.coefficients(F, Fb, alpha_por)
+        u_b = self.boundary_velocity(U, ub)
+        P, N, Pb = self.P, self.N, self.Pb
+        # momentum
+        Rm = []
+        for k in range(self.dim):
+            b = torch.zeros(self.nc, dtype=self.dt, device=self.device).index_add(0, Pb, (Db + torch.relu(-Fb)) * u_b[:, k])
+            b = b - g[:, k] * self.vol
+            AU = diag * U[:, k]
+            AU = AU.index_add(0, P, aPN * U[N, k]).index_add(0, N, aNP * U[P, k])
+            Rm.append(b - AU)
+        Rm = torch.stack(Rm, dim=1)
+        # continuity
+        Rc = self._scatter(F, -F, Fb)
+        # pressure gradient
+        pb = self.boundary_pressure(p, g)
+        Rg = g - self.green_gauss(p, pb)
+        # Rhie-Chow
+        diag_r = diag / self.au
+        denom = diag_r - sum_nb if self.simplec else diag_r
+        dP = self.vol / denom
+        dF = self.w * dP[P] + (1.0 - self.w) * dP[N]
+        uf = self.w[:, None] * U[P] + (1.0 - self.w)[:, None] * U[N]
+        gf = self.w[:, None] * g[P] + (1.0 - self.w)[:, None] * g[N]
+        RF = F - rho * ((uf * self.S).sum(1) - dF * self.alpha * (p[N] - p[P] - (gf * self.d).sum(1)))
+        fb_in = rho * (ub * self.Sb).sum(1) * self.m_inlet
+        fb_pr = rho * ((U[Pb] * self.Sb).sum(1) - dP[Pb] * self.alpha_b * (self.pb_fixed - p[Pb] - (g[Pb] * self.db).sum(1)))
+        RFb = Fb - (fb_in + fb_pr * self.m_pres)
+        return self.pack(Rm, Rc, Rg, RF, RFb)
+
+    def objective(self, x, ub):
+        """J = p_in - p_out (area-weighted mean boundary pressures) + sum 2 mu V |sym grad U|^2."""
+        import torch
+
+        U, p, g, F, Fb = self.split(x)
+        pb = self.boundary_pressure(p, g)
+        a_in, a_out = self.Sbm * self.inlet, self.Sbm * self.outlet
+        J = (pb * a_in).sum() / a_in.sum() - (pb * a_out).sum() / a_out.sum()
+        u_b = self.boundary_velocity(U, ub)
+        G = torch.stack([self.ls_gradient(U[:, k], u_b[:, k]) for k in range(self.dim)], dim=1)  # [nc, k, a]
+        E = 0.5 * (G + G.transpose(1, 2))
+        return J + (2.0 * self.mu * self.vol * (E * E).sum((1, 2))).sum()
+
+
+def state_from_oracle(o):
+    """x (reference numbering) of a converged oracle state: U, p, the Green-Gauss gradient of its
+    last iteration, F, Fb."""
+    return o.U.copy(), o.p.copy(), np.asarray(o._gp).copy(), o.F.copy(), o.Fb.copy()
+
+
+def relax_from(o):
+    """(relax_u, simplec) of a solver or the oracle at its current iteration."""
+    return float(o.relax_u), o.algo == "SIMPLEC"
+
+
+def bc_from_oracle(o):
+    return {"m_wall": o.m_wall, "m_inlet": o.m_inlet, "m_pres": o.m_pres, "m_dirvel": o.m_dirvel,
+            "pb_fixed": o.pb_fixed}
+
+
+# ================================================================================== device adjoint
+class DeviceAdjoint:
+    """The discrete adjoint of a converged ``SimpleSolver`` on the device (device numbering).
+
+    ``vjp`` applies (dR/dx)^T through the CUDA kernel ``b2s_residual_vjp_d``; ``solve`` finds
+    lambda with (dR/dx)^T lambda = dJ/dx by restarted GMRES, right-preconditioned by one sweep of
+    the transposed SIMPLE block elimination: the pressure-correction matrix (the Schur complement
+    of the flux unknowns; SA-AMG PCG of the solver's hierarchy), the flux adjoints from it, the
+    transposed momentum matrix (Jacobi-BiCGSTAB), then the gradient adjoint."""
+
+    def __init__(self, solver):
+        import torch
+
+        from .. import _lib
+
+        s = self.s = solver
+        fv = self.fv = s.fv
+        if s.energy:
+            raise NotImplementedError("the adjoint covers flows without the energy equation")
+        _check_scope(fv.host)
+        c = s._cur
+        nc, nf, nb, dim = fv.nc, fv.n_if, fv.n_bf, fv.dim
+        self.nc, self.nf, self.nb, self.dim = nc, nf, nb, dim
+        self.U = s._Up[c][1:].contiguous()
+        self.p = s._Up[c][0].contiguous()
+        self.g = s.gpf.contiguous()
+        self.F = s._F[c][: max(nf, 1)].contiguous()
+        self.Fb = s._Fb[c][: max(nb, 1)].contiguous()
+        self.sizes = [dim * nc, nc, dim * nc, nf, nb]
+        self.offs = np.cumsum([0] + self.sizes)
+        self.n = int(self.offs[-1])
+        dev = s.torch_device
+        self.work = torch.empty(4 * nc, dtype=torch.float64, device=dev)
+        self.relax_u, self.simplec = float(s.relax_u), s.algo == "SIMPLEC"
+        self.L = _lib.lib()
+        # transposed unrelaxed momentum matrix (its values through the slot maps)
+        t = fv.t
+        val = s.val_A.clone()
+        val[t["slot_diag"].long()] = s.diag
+        valT = val.clone()
+        if nf:
+            valT[t["slot_PN"].long()] = val[t["slot_NP"].long()]
+            valT[t["slot_NP"].long()] = val[t["slot_PN"].long()]
+        self.valT, self.invT = valT, 1.0 / s.diag
+        wb = self.L.b2s_bicgstab_workspace_bytes(nc, dim)
+        self.work_bicg = torch.empty(wb // 8 + 1, dtype=torch.float64, device=dev)
+        self.info = torch.zeros(4 * 16, dtype=torch.uint8, device=dev)
+        self.fP, self.fN, self.bP = t["fP"].long(), t["fN"].long(), t["bP"].long()
+        self.vjp_calls = 0
+
+    # ---------------------------------------------------------------- blocks
+    def split(self, v):
+        o, nc, dim = self.offs, self.nc, self.dim
+        return (v[o[0]:o[1]].view(dim, nc), v[o[1]:o[2]], v[o[2]:o[3]].view(dim, nc), v[o[3]:o[4]], v[o[4]:o[5]])
+
+    def vjp(self, lam, theta=False):
+        """(dR/dx)^T lam, and with theta also ((dR/dporosity)^T lam, (dR/dub)^T lam)."""
+        import torch
+
+        from .. import _lib
+
+        s, fv = self.s, self.fv
+        out = torch.empty_like(lam)
+        lm, lc, lg, lF, lFb = self.split(lam)
+        oU, op, og, oF, oFb = self.split(out)
+        opor = oub = None
+        if theta:
+            opor = torch.empty(self.nc, dtype=torch.float64, device=lam.device)
+            oub = torch.empty(self.dim, max(self.nb, 1), dtype=torch.float64, device=lam.device)
+        c = s.case
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        _lib.check(self.L.b2s_residual_vjp_d(fv.cmesh_ref, ctypes.byref(s.cbc), float(c.density), float(c.viscosity),
+                                             self.relax_u, int(self.simplec), self.U.data_ptr(), self.p.data_ptr(),
+                                             self.g.data_ptr(), self.F.data_ptr(), self.Fb.data_ptr(),
+                                             ptr(s.porosity), lm.data_ptr(), lc.data_ptr(), lg.data_ptr(),
+                                             lF.data_ptr(), lFb.data_ptr(), self.work.data_ptr(), oU.data_ptr(),
+                                             op.data_ptr(), og.data_ptr(), oF.data_ptr(), oFb.data_ptr(), ptr(opor),
+                                             ptr(oub), _lib.stream_ptr()), "b2s_residual_vjp_d")
+        self.vjp_calls += 1
+        return (out, opor, oub) if theta else out
+
+    def _vjp_blocks(self, lm=None, lF=None, lFb=None):
+        import torch
+
+        lam = torch.zeros(self.n, dtype=torch.float64, device=self.U.device)
+        b = self.split(lam)
+        if lm is not None:
+            b[0].copy_(lm)
+        if lF is not None:
+            b[3].copy_(lF)
+        if lFb is not None:
+            b[4].copy_(lFb)
+        return self.split(self.vjp(lam))
+
+    # ---------------------------------------------------------------- preconditioner
+    def precondition(self, r):
+        """Approximate solution z of (dR/dx)^T z = r by the transposed SIMPLE elimination."""
+        import torch
+
+        from .. import _lib
+
+        s = self.s
+        rU, rp, rg, rF, rFb = self.split(r)
+        # 1. continuity adjoint: Ap lc = rp - (dRF/dp)^T rF - (dRFb/dp)^T rFb
+        q = self._vjp_blocks(lF=rF, lFb=rFb)[1]
+        lc = torch.zeros_like(rp)
+        info = self.info.data_ptr()
+        s._amg.pcg((rp - q).contiguous(), lc, 1e-2, 100, s.singular_p, info)
+        # 2. flux adjoints
+        lF = rF - (lc[self.fP] - lc[self.fN]) if self.nf else rF
+        lFb = rFb - lc[self.bP] if self.nb else rFb
+        # 3. momentum adjoint: A^T lm = (dRF/dU)^T lF + (dRFb/dU)^T lFb - rU
+        t = self._vjp_blocks(lF=lF, lFb=lFb)[0]
+        rhs = (t - rU).contiguous()
+        lm = torch.zeros_like(rhs)
+        fv = self.fv
+        _lib.check(self.L.b2s_bicgstab_jacobi_d(self.nc, self.dim, fv.rowptr.data_ptr(), fv.col.data_ptr(),
+                                                self.valT.data_ptr(), rhs.data_ptr(), self.invT.data_ptr(),
+                                                lm.data_ptr(), 1e-3, 100, 1, self.work_bicg.data_ptr(),
+                                                self.work_bicg.numel() * 8, info, _lib.stream_ptr()),
+                   "b2s_bicgstab_jacobi_d")
+        # 4. gradient adjoint: lg = rg - (the other residuals' g-terms)
+        og = self._vjp_blocks(lm=lm, lF=lF, lFb=lFb)[2]
+        lg = rg - og
+        return torch.cat([lm.reshape(-1), lc, lg.reshape(-1), lF, lFb])
+
+    # ---------------------------------------------------------------- GMRES
+    def solve(self, rhs, tol=1e-11, restart=40, maxiter=2000):
+        """lambda with (dR/dx)^T lambda = rhs: right-preconditioned restarted GMRES (modified
+        Gram-Schmidt, Givens rotations). Returns (lambda, iterations, relative residual)."""
+        import torch
+
+        x = torch.zeros_like(rhs)
+        bnorm = float(torch.linalg.vector_norm(rhs))
+        if bnorm == 0.0:
+            return x, 0, 0.0
+        its, rel = 0, 1.0
+        while its < maxiter:
+            r = rhs - self.vjp(x)
+            beta = float(torch.linalg.vector_norm(r))
+            rel = beta / bnorm
+            if rel < tol:
+                break
+            V = [r / beta]
+            Z = []
+            H = np.zeros((restart + 1, restart))
+            cs, sn = np.zeros(restart), np.zeros(restart)
+            e = np.zeros(restart + 1)
+            e[0] = beta
+            k_used = 0
+            for k in range(restart):
+                z = self.precondition(V[k])
+                Z.append(z)
+                w = self.vjp(z)
+                for i in range(k + 1):
+                    H[i, k] = float(torch.dot(w, V[i]))
+                    w = w - H[i, k] * V[i]
+                H[k + 1, k] = float(torch.linalg.vector_norm(w))
+                V.append(w / H[k + 1, k] if H[k + 1, k] > 0 else w)
+                for i in range(k):
+                    a, b = H[i, k], H[i + 1, k]
+                    H[i, k], H[i + 1, k] = cs[i] * a + sn[i] * b, -sn[i] * a + cs[i] * b
+                den = np.hypot(H[k, k], H[k + 1, k])
+                cs[k], sn[k] = (H[k, k] / den, H[k + 1, k] / den) if den > 0 else (1.0, 0.0)
+                H[k, k], H[k + 1, k] = den, 0.0
+                e[k + 1], e[k] = -sn[k] * e[k], cs[k] * e[k]
+                its += 1
+                k_used = k + 1
+                rel = abs(e[k + 1]) / bnorm
+                if rel < tol or its >= maxiter:
+                    break
+            y = np.linalg.solve(np.triu(H[:k_used, :k_used]), e[:k_used])
+            for i in range(k_used):
+                x = x + float(y[i]) * Z[i]
+        r = rhs - self.vjp(x)
+        return x, its, float(torch.linalg.vector_norm(r)) / bnorm
+
+
+def objective_gradient(solver, inlet_zone, outlet_zone=None):
+    """J and its partial derivatives (reference numbering, host): dJ/dx as device blocks of the
+    adjoint's x and dJ/dub [nb, dim], by autograd of the plain-PyTorch objective."""
+    import torch
+
+    s = solver
+    h = s.fv.host
+    bc = {"m_wall": s.m_wall_h, "m_inlet": s.m_inlet_h, "m_pres": s.m_pres_h, "m_dirvel": s.m_dirvel_h,
+          "pb_fixed": s._pb_fixed_h}
+    zin = s.mesh.zone_by_name(inlet_zone)
+    inlet = (h.bzone == zin.id).astype(np.float64)
+    outlet = None
+    if outlet_zone is not None:
+        outlet = (h.bzone == s.mesh.zone_by_name(outlet_zone).id).astype(np.float64)
+    R = TorchResidual(h, bc, s.case, relax_u=s.relax_u, simplec=s.algo == "SIMPLEC", inlet_mask=inlet,
+                      outlet_mask=outlet)
+    fv = s.fv
+    c = s._cur
+    U = torch.as_tensor(fv.cells_to_host(s._Up[c][1:]))
+    p = torch.as_tensor(fv.cells_to_host(s._Up[c][0]))
+    g = torch.as_tensor(fv.cells_to_host(s.gpf))
+    F = torch.as_tensor(fv.faces_to_host(s._F[c][: h.n_if])) if h.n_if else torch.zeros(0, dtype=torch.float64)
+    Fb = torch.as_tensor(fv.bfaces_to_host(s._Fb[c][: h.n_bf])) if h.n_bf else torch.zeros(0, dtype=torch.float64)
+    with torch.enable_grad():  # also inside an autograd.Function's forward
+        x = R.pack(U, p, g, F, Fb).requires_grad_(True)
+        ub = torch.as_tensor(np.asarray(s.ub_fixed, dtype=np.float64)).requires_grad_(True)
+        J = R.objective(x, ub)
+        gx, gub = torch.autograd.grad(J, (x, ub))
+    gU, gp, gg, gF, gFb = R.split(gx)
+    parts = [fv.cells_to_device(gU.numpy()).reshape(-1), fv.cells_to_device(gp.numpy()),
+             fv.cells_to_device(gg.numpy()).reshape(-1)]
+    if h.n_if:
+        parts.append(fv.faces_to_device(gF.numpy()))
+    if h.n_bf:
+        parts.append(fv.bfaces_to_device(gFb.numpy()))
+    return float(J.detach()), torch.cat(parts), gub.numpy(), R
+
+
+def adjoint_gradient(solver, inlet_zone, outlet_zone=None, tol=1e-11):
+    """dJ/d(porosity) [nc] and dJ/d(fixed boundary velocities) [nb, dim] (reference numbering)
+    of a converged solver, with J the objective of ``TorchResidual.objective``."""
+    J, gx, gub, _ = objective_gradient(solver, inlet_zone, outlet_zone)
+    adj = DeviceAdjoint(solver)
+    lam, its, rel = adj.solve(gx, tol=tol)
+    _, opor, oub = adj.vjp(lam, theta=True)
+    fv = solver.fv
+    d_por = -fv.cells_to_host(opor)
+    d_ub = gub - fv.bfaces_to_host(oub[:, : fv.n_bf]) if fv.n_bf else gub
+    return {"J": J, "d_porosity": d_por, "d_ub": d_ub, "gmres_iterations": its, "gmres_residual": rel,
+            "vjp_calls": adj.vjp_calls}
+
+
+class PorousChannel:
+    """A steady flow whose Brinkman porosity [nc] and inlet speed are the parameters: ``solve``
+    runs the device solver to convergence (warm-started from the previous solution), ``J`` and
+    ``gradient`` are the objective and its adjoint gradient at the last solution."""
+
+    def __init__(self, mesh, case, inlet_zone, outlet_zone, solver_cls=None, direction=(1.0, 0.0)):
+        from .simple import SimpleSolver
+
+        self.mesh, self.case = mesh, case
+        self.inlet_zone, self.outlet_zone = inlet_zone, outlet_zone
+        self.solver = (solver_cls or SimpleSolver)(mesh, case)
+        self.direction = np.asarray(direction, dtype=np.float64)
+        self._state = None
+
+    def solve(self, porosity, u_in):
+        s = self.solver
+        s.set_porosity(np.asarray(porosity, dtype=np.float64))
+        n = int((s.fv.host.bzone == self.mesh.zone_by_name(self.inlet_zone).id).sum())
+        s.set_boundary_velocity(self.inlet_zone, np.tile(u_in * self.direction, (n, 1)))
+        if self._state is not None:
+            s.load_state(self._state)
+        else:
+            s.initialize({})
+        s.iteration = 0
+        s.converged = False
+        s.run()
+        if not s.converged:
+            raise RuntimeError("the flow did not converge")
+        self._state = s.state_dict()
+        return s
+
+    def J(self):
+        return objective_gradient(self.solver, self.inlet_zone, self.outlet_zone)[0]
+
+    def gradient(self, tol=1e-11):
+        """(J, dJ/dporosity [nc], dJ/du_in, solver details)."""
+        g = adjoint_gradient(self.solver, self.inlet_zone, self.outlet_zone, tol=tol)
+        inlet = self.solver.fv.host.bzone == self.mesh.zone_by_name(self.inlet_zone).id
+        d_uin = float((g["d_ub"][inlet] @ self.direction).sum())
+        return g["J"], g["d_porosity"], d_uin, g
+
+
+def porous_objective(problem: PorousChannel):
+    """A ``torch.autograd.Function`` J(porosity, u_in) of ``problem``: the forward pass solves the
+    flow, the backward pass the discrete adjoint (float64 CPU tensors, reference numbering)."""
+    import torch
+
+    class _Objective(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, porosity, u_in):
+            problem.solve(porosity.detach().cpu().numpy(), float(u_in))
+            J, d_por, d_uin, _ = problem.gradient()
+            ctx.save_for_backward(torch.as_tensor(d_por), torch.as_tensor(d_uin))
+            return torch.as_tensor(J, dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            d_por, d_uin = ctx.saved_tensors
+            return gJ * d_por, gJ * d_uin
+
+    return _Objective.apply

@@ -75,6 +75,7 @@ class BatchSimpleSolver(MixedSimpleSolver):
         self.mu_case = np.array([float(c.viscosity) for c in cases])
         super().__init__(union_mesh(self.meshes), _union_case(cases, meshes), max_coarse=max_coarse,
                          amg_theta=amg_theta)
+        self.reaggregate = False  # the batch hierarchy is set up once (aggregates per case)
         self.case_iteration = 0
         self.case_converged_at = np.full(self.ncase, -1, dtype=np.int64)
         self._res_max5_case = np.zeros(self.ncase)

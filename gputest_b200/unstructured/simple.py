@@ -150,11 +150,13 @@ class SimpleSolver:
         self._amg_age = 10 ** 9
         self.amg_rebuild = 10
         self.amg_setups = 0
-        # False: aggregates fixed at the first set-up, every numeric quantity rebuilt on the device.
-        # True: additionally redo the host set-up whenever the strength graph changed, which is what
-        # the reference does at each rebuild (it re-aggregates every time) - exact, but a host
-        # round trip of the pressure matrix per rebuild.
-        self.reaggregate = False
+        # True (the reference's behaviour: it re-aggregates at every rebuild): every numeric
+        # quantity is rebuilt on the device, and the host set-up is redone when the strength graph
+        # of some level changed since the last one (a device check; a host round trip of the
+        # pressure matrix only then). False: aggregates fixed at the first set-up - faster, but
+        # with a preconditioner the reference never builds, which on strongly varying coefficients
+        # (Brinkman porosity) can stall the outer iteration.
+        self.reaggregate = True
         self.max_coarse = int(max_coarse)
         self.amg_theta = float(amg_theta)
         self.last_linear = {}

@@ -431,6 +431,26 @@ B2S_API int b2s_pcg_groups_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, con
                                    double min_inner_tol, void* work, int64_t work_bytes, b2s_solve_info* info,
                                    b2s_stream_t s);
 
+/* ----------------------------------------------------------------------------------------- */
+/* Discrete adjoint. No counterpart in the reference (it has no derivatives).                   */
+
+/* Vector-Jacobian product of the steady residual R(x; theta) of the outer iteration with
+ * upwind convection on a mesh without non-orthogonal terms, the unknowns being
+ * x = (U [dim][nc], p [nc], g [dim][nc] the Green-Gauss pressure gradient, F [nf], Fb [nb]) and
+ * theta = (porosity [nc], the fixed boundary velocities bc->ub_fixed):
+ *   R_m = b - A U, R_c = Cdiff F + Cb Fb, R_g = g - GG(p, p_b), R_F = F - RhieChow(U, p, g, dP),
+ *   R_Fb = Fb - (inlet flux + Rhie-Chow pressure-face flux), dP = V / (a_P / relax_u - sum a_nb)
+ *   (simplec != 0) or V / (a_P / relax_u).
+ * Given lambda = (lm [dim][nc], lc [nc], lg [dim][nc], lF [nf], lFb [nb]) it writes
+ * (dR/dx)^T lambda into (oU, op, og, oF, oFb) and, when the pointers are set, (dR/dporosity)^T
+ * lambda into opor [nc] and (dR/dub)^T lambda into oub [dim][nb]. work holds 4 nc doubles. */
+B2S_API int b2s_residual_vjp_d(const b2s_mesh* m, const b2s_bc* bc, double rho, double mu, double relax_u,
+                               int simplec, const double* U, const double* p, const double* g, const double* F,
+                               const double* Fb, const double* porosity, const double* lm, const double* lc,
+                               const double* lg, const double* lF, const double* lFb, double* work, double* oU,
+                               double* op, double* og, double* oF, double* oFb, double* opor, double* oub,
+                               b2s_stream_t s);
+
 #ifdef __cplusplus
 }
 #endif

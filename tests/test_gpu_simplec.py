@@ -198,3 +198,26 @@ def test_coarse_inverse_of_every_shared_memory_size():
     fo, fs = o.fields(), s.fields()
     for k in ("x-velocity", "y-velocity", "pressure"):
         assert _rel(fs[k], fo[k]) < 1e-9, k
+
+
+def test_porous_channel_iterates_equal_oracle():
+    """Brinkman porosity (alpha V on the momentum diagonal, also in the SIMPLE coefficient) with
+    SIMPLE and fixed relaxation, the adjoint workload's setting."""
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    m = cartesian_mesh_2d(24, 8, 4.0, 1.0, names=("in", "out", "bottom", "top"))
+    case = UnstructuredCase(boundaries={"in": BoundarySpec("inlet", velocity=[1.0, 0.0]), "out": BoundarySpec("outlet"),
+                                        "bottom": BoundarySpec("wall"), "top": BoundarySpec("wall")},
+                            viscosity=1 / 200, scheme="upwind", tol=0.0, max_iter=100, algorithm="SIMPLE",
+                            relax_u=0.3, relax_p=0.3, pressure_tol=TIGHT)
+    por = 1e4 / (1 + np.exp(-8 * np.random.default_rng(0).standard_normal(m.n_cells)))
+    o = OracleSimple(m, case, porosity=por)
+    s = SimpleSolver(m, case, max_coarse=300)
+    s.set_porosity(por)
+    s.reaggregate = True
+    for it in range(40):
+        o.step()
+        s.step()
+    fo, fs = o.fields(), s.fields()
+    for k in ("x-velocity", "y-velocity", "pressure"):
+        assert _rel(fs[k], fo[k]) < 1e-9, k
