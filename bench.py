@@ -116,6 +116,80 @@ def make_batch_workload(ncase=256, seed=2, lo=1e3, hi=6.4e4):
     return meshes, cases, kinds
 
 
+def make_adjoint_workload(nx=512, ny=128, seed=3, corr=0.1):
+    """The adjoint workload: a 4 x 1 channel of nx x ny quads, Re 200 (u_in 1, viscosity 1/200),
+    upwind convection, SIMPLE with relaxation 0.3 / 0.3 (the relaxation the stability guard
+    settles on for porosity contrasts of 1e4); Brinkman porosity alpha = 1e4 sigmoid(8 g), g a
+    Gaussian random field of correlation length ``corr`` (white noise from default_rng(seed),
+    filtered by exp(-k^2 corr^2 / 2) in Fourier space, unit variance) sampled at the cell centres."""
+    import numpy as np
+
+    from gputest_b200.mesh.unstructured import cartesian_mesh_2d, compute_geometry
+    from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase
+
+    mesh = cartesian_mesh_2d(nx, ny, 4.0, 1.0, names=("in", "out", "bottom", "top"))
+    case = UnstructuredCase(boundaries={"in": BoundarySpec("inlet", velocity=[1.0, 0.0]), "out": BoundarySpec("outlet"),
+                                        "bottom": BoundarySpec("wall"), "top": BoundarySpec("wall")},
+                            viscosity=1.0 / 200.0, scheme="upwind", tol=1e-12, max_iter=200000, algorithm="SIMPLE",
+                            relax_u=0.3, relax_p=0.3)
+    rng = np.random.default_rng(seed)
+    white = rng.standard_normal((ny, nx))
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=4.0 / nx)
+    ky = 2 * np.pi * np.fft.fftfreq(ny, d=1.0 / ny)
+    K2 = ky[:, None] ** 2 + kx[None, :] ** 2
+    g = np.real(np.fft.ifft2(np.fft.fft2(white) * np.exp(-0.5 * K2 * corr ** 2)))
+    g = (g - g.mean()) / g.std()
+    xc = compute_geometry(mesh).cell_centre
+    i = np.clip((xc[:, 0] / (4.0 / nx)).astype(int), 0, nx - 1)
+    j = np.clip((xc[:, 1] / (1.0 / ny)).astype(int), 0, ny - 1)
+    por = 1e4 / (1.0 + np.exp(-8.0 * g[j, i]))
+    return mesh, case, por
+
+
+def run_adjoint(args):
+    """dJ/d(porosity) and dJ/du_in by the discrete adjoint against central differences along
+    ``args.fd_dirs`` random directions (step 1e-6; porosity directions relative to alpha)."""
+    import numpy as np
+    import torch
+
+    from gputest_b200.unstructured.adjoint import PorousChannel
+
+    mesh, case, por = make_adjoint_workload()
+    prob = PorousChannel(mesh, case, "in", "out")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    s = prob.solve(por, 1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    primal_ms, its = e0.elapsed_time(e1), s.iteration
+    t0 = time.perf_counter()
+    J, d_por, d_uin, info = prob.gradient()
+    torch.cuda.synchronize()
+    adj_s = time.perf_counter() - t0
+    rng = np.random.default_rng(11)
+    h, errs, fd_its = 1e-6, [], []
+    for _ in range(args.fd_dirs):
+        d = rng.standard_normal(por.size) * por
+        d /= np.abs(d / por).max()
+        prob.solve(por + h * d, 1.0)
+        fd_its.append(prob.solver.iteration)
+        Jp = prob.J()
+        prob.solve(por - h * d, 1.0)
+        Jm = prob.J()
+        fd = (Jp - Jm) / (2 * h)
+        errs.append(abs(float(d_por @ d) - fd) / max(abs(fd), 1e-300))
+    prob.solve(por, 1.0 + h)
+    Jp = prob.J()
+    prob.solve(por, 1.0 - h)
+    Jm = prob.J()
+    fd_u = (Jp - Jm) / (2 * h)
+    return {"J": J, "primal_ms": primal_ms, "primal_iterations": its, "adjoint_seconds": adj_s,
+            "gmres_iterations": info["gmres_iterations"], "gmres_residual": info["gmres_residual"],
+            "vjp_calls": info["vjp_calls"], "fd_rel_errors_porosity": errs, "dJ_du_in": d_uin, "fd_dJ_du_in": fd_u,
+            "fd_rel_error_u_in": abs(d_uin - fd_u) / max(abs(fd_u), 1e-300), "fd_warm_iterations": fd_its,
+            "cells": mesh.n_cells}
+
+
 # ---------------------------------------------------------------------------------- byte models
 def stage_bytes(solver, stage, step_info):
     """Algorithmic DRAM bytes of one launch of a stage: every array the stage's kernels read
@@ -454,6 +528,7 @@ def main():
     ap.add_argument("--batch-cases", type=int, default=256, help="c4: cases in the sweep")
     ap.add_argument("--batch-sample", type=int, default=24, help="c4: cases timed one at a time")
     ap.add_argument("--converge-max-iter", type=int, default=6000, help="c4: outer-iteration cap of --converge")
+    ap.add_argument("--fd-dirs", type=int, default=16, help="c5: random finite-difference directions")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -493,6 +568,26 @@ def main():
     dev = torch.cuda.current_device()
     if args.config == "c4":
         return main_batch(args, rank, world, dev)
+    if args.config == "c5":
+        r = run_adjoint(args)
+        if rank == 0:
+            worst = max(r["fd_rel_errors_porosity"] + [r["fd_rel_error_u_in"]])
+            line = {"metric": "adjoint dJ/d(porosity, u_in) max relative error vs central FD", "value": worst,
+                    "unit": "relative error", "n_gpus": world, "steps": r["primal_iterations"], "warmup": 0,
+                    "ms_per_step": r["primal_ms"] / max(r["primal_iterations"], 1), "higher_is_better": False,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                    "config": {"workload": "porous channel 4x1, 512x128 quads (65,536 cells), Re 200, Brinkman "
+                                           "alpha = 1e4 sigmoid(8 g), g a Gaussian random field (corr 0.1, seed 3), "
+                                           "J = p_in - p_out + viscous dissipation",
+                               "fd": f"{args.fd_dirs} random directions + u_in, central, step 1e-6"},
+                    "primal_cell_iters_per_s": r["cells"] * r["primal_iterations"] / (r["primal_ms"] / 1e3),
+                    "adjoint": {k: r[k] for k in ("adjoint_seconds", "gmres_iterations", "gmres_residual",
+                                                  "vjp_calls")},
+                    "dJ_du_in": r["dJ_du_in"], "fd_dJ_du_in": r["fd_dJ_du_in"],
+                    "fd_rel_errors_porosity": r["fd_rel_errors_porosity"], "J": r["J"],
+                    "gpu_launches": None}
+            print(json.dumps(line), flush=True)
+        return
     mesh, case, desc, inlet, skw = make_workload(args.config)
     Solver = MixedSimpleSolver if args.precision == "mixed" else SimpleSolver
     mk = lambda c: Solver(mesh, c, **skw)  # noqa: E731

@@ -268,6 +268,8 @@ class DeviceAdjoint:
         self.info = torch.zeros(4 * 16, dtype=torch.uint8, device=dev)
         self.fP, self.fN, self.bP = t["fP"].long(), t["fN"].long(), t["bP"].long()
         self.vjp_calls = 0
+        self.inner_tol = 1e-6  # relative tolerance of the preconditioner's pressure and momentum solves
+        self.sweeps = 1
 
     # ---------------------------------------------------------------- blocks
     def split(self, v):
@@ -315,6 +317,14 @@ class DeviceAdjoint:
 
     # ---------------------------------------------------------------- preconditioner
     def precondition(self, r):
+        """``sweeps`` steps of the stationary iteration z += M^-1 (r - (dR/dx)^T z) from z = 0, M the
+        transposed SIMPLE elimination of ``_sweep``."""
+        z = self._sweep(r)
+        for _ in range(self.sweeps - 1):
+            z = z + self._sweep(r - self.vjp(z))
+        return z
+
+    def _sweep(self, r):
         """Approximate solution z of (dR/dx)^T z = r by the transposed SIMPLE elimination."""
         import torch
 
@@ -326,7 +336,7 @@ class DeviceAdjoint:
         q = self._vjp_blocks(lF=rF, lFb=rFb)[1]
         lc = torch.zeros_like(rp)
         info = self.info.data_ptr()
-        s._amg.pcg((rp - q).contiguous(), lc, 1e-2, 100, s.singular_p, info)
+        s._amg.pcg((rp - q).contiguous(), lc, self.inner_tol, 200, s.singular_p, info)
         # 2. flux adjoints
         lF = rF - (lc[self.fP] - lc[self.fN]) if self.nf else rF
         lFb = rFb - lc[self.bP] if self.nb else rFb
@@ -337,7 +347,7 @@ class DeviceAdjoint:
         fv = self.fv
         _lib.check(self.L.b2s_bicgstab_jacobi_d(self.nc, self.dim, fv.rowptr.data_ptr(), fv.col.data_ptr(),
                                                 self.valT.data_ptr(), rhs.data_ptr(), self.invT.data_ptr(),
-                                                lm.data_ptr(), 1e-3, 100, 1, self.work_bicg.data_ptr(),
+                                                lm.data_ptr(), self.inner_tol, 200, 1, self.work_bicg.data_ptr(),
                                                 self.work_bicg.numel() * 8, info, _lib.stream_ptr()),
                    "b2s_bicgstab_jacobi_d")
         # 4. gradient adjoint: lg = rg - (the other residuals' g-terms)
@@ -346,9 +356,10 @@ class DeviceAdjoint:
         return torch.cat([lm.reshape(-1), lc, lg.reshape(-1), lF, lFb])
 
     # ---------------------------------------------------------------- GMRES
-    def solve(self, rhs, tol=1e-11, restart=40, maxiter=2000):
-        """lambda with (dR/dx)^T lambda = rhs: right-preconditioned restarted GMRES (modified
-        Gram-Schmidt, Givens rotations). Returns (lambda, iterations, relative residual)."""
+    def solve(self, rhs, tol=1e-11, restart=60, maxiter=2000, history=None):
+        """lambda with (dR/dx)^T lambda = rhs: flexible restarted GMRES (the preconditioner
+        contains inner Krylov solves; modified Gram-Schmidt, Givens rotations). Returns (lambda,
+        iterations, relative residual); ``history`` (a list) receives the residual per cycle."""
         import torch
 
         x = torch.zeros_like(rhs)
@@ -360,6 +371,8 @@ class DeviceAdjoint:
             r = rhs - self.vjp(x)
             beta = float(torch.linalg.vector_norm(r))
             rel = beta / bnorm
+            if history is not None:
+                history.append((its, rel))
             if rel < tol:
                 break
             V = [r / beta]

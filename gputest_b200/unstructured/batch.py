@@ -162,6 +162,7 @@ class BatchSimpleSolver(MixedSimpleSolver):
         import torch
 
         torch.cuda.current_stream().synchronize()
+        self._graphs.clear()  # captured iterations reference the old hierarchy's buffers
         self.val_P.copy_(self.val_P32)
         A_host = self.fv.matrix_to_host(self.val_P)
         self._amg = AMGHierarchy(A_host, self.fv.perm, self.fv.rowptr, self.fv.col, self.fv.t["slot_diag"],

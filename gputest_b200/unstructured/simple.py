@@ -373,6 +373,10 @@ class SimpleSolver:
 
     def set_porosity(self, alpha) -> None:
         """Implicit Brinkman drag: alpha_i V_i added to the momentum diagonal (None removes it)."""
+        if alpha is not None and self.porosity is not None:
+            self.porosity.copy_(self.fv.cells_to_device(np.asarray(alpha, dtype=np.float64)))
+            return
+        self._graphs.clear()  # captured iterations hold the previous buffer's address
         self.porosity = None if alpha is None else self.fv.cells_to_device(np.asarray(alpha, dtype=np.float64))
 
     def initialize(self, fields: dict) -> None:
@@ -395,6 +399,7 @@ class SimpleSolver:
 
     def set_sources(self, momentum=None, energy=None) -> None:
         """Volumetric sources (``flowtrace/unstructured/simple.py:164-182``)."""
+        self._graphs.clear()  # captured iterations hold the previous buffers' addresses
         vol = self.fv.host.vol
         self.mom_source = None if momentum is None else self.fv.cells_to_device(
             np.asarray(momentum, dtype=np.float64).reshape(self.nc, self.dim) * vol[:, None])
@@ -416,6 +421,8 @@ class SimpleSolver:
         import torch
 
         torch.cuda.current_stream().synchronize()
+        # captured iterations reference the old hierarchy's buffers, which are freed with it
+        self._graphs.clear()
         A_host = self.fv.matrix_to_host(self.val_P)
         self._amg = AMGHierarchy(A_host, self.fv.perm, self.fv.rowptr, self.fv.col, self.fv.t["slot_diag"],
                                  self.val_P, self.fv.slot_ref, singular=self.singular_p, max_coarse=self.max_coarse,
@@ -575,7 +582,7 @@ class SimpleSolver:
         return (self._cur, self._lag, self._lagT, self.relax_u, self.relax_p, self.algo,
                 None if self.porosity is None else self.porosity.data_ptr(),
                 None if self.mom_source is None else self.mom_source.data_ptr(),
-                None if self.energy_source is None else self.energy_source.data_ptr(), id(self._amg))
+                None if self.energy_source is None else self.energy_source.data_ptr(), self.amg_setups)
 
     def _launch_graph(self):
         """Replay (capturing on first use) the CUDA graph of an outer iteration that needs no
