@@ -154,7 +154,8 @@ def run_adjoint(args):
 
     from gputest_b200.unstructured.adjoint import PorousChannel
 
-    mesh, case, por = make_adjoint_workload()
+    nx, ny = (int(v) for v in args.adj_grid.split("x"))
+    mesh, case, por = make_adjoint_workload(nx, ny)
     prob = PorousChannel(mesh, case, "in", "out")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -529,6 +530,7 @@ def main():
     ap.add_argument("--batch-sample", type=int, default=24, help="c4: cases timed one at a time")
     ap.add_argument("--converge-max-iter", type=int, default=6000, help="c4: outer-iteration cap of --converge")
     ap.add_argument("--fd-dirs", type=int, default=16, help="c5: random finite-difference directions")
+    ap.add_argument("--adj-grid", default="512x128", help="c5: channel grid nx x ny")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -576,9 +578,9 @@ def main():
                     "unit": "relative error", "n_gpus": world, "steps": r["primal_iterations"], "warmup": 0,
                     "ms_per_step": r["primal_ms"] / max(r["primal_iterations"], 1), "higher_is_better": False,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                    "config": {"workload": "porous channel 4x1, 512x128 quads (65,536 cells), Re 200, Brinkman "
-                                           "alpha = 1e4 sigmoid(8 g), g a Gaussian random field (corr 0.1, seed 3), "
-                                           "J = p_in - p_out + viscous dissipation",
+                    "config": {"workload": f"porous channel 4x1, {args.adj_grid} quads ({r['cells']:,} cells), Re 200, "
+                                           "Brinkman alpha = 1e4 sigmoid(8 g), g a Gaussian random field (corr 0.1, "
+                                           "seed 3), J = p_in - p_out + viscous dissipation",
                                "fd": f"{args.fd_dirs} random directions + u_in, central, step 1e-6"},
                     "primal_cell_iters_per_s": r["cells"] * r["primal_iterations"] / (r["primal_ms"] / 1e3),
                     "adjoint": {k: r[k] for k in ("adjoint_seconds", "gmres_iterations", "gmres_residual",

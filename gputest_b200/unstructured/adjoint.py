@@ -473,6 +473,7 @@ class PorousChannel:
         self.mesh, self.case = mesh, case
         self.inlet_zone, self.outlet_zone = inlet_zone, outlet_zone
         self.solver = (solver_cls or SimpleSolver)(mesh, case)
+        self.solver.reaggregate = True  # aggregates follow the strongly varying coefficients
         self.direction = np.asarray(direction, dtype=np.float64)
         self._state = None
 

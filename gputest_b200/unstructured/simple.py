@@ -150,13 +150,14 @@ class SimpleSolver:
         self._amg_age = 10 ** 9
         self.amg_rebuild = 10
         self.amg_setups = 0
-        # True (the reference's behaviour: it re-aggregates at every rebuild): every numeric
-        # quantity is rebuilt on the device, and the host set-up is redone when the strength graph
-        # of some level changed since the last one (a device check; a host round trip of the
-        # pressure matrix only then). False: aggregates fixed at the first set-up - faster, but
-        # with a preconditioner the reference never builds, which on strongly varying coefficients
-        # (Brinkman porosity) can stall the outer iteration.
-        self.reaggregate = True
+        # False: aggregates fixed at the first set-up, every numeric quantity rebuilt on the device
+        # (no host work after the first iteration). True: the reference's behaviour (it
+        # re-aggregates at every rebuild) - the host set-up is redone whenever the strength graph
+        # of some level changed (a device check), a host round trip of the pressure matrix each
+        # time. Fixed aggregates give a preconditioner the reference never builds; on strongly
+        # varying coefficients (Brinkman porosity) that can stall the outer iteration, so
+        # porous problems (``adjoint.PorousChannel``) turn re-aggregation on.
+        self.reaggregate = False
         self.max_coarse = int(max_coarse)
         self.amg_theta = float(amg_theta)
         self.last_linear = {}

@@ -214,7 +214,7 @@ def test_porous_channel_iterates_equal_oracle():
     o = OracleSimple(m, case, porosity=por)
     s = SimpleSolver(m, case, max_coarse=300)
     s.set_porosity(por)
-    s.reaggregate = True
+    s.reaggregate = True  # the reference re-aggregates at every rebuild
     for it in range(40):
         o.step()
         s.step()
