@@ -410,6 +410,12 @@ class DeviceAdjoint:
         return x, its, float(torch.linalg.vector_norm(r)) / bnorm
 
 
+def torch_norm(v):
+    import torch
+
+    return float(torch.linalg.vector_norm(v))
+
+
 def objective_gradient(solver, inlet_zone, outlet_zone=None):
     """J and its partial derivatives (reference numbering, host): dJ/dx as device blocks of the
     adjoint's x and dJ/dub [nb, dim], by autograd of the plain-PyTorch objective."""
@@ -448,12 +454,19 @@ def objective_gradient(solver, inlet_zone, outlet_zone=None):
     return float(J.detach()), torch.cat(parts), gub.numpy(), R
 
 
-def adjoint_gradient(solver, inlet_zone, outlet_zone=None, tol=1e-11):
+def adjoint_gradient(solver, inlet_zone, outlet_zone=None, tol=1e-11, method="gmres"):
     """dJ/d(porosity) [nc] and dJ/d(fixed boundary velocities) [nb, dim] (reference numbering)
-    of a converged solver, with J the objective of ``TorchResidual.objective``."""
+    of a converged solver, with J the objective of ``TorchResidual.objective``. ``method``:
+    "gmres" (the device solve ``DeviceAdjoint.solve``) or "direct" (the Jacobian assembled from
+    compressed device VJPs and a sparse LU of its transpose on the host; Cartesian meshes)."""
     J, gx, gub, _ = objective_gradient(solver, inlet_zone, outlet_zone)
     adj = DeviceAdjoint(solver)
-    lam, its, rel = adj.solve(gx, tol=tol)
+    if method == "direct":
+        lam, _ = direct_adjoint(adj, gx)
+        its = 0
+        rel = float(torch_norm(adj.vjp(lam) - gx) / torch_norm(gx))
+    else:
+        lam, its, rel = adj.solve(gx, tol=tol)
     _, opor, oub = adj.vjp(lam, theta=True)
     fv = solver.fv
     d_por = -fv.cells_to_host(opor)
@@ -476,6 +489,7 @@ class PorousChannel:
         self.solver.reaggregate = True  # aggregates follow the strongly varying coefficients
         self.direction = np.asarray(direction, dtype=np.float64)
         self._state = None
+        self.method = "gmres"
 
     def solve(self, porosity, u_in):
         s = self.solver
@@ -497,9 +511,10 @@ class PorousChannel:
     def J(self):
         return objective_gradient(self.solver, self.inlet_zone, self.outlet_zone)[0]
 
-    def gradient(self, tol=1e-11):
-        """(J, dJ/dporosity [nc], dJ/du_in, solver details)."""
-        g = adjoint_gradient(self.solver, self.inlet_zone, self.outlet_zone, tol=tol)
+    def gradient(self, tol=1e-11, method=None):
+        """(J, dJ/dporosity [nc], dJ/du_in, solver details); ``method`` as ``adjoint_gradient``
+        (default ``self.method``)."""
+        g = adjoint_gradient(self.solver, self.inlet_zone, self.outlet_zone, tol=tol, method=method or self.method)
         inlet = self.solver.fv.host.bzone == self.mesh.zone_by_name(self.inlet_zone).id
         d_uin = float((g["d_ub"][inlet] @ self.direction).sum())
         return g["J"], g["d_porosity"], d_uin, g
@@ -524,3 +539,113 @@ def porous_objective(problem: PorousChannel):
             return gJ * d_por, gJ * d_uin
 
     return _Objective.apply
+
+
+# ================================================================================== exact Jacobian
+def grid_coordinates(xc):
+    """Integer lattice coordinates (i, j[, k]) of the cell centres of a Cartesian mesh."""
+    out = []
+    for a in range(xc.shape[1]):
+        u = np.unique(np.round(xc[:, a], 12))
+        h = np.diff(u).min() if u.size > 1 else 1.0
+        out.append(np.rint((xc[:, a] - u[0]) / h).astype(np.int64))
+    return np.stack(out, axis=1)
+
+
+def _descriptors(dim, nc, cell_ij, fP, fN, bP, Sb):
+    """Home cell and type of every entry of the adjoint's block layout (U [dim][nc], p [nc],
+    g [dim][nc], F [nf], Fb [nb]). Entries of one type have at most one per cell: interior faces
+    are typed by the owner-to-neighbour lattice step, boundary faces by their side."""
+    home, typ = [], []
+    for k in range(dim):
+        home.append(np.arange(nc))
+        typ.append(np.full(nc, k))
+    home.append(np.arange(nc))
+    typ.append(np.full(nc, dim))
+    for k in range(dim):
+        home.append(np.arange(nc))
+        typ.append(np.full(nc, dim + 1 + k))
+    base = 2 * dim + 1
+    if fP.size:
+        step = cell_ij[fN] - cell_ij[fP]
+        ax = np.argmax(np.abs(step), axis=1)
+        home.append(fP)
+        typ.append(base + ax * 2 + (step[np.arange(step.shape[0]), ax] > 0))
+    base += 2 * dim
+    if bP.size:
+        ax = np.argmax(np.abs(Sb), axis=1)
+        home.append(bP)
+        typ.append(base + ax * 2 + (Sb[np.arange(Sb.shape[0]), ax] > 0))
+    return np.concatenate(home), np.concatenate(typ)
+
+
+def assemble_jacobian(vjp, home, typ, cell_ij, n):
+    """The sparse Jacobian dR/dx from reverse products with compressed seeds. Every residual
+    depends only on unknowns whose home cells lie within two lattice steps of its own, so the rows
+    of one type whose home cells are congruent modulo 5 in every direction share no unknown: one
+    product per (type, colour) recovers all of them. ``vjp`` maps a float64 numpy vector (a
+    combination of residual rows) to the numpy vector lambda^T dR/dx."""
+    import scipy.sparse as sp
+
+    dim = cell_ij.shape[1]
+    shape = np.array([int(v) + 1 for v in cell_ij.max(axis=0)])
+    cell_at = np.full(tuple(shape), -1, dtype=np.int64)
+    cell_at[tuple(cell_ij.T)] = np.arange(cell_ij.shape[0])
+    ntype = int(typ.max()) + 1
+    flat_of = np.full((ntype, cell_ij.shape[0]), -1, dtype=np.int64)
+    flat_of[typ, home] = np.arange(n)
+    hij = cell_ij[home]
+    color = np.zeros(n, dtype=np.int64)
+    for a in range(dim):
+        color = color * 5 + hij[:, a] % 5
+    rows, cols, vals = [], [], []
+    for t in range(ntype):
+        for k in np.unique(color[typ == t]):
+            seed = (typ == t) & (color == k)
+            out = np.asarray(vjp(seed.astype(np.float64)))
+            u = np.flatnonzero(out)
+            if not u.size:
+                continue
+            ck = np.array([(k // 5 ** (dim - 1 - a)) % 5 for a in range(dim)])
+            rij = hij[u] + ((ck[None, :] - hij[u] + 2) % 5) - 2
+            ok = np.all((rij >= 0) & (rij < shape[None, :]), axis=1)
+            cell_r = np.full(u.size, -1, dtype=np.int64)
+            cell_r[ok] = cell_at[tuple(rij[ok].T)]
+            r = np.where(cell_r >= 0, flat_of[t, np.maximum(cell_r, 0)], -1)
+            keep = r >= 0
+            rows.append(r[keep])
+            cols.append(u[keep])
+            vals.append(out[u[keep]])
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+
+
+def device_jacobian(adj):
+    """dR/dx of a ``DeviceAdjoint`` in its device block layout, by compressed CUDA VJPs."""
+    import torch
+
+    fv = adj.fv
+    ij = grid_coordinates(fv.host.xc)[fv.perm]
+    t = fv.t
+    z = np.zeros(0, dtype=np.int64)
+    fP = t["fP"].cpu().numpy().astype(np.int64) if fv.n_if else z
+    fN = t["fN"].cpu().numpy().astype(np.int64) if fv.n_if else z
+    bP = t["bP"].cpu().numpy().astype(np.int64) if fv.n_bf else z
+    Sb = t["Sb"].cpu().numpy().reshape(fv.dim, -1)[:, : fv.n_bf].T if fv.n_bf else np.zeros((0, fv.dim))
+    home, typ = _descriptors(fv.dim, fv.nc, ij, fP, fN, bP, Sb)
+    dev = adj.U.device
+
+    def vjp(lam):
+        return adj.vjp(torch.as_tensor(lam, device=dev)).cpu().numpy()
+
+    return assemble_jacobian(vjp, home, typ, ij, adj.n)
+
+
+def direct_adjoint(adj, rhs):
+    """lambda with (dR/dx)^T lambda = rhs: the Jacobian assembled from compressed device VJPs,
+    then a sparse LU of its transpose on the host. Returns (lambda on rhs's device, J)."""
+    import scipy.sparse.linalg as spla
+    import torch
+
+    J = device_jacobian(adj)
+    lam = spla.splu(J.T.tocsc()).solve(rhs.detach().cpu().numpy())
+    return torch.as_tensor(lam, device=rhs.device), J

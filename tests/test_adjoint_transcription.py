@@ -84,3 +84,42 @@ def test_exact_discrete_adjoint_matches_central_differences():
         assert float(d_por @ d) == pytest.approx(fd, rel=1e-5)
     fd = (Jof(_solve(m, case, por, 1 + h, start=st)) - Jof(_solve(m, case, por, 1 - h, start=st))) / (2 * h)
     assert d_uin == pytest.approx(fd, rel=1e-5)
+
+
+def test_compressed_reverse_products_recover_the_exact_jacobian():
+    """``assemble_jacobian`` (one reverse product per residual type and lattice colour) against the
+    dense autograd Jacobian of the transcription, in the adjoint's block layout."""
+    import torch
+
+    from gputest_b200.unstructured.adjoint import _descriptors, assemble_jacobian, grid_coordinates
+
+    m, case, por = _channel()
+    o = _solve(m, case, por)
+    ru, sc = relax_from(o)
+    R = TorchResidual(o.fv, bc_from_oracle(o), case, relax_u=ru, simplec=sc)
+    h = o.fv
+    nc, dim = h.nc, h.dim
+
+    def to_ref(v):  # block layout (U [dim][nc], p, g [dim][nc], F, Fb) -> transcription layout
+        v = torch.as_tensor(v)
+        a = np.cumsum([0, dim * nc, nc, dim * nc])
+        return torch.cat([v[a[0]:a[1]].reshape(dim, nc).T.reshape(-1), v[a[1]:a[2]],
+                          v[a[2]:a[3]].reshape(dim, nc).T.reshape(-1), v[a[3]:]])
+
+    def to_blk(v):
+        U, p, g, F, Fb = R.split(v)
+        return torch.cat([U.T.reshape(-1), p, g.T.reshape(-1), F, Fb])
+
+    x = _x(R, o)
+    al, ub = torch.as_tensor(por), torch.as_tensor(o.ub_fixed)
+    xr = x.clone().requires_grad_(True)
+    r = R.residual(xr, al, ub)
+
+    def vjp(lam):
+        return to_blk(torch.autograd.grad(r, xr, to_ref(lam), retain_graph=True)[0]).numpy()
+
+    ij = grid_coordinates(h.xc)
+    home, typ = _descriptors(dim, nc, ij, h.P, h.N, h.Pb, h.Sb)
+    J = assemble_jacobian(vjp, home, typ, ij, x.numel()).toarray()
+    Jd = torch.autograd.functional.jacobian(lambda v: to_blk(R.residual(to_ref(v), al, ub)), to_blk(x)).numpy()
+    assert np.abs(J - Jd).max() <= 1e-12 * np.abs(Jd).max()
