@@ -157,16 +157,20 @@ def run_adjoint(args):
     nx, ny = (int(v) for v in args.adj_grid.split("x"))
     mesh, case, por = make_adjoint_workload(nx, ny)
     prob = PorousChannel(mesh, case, "in", "out")
+    prob.method = args.adj_method
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     s = prob.solve(por, 1.0)
     e1.record()
     torch.cuda.synchronize()
     primal_ms, its = e0.elapsed_time(e1), s.iteration
+    log = lambda *a: print("[c5]", *a, file=sys.stderr, flush=True)  # noqa: E731
+    log(f"primal: {its} iterations, {primal_ms / 1e3:.1f} s")
     t0 = time.perf_counter()
     J, d_por, d_uin, info = prob.gradient()
     torch.cuda.synchronize()
     adj_s = time.perf_counter() - t0
+    log(f"adjoint ({info['method']}): {adj_s:.1f} s, residual {info['residual']:.2e}")
     rng = np.random.default_rng(11)
     h, errs, fd_its = 1e-6, [], []
     for _ in range(args.fd_dirs):
@@ -179,13 +183,16 @@ def run_adjoint(args):
         Jm = prob.J()
         fd = (Jp - Jm) / (2 * h)
         errs.append(abs(float(d_por @ d) - fd) / max(abs(fd), 1e-300))
+        log(f"direction {len(errs)}: adjoint {float(d_por @ d):.12e} fd {fd:.12e} rel {errs[-1]:.2e}")
     prob.solve(por, 1.0 + h)
     Jp = prob.J()
     prob.solve(por, 1.0 - h)
     Jm = prob.J()
     fd_u = (Jp - Jm) / (2 * h)
     return {"J": J, "primal_ms": primal_ms, "primal_iterations": its, "adjoint_seconds": adj_s,
-            "gmres_iterations": info["gmres_iterations"], "gmres_residual": info["gmres_residual"],
+            "method": info["method"], "iterations": info["iterations"], "residual": info["residual"],
+            "direct": {k: info[k] for k in ("assemble_s", "factor_s", "solve_s", "jacobian_nnz", "lu_fill",
+                                            "residuals") if k in info},
             "vjp_calls": info["vjp_calls"], "fd_rel_errors_porosity": errs, "dJ_du_in": d_uin, "fd_dJ_du_in": fd_u,
             "fd_rel_error_u_in": abs(d_uin - fd_u) / max(abs(fd_u), 1e-300), "fd_warm_iterations": fd_its,
             "cells": mesh.n_cells}
@@ -531,6 +538,8 @@ def main():
     ap.add_argument("--converge-max-iter", type=int, default=6000, help="c4: outer-iteration cap of --converge")
     ap.add_argument("--fd-dirs", type=int, default=16, help="c5: random finite-difference directions")
     ap.add_argument("--adj-grid", default="512x128", help="c5: channel grid nx x ny")
+    ap.add_argument("--adj-method", default="direct", choices=("direct", "gmres"),
+                    help="c5: adjoint solve (sparse LU of the assembled Jacobian, or preconditioned GMRES)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -583,7 +592,7 @@ def main():
                                            "seed 3), J = p_in - p_out + viscous dissipation",
                                "fd": f"{args.fd_dirs} random directions + u_in, central, step 1e-6"},
                     "primal_cell_iters_per_s": r["cells"] * r["primal_iterations"] / (r["primal_ms"] / 1e3),
-                    "adjoint": {k: r[k] for k in ("adjoint_seconds", "gmres_iterations", "gmres_residual",
+                    "adjoint": {k: r[k] for k in ("adjoint_seconds", "method", "iterations", "residual", "direct",
                                                   "vjp_calls")},
                     "dJ_du_in": r["dJ_du_in"], "fd_dJ_du_in": r["fd_dJ_du_in"],
                     "fd_rel_errors_porosity": r["fd_rel_errors_porosity"], "J": r["J"],
