@@ -21,6 +21,7 @@ constexpr int kThreads = 256;        // ordinary kernels
 constexpr int kCoopThreads = 1024;   // cooperative kernels: one block per SM
 constexpr int kMaxCoopBlocks = 1184; // 148 SMs x 8
 constexpr int kWarps = kCoopThreads / 32;
+constexpr int kBicgVectors = 11;  // work vectors per right-hand side of the Jacobi-BiCGSTAB kernel
 
 __host__ __device__ inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
@@ -52,10 +53,11 @@ __device__ __forceinline__ void block_sum(const double (&v)[NQ], double* smem, d
     if (lane == 0) smem[warp * NQ + q] = s;
   }
   __syncthreads();
-  if (threadIdx.x < NQ) {
-    double s = 0.0;
-    for (int w = 0; w < nw; ++w) s += smem[w * NQ + threadIdx.x];
-    smem[nw * NQ + threadIdx.x] = s;
+  // warp w sums quantities w, w + nw, ... over the warp partials by a shuffle tree
+  for (int q = warp; q < NQ; q += nw) {
+    double s = lane < nw ? smem[lane * NQ + q] : 0.0;
+    s = warp_sum(s);
+    if (lane == 0) smem[nw * NQ + q] = s;
   }
   __syncthreads();
 #pragma unroll
@@ -85,13 +87,13 @@ __device__ __forceinline__ double warp_total(const double* part, int nb, int nq,
 }
 
 // Totals of nq partial sums (nb blocks each); every thread of the block gets tot[0..nq).
+// Warp w reduces quantities w, w + nwarps, ... so the totals' loads are in flight together.
 // smem must hold nq doubles.
 __device__ __forceinline__ void grid_totals(const double* part, int nb, int nq, double* smem) {
-  if (threadIdx.x < 32) {
-    for (int q = 0; q < nq; ++q) {
-      double t = warp_total(part, nb, nq, q);
-      if (threadIdx.x == 0) smem[q] = t;
-    }
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int q = warp; q < nq; q += nw) {
+    double t = warp_total(part, nb, nq, q);
+    if ((threadIdx.x & 31) == 0) smem[q] = t;
   }
   __syncthreads();
 }

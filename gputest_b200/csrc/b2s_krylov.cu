@@ -70,14 +70,17 @@ using BicgArgs = BicgArgsT<double>;
 
 enum { ACTIVE = 0, CONVERGED = 1, STOPPED = 2 };
 
-// Three grid phases per iteration (the reference's algorithm has five dependent steps):
-//   1. p = r + beta (p_old - omega v_old), h = inv p, v = A h with every neighbour's h evaluated
-//      on the fly from p_old, v_old and r (same arithmetic as storing it), r_hat.v;
-//   2. s = r - alpha v, hs = inv s, and t = A hs evaluated the same way, with s.s, t.t, t.s
+// Three grid phases per iteration (the reference's algorithm has five dependent steps). The
+// Jacobi-preconditioned vectors a neighbour's row needs are kept as u = inv r, w = inv (p - omega v)
+// and z = inv v, so that every matrix entry gathers two values:
+//   1. p = r + beta (p - omega v), h = inv p = u + beta w, v = A h with the neighbours' h
+//      formed from their u and w, z = inv v; r_hat.v;
+//   2. s = r - alpha v, hs = inv s = u - alpha z, t = A hs formed the same way; s.s, t.t, t.s
 //      (t is wasted only on the iteration where |s| converges);
-//   3. r = s - omega t, r.r, r_hat.r.
-// p and v alternate between two buffers so that neighbours read the previous iteration's values.
+//   3. r = s - omega t, u = inv r, w = inv (p - omega v); r.r, r_hat.r.
 // x gets alpha h + omega hs one phase later (after the breakdown test), as the reference does.
+// Every row reads and writes only its own p, v, h, hs, s and t; u, w and z are written in the
+// phase before the one that gathers them. Storage is T; the arithmetic is double.
 template <int NR, class T>
 __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) {
   cg::grid_group grid = cg::this_grid();
@@ -87,33 +90,34 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   double* part[2] = {a.part0, a.part1};
   int pb = 0;
-  T *r[NR], *rh[NR], *pp[2][NR], *vv[2][NR], *h[NR], *s[NR], *hs[NR], *t[NR], *x[NR];
+  T *r[NR], *rh[NR], *p[NR], *v[NR], *h[NR], *s[NR], *hs[NR], *t[NR], *u[NR], *w[NR], *z[NR], *x[NR];
   const T* b[NR];
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
-    T* w = a.work + (int64_t)10 * k * n;
-    r[k] = w;
-    rh[k] = w + n;
-    pp[0][k] = w + 2 * (int64_t)n;
-    vv[0][k] = w + 3 * (int64_t)n;
-    h[k] = w + 4 * (int64_t)n;
-    s[k] = w + 5 * (int64_t)n;
-    hs[k] = w + 6 * (int64_t)n;
-    t[k] = w + 7 * (int64_t)n;
-    pp[1][k] = w + 8 * (int64_t)n;
-    vv[1][k] = w + 9 * (int64_t)n;
+    T* wk = a.work + (int64_t)kBicgVectors * k * n;
+    r[k] = wk;
+    rh[k] = wk + n;
+    p[k] = wk + 2 * (int64_t)n;
+    v[k] = wk + 3 * (int64_t)n;
+    h[k] = wk + 4 * (int64_t)n;
+    s[k] = wk + 5 * (int64_t)n;
+    hs[k] = wk + 6 * (int64_t)n;
+    t[k] = wk + 7 * (int64_t)n;
+    u[k] = wk + 8 * (int64_t)n;
+    w[k] = wk + 9 * (int64_t)n;
+    z[k] = wk + 10 * (int64_t)n;
     x[k] = a.x + (int64_t)k * n;
     b[k] = a.b + (int64_t)k * n;
   }
   const T* inv = a.inv;
-  int cur = 0;  // p, v of the previous iteration are pp[cur], vv[cur]
-  // ---- r = b - A x, r_hat = r, p = v = 0
+  // ---- r = b - A x, r_hat = r, u = inv r, p = v = w = 0
   {
     double acc[3 * NR];
 #pragma unroll
     for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
     for (int i = gt; i < n; i += gs) {
       const int j0 = a.rowptr[i], j1 = a.rowptr[i + 1];
+      const double iv = inv[i];
       double ax[NR];
 #pragma unroll
       for (int k = 0; k < NR; ++k) ax[k] = 0.0;
@@ -131,8 +135,10 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
         if (a.zero_x0) x[k][i] = 0.0;
         r[k][i] = ri;
         rh[k][i] = ri;
-        pp[0][k][i] = 0.0;
-        vv[0][k][i] = 0.0;
+        u[k][i] = iv * ri;
+        p[k][i] = 0.0;
+        v[k][i] = 0.0;
+        w[k][i] = 0.0;
         acc[k] += ri * ri;
         acc[NR + k] += bi * bi;
       }
@@ -176,22 +182,11 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
       rho[k] = rho_new[k];
       any = true;
     }
-    // ---- phase 1: deferred x update; p, h, v = A h; r_hat.v
+    // ---- phase 1: deferred x update; p, h, v = A h, z = inv v; r_hat.v
     {
       double acc[3 * NR];
 #pragma unroll
       for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
-      T* po[NR];
-      T* vo[NR];
-      T* pn[NR];
-      T* vn[NR];
-#pragma unroll
-      for (int k = 0; k < NR; ++k) {
-        po[k] = pp[cur][k];
-        vo[k] = vv[cur][k];
-        pn[k] = pp[cur ^ 1][k];
-        vn[k] = vv[cur ^ 1][k];
-      }
       for (int i = gt; i < n; i += gs) {
         const double iv = inv[i];
 #pragma unroll
@@ -205,18 +200,17 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
         for (int j = j0; j < j1; ++j) {
           const double aij = a.val[j];
           const int c = a.col[j];
-          const double ic = inv[c];
 #pragma unroll
           for (int k = 0; k < NR; ++k)
-            if (st[k] == ACTIVE) av_[k] += aij * (ic * (r[k][c] + beta[k] * (po[k][c] - omega[k] * vo[k][c])));
+            if (st[k] == ACTIVE) av_[k] += aij * ((double)u[k][c] + beta[k] * w[k][c]);
         }
 #pragma unroll
         for (int k = 0; k < NR; ++k)
           if (st[k] == ACTIVE) {
-            const double pi = r[k][i] + beta[k] * (po[k][i] - omega[k] * vo[k][i]);
-            pn[k][i] = pi;
-            h[k][i] = iv * pi;
-            vn[k][i] = av_[k];
+            p[k][i] = r[k][i] + beta[k] * (p[k][i] - omega[k] * v[k][i]);
+            h[k][i] = (double)u[k][i] + beta[k] * w[k][i];
+            v[k][i] = av_[k];
+            z[k][i] = iv * av_[k];
             acc[k] += rh[k][i] * av_[k];
           }
       }
@@ -225,7 +219,6 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
       if (!any) break;
       grid_reduce<3 * NR>(grid, acc, red, part[pb], tot);
       pb ^= 1;
-      cur ^= 1;
     }
     any = false;
 #pragma unroll
@@ -243,16 +236,12 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
     }
     __syncthreads();
     if (!any) break;
-    // ---- phase 2: s = r - alpha v, hs = inv s, t = A hs; s.s, t.t, t.s
+    // ---- phase 2: s = r - alpha v, hs = u - alpha z, t = A hs; s.s, t.t, t.s
     {
       double acc[3 * NR];
 #pragma unroll
       for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
-      T* v[NR];
-#pragma unroll
-      for (int k = 0; k < NR; ++k) v[k] = vv[cur][k];
       for (int i = gt; i < n; i += gs) {
-        const double iv = inv[i];
         const int j0 = a.rowptr[i], j1 = a.rowptr[i + 1];
         double at[NR];
 #pragma unroll
@@ -260,17 +249,16 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
         for (int j = j0; j < j1; ++j) {
           const double aij = a.val[j];
           const int c = a.col[j];
-          const double ic = inv[c];
 #pragma unroll
           for (int k = 0; k < NR; ++k)
-            if (st[k] == ACTIVE) at[k] += aij * (ic * (r[k][c] - alpha[k] * v[k][c]));
+            if (st[k] == ACTIVE) at[k] += aij * ((double)u[k][c] - alpha[k] * z[k][c]);
         }
 #pragma unroll
         for (int k = 0; k < NR; ++k)
           if (st[k] == ACTIVE) {
             const double si = r[k][i] - alpha[k] * v[k][i];
             s[k][i] = si;
-            hs[k][i] = iv * si;
+            hs[k][i] = (double)u[k][i] - alpha[k] * z[k][i];
             t[k][i] = at[k];
             acc[k] += si * si;
             acc[NR + k] += at[k] * at[k];
@@ -296,18 +284,22 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
       any = true;
     }
     __syncthreads();
-    // ---- phase 3: r = s - omega t; r.r, r_hat.r (systems converged in phase 2 take x += alpha h)
+    // ---- phase 3: r = s - omega t, u = inv r, w = inv (p - omega v); r.r, r_hat.r (systems
+    // converged in phase 2 take x += alpha h)
     {
       double acc[3 * NR];
 #pragma unroll
       for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
       for (int i = gt; i < n; i += gs) {
+        const double iv = inv[i];
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
           if (pend_a[k]) x[k][i] = x[k][i] + alpha[k] * h[k][i];
           if (st[k] == ACTIVE) {
             const double ri = s[k][i] - omega[k] * t[k][i];
             r[k][i] = ri;
+            u[k][i] = iv * ri;
+            w[k][i] = iv * (p[k][i] - omega[k] * v[k][i]);
             acc[k] += ri * ri;
             acc[NR + k] += rh[k][i] * ri;
           }
@@ -411,42 +403,60 @@ struct PcgArgsT {
 };
 using PcgArgs = PcgArgsT<double>;
 
-// Rows of a V-cycle phase. Levels whose rows average at least kWideRow entries (the dense
-// coarse levels of 3-D hierarchies) are walked one warp per row, lanes striding the row and a
-// shuffle sum at the end; the others one thread per row in stored order.
-constexpr int kWideRow = 24;
-
+// Rows of a V-cycle phase, walked by groups of g lanes (g a power of two, 1..32): a group takes
+// a row, its lanes stride the row's entries, and an xor-shuffle tree over the group sums them.
+// A phase is latency-bound when one group walks many rows one after another, so g is the
+// largest size that still leaves at most one row per group (the phase's threads over the rows),
+// capped by the mean row length (no more lanes than entries) and raised to keep at most 32
+// entries per lane. Whole warps step through the rows together (a row index past the end
+// contributes nothing) so every lane takes part in the shuffles. The phase's thread count and
+// the warps' first thread indices are multiples of 32.
 struct Rows {
-  int first, stride, lane, step;
-  bool wide;
-  __device__ __forceinline__ Rows(bool w, int t, int n)
-      : first(w ? t >> 5 : t), stride(w ? n >> 5 : n), lane(w ? (t & 31) : 0), step(w ? 32 : 1), wide(w) {}
-  __device__ __forceinline__ double total(double s) const { return wide ? warp_sum(s) : s; }
+  int first, stride, sub, lane, g;
+  __device__ __forceinline__ Rows(int n, int64_t nnz, int t, int nthreads) {
+    const int64_t avg = n > 0 ? (nnz + n - 1) / n : 1;
+    int gg = 1;
+    while (gg < 32 && (int64_t)n * (gg * 2) <= nthreads && avg > gg) gg <<= 1;
+    while (gg < 32 && avg > 32 * (int64_t)gg) gg <<= 1;
+    g = gg;
+    const int gpw = 32 / gg;
+    first = (t >> 5) * gpw;
+    stride = (nthreads >> 5) * gpw;
+    sub = (t & 31) / gg;
+    lane = (t & 31) & (gg - 1);
+  }
+  __device__ __forceinline__ double total(double s) const {
+    for (int o = g >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+  }
   __device__ __forceinline__ bool writer() const { return lane == 0; }
 };
-
-__device__ __forceinline__ bool wide_level(int n, int64_t nnz) { return nnz >= (int64_t)kWideRow * n; }
 
 // One damped-Jacobi step y = x + (w Dinv)(b - A x); x == NULL means x = w Dinv b (fused).
 template <class T>
 __device__ __forceinline__ void jacobi_step(const b2s_amg_level& L, const LvVals<T>& V, double w, const T* b,
                                             const T* x, T* y, int gt, int gs) {
-  const Rows R(wide_level(L.n, L.nnz), gt, gs);
-  for (int i = R.first; i < L.n; i += R.stride) {
-    double s = 0.0, xi;
-    const double wd = w * V.dinv[i];
-    if (x) {
-      for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.step) s += V.val[j] * x[L.col[j]];
-      xi = x[i];
-    } else {
-      for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.step) {
-        const int c = L.col[j];
-        s += V.val[j] * ((w * V.dinv[c]) * b[c]);
+  const Rows R(L.n, L.nnz, gt, gs);
+  for (int i0 = R.first; i0 < L.n; i0 += R.stride) {
+    const int i = i0 + R.sub;
+    const bool act = i < L.n;
+    double s = 0.0;
+    if (act) {
+      if (x) {
+        for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.g) s += V.val[j] * x[L.col[j]];
+      } else {
+        for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.g) {
+          const int c = L.col[j];
+          s += V.val[j] * ((w * V.dinv[c]) * b[c]);
+        }
       }
-      xi = wd * b[i];
     }
     s = R.total(s);
-    if (R.writer()) y[i] = xi + wd * (b[i] - s);
+    if (act && R.writer()) {
+      const double wd = w * V.dinv[i];
+      const double xi = x ? (double)x[i] : wd * b[i];
+      y[i] = xi + wd * (b[i] - s);
+    }
   }
 }
 
@@ -489,23 +499,29 @@ __device__ __forceinline__ T* vdown(const PcgArgsT<T>& a, int l, const T* b, con
   ph.sync();
   T* Rv = a.lv[l].r;
   {
-    const Rows R(wide_level(lv.n, lv.nnz), ph.t, ph.n);
-    for (int i = R.first; i < lv.n; i += R.stride) {
+    const Rows R(lv.n, lv.nnz, ph.t, ph.n);
+    for (int i0 = R.first; i0 < lv.n; i0 += R.stride) {
+      const int i = i0 + R.sub;
+      const bool act = i < lv.n;
       double s = 0.0;
-      for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.step) s += V.val[j] * c[lv.col[j]];
+      if (act)
+        for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.g) s += V.val[j] * c[lv.col[j]];
       s = R.total(s);
-      if (R.writer()) Rv[i] = b[i] - s;
+      if (act && R.writer()) Rv[i] = b[i] - s;
     }
   }
   ph.sync();
   T* bn = (l + 1 < L) ? a.lv[l + 1].b : a.cb;
   {
-    const Rows R(wide_level(lv.nc, lv.p_nnz), ph.t, ph.n);
-    for (int I = R.first; I < lv.nc; I += R.stride) {
+    const Rows R(lv.nc, lv.p_nnz, ph.t, ph.n);
+    for (int I0 = R.first; I0 < lv.nc; I0 += R.stride) {
+      const int I = I0 + R.sub;
+      const bool act = I < lv.nc;
       double s = 0.0;
-      for (int j = lv.r_rowptr[I] + R.lane; j < lv.r_rowptr[I + 1]; j += R.step) s += V.r_val[j] * Rv[lv.r_col[j]];
+      if (act)
+        for (int j = lv.r_rowptr[I] + R.lane; j < lv.r_rowptr[I + 1]; j += R.g) s += V.r_val[j] * Rv[lv.r_col[j]];
       s = R.total(s);
-      if (R.writer()) bn[I] = s;
+      if (act && R.writer()) bn[I] = s;
     }
   }
   ph.sync();
@@ -526,13 +542,16 @@ __device__ __forceinline__ T* vup(const PcgArgsT<T>& a, int l, const T* b, T* c,
   const bool want = stats != nullptr;
   double acc[3] = {0.0, 0.0, 0.0};
   {
-    const Rows R(wide_level(lv.n, lv.p_nnz), ph.t, ph.n);
-    for (int i = R.first; i < lv.n; i += R.stride) {
+    const Rows R(lv.n, lv.p_nnz, ph.t, ph.n);
+    for (int i0 = R.first; i0 < lv.n; i0 += R.stride) {
+      const int i = i0 + R.sub;
+      const bool act = i < lv.n;
       double s = 0.0;
-      for (int j = lv.p_rowptr[i] + R.lane; j < lv.p_rowptr[i + 1]; j += R.step) s += V.p_val[j] * xc[lv.p_col[j]];
+      if (act)
+        for (int j = lv.p_rowptr[i] + R.lane; j < lv.p_rowptr[i + 1]; j += R.g) s += V.p_val[j] * xc[lv.p_col[j]];
       s = R.total(s);
-      const double zi = c[i] + s;
-      if (R.writer()) {
+      if (act && R.writer()) {
+        const double zi = c[i] + s;
         c[i] = zi;
         if (want && h.sweeps == 0) {
           acc[0] += zi;
@@ -542,16 +561,19 @@ __device__ __forceinline__ T* vup(const PcgArgsT<T>& a, int l, const T* b, T* c,
       }
     }
   }
-  const Rows R(wide_level(lv.n, lv.nnz), ph.t, ph.n);
+  const Rows R(lv.n, lv.nnz, ph.t, ph.n);
   for (int sw = 0; sw < h.sweeps; ++sw) {
     ph.sync();
     const bool last = sw + 1 == h.sweeps;
-    for (int i = R.first; i < lv.n; i += R.stride) {
+    for (int i0 = R.first; i0 < lv.n; i0 += R.stride) {
+      const int i = i0 + R.sub;
+      const bool act = i < lv.n;
       double s = 0.0;
-      for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.step) s += V.val[j] * c[lv.col[j]];
+      if (act)
+        for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.g) s += V.val[j] * c[lv.col[j]];
       s = R.total(s);
-      const double zi = c[i] + (w * V.dinv[i]) * (b[i] - s);
-      if (R.writer()) {
+      if (act && R.writer()) {
+        const double zi = c[i] + (w * V.dinv[i]) * (b[i] - s);
         o[i] = zi;
         if (want && last) {
           acc[0] += zi;
@@ -1024,7 +1046,7 @@ int b2s_spmv_d(int32_t n, int k, const int32_t* rowptr, const int32_t* col, cons
 
 int64_t b2s_bicgstab_workspace_bytes(int32_t n, int nrhs) {
   if (n <= 0 || nrhs < 1 || nrhs > 3) return -1;
-  return (int64_t)sizeof(double) * ((int64_t)10 * nrhs * n + (int64_t)2 * kMaxCoopBlocks * 3 * nrhs);
+  return (int64_t)sizeof(double) * ((int64_t)kBicgVectors * nrhs * n + (int64_t)2 * kMaxCoopBlocks * 3 * nrhs);
 }
 
 int b2s_bicgstab_jacobi_d(int32_t n, int nrhs, const int32_t* rowptr, const int32_t* col, const double* val,
@@ -1049,7 +1071,7 @@ int b2s_bicgstab_jacobi_d(int32_t n, int nrhs, const int32_t* rowptr, const int3
   a.rel = relative_to_initial ? 1 : 0;
   a.zero_x0 = 0;
   a.work = (double*)work;
-  a.part0 = a.work + (int64_t)10 * nrhs * n;
+  a.part0 = a.work + (int64_t)kBicgVectors * nrhs * n;
   a.part1 = a.part0 + (int64_t)kMaxCoopBlocks * 3 * nrhs;
   a.info = info;
   a.out64 = nullptr;
@@ -1059,7 +1081,7 @@ int b2s_bicgstab_jacobi_d(int32_t n, int nrhs, const int32_t* rowptr, const int3
 
 int64_t b2s_bicgstab_f32_workspace_bytes(int32_t n, int nrhs) {
   if (n <= 0 || nrhs < 1 || nrhs > 3) return -1;
-  return (int64_t)sizeof(float) * ((int64_t)10 * nrhs * n) + (int64_t)sizeof(double) * 2 * kMaxCoopBlocks * 3 * nrhs;
+  return (int64_t)sizeof(float) * ((int64_t)kBicgVectors * nrhs * n) + (int64_t)sizeof(double) * 2 * kMaxCoopBlocks * 3 * nrhs;
 }
 
 int b2s_bicgstab_jacobi_f32_d(int32_t n, int nrhs, const int32_t* rowptr, const int32_t* col, const float* val,
@@ -1084,7 +1106,7 @@ int b2s_bicgstab_jacobi_f32_d(int32_t n, int nrhs, const int32_t* rowptr, const 
   a.rel = relative_to_initial ? 1 : 0;
   a.zero_x0 = zero_x0 ? 1 : 0;
   a.work = (float*)work;
-  a.part0 = (double*)((char*)work + sizeof(float) * (int64_t)10 * nrhs * n);
+  a.part0 = (double*)((char*)work + sizeof(float) * (int64_t)kBicgVectors * nrhs * n);
   a.part1 = a.part0 + (int64_t)kMaxCoopBlocks * 3 * nrhs;
   a.info = info;
   a.out64 = out64;

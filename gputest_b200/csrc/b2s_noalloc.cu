@@ -15,7 +15,7 @@
 // device (make that first call before any stream capture). Every call on a device shares the
 // one array, so calls that overlap on the GPU (concurrent streams, or several host threads)
 // race on it: serialise them. The solve initialises every scratch value it reads before reading
-// it (r, r_hat, p and v are set in its first phase, the rest are written before use), so the
+// it (r, r_hat, u, p, v and w are set in its first phase, the rest are written before use), so the
 // contents left by the previous call do not matter.
 #include <mutex>
 
@@ -24,7 +24,7 @@
 namespace {
 
 constexpr int64_t kScratchDoubles =
-    (int64_t)10 * B2S_NOALLOC_MAX_UNKNOWNS + (int64_t)2 * b2s::kMaxCoopBlocks * 3 * 3;
+    (int64_t)b2s::kBicgVectors * B2S_NOALLOC_MAX_UNKNOWNS + (int64_t)2 * b2s::kMaxCoopBlocks * 3 * 3;
 
 __device__ __align__(256) double g_bicgstab_scratch[kScratchDoubles];
 
