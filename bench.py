@@ -620,17 +620,21 @@ def main():
         s.step()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     launches0 = s.kernel_launches
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    ev = []
     infos = []
     smi, smi_fh = (sample_clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
                    if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else sample_clocks(f"/tmp/clocks_rank{rank}.csv"))
-    barrier()
-    for k in range(K):
+
+    def before():  # L2 flush between timed iterations, outside their events
         flush.zero_()
-        ev[k][0].record()
-        s.step()
-        ev[k][1].record()
-        infos.append(dict(s.last_linear))
+        ev.append((torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)))
+        ev[-1][0].record()
+
+    def after():
+        ev[-1][1].record()
+
+    barrier()
+    s.run(max_steps=K, hooks=(before, after, lambda: infos.append(dict(s.last_linear))))
     barrier()
     if smi is not None:
         smi.terminate()
@@ -682,8 +686,7 @@ def main():
     s2 = mk(run_case)
     if inlet is not None:
         inlet(s2)
-    for _ in range(W + K):
-        s2.step()
+    s2.run(max_steps=W + K)
     f = s2.fields()
     e1.record()
     torch.cuda.synchronize()

@@ -44,6 +44,29 @@ __device__ __forceinline__ void grid_reduce(cg::grid_group& grid, const double (
   grid_totals(part, gridDim.x, NQ, tot);
 }
 
+// Entries of a row issued as one straight-line block (predicated on the row's length) before
+// the rest are walked in a loop: their loads are in flight together.
+constexpr int kRowUnroll = 8;
+
+// Rows [0, n) of a grid phase, one thread per row: emit(i, s) with s[k] the sum over row i's
+// entries j of entry(j, k). Each row's first kRowUnroll entries are issued as one straight-line
+// block so that their loads are in flight together; the sums keep the entries' stored order.
+template <int NR, class Entry, class Emit>
+__device__ __forceinline__ void walk_rows_nr(int n, int gt, int gs, const int32_t* __restrict__ rowptr, Entry entry,
+                                             Emit emit) {
+  for (int i = gt; i < n; i += gs) {
+    const int ja = rowptr[i], jae = rowptr[i + 1];
+    double sa[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) sa[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < kRowUnroll; ++k)
+      if (ja + k < jae) entry(ja + k, sa);
+    for (int j = ja + kRowUnroll; j < jae; ++j) entry(j, sa);
+    emit(i, sa);
+  }
+}
+
 // ---------------------------------------------------------------------------------- BiCGSTAB
 // T is the storage type of the matrix values and the vectors (double, or float for the
 // mixed-precision path); scalars and every reduction are accumulated in double.
@@ -187,32 +210,36 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
       double acc[3 * NR];
 #pragma unroll
       for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
-      for (int i = gt; i < n; i += gs) {
-        const double iv = inv[i];
+      auto xupd = [&](int i) {
 #pragma unroll
         for (int k = 0; k < NR; ++k)
           if (pend[k]) x[k][i] = (x[k][i] + alpha[k] * h[k][i]) + omega[k] * hs[k][i];
-        if (!any) continue;
-        const int j0 = a.rowptr[i], j1 = a.rowptr[i + 1];
-        double av_[NR];
+      };
+      if (!any) {
+        for (int i = gt; i < n; i += gs) xupd(i);
+      } else {
+        walk_rows_nr<NR>(
+            n, gt, gs, a.rowptr,
+            [&](int j, double (&sv)[NR]) {
+              const double aij = a.val[j];
+              const int c = a.col[j];
 #pragma unroll
-        for (int k = 0; k < NR; ++k) av_[k] = 0.0;
-        for (int j = j0; j < j1; ++j) {
-          const double aij = a.val[j];
-          const int c = a.col[j];
+              for (int k = 0; k < NR; ++k)
+                if (st[k] == ACTIVE) sv[k] += aij * ((double)u[k][c] + beta[k] * w[k][c]);
+            },
+            [&](int i, const double (&av_)[NR]) {
+              xupd(i);
+              const double iv = inv[i];
 #pragma unroll
-          for (int k = 0; k < NR; ++k)
-            if (st[k] == ACTIVE) av_[k] += aij * ((double)u[k][c] + beta[k] * w[k][c]);
-        }
-#pragma unroll
-        for (int k = 0; k < NR; ++k)
-          if (st[k] == ACTIVE) {
-            p[k][i] = r[k][i] + beta[k] * (p[k][i] - omega[k] * v[k][i]);
-            h[k][i] = (double)u[k][i] + beta[k] * w[k][i];
-            v[k][i] = av_[k];
-            z[k][i] = iv * av_[k];
-            acc[k] += rh[k][i] * av_[k];
-          }
+              for (int k = 0; k < NR; ++k)
+                if (st[k] == ACTIVE) {
+                  p[k][i] = r[k][i] + beta[k] * (p[k][i] - omega[k] * v[k][i]);
+                  h[k][i] = (double)u[k][i] + beta[k] * w[k][i];
+                  v[k][i] = av_[k];
+                  z[k][i] = iv * av_[k];
+                  acc[k] += rh[k][i] * av_[k];
+                }
+            });
       }
 #pragma unroll
       for (int k = 0; k < NR; ++k) pend[k] = false;
@@ -241,30 +268,28 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
       double acc[3 * NR];
 #pragma unroll
       for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
-      for (int i = gt; i < n; i += gs) {
-        const int j0 = a.rowptr[i], j1 = a.rowptr[i + 1];
-        double at[NR];
+      walk_rows_nr<NR>(
+          n, gt, gs, a.rowptr,
+          [&](int j, double (&sv)[NR]) {
+            const double aij = a.val[j];
+            const int c = a.col[j];
 #pragma unroll
-        for (int k = 0; k < NR; ++k) at[k] = 0.0;
-        for (int j = j0; j < j1; ++j) {
-          const double aij = a.val[j];
-          const int c = a.col[j];
+            for (int k = 0; k < NR; ++k)
+              if (st[k] == ACTIVE) sv[k] += aij * ((double)u[k][c] - alpha[k] * z[k][c]);
+          },
+          [&](int i, const double (&at)[NR]) {
 #pragma unroll
-          for (int k = 0; k < NR; ++k)
-            if (st[k] == ACTIVE) at[k] += aij * ((double)u[k][c] - alpha[k] * z[k][c]);
-        }
-#pragma unroll
-        for (int k = 0; k < NR; ++k)
-          if (st[k] == ACTIVE) {
-            const double si = r[k][i] - alpha[k] * v[k][i];
-            s[k][i] = si;
-            hs[k][i] = (double)u[k][i] - alpha[k] * z[k][i];
-            t[k][i] = at[k];
-            acc[k] += si * si;
-            acc[NR + k] += at[k] * at[k];
-            acc[2 * NR + k] += at[k] * si;
-          }
-      }
+            for (int k = 0; k < NR; ++k)
+              if (st[k] == ACTIVE) {
+                const double si = r[k][i] - alpha[k] * v[k][i];
+                s[k][i] = si;
+                hs[k][i] = (double)u[k][i] - alpha[k] * z[k][i];
+                t[k][i] = at[k];
+                acc[k] += si * si;
+                acc[NR + k] += at[k] * at[k];
+                acc[2 * NR + k] += at[k] * si;
+              }
+          });
       grid_reduce<3 * NR>(grid, acc, red, part[pb], tot);
       pb ^= 1;
     }
@@ -432,31 +457,66 @@ struct Rows {
   __device__ __forceinline__ bool writer() const { return lane == 0; }
 };
 
+// The rows [0, n) of a phase: emit(i, sum over row i's entries j of entry(j)). With one lane per
+// row and more rows than lanes, two rows are walked together, the first kRowUnroll entries of
+// both in one straight-line block, so that both rows' loads are in flight at once; each row's
+// sum keeps the entries' stored order, and every lane emits its rows in increasing order.
+template <class Entry, class Emit>
+__device__ __forceinline__ void walk_rows(const Rows& R, int n, const int32_t* __restrict__ rowptr, Entry entry,
+                                          Emit emit) {
+  if (R.g == 1 && n > R.stride) {
+    for (int i0 = R.first; i0 < n; i0 += 2 * R.stride) {
+      const int ia = i0 + R.sub, ib = ia + R.stride;
+      int ja = 0, jae = 0, jb = 0, jbe = 0;
+      if (ia < n) {
+        ja = rowptr[ia];
+        jae = rowptr[ia + 1];
+      }
+      if (ib < n) {
+        jb = rowptr[ib];
+        jbe = rowptr[ib + 1];
+      }
+      double sa = 0.0, sb = 0.0;
+#pragma unroll
+      for (int k = 0; k < kRowUnroll; ++k) {
+        if (ja + k < jae) sa += entry(ja + k);
+        if (jb + k < jbe) sb += entry(jb + k);
+      }
+      for (int j = ja + kRowUnroll; j < jae; ++j) sa += entry(j);
+      for (int j = jb + kRowUnroll; j < jbe; ++j) sb += entry(j);
+      if (ia < n) emit(ia, sa);
+      if (ib < n) emit(ib, sb);
+    }
+  } else {
+    for (int i0 = R.first; i0 < n; i0 += R.stride) {
+      const int i = i0 + R.sub;
+      const bool act = i < n;
+      double s = 0.0;
+      if (act)
+        for (int j = rowptr[i] + R.lane; j < rowptr[i + 1]; j += R.g) s += entry(j);
+      s = R.total(s);
+      if (act && R.writer()) emit(i, s);
+    }
+  }
+}
+
 // One damped-Jacobi step y = x + (w Dinv)(b - A x); x == NULL means x = w Dinv b (fused).
 template <class T>
 __device__ __forceinline__ void jacobi_step(const b2s_amg_level& L, const LvVals<T>& V, double w, const T* b,
                                             const T* x, T* y, int gt, int gs) {
   const Rows R(L.n, L.nnz, gt, gs);
-  for (int i0 = R.first; i0 < L.n; i0 += R.stride) {
-    const int i = i0 + R.sub;
-    const bool act = i < L.n;
-    double s = 0.0;
-    if (act) {
-      if (x) {
-        for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.g) s += V.val[j] * x[L.col[j]];
-      } else {
-        for (int j = L.rowptr[i] + R.lane; j < L.rowptr[i + 1]; j += R.g) {
-          const int c = L.col[j];
-          s += V.val[j] * ((w * V.dinv[c]) * b[c]);
-        }
-      }
-    }
-    s = R.total(s);
-    if (act && R.writer()) {
-      const double wd = w * V.dinv[i];
-      const double xi = x ? (double)x[i] : wd * b[i];
-      y[i] = xi + wd * (b[i] - s);
-    }
+  auto emit = [&](int i, double s) {
+    const double wd = w * V.dinv[i];
+    const double xi = x ? (double)x[i] : wd * b[i];
+    y[i] = xi + wd * (b[i] - s);
+  };
+  if (x) {
+    walk_rows(R, L.n, L.rowptr, [&](int j) { return (double)V.val[j] * x[L.col[j]]; }, emit);
+  } else {
+    walk_rows(R, L.n, L.rowptr, [&](int j) {
+      const int c = L.col[j];
+      return (double)V.val[j] * ((w * V.dinv[c]) * b[c]);
+    }, emit);
   }
 }
 
@@ -498,32 +558,12 @@ __device__ __forceinline__ T* vdown(const PcgArgsT<T>& a, int l, const T* b, con
   }
   ph.sync();
   T* Rv = a.lv[l].r;
-  {
-    const Rows R(lv.n, lv.nnz, ph.t, ph.n);
-    for (int i0 = R.first; i0 < lv.n; i0 += R.stride) {
-      const int i = i0 + R.sub;
-      const bool act = i < lv.n;
-      double s = 0.0;
-      if (act)
-        for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.g) s += V.val[j] * c[lv.col[j]];
-      s = R.total(s);
-      if (act && R.writer()) Rv[i] = b[i] - s;
-    }
-  }
+  walk_rows(Rows(lv.n, lv.nnz, ph.t, ph.n), lv.n, lv.rowptr,
+            [&](int j) { return (double)V.val[j] * c[lv.col[j]]; }, [&](int i, double s) { Rv[i] = b[i] - s; });
   ph.sync();
   T* bn = (l + 1 < L) ? a.lv[l + 1].b : a.cb;
-  {
-    const Rows R(lv.nc, lv.p_nnz, ph.t, ph.n);
-    for (int I0 = R.first; I0 < lv.nc; I0 += R.stride) {
-      const int I = I0 + R.sub;
-      const bool act = I < lv.nc;
-      double s = 0.0;
-      if (act)
-        for (int j = lv.r_rowptr[I] + R.lane; j < lv.r_rowptr[I + 1]; j += R.g) s += V.r_val[j] * Rv[lv.r_col[j]];
-      s = R.total(s);
-      if (act && R.writer()) bn[I] = s;
-    }
-  }
+  walk_rows(Rows(lv.nc, lv.p_nnz, ph.t, ph.n), lv.nc, lv.r_rowptr,
+            [&](int j) { return (double)V.r_val[j] * Rv[lv.r_col[j]]; }, [&](int I, double s) { bn[I] = s; });
   ph.sync();
   return c;
 }
@@ -541,47 +581,31 @@ __device__ __forceinline__ T* vup(const PcgArgsT<T>& a, int l, const T* b, T* c,
   T* o = (c == a.lv[l].x) ? a.lv[l].y : a.lv[l].x;
   const bool want = stats != nullptr;
   double acc[3] = {0.0, 0.0, 0.0};
-  {
-    const Rows R(lv.n, lv.p_nnz, ph.t, ph.n);
-    for (int i0 = R.first; i0 < lv.n; i0 += R.stride) {
-      const int i = i0 + R.sub;
-      const bool act = i < lv.n;
-      double s = 0.0;
-      if (act)
-        for (int j = lv.p_rowptr[i] + R.lane; j < lv.p_rowptr[i + 1]; j += R.g) s += V.p_val[j] * xc[lv.p_col[j]];
-      s = R.total(s);
-      if (act && R.writer()) {
-        const double zi = c[i] + s;
-        c[i] = zi;
-        if (want && h.sweeps == 0) {
-          acc[0] += zi;
-          acc[1] += rr[i] * zi;
-          acc[2] += rr[i];
-        }
-      }
-    }
-  }
+  walk_rows(Rows(lv.n, lv.p_nnz, ph.t, ph.n), lv.n, lv.p_rowptr,
+            [&](int j) { return (double)V.p_val[j] * xc[lv.p_col[j]]; },
+            [&](int i, double s) {
+              const double zi = c[i] + s;
+              c[i] = zi;
+              if (want && h.sweeps == 0) {
+                acc[0] += zi;
+                acc[1] += rr[i] * zi;
+                acc[2] += rr[i];
+              }
+            });
   const Rows R(lv.n, lv.nnz, ph.t, ph.n);
   for (int sw = 0; sw < h.sweeps; ++sw) {
     ph.sync();
     const bool last = sw + 1 == h.sweeps;
-    for (int i0 = R.first; i0 < lv.n; i0 += R.stride) {
-      const int i = i0 + R.sub;
-      const bool act = i < lv.n;
-      double s = 0.0;
-      if (act)
-        for (int j = lv.rowptr[i] + R.lane; j < lv.rowptr[i + 1]; j += R.g) s += V.val[j] * c[lv.col[j]];
-      s = R.total(s);
-      if (act && R.writer()) {
-        const double zi = c[i] + (w * V.dinv[i]) * (b[i] - s);
-        o[i] = zi;
-        if (want && last) {
-          acc[0] += zi;
-          acc[1] += rr[i] * zi;
-          acc[2] += rr[i];
-        }
-      }
-    }
+    walk_rows(R, lv.n, lv.rowptr, [&](int j) { return (double)V.val[j] * c[lv.col[j]]; },
+              [&](int i, double s) {
+                const double zi = c[i] + (w * V.dinv[i]) * (b[i] - s);
+                o[i] = zi;
+                if (want && last) {
+                  acc[0] += zi;
+                  acc[1] += rr[i] * zi;
+                  acc[2] += rr[i];
+                }
+              });
     T* tmp = c;
     c = o;
     o = tmp;
@@ -776,18 +800,19 @@ __device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const 
     const T* po = pbuf[pc ^ 1];
     {
       double acc[2] = {0.0, 0.0};
-      for (int i = gt; i < n; i += gs) {
-        double s = 0.0;
-        for (int j = a.rowptr[i]; j < a.rowptr[i + 1]; ++j) {
-          const int c = a.col[j];
-          const double pj = first ? z[c] - zm : (z[c] - zm) + beta * po[c];
-          s += a.val[j] * pj;
-        }
-        const double pi = first ? z[i] - zm : (z[i] - zm) + beta * po[i];
-        pn[i] = pi;
-        q[i] = s;
-        acc[0] += pi * s;
-      }
+      walk_rows_nr<1>(
+          n, gt, gs, a.rowptr,
+          [&](int j, double (&sv)[1]) {
+            const int c = a.col[j];
+            const double pj = first ? z[c] - zm : (z[c] - zm) + beta * po[c];
+            sv[0] += a.val[j] * pj;
+          },
+          [&](int i, const double (&sv)[1]) {
+            const double pi = first ? z[i] - zm : (z[i] - zm) + beta * po[i];
+            pn[i] = pi;
+            q[i] = sv[0];
+            acc[0] += pi * sv[0];
+          });
       grid_reduce<2>(grid, acc, red, part[pb], tot);
       pb ^= 1;
     }

@@ -395,6 +395,23 @@ class BatchSimpleSolver(MixedSimpleSolver):
         self.converged = bool(np.all(self.case_converged_at >= 0))
         return 1.0
 
+    def run(self, max_steps=None, hooks=None) -> int:
+        """Step until every case converged or ``max_iter`` (or ``max_steps``), one iteration at a
+        time (the per-case guard reads each iteration's report before the next one starts).
+        ``hooks`` as ``SimpleSolver.run``."""
+        before, after, done = (tuple(hooks) + (None,) * 3)[:3] if hooks is not None else (None, None, None)
+        n = 0
+        while not self.finished and (max_steps is None or n < max_steps):
+            if before:
+                before()
+            self.step()
+            if after:
+                after()
+            if done:
+                done()
+            n += 1
+        return n
+
     @property
     def finished(self) -> bool:
         return self.converged or self.iteration >= self.case.max_iter

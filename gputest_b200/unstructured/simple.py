@@ -284,7 +284,12 @@ class SimpleSolver:
         self.q_of = torch.arange(self.NQ, dtype=torch.int32, device=dev)
         ninfo = dim + 2
         self.report = torch.zeros(self.NQ * 8 + ninfo * INFO_DTYPE.itemsize, dtype=torch.uint8, device=dev)
-        self.report_host = torch.zeros_like(self.report, device="cpu").pin_memory()
+        # two pinned host copies of the report, each with the event that marks its copy done, so
+        # that run() can enqueue the next iteration while the host reads this one's report
+        self.report_hosts = [torch.zeros_like(self.report, device="cpu").pin_memory() for _ in range(2)]
+        self.report_host = self.report_hosts[0]
+        self._rep_events = [torch.cuda.Event() for _ in range(2)]
+        self._rep_slot = 0
         self.scal = self.report[: self.NQ * 8].view(torch.float64)
         base = self.report.data_ptr() + self.NQ * 8
         self.info_mom = base
@@ -567,14 +572,22 @@ class SimpleSolver:
                                            self.work_bicg.data_ptr(), self.work_bicg.numel() * 8, self.info_T, s),
                    "b2s_bicgstab_jacobi_d")
 
-    def _read_report(self):
-        import torch
-
+    def _queue_report(self) -> int:
+        """Enqueue the copy of the report into the next pinned host buffer; returns its slot."""
+        slot = self._rep_slot
+        self._rep_slot ^= 1
+        self.report_host = self.report_hosts[slot]
         self.report_host.copy_(self.report, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        self._rep_events[slot].record()
+        return slot
+
+    def _read_report(self, slot=None):
+        if slot is None:
+            slot = self._queue_report()
+        self._rep_events[slot].synchronize()
         if self._events:
             self._resolve_stage_events()
-        raw = self.report_host.numpy()
+        raw = self.report_hosts[slot].numpy()
         scal = raw[: self.NQ * 8].view(np.float64).copy()
         infos = read_info(raw[self.NQ * 8:])
         return scal, infos
@@ -606,14 +619,35 @@ class SimpleSolver:
         self._amg_age += 1
         return old, new
 
-    def step(self) -> float:
-        """One outer iteration (``flowtrace/unstructured/simple.py:500-703``)."""
-        if self.finished:
-            return 0.0
-        self._capture = None
-        c, dim = self.case, self.dim
+    def _lagged(self):
+        """Buffers an iteration overwrites in place and the next one reads (lagged gradients)."""
+        out = [self.gUp]
+        if self.case.pressure_gradient == "green-gauss":
+            out.append(self.gpf)
+        if self.energy and getattr(self, "gT", None) is not None:
+            out.append(self.gT)
+        return out
+
+    def _save_lagged(self):
+        if getattr(self, "_lag_bak", None) is None:
+            self._lag_bak = [t.clone() for t in self._lagged()]
+        else:
+            for b, t in zip(self._lag_bak, self._lagged()):
+                b.copy_(t)
+
+    def _restore_lagged(self):
+        for b, t in zip(self._lag_bak, self._lagged()):
+            t.copy_(b)
+
+    def _graph_ready(self) -> bool:
+        """The next iteration replays a CUDA graph: no AMG rebuild is due and no host work."""
         rebuild_due = self._amg is None or self._amg_age >= self.amg_rebuild
-        if self.use_graphs and not rebuild_due and self._lag and not self.profile_stages:
+        return self.use_graphs and not rebuild_due and self._lag and not self.profile_stages
+
+    def _enqueue_iteration(self):
+        """Enqueue one outer iteration and the copy of its report; the state pointer moves to the
+        iteration's output. Returns (old, new, report slot)."""
+        if self._graph_ready():
             try:
                 old, new = self._launch_graph()
             except RuntimeError:
@@ -622,7 +656,23 @@ class SimpleSolver:
                 old, new = self._launch()
         else:
             old, new = self._launch()
-        scal, infos = self._read_report()
+        slot = self._queue_report()
+        self._cur = new
+        return old, new, slot
+
+    def step(self) -> float:
+        """One outer iteration (``flowtrace/unstructured/simple.py:500-703``)."""
+        if self.finished:
+            return 0.0
+        self._capture = None
+        return self._finish_iteration(self._enqueue_iteration())
+
+    def _finish_iteration(self, ticket) -> float:
+        """Read an enqueued iteration's report (waiting for it) and apply the host side of the
+        iteration: residuals, the stability guard and the convergence test."""
+        old, new, slot = ticket
+        c, dim = self.case, self.dim
+        scal, infos = self._read_report(slot)
         self._cur = new
         mom_info, p_info = infos[:dim], infos[dim]
         res = {}
@@ -659,12 +709,58 @@ class SimpleSolver:
             self.converged = True
         return 1.0
 
-    def run(self, max_steps=None) -> int:
-        """Step until finished (or ``max_steps``); returns the number of steps taken."""
+    def run(self, max_steps=None, hooks=None) -> int:
+        """Step until finished (or ``max_steps``); returns the number of steps taken.
+
+        The same iterates as calling ``step()`` that many times, pipelined: while the host reads
+        iteration k's report (residuals, guard, convergence), iteration k+1 is already enqueued
+        when it is a graph replay (no AMG rebuild or other host work due). If iteration k ends
+        the run (converged, or a guard roll-back) the enqueued k+1 is discarded: its output went
+        to a state buffer that is not the current one, and the lagged gradients it overwrote in
+        place are put back from a device copy taken before it was enqueued (a guard roll-back
+        drops the lagged terms anyway). No iteration past ``max_steps`` or the case's
+        ``max_iter`` is enqueued. ``hooks`` = (before, after[, done]): callables run around the
+        enqueueing of each iteration (e.g. to record CUDA events) and after the host side of
+        each kept iteration."""
+        before, after, done = (tuple(hooks) + (None,) * 3)[:3] if hooks is not None else (None, None, None)
+
+        def enqueue():
+            if before:
+                before()
+            self._capture = None
+            t = self._enqueue_iteration()
+            if after:
+                after()
+            return t
+
         n = 0
+        ticket = None
         while not self.finished and (max_steps is None or n < max_steps):
-            self.step()
+            if ticket is None:
+                ticket = enqueue()
+            nxt = None
+            more = (max_steps is None or n + 1 < max_steps) and self.iteration + 1 < self.case.max_iter
+            if more and self._graph_ready():
+                age = self._amg_age
+                self._save_lagged()
+                nxt = enqueue()
+            guard_before = len(getattr(self, "guard_events", []))
+            self._finish_iteration(ticket)
             n += 1
+            if done:
+                done()
+            stop = self.finished or (max_steps is not None and n >= max_steps)
+            rolled = len(getattr(self, "guard_events", [])) != guard_before
+            if nxt is not None and (stop or rolled):
+                # discard the speculative iteration: the state stays where iteration k (or the
+                # guard's restore, which drops the lagged terms) left it
+                if not rolled:
+                    self._amg_age = age
+                    self._restore_lagged()
+                nxt = None
+            elif nxt is not None:
+                self._cur = nxt[1]
+            ticket = nxt
         return n
 
     # ------------------------------------------------------------------ guard and state
