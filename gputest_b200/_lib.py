@@ -13,7 +13,7 @@ from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "csrc", "libb2simplec.so")
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 B2S_OK = 0
 _ERRORS = {-1: "invalid argument", -2: "kernel launch failed", -3: "work space too small", -4: "no usable CUDA device",
@@ -53,7 +53,8 @@ class AmgLevel(ctypes.Structure):
     _fields_ = [("n", I32), ("nnz", I32), ("nc", I32), ("p_nnz", I32), ("w_nnz", I32)] + [
         (name, P) for name in ("rowptr", "col", "val", "diag_slot", "dinv", "agg", "tval", "x0", "p_rowptr", "p_col",
                                "p_val", "r_rowptr", "r_col", "r_from_p", "r_val", "w_rowptr", "w_col", "w_val", "rho",
-                               "strong", "group_ptr")]
+                               "strong", "group_ptr", "p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te",
+                               "c_ts")] + [("c_nnz", I32), ("pad_", I32)]
 
 
 class Amg32(ctypes.Structure):

@@ -175,6 +175,41 @@ __global__ void pvals_k(b2s_amg_level L, int ngroups) {
   }
 }
 
+// The same P from the level's term lists: thread per row, each slot's terms in list order (the
+// order pvals_k adds them), no search.
+__global__ void pvals_terms_k(b2s_amg_level L) {
+  const double c = (4.0 / 3.0) / *L.rho;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+    const double di = L.dinv[i];
+    const int ai = L.agg[i];
+    for (int s = L.p_rowptr[i]; s < L.p_rowptr[i + 1]; ++s) {
+      const int J = L.p_col[s];
+      const double tJ = L.tval[J];
+      double acc = 0.0;
+      for (int t = L.p_tptr[s]; t < L.p_tptr[s + 1]; ++t) acc += (di * L.val[L.p_tj[t]]) * tJ;
+      L.p_val[s] = ((J == ai) ? tJ : 0.0) - c * acc;
+    }
+  }
+}
+
+// W = A P from the term lists: thread per W entry, terms in the order wvals_k adds them.
+__global__ void wvals_terms_k(b2s_amg_level L) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.w_nnz; s += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int t = L.w_tptr[s]; t < L.w_tptr[s + 1]; ++t) acc += L.val[L.w_tj[t]] * L.p_val[L.w_te[t]];
+    L.w_val[s] = acc;
+  }
+}
+
+// A_c = R W from the term lists: thread per A_c entry, terms in R-entry order (as acvals_k).
+__global__ void acvals_terms_k(b2s_amg_level L, double* __restrict__ cval) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.c_nnz; s += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int t = L.c_tptr[s]; t < L.c_tptr[s + 1]; ++t) acc += L.r_val[L.c_te[t]] * L.w_val[L.c_ts[t]];
+    cval[s] = acc;
+  }
+}
+
 __global__ void rvals_k(b2s_amg_level L) {
   const int nnz = L.p_nnz;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x)
@@ -442,15 +477,21 @@ int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stre
       if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
         return B2S_ERR_LAUNCH;
     }
-    pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L, h->ngroups);
+    const bool terms = h->ngroups == 0 && L.p_tptr && L.p_tj && L.w_tptr && L.w_tj && L.w_te;
+    if (terms) pvals_terms_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+    else pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L, h->ngroups);
     rvals_k<<<grid_for(L.p_nnz), kThreads, 0, st>>>(L);
-    wvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+    if (terms) wvals_terms_k<<<grid_for(L.w_nnz), kThreads, 0, st>>>(L);
+    else wvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
     B2S_LAUNCH_CHECK();
     const bool last = l + 1 == h->nlevels;
     const int32_t* crow = last ? h->coarse_rowptr : h->levels[l + 1].rowptr;
     const int32_t* ccol = last ? h->coarse_col : h->levels[l + 1].col;
     double* cval = last ? h->coarse_val : h->levels[l + 1].val;
-    acvals_k<<<(unsigned)cdiv(L.nc, kGalWarps), kGalWarps * 32, 0, st>>>(L, crow, ccol, cval);
+    if (terms && L.c_tptr && L.c_te && L.c_ts && L.c_nnz > 0)
+      acvals_terms_k<<<grid_for(L.c_nnz), kThreads, 0, st>>>(L, cval);
+    else
+      acvals_k<<<(unsigned)cdiv(L.nc, kGalWarps), kGalWarps * 32, 0, st>>>(L, crow, ccol, cval);
     B2S_LAUNCH_CHECK();
   }
   if (h->ngroups > 0) {  // one dense block per case, each at most kSmemCoarse rows (checked at set-up)

@@ -76,6 +76,64 @@ def _pattern(M) -> sp.csr_matrix:
     return M
 
 
+TERM_CAP = 1 << 26  # largest term list built per product (larger products keep the row-owned kernel)
+
+
+def _expand(ptr, idx):
+    """For each i in idx, the positions ptr[i] .. ptr[i+1]-1, concatenated; with the index of
+    the idx entry each position came from."""
+    lens = (ptr[idx + 1] - ptr[idx]).astype(np.int64)
+    src = np.repeat(np.arange(idx.size, dtype=np.int64), lens)
+    start = np.repeat(ptr[idx].astype(np.int64) - (np.cumsum(lens) - lens), lens)
+    return src, start + np.arange(int(lens.sum()), dtype=np.int64)
+
+
+def _slot_lists(slot, nslot):
+    """Stable grouping of terms (in generation order) by output slot: (ptr, term order)."""
+    order = np.argsort(slot, kind="stable")
+    ptr = np.concatenate([[0], np.cumsum(np.bincount(slot, minlength=nslot))])
+    return ptr, order
+
+
+def term_lists(rp, cl, agg, na, Pp, Wp, Cp, r_col, r_rowptr, cap=TERM_CAP):
+    """Term lists of P, W = A P and A_c = R W on fixed patterns (see ``b2s_amg_level``): for
+    every output slot, the terms in the order the row-owned kernels add them (A entries in
+    stored order; then P entries in sorted order; R entries in R order, each W row once).
+    (rp, cl): the level's CSR in stored order; agg: aggregate of each row; Pp, Wp, Cp: sorted
+    patterns; r_col, r_rowptr: R = P^T. Returns a dict of int32 arrays; the A_c lists are left
+    out (None) when they would exceed ``cap`` terms."""
+    n = rp.size - 1
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
+    cl = cl.astype(np.int64)
+    out = {}
+    # P: A entry j of row i -> slot (i, agg[col j])
+    pkeys = np.repeat(np.arange(n, dtype=np.int64), np.diff(Pp.indptr)) * na + Pp.indices
+    sp_ = np.searchsorted(pkeys, rows * na + agg[cl])
+    out["p_tptr"], out["p_tj"] = _slot_lists(sp_, Pp.nnz)
+    # W: (A entry j, P entry e of row col j) -> slot (row j, col e)
+    wkeys = np.repeat(np.arange(n, dtype=np.int64), np.diff(Wp.indptr)) * na + Wp.indices
+    jj, e = _expand(Pp.indptr.astype(np.int64), cl)
+    if e.size > cap:
+        return None
+    sw = np.searchsorted(wkeys, rows[jj] * na + Pp.indices[e])
+    ptr, order = _slot_lists(sw, Wp.nnz)
+    out["w_tptr"], out["w_tj"], out["w_te"] = ptr, jj[order], e[order]
+    # A_c: (R entry q of coarse row I, W entry s of row r_col[q]) -> slot (I, col s)
+    nr = r_col.size
+    qrow = np.repeat(np.arange(r_rowptr.size - 1, dtype=np.int64), np.diff(r_rowptr))
+    lens = np.diff(Wp.indptr)[r_col]
+    if int(lens.sum()) > cap:
+        out["c_tptr"] = out["c_te"] = out["c_ts"] = None
+    else:
+        ckeys = np.repeat(np.arange(Cp.shape[0], dtype=np.int64), np.diff(Cp.indptr)) * na + Cp.indices
+        q, s_ = _expand(Wp.indptr.astype(np.int64), np.asarray(r_col, dtype=np.int64))
+        sc = np.searchsorted(ckeys, qrow[q] * na + Wp.indices[s_])
+        ptr, order = _slot_lists(sc, Cp.nnz)
+        out["c_tptr"], out["c_te"], out["c_ts"] = ptr, q[order], s_[order]
+        assert q.size == 0 or q.max() < nr
+    return out
+
+
 class AMGHierarchy:
     """Fixed-pattern SA-AMG hierarchy whose numeric part lives on the device.
 
@@ -166,6 +224,7 @@ class AMGHierarchy:
         rp = np.asarray(rowptr.cpu().numpy(), dtype=np.int64)
         cl = np.asarray(col.cpu().numpy(), dtype=np.int64)
         Apat = sp.csr_matrix((np.ones(cl.size), cl, rp), shape=(n0, n0))
+        lv_rp, lv_cl = rp, cl  # the current level's CSR in stored order
         # the hierarchy's own copy of the level-0 values: like the reference's preconditioner
         # object, the V-cycle keeps the matrix of the last rebuild until the next one
         self.src_val = val
@@ -218,12 +277,20 @@ class AMGHierarchy:
             if batched:
                 bufs["group_ptr"] = i32(np.concatenate([[0], np.cumsum(np.bincount(level_groups[l],
                                                                                     minlength=ngroups))]))
+            else:
+                tl = term_lists(lv_rp, lv_cl, agg_l.astype(np.int64), na, Pp, Wp, Cp, r_col, r_rowptr)
+                if tl is not None:
+                    for k, v in tl.items():
+                        if v is not None:
+                            bufs[k] = i32(v)
+                    L.c_nnz = Cp.nnz
             for k, v in bufs.items():
                 setattr(L, k, v.data_ptr())
             self._keep.append(bufs)
             self.sizes.append(n)
             # next level: pattern Cp in aggregate numbering
             Apat = Cp
+            lv_rp, lv_cl = Cp.indptr.astype(np.int64), Cp.indices.astype(np.int64)
             level_rowptr, level_col = i32(Cp.indptr), i32(Cp.indices)
             level_val = torch.empty(Cp.nnz, dtype=torch.float64, device=dev)
             rows = np.repeat(np.arange(Cp.shape[0]), np.diff(Cp.indptr))

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define B2S_ABI_VERSION 2
+#define B2S_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define B2S_API __attribute__((visibility("default")))
@@ -278,6 +278,23 @@ typedef struct b2s_amg_level {
   double* rho;                 /* [1] spectral radius estimate (device); batches: [ngroups] */
   const uint8_t* strong;       /* [nnz] strength of each entry at set-up (1: strong), or NULL */
   const int32_t* group_ptr;    /* batches: [ngroups+1] rows of each case on this level, or NULL */
+  /* Optional term lists of the fixed-pattern products (single systems; NULL: the row-owned
+   * kernels locate each term's slot by binary search). The terms of slot s are t in
+   * [x_tptr[s], x_tptr[s+1]), listed in the order the row-owned kernels add them, so both give
+   * the same values bit for bit:
+   *   P slot s (row i):  sum_t (dinv_i a[p_tj[t]]) tval[col]       (A entries of row i)
+   *   W slot s:          sum_t a[w_tj[t]] p[w_te[t]]               (A entry, P entry)
+   *   A_c slot s:        sum_t r[c_te[t]] w[c_ts[t]]               (R entry, W entry) */
+  const int32_t* p_tptr;       /* [p_nnz+1] */
+  const int32_t* p_tj;         /* [nnz] */
+  const int32_t* w_tptr;       /* [w_nnz+1] */
+  const int32_t* w_tj;
+  const int32_t* w_te;
+  const int32_t* c_tptr;       /* [c_nnz+1], or NULL (the warp-per-row Galerkin kernel) */
+  const int32_t* c_te;
+  const int32_t* c_ts;
+  int32_t c_nnz;               /* entries of the next level's matrix */
+  int32_t pad_;
 } b2s_amg_level;
 
 typedef struct b2s_amg {

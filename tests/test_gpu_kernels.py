@@ -157,3 +157,52 @@ def test_amg_vcycle_and_pcg_match_the_reference_hierarchy(torch_cuda, name):
         assert np.abs(Ap @ fv.cells_to_host(x) - b).max() <= 10 * tol * np.abs(b).max() + 1e-14
         if i.iterations == ir.iterations:
             assert _rel(fv.cells_to_host(x), xr) < 1e-6
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_amg_term_list_rebuild_equals_the_row_owned_rebuild(dim):
+    """The rebuild from the set-up's term lists (thread per P row / W entry / A_c entry) gives
+    the same hierarchy bit for bit as the row-owned kernels that locate each term's slot by
+    binary search (selected by clearing the term-list pointers)."""
+    import torch
+
+    from gputest_b200.mesh.unstructured import box_mesh_3d, cartesian_mesh_2d
+    from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    if dim == 2:
+        mesh = cartesian_mesh_2d(48, 48, triangulate=True, jitter=0.2)
+        top = [1.0, 0.0]
+    else:
+        mesh = box_mesh_3d(16, 12, 10, jitter=0.1, seed=1, names=("wall", "wall", "wall", "top", "wall", "wall"))
+        top = [1.0, 0.0, 0.0]
+    case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=top), "wall": BoundarySpec("wall")},
+                            viscosity=0.01, max_iter=10, tol=0.0)
+    s = SimpleSolver(mesh, case, amg_theta=0.0)
+    for _ in range(3):
+        s.step()
+    amg, h = s._amg, s._amg.c
+    assert h.nlevels >= 2 and all(h.levels[l].p_tptr and h.levels[l].w_tptr for l in range(h.nlevels))
+    assert h.levels[0].c_tptr
+    bufs = [b for b in amg._keep if "p_val" in b]
+    nxt = [b["val"] for b in amg._keep if "diag" in b]
+
+    def values():
+        torch.cuda.synchronize()
+        out = [t.clone() for b in bufs for t in (b["p_val"], b["w_val"], b["rho"])]
+        return out + [t.clone() for t in nxt] + [amg.coarse_inv.clone()]
+
+    amg.rebuild()
+    a = values()
+    names = ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te", "c_ts")
+    saved = [[getattr(h.levels[l], k) for k in names] for l in range(h.nlevels)]
+    for l in range(h.nlevels):
+        for k in names:
+            setattr(h.levels[l], k, None)
+    amg.rebuild()
+    b = values()
+    for l in range(h.nlevels):
+        for k, v in zip(names, saved[l]):
+            setattr(h.levels[l], k, v)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)

@@ -176,3 +176,78 @@ def test_union_mesh_keeps_every_case_and_its_geometry():
     assert np.all(np.diff(gd) >= 0)
     # no interior face joins two cases
     assert np.all(g[fv.host.P] == g[fv.host.N])
+
+
+def test_amg_term_lists_reproduce_the_row_owned_products_bit_for_bit():
+    """The term lists of P, W = A P and A_c = R W (``linalg.amg.term_lists``), summed slot by
+    slot in list order, equal the row-owned products of the rebuild kernels (pvals_k, wvals_k,
+    acvals_k, restated here as loops) exactly, on a random pattern with unsorted stored rows."""
+    import scipy.sparse as sp
+
+    from gputest_b200.linalg.amg import _pattern, term_lists
+
+    rng = np.random.default_rng(4)
+    n, na = 80, 17
+    M = sp.random(n, n, density=0.06, random_state=5) + sp.eye(n)
+    M = sp.csr_matrix(M + M.T)
+    rp, cl = M.indptr.astype(np.int64), M.indices.astype(np.int64).copy()
+    for i in range(n):  # stored order within rows need not be sorted
+        seg = cl[rp[i]:rp[i + 1]]
+        cl[rp[i]:rp[i + 1]] = seg[rng.permutation(seg.size)]
+    agg = rng.integers(0, na, n)
+    agg[:na] = np.arange(na)
+    Apat = sp.csr_matrix((np.ones(cl.size), cl, rp), shape=(n, n))
+    T = sp.csr_matrix((np.ones(n), (np.arange(n), agg)), shape=(n, na))
+    Pp = _pattern(_pattern(Apat) @ T)
+    Wp = _pattern(_pattern(Apat) @ Pp)
+    Cp = _pattern(Pp.T.tocsr() @ Wp)
+    prow = np.repeat(np.arange(n), np.diff(Pp.indptr))
+    order = np.lexsort((prow, Pp.indices))
+    r_col = prow[order]
+    r_rowptr = np.concatenate([[0], np.cumsum(np.bincount(Pp.indices, minlength=na))])
+    a, dinv, tval = rng.standard_normal(cl.size), 1 / (1 + rng.random(n)), 1 / np.sqrt(1 + rng.random(na))
+    c = 4.0 / 3.0 / 1.7
+    # row-owned products in the kernels' order
+    p = np.zeros(Pp.nnz)
+    for i in range(n):
+        p0, p1 = Pp.indptr[i], Pp.indptr[i + 1]
+        for j in range(rp[i], rp[i + 1]):
+            J = agg[cl[j]]
+            s = p0 + int(np.searchsorted(Pp.indices[p0:p1], J))
+            p[s] += (dinv[i] * a[j]) * tval[J]
+        for s in range(p0, p1):
+            J = Pp.indices[s]
+            p[s] = (tval[J] if J == agg[i] else 0.0) - c * p[s]
+    w = np.zeros(Wp.nnz)
+    for i in range(n):
+        w0, w1 = Wp.indptr[i], Wp.indptr[i + 1]
+        for j in range(rp[i], rp[i + 1]):
+            k = cl[j]
+            for e in range(Pp.indptr[k], Pp.indptr[k + 1]):
+                s = w0 + int(np.searchsorted(Wp.indices[w0:w1], Pp.indices[e]))
+                w[s] += a[j] * p[e]
+    r = p[order]
+    ac = np.zeros(Cp.nnz)
+    for I in range(na):
+        c0, c1 = Cp.indptr[I], Cp.indptr[I + 1]
+        for q in range(r_rowptr[I], r_rowptr[I + 1]):
+            i = r_col[q]
+            for s in range(Wp.indptr[i], Wp.indptr[i + 1]):
+                t = c0 + int(np.searchsorted(Cp.indices[c0:c1], Wp.indices[s]))
+                ac[t] += r[q] * w[s]
+    # the same from the term lists
+    tl = term_lists(rp, cl, agg, na, Pp, Wp, Cp, r_col, r_rowptr)
+    p2 = np.empty(Pp.nnz)
+    for i in range(n):
+        for s in range(Pp.indptr[i], Pp.indptr[i + 1]):
+            J = Pp.indices[s]
+            acc = 0.0
+            for t in range(tl["p_tptr"][s], tl["p_tptr"][s + 1]):
+                acc += (dinv[i] * a[tl["p_tj"][t]]) * tval[J]
+            p2[s] = (tval[J] if J == agg[i] else 0.0) - c * acc
+    w2 = np.array([sum((a[tl["w_tj"][t]] * p2[tl["w_te"][t]] for t in range(tl["w_tptr"][s], tl["w_tptr"][s + 1])),
+                       0.0) for s in range(Wp.nnz)])
+    ac2 = np.array([sum((r[tl["c_te"][t]] * w2[tl["c_ts"][t]] for t in range(tl["c_tptr"][s], tl["c_tptr"][s + 1])),
+                        0.0) for s in range(Cp.nnz)])
+    assert np.array_equal(p, p2) and np.array_equal(w, w2) and np.array_equal(ac, ac2)
+    assert tl["c_tptr"][-1] == sum(np.diff(Wp.indptr)[r_col])
