@@ -328,23 +328,24 @@ __device__ __forceinline__ void gj_inverse(int n, int r0, const int32_t* __restr
   }
   // In-place Gauss-Jordan inversion. The coarse matrix is symmetric positive definite (a
   // Galerkin product of the SPD pressure-correction matrix, shifted when singular), so no
-  // pivoting is needed. Step k copies pivot row and column, then updates every entry at once:
-  //   M[k][k] = 1/p, M[k][c] = M[k][c]/p, M[r][k] = -M[r][k]/p, M[r][c] -= M[r][k] M[k][c]/p.
+  // pivoting is needed. Step k copies the pivot column and the pivot row scaled by 1/p (one
+  // division per step), then updates every entry at once:
+  //   M[k][k] = 1/p, M[k][c] = M[k][c]/p, M[r][k] = -M[r][k]/p, M[r][c] -= M[r][k] (M[k][c]/p).
   for (int k = 0; k < n; ++k) {
+    const double rp = 1.0 / M[(int64_t)k * n + k];
     for (int i = tid; i < n; i += nt) {
-      rowk[i] = M[(int64_t)k * n + i];
+      rowk[i] = M[(int64_t)k * n + i] * rp;
       colk[i] = M[(int64_t)i * n + k];
     }
     __syncthreads();
-    const double piv = rowk[k];
     for (int r = tid >> 5; r < n; r += nt >> 5) {  // rows over warps, columns over lanes
       double* Mr = M + (int64_t)r * n;
       const double cr = colk[r];
       for (int c = tid & 31; c < n; c += 32) {
         double v;
-        if (r == k) v = (c == k) ? 1.0 / piv : rowk[c] / piv;
-        else if (c == k) v = -cr / piv;
-        else v = Mr[c] - cr * (rowk[c] / piv);
+        if (r == k) v = (c == k) ? rp : rowk[c];
+        else if (c == k) v = -cr * rp;
+        else v = Mr[c] - cr * rowk[c];
         Mr[c] = v;
       }
     }

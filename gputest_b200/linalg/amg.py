@@ -81,56 +81,72 @@ TERM_CAP = 1 << 26  # largest term list built per product (larger products keep 
 
 def _expand(ptr, idx):
     """For each i in idx, the positions ptr[i] .. ptr[i+1]-1, concatenated; with the index of
-    the idx entry each position came from."""
-    lens = (ptr[idx + 1] - ptr[idx]).astype(np.int64)
-    src = np.repeat(np.arange(idx.size, dtype=np.int64), lens)
-    start = np.repeat(ptr[idx].astype(np.int64) - (np.cumsum(lens) - lens), lens)
-    return src, start + np.arange(int(lens.sum()), dtype=np.int64)
+    the idx entry each position came from (int64 torch tensors on one device)."""
+    import torch
+
+    lens = ptr[idx + 1] - ptr[idx]
+    src = torch.repeat_interleave(torch.arange(idx.numel(), device=idx.device), lens)
+    start = torch.repeat_interleave(ptr[idx] - (torch.cumsum(lens, 0) - lens), lens)
+    return src, start + torch.arange(src.numel(), device=idx.device)
 
 
 def _slot_lists(slot, nslot):
     """Stable grouping of terms (in generation order) by output slot: (ptr, term order)."""
-    order = np.argsort(slot, kind="stable")
-    ptr = np.concatenate([[0], np.cumsum(np.bincount(slot, minlength=nslot))])
+    import torch
+
+    order = torch.sort(slot, stable=True).indices
+    ptr = torch.zeros(nslot + 1, dtype=torch.int64, device=slot.device)
+    ptr[1:] = torch.cumsum(torch.bincount(slot, minlength=nslot), 0)
     return ptr, order
 
 
-def term_lists(rp, cl, agg, na, Pp, Wp, Cp, r_col, r_rowptr, cap=TERM_CAP):
+def _row_keys(indptr, indices, ncols):
+    """row * ncols + column of every stored entry of a CSR pattern (sorted when the pattern is)."""
+    import torch
+
+    rows = torch.repeat_interleave(torch.arange(indptr.numel() - 1, device=indptr.device), indptr[1:] - indptr[:-1])
+    return rows * ncols + indices
+
+
+def term_lists(rp, cl, agg, na, Pp, Wp, Cp, r_col, r_rowptr, cap=TERM_CAP, device="cpu"):
     """Term lists of P, W = A P and A_c = R W on fixed patterns (see ``b2s_amg_level``): for
     every output slot, the terms in the order the row-owned kernels add them (A entries in
     stored order; then P entries in sorted order; R entries in R order, each W row once).
     (rp, cl): the level's CSR in stored order; agg: aggregate of each row; Pp, Wp, Cp: sorted
-    patterns; r_col, r_rowptr: R = P^T. Returns a dict of int32 arrays; the A_c lists are left
-    out (None) when they would exceed ``cap`` terms."""
-    n = rp.size - 1
-    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
-    cl = cl.astype(np.int64)
+    scipy patterns; r_col, r_rowptr: R = P^T. Computed with torch on ``device`` (sorts and
+    searches on the GPU at set-up); returns a dict of int32 tensors there, or None when the W
+    lists would exceed ``cap`` terms; the A_c lists are None when they would."""
+    import torch
+
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=device)  # noqa: E731
+    rp_t, cl_t, agg_t = T(rp), T(cl), T(agg)
+    p_ptr, p_idx, w_ptr, w_idx = T(Pp.indptr), T(Pp.indices), T(Wp.indptr), T(Wp.indices)
+    n = rp_t.numel() - 1
+    rows = torch.repeat_interleave(torch.arange(n, device=device), rp_t[1:] - rp_t[:-1])
+    i32 = lambda t: t.to(torch.int32).contiguous()  # noqa: E731
     out = {}
     # P: A entry j of row i -> slot (i, agg[col j])
-    pkeys = np.repeat(np.arange(n, dtype=np.int64), np.diff(Pp.indptr)) * na + Pp.indices
-    sp_ = np.searchsorted(pkeys, rows * na + agg[cl])
-    out["p_tptr"], out["p_tj"] = _slot_lists(sp_, Pp.nnz)
+    sp_ = torch.searchsorted(_row_keys(p_ptr, p_idx, na), rows * na + agg_t[cl_t])
+    ptr, order = _slot_lists(sp_, Pp.nnz)
+    out["p_tptr"], out["p_tj"] = i32(ptr), i32(order)
     # W: (A entry j, P entry e of row col j) -> slot (row j, col e)
-    wkeys = np.repeat(np.arange(n, dtype=np.int64), np.diff(Wp.indptr)) * na + Wp.indices
-    jj, e = _expand(Pp.indptr.astype(np.int64), cl)
-    if e.size > cap:
-        return None
-    sw = np.searchsorted(wkeys, rows[jj] * na + Pp.indices[e])
-    ptr, order = _slot_lists(sw, Wp.nnz)
-    out["w_tptr"], out["w_tj"], out["w_te"] = ptr, jj[order], e[order]
-    # A_c: (R entry q of coarse row I, W entry s of row r_col[q]) -> slot (I, col s)
-    nr = r_col.size
-    qrow = np.repeat(np.arange(r_rowptr.size - 1, dtype=np.int64), np.diff(r_rowptr))
-    lens = np.diff(Wp.indptr)[r_col]
+    lens = p_ptr[cl_t + 1] - p_ptr[cl_t]
     if int(lens.sum()) > cap:
+        return None
+    jj, e = _expand(p_ptr, cl_t)
+    sw = torch.searchsorted(_row_keys(w_ptr, w_idx, na), rows[jj] * na + p_idx[e])
+    ptr, order = _slot_lists(sw, Wp.nnz)
+    out["w_tptr"], out["w_tj"], out["w_te"] = i32(ptr), i32(jj[order]), i32(e[order])
+    # A_c: (R entry q of coarse row I, W entry s of row r_col[q]) -> slot (I, col s)
+    rc, rr = T(r_col), T(r_rowptr)
+    if int((w_ptr[rc + 1] - w_ptr[rc]).sum()) > cap:
         out["c_tptr"] = out["c_te"] = out["c_ts"] = None
-    else:
-        ckeys = np.repeat(np.arange(Cp.shape[0], dtype=np.int64), np.diff(Cp.indptr)) * na + Cp.indices
-        q, s_ = _expand(Wp.indptr.astype(np.int64), np.asarray(r_col, dtype=np.int64))
-        sc = np.searchsorted(ckeys, qrow[q] * na + Wp.indices[s_])
-        ptr, order = _slot_lists(sc, Cp.nnz)
-        out["c_tptr"], out["c_te"], out["c_ts"] = ptr, q[order], s_[order]
-        assert q.size == 0 or q.max() < nr
+        return out
+    qrow = torch.repeat_interleave(torch.arange(rr.numel() - 1, device=device), rr[1:] - rr[:-1])
+    q, s_ = _expand(w_ptr, rc)
+    sc = torch.searchsorted(_row_keys(T(Cp.indptr), T(Cp.indices), na), qrow[q] * na + w_idx[s_])
+    ptr, order = _slot_lists(sc, Cp.nnz)
+    out["c_tptr"], out["c_te"], out["c_ts"] = i32(ptr), i32(q[order]), i32(s_[order])
     return out
 
 
@@ -278,11 +294,11 @@ class AMGHierarchy:
                 bufs["group_ptr"] = i32(np.concatenate([[0], np.cumsum(np.bincount(level_groups[l],
                                                                                     minlength=ngroups))]))
             else:
-                tl = term_lists(lv_rp, lv_cl, agg_l.astype(np.int64), na, Pp, Wp, Cp, r_col, r_rowptr)
+                tl = term_lists(lv_rp, lv_cl, agg_l, na, Pp, Wp, Cp, r_col, r_rowptr, device=dev)
                 if tl is not None:
                     for k, v in tl.items():
                         if v is not None:
-                            bufs[k] = i32(v)
+                            bufs[k] = v
                     L.c_nnz = Cp.nnz
             for k, v in bufs.items():
                 setattr(L, k, v.data_ptr())

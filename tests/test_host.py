@@ -236,7 +236,7 @@ def test_amg_term_lists_reproduce_the_row_owned_products_bit_for_bit():
                 t = c0 + int(np.searchsorted(Cp.indices[c0:c1], Wp.indices[s]))
                 ac[t] += r[q] * w[s]
     # the same from the term lists
-    tl = term_lists(rp, cl, agg, na, Pp, Wp, Cp, r_col, r_rowptr)
+    tl = {k: v.numpy() for k, v in term_lists(rp, cl, agg, na, Pp, Wp, Cp, r_col, r_rowptr).items()}
     p2 = np.empty(Pp.nnz)
     for i in range(n):
         for s in range(Pp.indptr[i], Pp.indptr[i + 1]):
