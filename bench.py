@@ -354,7 +354,8 @@ def run_batch(args, rank, world):
     for c in bs.cases + [bs.case]:
         c.tol = 0.0
     setup_s = time.perf_counter() - t0
-    for _ in range(W):
+    tuning = bs.autotune()  # team shapes of the per-case Krylov solves, timed on this batch
+    for _ in range(W):  # after the tuning: the graphs are captured with the chosen shapes
         bs.step()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
@@ -428,6 +429,9 @@ def run_batch(args, rank, world):
     return {"value": value, "ms": ms_max, "ncell": ncell, "ncase": len(meshes), "setup_s": setup_s,
             "launches": launches, "times": times, "infos": infos, "one_at_a_time": one, "seq_ms": seq_ms,
             "sample": samp, "solver": bs, "converge": conv,
+            "autotune": {"momentum": list(tuning["momentum"]), "pressure": list(tuning["pressure"]),
+                         "fields": ["cluster_blocks", "block_threads", "wide_row"],
+                         "ms_momentum_pressure": {"x".join(map(str, k)): v for k, v in tuning["ms"].items()}},
             "kinds": {"cavity": kinds.count("cavity"), "channel": kinds.count("channel")}}
 
 
@@ -517,7 +521,7 @@ def main_batch(args, rank, world, dev):
                          "traffic": None, "algorithmic_bytes_per_launch": byts / K,
                          "stage_ms_per_step": {k: v / K for k, v in sorted(times.items(), key=lambda kv: -kv[1])}},
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": r["launches"], "setup_seconds": r["setup_s"],
-            "to_convergence": r["converge"]}
+            "autotune": r["autotune"], "to_convergence": r["converge"]}
     print(json.dumps(line), flush=True)
 
 

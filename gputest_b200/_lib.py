@@ -31,6 +31,11 @@ class Mesh(ctypes.Structure):
         ("tiles", P), ("ntiles", I32), ("pad_", I32)]
 
 
+class TeamConfig(ctypes.Structure):
+    """``b2s_team_config``: the thread-block cluster that solves one case of a batch."""
+    _fields_ = [("cluster_blocks", I32), ("block_threads", I32), ("wide_row", I32), ("pad_", I32)]
+
+
 class BC(ctypes.Structure):
     _fields_ = [(name, P) for name in ("m_wall", "m_inlet", "m_pres", "m_sym", "m_dirvel", "ub_fixed", "pb_fixed",
                                        "m_tfix", "m_tflux", "m_out", "tval")]
@@ -117,11 +122,11 @@ _SIGS = {
     "b2s_remove_group_means_d": ([P, P, P, ctypes.c_int, ctypes.c_int, P, P, P, P, P], ctypes.c_int),
     "b2s_bicgstab_groups_workspace_bytes": ([I32, ctypes.c_int, ctypes.c_int], I64),
     "b2s_bicgstab_groups_f32_d": ([ctypes.c_int, P, P, I32, ctypes.c_int, P, P, P, P, P, P, F64, ctypes.c_int,
-                                   ctypes.c_int, ctypes.c_int, P, P, P, I64, P, P], ctypes.c_int),
+                                   ctypes.c_int, ctypes.c_int, P, P, P, I64, P, P, P], ctypes.c_int),
     "b2s_pcg_groups_workspace_bytes": ([P], I64),
     "b2s_residual_vjp_d": ([P, P, F64, F64, F64, ctypes.c_int] + [P] * 18 + [P], ctypes.c_int),
     "b2s_pcg_groups_mixed_d": ([P, P, P, P, P, P, P, I32, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, F64, P, I64,
-                                P, P], ctypes.c_int),
+                                P, P, P], ctypes.c_int),
 }
 
 _lib: Optional[ctypes.CDLL] = None

@@ -55,12 +55,12 @@ __global__ void remove_group_means_k(b2s_mesh m, double* __restrict__ x, const d
 }
 
 // ---------------------------------------------------------------------------------- case teams
-// A case is solved by a team: the blocks of one thread-block cluster (kClusterBlocks blocks,
-// each on its own SM). Rows are dealt over all the team's threads; a team barrier is the
+// A case is solved by a team: the blocks of one thread-block cluster (b2s_team_config: 1-8
+// blocks of up to 1024 threads, 4 x 1024 by default; the autotuner of the batch solver picks it). Rows are dealt over all the team's threads; a team barrier is the
 // cluster barrier (which also orders the team's global-memory accesses), and a team sum adds
 // the block sums of the team's blocks read from their shared memory (distributed shared
 // memory), in rank order, so that every thread of the team gets the same bits.
-constexpr int kClusterBlocks = 4;
+constexpr int kClusterBlocks = 4;  // default team shape
 
 struct Team {
   int t, n;      // this thread's index in the team and the team's size
@@ -117,7 +117,13 @@ struct BRows {
   __device__ __forceinline__ bool writer() const { return lane == 0; }
 };
 
-constexpr int kBatchWideRow = 24;
+constexpr int kBatchWideRow = 24;  // default: rows averaging this many entries go one warp per row
+
+// Whether a range of rows is walked one warp per row (wide_row > 0 and rows averaging at least
+// wide_row entries).
+__device__ __forceinline__ bool wide_rows(int64_t nnz, int64_t rows, int wide_row) {
+  return wide_row > 0 && nnz >= (int64_t)wide_row * rows;
+}
 
 // ---------------------------------------------------------------------------------- BiCGSTAB
 template <class T>
@@ -134,6 +140,7 @@ struct BicgGroupArgs {
   double tol;
   int maxiter, rel, zero_x0;
   T* work;        // 7 [nr][n] vectors
+  int wide_row;   // rows-per-warp switch (b2s_team_config)
   b2s_solve_info* info;  // [ngroups][nr]
   double* out64;  // when set: out64 = base64 + x
   const double* base64;
@@ -162,7 +169,7 @@ __device__ void bicgstab_group(const BicgGroupArgs<T>& a, int lo, int hi, double
     b[k] = a.b + (int64_t)k * n;
   }
   const T* inv = a.inv;
-  const bool wide = nnz >= (int64_t)kBatchWideRow * (hi - lo);
+  const bool wide = wide_rows(nnz, hi - lo, a.wide_row);
   // r = b - A x, r_hat = r, p = v = 0
   double acc[2 * NR];
 #pragma unroll
@@ -447,6 +454,7 @@ struct PcgGroupArgs {
   T* d;    // float correction of a pass
   const int32_t* order;
   const int32_t* project;  // [ngroups] singular cases
+  int wide_row;            // rows-per-warp switch (b2s_team_config)
   double tol;
   int maxiter, maxpass;
   double min_inner_tol;
@@ -468,7 +476,7 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
     const T* b = (l == 0) ? rhs0 : (const T*)a.lb[l];
     const T* val = a.lval[l];
     const T* dinv = a.ldinv[l];
-    const bool wide = lv.nnz >= (int64_t)kBatchWideRow * lv.n;
+    const bool wide = wide_rows(lv.nnz, lv.n, a.wide_row);
     T* X = a.lx[l];
     T* Y = a.ly[l];
     T* c = X;
@@ -518,7 +526,7 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
     const int chi = (l + 1 < L) ? h.levels[l + 1].group_ptr[g + 1] : h.coarse_group_ptr[g + 1];
     T* bn = (l + 1 < L) ? a.lb[l + 1] : a.cb;
     {
-      const BRows R(lv.p_nnz >= (int64_t)kBatchWideRow * lv.nc, clo, tm);
+      const BRows R(wide_rows(lv.p_nnz, lv.nc, a.wide_row), clo, tm);
       for (int I = R.first; I < chi; I += R.stride) {
         double s = 0.0;
         for (int j = lv.r_rowptr[I] + R.lane; j < lv.r_rowptr[I + 1]; j += R.step) s += (double)a.lrval[l][j] * (double)Rv[lv.r_col[j]];
@@ -549,12 +557,12 @@ __device__ T* vcycle_group(const PcgGroupArgs<T>& a, int g, const T* rhs0, doubl
     const T* b = (l == 0) ? rhs0 : (const T*)a.lb[l];
     const T* val = a.lval[l];
     const T* dinv = a.ldinv[l];
-    const bool wide = lv.nnz >= (int64_t)kBatchWideRow * lv.n;
+    const bool wide = wide_rows(lv.nnz, lv.n, a.wide_row);
     const T* xc = (l + 1 < L) ? (const T*)cur[l + 1] : (const T*)a.cx;
     T* c = cur[l];
     T* o = (c == a.lx[l]) ? a.ly[l] : a.lx[l];
     {
-      const BRows R(lv.p_nnz >= (int64_t)kBatchWideRow * lv.n, lo, tm);
+      const BRows R(wide_rows(lv.p_nnz, lv.n, a.wide_row), lo, tm);
       for (int i = R.first; i < hi; i += R.stride) {
         double s = 0.0;
         for (int j = lv.p_rowptr[i] + R.lane; j < lv.p_rowptr[i + 1]; j += R.step) s += (double)a.lpval[l][j] * (double)xc[lv.p_col[j]];
@@ -775,17 +783,28 @@ __global__ void __launch_bounds__(kBatchThreads) pcg_groups_k(PcgGroupArgs<T> a)
 
 using namespace b2s;
 
-// Launch one team (a cluster of kClusterBlocks blocks) per case up to the number of clusters that
-// fit on the device at once; the teams then walk the case list.
-static int launch_teams(const void* kernel, int ngroups, void** args, b2s_stream_t s) {
+// The team shape of a call: the caller's configuration, or the default.
+static int team_shape(const b2s_team_config* team, b2s_team_config* out) {
+  b2s_team_config t = {kClusterBlocks, kBatchThreads, kBatchWideRow, 0};
+  if (team) t = *team;
+  if (t.cluster_blocks < 1 || t.cluster_blocks > 8 || t.block_threads < 64 || t.block_threads > kBatchThreads ||
+      t.block_threads % 32 != 0 || t.wide_row < 0)
+    return B2S_ERR_ARG;
+  *out = t;
+  return B2S_OK;
+}
+
+// Launch one team (a cluster of team.cluster_blocks blocks) per case up to the number of
+// clusters that fit on the device at once; the teams then walk the case list.
+static int launch_teams(const void* kernel, int ngroups, void** args, const b2s_team_config& team, b2s_stream_t s) {
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kClusterBlocks;
+  attr[0].val.clusterDim.x = (unsigned)team.cluster_blocks;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kClusterBlocks, 1, 1);
-  cfg.blockDim = dim3(kBatchThreads, 1, 1);
+  cfg.gridDim = dim3((unsigned)team.cluster_blocks, 1, 1);
+  cfg.blockDim = dim3((unsigned)team.block_threads, 1, 1);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = (cudaStream_t)s;
   cfg.attrs = attr;
@@ -793,18 +812,18 @@ static int launch_teams(const void* kernel, int ngroups, void** args, b2s_stream
   int ncl = 0;
   if (cudaOccupancyMaxActiveClusters(&ncl, kernel, &cfg) != cudaSuccess || ncl < 1) return B2S_ERR_DEVICE;
   if (ncl > ngroups) ncl = ngroups;
-  cfg.gridDim = dim3((unsigned)(ncl * kClusterBlocks), 1, 1);
+  cfg.gridDim = dim3((unsigned)(ncl * team.cluster_blocks), 1, 1);
   if (cudaLaunchKernelExC(&cfg, kernel, args) != cudaSuccess) return B2S_ERR_LAUNCH;
   B2S_LAUNCH_CHECK();
   return B2S_OK;
 }
 
 template <class T>
-static int launch_bicg_groups(BicgGroupArgs<T>& a, b2s_stream_t s) {
+static int launch_bicg_groups(BicgGroupArgs<T>& a, const b2s_team_config& team, b2s_stream_t s) {
   void* args[] = {&a};
   const void* k = a.nr == 1 ? (const void*)bicgstab_groups_k<1, T>
                   : a.nr == 2 ? (const void*)bicgstab_groups_k<2, T> : (const void*)bicgstab_groups_k<3, T>;
-  return launch_teams(k, a.ngroups, args, s);
+  return launch_teams(k, a.ngroups, args, team, s);
 }
 
 extern "C" {
@@ -845,10 +864,12 @@ int b2s_bicgstab_groups_f32_d(int ngroups, const int32_t* group_ptr, const int32
                               const int32_t* rowptr, const int32_t* col, const float* val, const float* b,
                               const float* inv_diag, float* x, double tol, int maxiter, int relative_to_initial,
                               int zero_x0, double* out64, const double* base64, void* work, int64_t work_bytes,
-                              b2s_solve_info* info, b2s_stream_t s) {
+                              b2s_solve_info* info, const b2s_team_config* team, b2s_stream_t s) {
   if (ngroups <= 0 || !group_ptr || !order || n <= 0 || nrhs < 1 || nrhs > 3 || !rowptr || !col || !val || !b ||
       !inv_diag || !x || !work || !info || maxiter < 0 || ((out64 == nullptr) != (base64 == nullptr)))
     return B2S_ERR_ARG;
+  b2s_team_config tc;
+  if (team_shape(team, &tc) != B2S_OK) return B2S_ERR_ARG;
   if (work_bytes < b2s_bicgstab_groups_workspace_bytes(n, nrhs, 1)) return B2S_ERR_WORKSPACE;
   BicgGroupArgs<float> a;
   a.ngroups = ngroups;
@@ -870,7 +891,8 @@ int b2s_bicgstab_groups_f32_d(int ngroups, const int32_t* group_ptr, const int32
   a.info = info;
   a.out64 = out64;
   a.base64 = base64;
-  return launch_bicg_groups(a, s);
+  a.wide_row = tc.wide_row;
+  return launch_bicg_groups(a, tc, s);
 }
 
 static bool amg_groups_ok(const b2s_amg* h, const b2s_amg_f32* h32) {
@@ -898,10 +920,12 @@ int b2s_pcg_groups_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const int32
                            const b2s_mesh* m, const double* cf, const double* cb, int32_t n, const int32_t* rowptr,
                            const int32_t* col, const float* val, const double* b, double* x, double tol, int maxiter,
                            int maxpass, double min_inner_tol, void* work, int64_t work_bytes, b2s_solve_info* info,
-                           b2s_stream_t s) {
+                           const b2s_team_config* team, b2s_stream_t s) {
   if (!amg_groups_ok(h, h32) || !order || !project || !m || !cf || (!cb && m->nb) || !rowptr || !col || !val || !b ||
       !x || !work || !info || maxiter < 0 || maxpass < 1 || !(min_inner_tol > 0.0))
     return B2S_ERR_ARG;
+  b2s_team_config tc;
+  if (team_shape(team, &tc) != B2S_OK) return B2S_ERR_ARG;
   if (n != (h->nlevels ? h->levels[0].n : h->coarse_n) || n != m->nc) return B2S_ERR_ARG;
   if (work_bytes < b2s_pcg_groups_workspace_bytes(h)) return B2S_ERR_WORKSPACE;
   PcgGroupArgs<float> a;
@@ -945,8 +969,9 @@ int b2s_pcg_groups_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const int32
   a.maxpass = maxpass;
   a.min_inner_tol = min_inner_tol;
   a.info = info;
+  a.wide_row = tc.wide_row;
   void* args[] = {&a};
-  return launch_teams((const void*)pcg_groups_k<float>, h->ngroups, args, s);
+  return launch_teams((const void*)pcg_groups_k<float>, h->ngroups, args, tc, s);
 }
 
 }  // extern "C"

@@ -433,13 +433,15 @@ class AMGHierarchy:
                                             info, _lib.stream_ptr(stream)), "b2s_pcg_amg_d")
 
     def pcg_groups_mixed(self, mesh_ref, order, project, cf, cb, b, x, tol, maxiter, info, maxpass=8,
-                         min_inner_tol=1e-5, stream=None):
+                         min_inner_tol=1e-5, stream=None, team=None):
         """Per-case refined solves of a batch hierarchy (``b2s_pcg_groups_mixed_d``): order and
-        project are device int32 tensors [ngroups]; info the device address of ngroups records."""
+        project are device int32 tensors [ngroups]; info the device address of ngroups records;
+        team a ``_lib.TeamConfig`` (None: the library's default team shape)."""
         _lib.check(_lib.lib().b2s_pcg_groups_mixed_d(self.cref, self.c32ref, order.data_ptr(), project.data_ptr(),
                                                      mesh_ref, cf.data_ptr(), cb.data_ptr(), self.n0,
                                                      self.rowptr0.data_ptr(), self.col0.data_ptr(),
                                                      self.src_val32.data_ptr(), b.data_ptr(), x.data_ptr(), float(tol),
                                                      int(maxiter), int(maxpass), float(min_inner_tol),
                                                      self.work_mixed.data_ptr(), self.work_mixed.numel() * 8, info,
+                                                     None if team is None else ctypes.byref(team),
                                                      _lib.stream_ptr(stream)), "b2s_pcg_groups_mixed_d")

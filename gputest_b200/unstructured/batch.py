@@ -63,6 +63,12 @@ def _union_case(cases: Sequence[UnstructuredCase], meshes: Sequence[Unstructured
 class BatchSimpleSolver(MixedSimpleSolver):
     """Many independent cases (list of meshes and cases of one dimension) solved together."""
 
+    # team shapes of the per-case Krylov solves (``b2s_team_config``: blocks per cluster, threads
+    # per block, rows-per-warp switch), one per solve; ``autotune`` picks among TEAM_CANDIDATES on
+    # the batch itself
+    DEFAULT_TEAM = (4, 1024, 24)
+    TEAM_CANDIDATES = tuple((cb, bt, wr) for cb in (2, 4, 8) for bt in (512, 1024) for wr in (16, 24, 48))
+
     def __init__(self, meshes: List[UnstructuredMesh], cases: List[UnstructuredCase], max_coarse: int = 150,
                  amg_theta: float = 0.08):
         if len(meshes) != len(cases) or not meshes:
@@ -76,6 +82,9 @@ class BatchSimpleSolver(MixedSimpleSolver):
         super().__init__(union_mesh(self.meshes), _union_case(cases, meshes), max_coarse=max_coarse,
                          amg_theta=amg_theta)
         self.reaggregate = False  # the batch hierarchy is set up once (aggregates per case)
+        self.team = _lib.TeamConfig(*self.DEFAULT_TEAM, 0)  # pressure-correction solve
+        self.team_momentum = _lib.TeamConfig(*self.DEFAULT_TEAM, 0)
+        self.tuning = None
         self.case_iteration = 0
         self.case_converged_at = np.full(self.ncase, -1, dtype=np.int64)
         self._res_max5_case = np.zeros(self.ncase)
@@ -304,7 +313,8 @@ class BatchSimpleSolver(MixedSimpleSolver):
                                                self.r32.data_ptr(), self.inv32.data_ptr(), self.dU32.data_ptr(), 0.1,
                                                30, 1, 1, self.Ustar.data_ptr(), Up[1:].data_ptr(),
                                                self.work_bicg_g.data_ptr(), self.work_bicg_g.numel() * 8,
-                                               self.info_mom_g, s), "b2s_bicgstab_groups_f32_d")
+                                               self.info_mom_g, ctypes.byref(self.team_momentum), s),
+                   "b2s_bicgstab_groups_f32_d")
         self._mark("momentum_solve")
         _lib.check(L.b2s_pressure_assemble_mixed_d(m, bc, pr, self.Ustar.data_ptr(), Up.data_ptr(), gp.data_ptr(),
                                                    self.dP.data_ptr(), self.Fst.data_ptr(), self.cf.data_ptr(),
@@ -318,7 +328,7 @@ class BatchSimpleSolver(MixedSimpleSolver):
         self._mark("amg_rebuild")
         self._amg.pcg_groups_mixed(m, self.g_order, self.g_singular, self.cf, self.cb, self.rhs_p, self.pp,
                                    self.case.pressure_tol, 200, self.info_p_g, maxpass=self.REFINE_PASSES,
-                                   min_inner_tol=self.INNER_TOL_FLOOR)
+                                   min_inner_tol=self.INNER_TOL_FLOOR, team=self.team)
         self.kernel_launches += 1
         self._mark("pressure_solve")
         Upn, Fn, Fbn = self._Up[new], self._F[new], self._Fb[new]
@@ -394,6 +404,82 @@ class BatchSimpleSolver(MixedSimpleSolver):
         self.case_converged_at[newly] = self.iteration
         self.converged = bool(np.all(self.case_converged_at >= 0))
         return 1.0
+
+    def autotune(self, candidates=None, reps=5, margin=0.05) -> dict:
+        """Pick the team shapes of the per-case Krylov solves (``b2s_team_config``: blocks per
+        thread-block cluster, threads per block, the mean row length from which rows are walked
+        one warp per row), one for the momentum Jacobi-BiCGSTAB and one for the refined
+        pressure-correction AMG-PCG, by timing every candidate on this batch's current systems
+        (those of the last outer iteration; one is run first if none has): each solve ``reps``
+        times after one untimed call, CUDA events, median. A candidate replaces the current shape
+        only when it is faster by more than ``margin`` (timing noise must not pick a shape). The
+        timed solves write scratch copies, so the solver's state is unchanged; captured graphs
+        are dropped (they hold the previous shapes). A candidate the device cannot launch is
+        skipped. Returns {"momentum": shape, "pressure": shape, "ms": {candidate: (momentum ms,
+        pressure ms) or None}}."""
+        import torch
+
+        if self._amg is None or self.iteration == 0:
+            self.step()
+        L, fv, ng, dim, nc = _lib.lib(), self.fv, self.ncase, self.dim, self.nc
+        s = _lib.stream_ptr()
+        dev = self.torch_device
+        dU = torch.empty_like(self.dU32)
+        Ust = torch.empty_like(self.Ustar)
+        pp = torch.empty_like(self.pp)
+        info = torch.zeros(ng * max(dim, 1) * INFO_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        base = self._Up[self._cur][1:]
+        m = fv.cmesh_ref
+
+        def momentum(team):
+            _lib.check(L.b2s_bicgstab_groups_f32_d(ng, self.g_cells.data_ptr(), self.g_order.data_ptr(), nc, dim,
+                                                   fv.rowptr.data_ptr(), fv.col.data_ptr(), self.val_A32.data_ptr(),
+                                                   self.r32.data_ptr(), self.inv32.data_ptr(), dU.data_ptr(), 0.1, 30,
+                                                   1, 1, Ust.data_ptr(), base.data_ptr(), self.work_bicg_g.data_ptr(),
+                                                   self.work_bicg_g.numel() * 8, info.data_ptr(), ctypes.byref(team),
+                                                   s), "b2s_bicgstab_groups_f32_d")
+
+        def pressure(team):
+            self._amg.pcg_groups_mixed(m, self.g_order, self.g_singular, self.cf, self.cb, self.rhs_p, pp,
+                                       self.case.pressure_tol, 200, info.data_ptr(), maxpass=self.REFINE_PASSES,
+                                       min_inner_tol=self.INNER_TOL_FLOOR, team=team)
+
+        def timed(fn, team):
+            fn(team)
+            torch.cuda.synchronize()
+            ms = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                fn(team)
+                e1.record()
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            return float(np.median(ms))
+
+        cur_m = (self.team_momentum.cluster_blocks, self.team_momentum.block_threads, self.team_momentum.wide_row)
+        cur_p = (self.team.cluster_blocks, self.team.block_threads, self.team.wide_row)
+        cands = [tuple(c) for c in (candidates or self.TEAM_CANDIDATES)]
+        times = {}
+        for cand in dict.fromkeys(cands + [cur_m, cur_p]):
+            team = _lib.TeamConfig(*cand, 0)
+            try:
+                times[cand] = (timed(momentum, team), timed(pressure, team))
+            except RuntimeError:
+                times[cand] = None
+        ok = {k: v for k, v in times.items() if v is not None}
+        if not ok:
+            raise RuntimeError("no team shape could be launched")
+        choice = []
+        for q, cur in ((0, cur_m), (1, cur_p)):
+            best = min(ok, key=lambda k: ok[k][q])
+            keep = cur in ok and ok[best][q] > (1.0 - margin) * ok[cur][q]
+            choice.append(cur if keep else best)
+        self.team_momentum = _lib.TeamConfig(*choice[0], 0)
+        self.team = _lib.TeamConfig(*choice[1], 0)
+        self._graphs.clear()
+        self.tuning = {"momentum": choice[0], "pressure": choice[1], "ms": times}
+        return self.tuning
 
     def run(self, max_steps=None, hooks=None) -> int:
         """Step until every case converged or ``max_iter`` (or ``max_steps``), one iteration at a

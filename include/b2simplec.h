@@ -431,12 +431,23 @@ B2S_API int b2s_remove_group_means_d(const b2s_mesh* m, double* x, const double*
 /* Jacobi-BiCGSTAB in float of every case's rows (group_ptr [ngroups+1]) as separate systems,
  * with the semantics of b2s_bicgstab_jacobi_f32_d per case; order [ngroups] is the processing
  * order (largest first); info is [ngroups][nrhs]. */
+/* Shape of the team that solves one case of a batch: the blocks of one thread-block cluster.
+ * NULL selects the default (4 blocks of 1024 threads, rows averaging 24 or more entries walked one
+ * warp per row); the batch solver's autotuner times candidate shapes on the batch itself. */
+typedef struct b2s_team_config {
+  int32_t cluster_blocks;  /* blocks per team (1 .. 8) */
+  int32_t block_threads;   /* threads per block: a multiple of 32, 64 .. 1024 */
+  int32_t wide_row;        /* rows averaging at least this many entries go one warp per row (0: never) */
+  int32_t pad_;
+} b2s_team_config;
+
 B2S_API int64_t b2s_bicgstab_groups_workspace_bytes(int32_t n, int nrhs, int single);
 B2S_API int b2s_bicgstab_groups_f32_d(int ngroups, const int32_t* group_ptr, const int32_t* order, int32_t n, int nrhs,
                                       const int32_t* rowptr, const int32_t* col, const float* val, const float* b,
                                       const float* inv_diag, float* x, double tol, int maxiter,
                                       int relative_to_initial, int zero_x0, double* out64, const double* base64,
-                                      void* work, int64_t work_bytes, b2s_solve_info* info, b2s_stream_t s);
+                                      void* work, int64_t work_bytes, b2s_solve_info* info,
+                                      const b2s_team_config* team, b2s_stream_t s);
 
 /* The refined pressure-correction solve of b2s_pcg_amg_mixed_d per case, on a batch hierarchy
  * (h->ngroups > 0); project [ngroups] marks the singular cases, info is [ngroups]. */
@@ -446,7 +457,7 @@ B2S_API int b2s_pcg_groups_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, con
                                    int32_t n, const int32_t* rowptr, const int32_t* col, const float* val,
                                    const double* b, double* x, double tol, int maxiter, int maxpass,
                                    double min_inner_tol, void* work, int64_t work_bytes, b2s_solve_info* info,
-                                   b2s_stream_t s);
+                                   const b2s_team_config* team, b2s_stream_t s);
 
 /* ----------------------------------------------------------------------------------------- */
 /* Discrete adjoint. No counterpart in the reference (it has no derivatives).                   */

@@ -113,3 +113,46 @@ def test_batch_stability_guard_rolls_back_one_case_only():
     for _ in range(5):
         bs.step()
     assert np.isfinite(bs.case_residuals(1)["continuity"])
+
+
+@pytest.mark.parametrize("team", [(2, 512, 16), (8, 1024, 0)])
+def test_other_team_shapes_converge_to_the_same_fields(team):
+    """Non-default team shapes (blocks per cluster, threads per block, rows-per-warp switch; 0
+    never walks a row by a warp) solve every case to the fields of the case solved alone."""
+    from gputest_b200 import _lib
+    from gputest_b200.unstructured.batch import BatchSimpleSolver
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    meshes, cases = _cases()
+    bs = BatchSimpleSolver(meshes, cases)
+    bs.team = _lib.TeamConfig(*team, 0)
+    bs.team_momentum = _lib.TeamConfig(*team, 0)
+    bs.run()
+    assert bs.converged
+    for i, (m, c) in enumerate(zip(meshes, cases)):
+        s = SimpleSolver(m, c)
+        s.run()
+        ref, got = s.fields(), bs.case_fields(i)
+        for k in ref:
+            assert _rel(got[k], ref[k]) <= FIELD_TOL, (team, i, k)
+
+
+def test_autotune_times_the_candidates_and_keeps_the_fastest():
+    from gputest_b200.unstructured.batch import BatchSimpleSolver
+
+    meshes, cases = _cases(tol=0.0, max_iter=20)
+    bs = BatchSimpleSolver(meshes, cases)
+    cands = [(2, 512, 16), (4, 1024, 24), (8, 1024, 48)]
+    tuned = bs.autotune(candidates=cands, reps=2, margin=0.0)
+    ms = {k: v for k, v in tuned["ms"].items() if v is not None}
+    assert set(tuned["ms"]) == set(cands) and ms
+    assert tuned["momentum"] == min(ms, key=lambda k: ms[k][0])
+    assert tuned["pressure"] == min(ms, key=lambda k: ms[k][1])
+    assert (bs.team.cluster_blocks, bs.team.block_threads, bs.team.wide_row) == tuned["pressure"]
+    m = bs.team_momentum
+    assert (m.cluster_blocks, m.block_threads, m.wide_row) == tuned["momentum"]
+    it = bs.iteration
+    f0 = bs.fields()
+    bs.run(max_steps=3)
+    assert bs.iteration == it + 3 and all(np.all(np.isfinite(v)) for v in bs.fields().values())
+    assert f0.keys() == bs.fields().keys()

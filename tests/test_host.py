@@ -251,3 +251,37 @@ def test_amg_term_lists_reproduce_the_row_owned_products_bit_for_bit():
                         0.0) for s in range(Cp.nnz)])
     assert np.array_equal(p, p2) and np.array_equal(w, w2) and np.array_equal(ac, ac2)
     assert tl["c_tptr"][-1] == sum(np.diff(Wp.indptr)[r_col])
+
+
+def test_ctypes_structs_match_the_c_header_layout(tmp_path):
+    """Every struct of ``include/b2simplec.h`` and its ctypes mirror in ``gputest_b200/_lib.py``
+    have the same size and the same offset for every field (compiled with gcc against the header)."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    from gputest_b200 import _lib
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    pairs = {"b2s_mesh": _lib.Mesh, "b2s_bc": _lib.BC, "b2s_flow_params": _lib.FlowParams,
+             "b2s_solve_info": _lib.SolveInfo, "b2s_amg_level": _lib.AmgLevel, "b2s_amg": _lib.Amg,
+             "b2s_amg_f32": _lib.Amg32, "b2s_team_config": _lib.TeamConfig}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "b2simplec.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-std=c11", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
