@@ -192,7 +192,7 @@ def run_adjoint(args):
     return {"J": J, "primal_ms": primal_ms, "primal_iterations": its, "adjoint_seconds": adj_s,
             "method": info["method"], "iterations": info["iterations"], "residual": info["residual"],
             "direct": {k: info[k] for k in ("assemble_s", "factor_s", "solve_s", "jacobian_nnz", "lu_fill",
-                                            "residuals") if k in info},
+                                            "eliminated_gradients", "residuals") if k in info},
             "vjp_calls": info["vjp_calls"], "fd_rel_errors_porosity": errs, "dJ_du_in": d_uin, "fd_dJ_du_in": fd_u,
             "fd_rel_error_u_in": abs(d_uin - fd_u) / max(abs(fd_u), 1e-300), "fd_warm_iterations": fd_its,
             "cells": mesh.n_cells}

@@ -88,10 +88,12 @@ def test_exact_discrete_adjoint_matches_central_differences():
 
 def test_compressed_reverse_products_recover_the_exact_jacobian():
     """``assemble_jacobian`` (one reverse product per residual type and lattice colour) against the
-    dense autograd Jacobian of the transcription, in the adjoint's block layout."""
+    dense autograd Jacobian of the transcription, in the adjoint's block layout; and
+    ``TransposedSolver`` (gradient unknowns eliminated, sparse LU of the rest) against a dense
+    solve of the transposed system."""
     import torch
 
-    from gputest_b200.unstructured.adjoint import _descriptors, assemble_jacobian, grid_coordinates
+    from gputest_b200.unstructured.adjoint import TransposedSolver, _descriptors, assemble_jacobian, grid_coordinates
 
     m, case, por = _channel()
     o = _solve(m, case, por)
@@ -120,6 +122,14 @@ def test_compressed_reverse_products_recover_the_exact_jacobian():
 
     ij = grid_coordinates(h.xc)
     home, typ = _descriptors(dim, nc, ij, h.P, h.N, h.Pb, h.Sb)
-    J = assemble_jacobian(vjp, home, typ, ij, x.numel()).toarray()
+    Js = assemble_jacobian(vjp, home, typ, ij, x.numel())
+    J = Js.toarray()
     Jd = torch.autograd.functional.jacobian(lambda v: to_blk(R.residual(to_ref(v), al, ub)), to_blk(x)).numpy()
     assert np.abs(J - Jd).max() <= 1e-12 * np.abs(Jd).max()
+    # the transposed solve with the gradient unknowns eliminated
+    ts = TransposedSolver(Js, dim, nc)
+    assert ts.minv is not None
+    b = np.random.default_rng(2).standard_normal(J.shape[0])
+    y = ts.solve(b)
+    assert np.linalg.norm(Jd.T @ y - b) <= 1e-10 * np.linalg.norm(b)
+    assert np.allclose(y, np.linalg.solve(Jd.T, b), rtol=1e-8, atol=1e-10 * np.abs(y).max())
