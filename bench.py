@@ -198,6 +198,68 @@ def run_adjoint(args):
             "cells": mesh.n_cells}
 
 
+def run_probe(args):
+    """HBM bandwidth probe (``--config probe``): the C-ABI SpMV and the fused least-squares
+    gradient of 1 + dim fields (the gradients stage's kernel) on a 4,194,304-cell 3-D duct
+    (256 x 128 x 128 jittered hexahedra, ~350 MB of CSR: several times L2), K timed launches each
+    after W untimed, CUDA events on the launching stream; achieved = algorithmic bytes / time."""
+    import numpy as np
+    import torch
+
+    from gputest_b200 import _lib
+    from gputest_b200.mesh.unstructured import box_mesh_3d
+    from gputest_b200.unstructured.fvmesh import FVMesh
+
+    nx, ny, nz = (int(v) for v in args.probe_grid.split("x"))
+    t0 = time.perf_counter()
+    fv = FVMesh(box_mesh_3d(nx, ny, nz, 2.0, 1.0, 1.0, jitter=0.1, seed=1))
+    setup_s = time.perf_counter() - t0
+    L, s = _lib.lib(), _lib.stream_ptr()
+    nc, nf, nb, d, nnz = fv.nc, fv.n_if, fv.n_bf, fv.dim, fv.nnz
+    g = torch.Generator(device="cuda").manual_seed(0)
+    val = torch.rand(nnz, dtype=torch.float64, device="cuda", generator=g)
+    x = torch.rand(nc, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    k = 1 + d
+    phi = torch.rand(k, nc, dtype=torch.float64, device="cuda", generator=g)
+    phib = torch.rand(k, nb, dtype=torch.float64, device="cuda", generator=g)
+    grad = torch.empty(k, d, nc, dtype=torch.float64, device="cuda")
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        for a, b in ev:
+            a.record()
+            fn()
+            b.record()
+        torch.cuda.synchronize()
+        return float(np.median([a.elapsed_time(b) for a, b in ev])) / 1e3
+
+    spmv = lambda: _lib.check(L.b2s_spmv_d(nc, 1, fv.rowptr.data_ptr(), fv.col.data_ptr(), val.data_ptr(),  # noqa: E731
+                                           x.data_ptr(), y.data_ptr(), s), "b2s_spmv_d")
+    lsg = lambda: _lib.check(L.b2s_ls_gradient_d(fv.cmesh_ref, k, phi.data_ptr(), phib.data_ptr(),  # noqa: E731
+                                                 grad.data_ptr(), s), "b2s_ls_gradient_d")
+    sv = 8
+    bytes_spmv = nnz * (sv + 4) + 4 * (nc + 1) + 2 * nc * sv
+    geom = 8 * nf + nf * sv * (1 + d) + nb * (4 + sv * (1 + d)) + nc * sv * d * d + 4 * 3 * (nc + 1) + 4 * nf
+    bytes_lsg = geom + k * (nc + nb) * sv + k * nc * d * sv
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    out = {}
+    for name, fn, byts in (("spmv", spmv, bytes_spmv), ("ls_gradient_4_fields", lsg, bytes_lsg)):
+        t = timed(fn)
+        out[name] = {"ms": t * 1e3, "algorithmic_bytes": byts, "achieved_gbs": byts / t / 1e9,
+                     "frac": byts / t / 1e9 / hbm}
+    return {"cells": nc, "faces": nf, "nnz": nnz, "setup_s": setup_s, "kernels": out, "peak": hbm,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+
 # ---------------------------------------------------------------------------------- byte models
 def stage_bytes(solver, stage, step_info):
     """Algorithmic DRAM bytes of one launch of a stage: every array the stage's kernels read
@@ -542,6 +604,7 @@ def main():
     ap.add_argument("--converge-max-iter", type=int, default=6000, help="c4: outer-iteration cap of --converge")
     ap.add_argument("--fd-dirs", type=int, default=16, help="c5: random finite-difference directions")
     ap.add_argument("--adj-grid", default="512x128", help="c5: channel grid nx x ny")
+    ap.add_argument("--probe-grid", default="256x128x128", help="probe: duct grid nx x ny x nz")
     ap.add_argument("--adj-method", default="direct", choices=("direct", "gmres"),
                     help="c5: adjoint solve (sparse LU of the assembled Jacobian, or preconditioned GMRES)")
     args = ap.parse_args()
@@ -583,6 +646,20 @@ def main():
     dev = torch.cuda.current_device()
     if args.config == "c4":
         return main_batch(args, rank, world, dev)
+    if args.config == "probe":
+        r = run_probe(args)
+        if rank == 0:
+            best = max(r["kernels"].values(), key=lambda v: v["frac"])
+            line = {"metric": "HBM bandwidth probe: achieved / measured copy bandwidth", "value": best["frac"],
+                    "unit": "fraction", "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic", "config": {"workload": f"3-D duct {args.probe_grid} hexahedra "
+                                                                f"({r['cells']:,} cells), jitter 0.1h seed 1",
+                                                    "l2": "inputs larger than L2"},
+                    "kernels": r["kernels"], "peak_gbs": r["peak"], "peak_source": r["peak_source"],
+                    "setup_seconds": r["setup_s"]}
+            print(json.dumps(line), flush=True)
+        return
     if args.config == "c5":
         r = run_adjoint(args)
         if rank == 0:
