@@ -176,10 +176,20 @@ __global__ void pvals_k(b2s_amg_level L, int ngroups) {
 }
 
 // The same P from the level's term lists: thread per row, each slot's terms in list order (the
-// order pvals_k adds them), no search.
-__global__ void pvals_terms_k(b2s_amg_level L) {
-  const double c = (4.0 / 3.0) / *L.rho;
+// order pvals_k adds them), no search; batches take rho of the row's case, as pvals_k does.
+__global__ void pvals_terms_k(b2s_amg_level L, int ngroups) {
+  const double c0 = ngroups > 0 ? 0.0 : (4.0 / 3.0) / *L.rho;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+    double c = c0;
+    if (ngroups > 0) {
+      int lo = 0, hi = ngroups;  // the case g with group_ptr[g] <= i < group_ptr[g+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (L.group_ptr[mid] <= i) lo = mid;
+        else hi = mid;
+      }
+      c = (4.0 / 3.0) / L.rho[lo];
+    }
     const double di = L.dinv[i];
     const int ai = L.agg[i];
     for (int s = L.p_rowptr[i]; s < L.p_rowptr[i + 1]; ++s) {
@@ -478,8 +488,8 @@ int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stre
       if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
         return B2S_ERR_LAUNCH;
     }
-    const bool terms = h->ngroups == 0 && L.p_tptr && L.p_tj && L.w_tptr && L.w_tj && L.w_te;
-    if (terms) pvals_terms_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+    const bool terms = L.p_tptr && L.p_tj && L.w_tptr && L.w_tj && L.w_te;
+    if (terms) pvals_terms_k<<<grid_for(L.n), kThreads, 0, st>>>(L, h->ngroups);
     else pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L, h->ngroups);
     rvals_k<<<grid_for(L.p_nnz), kThreads, 0, st>>>(L);
     if (terms) wvals_terms_k<<<grid_for(L.w_nnz), kThreads, 0, st>>>(L);

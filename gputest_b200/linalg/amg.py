@@ -293,13 +293,12 @@ class AMGHierarchy:
             if batched:
                 bufs["group_ptr"] = i32(np.concatenate([[0], np.cumsum(np.bincount(level_groups[l],
                                                                                     minlength=ngroups))]))
-            else:
-                tl = term_lists(lv_rp, lv_cl, agg_l, na, Pp, Wp, Cp, r_col, r_rowptr, device=dev)
-                if tl is not None:
-                    for k, v in tl.items():
-                        if v is not None:
-                            bufs[k] = v
-                    L.c_nnz = Cp.nnz
+            tl = term_lists(lv_rp, lv_cl, agg_l, na, Pp, Wp, Cp, r_col, r_rowptr, device=dev)
+            if tl is not None:
+                for k, v in tl.items():
+                    if v is not None:
+                        bufs[k] = v
+                L.c_nnz = Cp.nnz
             for k, v in bufs.items():
                 setattr(L, k, v.data_ptr())
             self._keep.append(bufs)

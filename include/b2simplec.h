@@ -278,8 +278,8 @@ typedef struct b2s_amg_level {
   double* rho;                 /* [1] spectral radius estimate (device); batches: [ngroups] */
   const uint8_t* strong;       /* [nnz] strength of each entry at set-up (1: strong), or NULL */
   const int32_t* group_ptr;    /* batches: [ngroups+1] rows of each case on this level, or NULL */
-  /* Optional term lists of the fixed-pattern products (single systems; NULL: the row-owned
-   * kernels locate each term's slot by binary search). The terms of slot s are t in
+  /* Optional term lists of the fixed-pattern products (NULL: the row-owned kernels locate each
+   * term's slot by binary search). The terms of slot s are t in
    * [x_tptr[s], x_tptr[s+1]), listed in the order the row-owned kernels add them, so both give
    * the same values bit for bit:
    *   P slot s (row i):  sum_t (dinv_i a[p_tj[t]]) tval[col]       (A entries of row i)

@@ -159,7 +159,7 @@ def test_amg_vcycle_and_pcg_match_the_reference_hierarchy(torch_cuda, name):
             assert _rel(fv.cells_to_host(x), xr) < 1e-6
 
 
-@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("dim", [2, 3, "batch"])
 def test_amg_term_list_rebuild_equals_the_row_owned_rebuild(dim):
     """The rebuild from the set-up's term lists (thread per P row / W entry / A_c entry) gives
     the same hierarchy bit for bit as the row-owned kernels that locate each term's slot by
@@ -170,15 +170,23 @@ def test_amg_term_list_rebuild_equals_the_row_owned_rebuild(dim):
     from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase
     from gputest_b200.unstructured.simple import SimpleSolver
 
-    if dim == 2:
+    if dim == "batch":  # a block-diagonal batch hierarchy (per-case spectral radii)
+        from gputest_b200.unstructured.batch import BatchSimpleSolver
+
+        meshes = [cartesian_mesh_2d(n, n, jitter=0.15, seed=n) for n in (30, 18, 24)]
+        cases = [UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=[u, 0.0])}, viscosity=0.01,
+                                  max_iter=10, tol=0.0) for u in (1.0, 0.5, 2.0)]
+        s = BatchSimpleSolver(meshes, cases, max_coarse=40)
+    elif dim == 2:
         mesh = cartesian_mesh_2d(48, 48, triangulate=True, jitter=0.2)
         top = [1.0, 0.0]
     else:
         mesh = box_mesh_3d(16, 12, 10, jitter=0.1, seed=1, names=("wall", "wall", "wall", "top", "wall", "wall"))
         top = [1.0, 0.0, 0.0]
-    case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=top), "wall": BoundarySpec("wall")},
-                            viscosity=0.01, max_iter=10, tol=0.0)
-    s = SimpleSolver(mesh, case, amg_theta=0.0)
+    if dim != "batch":
+        case = UnstructuredCase(boundaries={"top": BoundarySpec("wall", velocity=top), "wall": BoundarySpec("wall")},
+                                viscosity=0.01, max_iter=10, tol=0.0)
+        s = SimpleSolver(mesh, case, amg_theta=0.0)
     for _ in range(3):
         s.step()
     amg, h = s._amg, s._amg.c
