@@ -47,7 +47,7 @@ import numpy as np
 
 from .. import _lib
 from ..linalg.amg import AMGHierarchy
-from ..linalg.krylov import INFO_DTYPE, KrylovInfo, info_buffer, read_info
+from ..linalg.krylov import INFO_DTYPE, read_info
 from ..mesh.unstructured import UnstructuredMesh
 from .case import FLUENT_TO_KIND, BoundarySpec, UnstructuredCase
 from .fvmesh import FVMesh
