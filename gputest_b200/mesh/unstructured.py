@@ -470,6 +470,69 @@ def extrude_to_3d(mesh2d: UnstructuredMesh, nz: int, lz: float,
     return sort_faces_by_zone(m)
 
 
+def extract_cells(mesh: UnstructuredMesh, keep, interface_type: str = "wall"):
+    """The sub-mesh of the cells where ``keep`` is True (``flowtrace/mesh/unstructured.py:714-779``):
+    the fluid part of a conjugate heat-transfer mesh. Faces between a kept and a dropped cell
+    become boundary faces of new zones ``interface-<dropped cell zone>`` (ids after the mesh's
+    largest, in order of the first face met), oriented out of the kept cell (a face kept through
+    its neighbour has its node loop reversed). Faces are then sorted by zone (interior zones
+    first, then by id). Returns (sub-mesh, face map: the original index of every sub-mesh face,
+    -(index + 1) where the loop was reversed, cell map: the original index of every sub-mesh
+    cell)."""
+    keep = np.asarray(keep, dtype=bool)
+    if mesh.periodic:
+        raise NotImplementedError("extracting cells from a mesh with periodic zones is not supported")
+    cmap = np.flatnonzero(keep)
+    new_id = np.full(mesh.n_cells, -1, dtype=np.int64)
+    new_id[cmap] = np.arange(cmap.size)
+    own, nei = mesh.owner, mesh.neighbour
+    ko = keep[own]
+    kn = (nei >= 0) & keep[np.maximum(nei, 0)]
+    whole = ko & (kn | (nei < 0))          # kept as it is (interior of the kept cells, or boundary)
+    iface = (ko ^ kn) & (nei >= 0)         # between a kept and a dropped cell
+    sel = np.flatnonzero(whole | iface)    # in face order
+    flip = iface[sel] & ~ko[sel]           # kept through the neighbour: reverse, neighbour becomes owner
+    dropped = np.where(ko[sel], np.maximum(nei[sel], 0), own[sel])
+    zones = {zid: z for zid, z in mesh.zones.items() if z.kind == "face"}
+    for z in mesh.cell_zones():
+        if np.any(keep[mesh.cell_zone == z.id]):
+            zones[z.id] = Zone(z.id, z.name, z.type, "cell")
+    fzone = mesh.face_zone[sel].copy()
+    is_if = iface[sel]
+    next_id = max(mesh.zones) + 1
+    iface_id = {}
+    for dz in mesh.cell_zone[dropped[is_if]].tolist():  # new zone ids in order of first appearance
+        if dz not in iface_id:
+            oz = mesh.zones[int(dz)]
+            iface_id[dz] = next_id
+            zones[next_id] = Zone(next_id, f"interface-{oz.name}", interface_type, "face")
+            next_id += 1
+    if is_if.any():
+        fzone[is_if] = np.array([iface_id[dz] for dz in mesh.cell_zone[dropped[is_if]].tolist()], dtype=np.int64)
+    owner = np.where(flip, new_id[np.maximum(nei[sel], 0)], new_id[own[sel]])
+    neighbour = np.where(is_if | (nei[sel] < 0), -1, new_id[np.maximum(nei[sel], 0)])
+    counts = np.diff(mesh.face_ptr)[sel]
+    ptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    f_of = np.repeat(np.arange(sel.size), counts)
+    pos = np.arange(int(counts.sum())) - ptr[f_of]
+    src = mesh.face_ptr[sel][f_of] + np.where(flip[f_of], counts[f_of] - 1 - pos, pos)
+    fmap = np.where(flip, -(sel + 1), sel)
+    present = set(fzone.tolist())
+    zones = {k: z for k, z in zones.items() if z.kind == "cell" or k in present}
+    sub = UnstructuredMesh(dim=mesh.dim, nodes=mesh.nodes, face_ptr=ptr, face_nodes=mesh.face_nodes[src],
+                           owner=owner.astype(np.int64), neighbour=neighbour.astype(np.int64), face_zone=fzone,
+                           n_cells=int(cmap.size), cell_zone=mesh.cell_zone[cmap], zones=zones,
+                           name=mesh.name + "-fluid")
+    zorder = sorted(sub.face_zones(), key=lambda z: (z.type != "interior", z.id))
+    rank = {z.id: r for r, z in enumerate(zorder)}
+    perm = np.argsort(np.array([rank[z] for z in fzone.tolist()]), kind="stable")
+    sub = sort_faces_by_zone(sub)
+    for z in sub.cell_zones():
+        w = np.flatnonzero(sub.cell_zone == z.id)
+        z.first, z.last = int(w[0]), int(w[-1])
+    return sub, fmap[perm], cmap
+
+
 def sort_faces_by_zone(mesh: UnstructuredMesh) -> UnstructuredMesh:
     """Faces reordered so each face zone is contiguous, interior zones first, then by zone id
     (stable within a zone); ``flowtrace/mesh/unstructured.py:783-810``."""

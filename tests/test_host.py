@@ -285,3 +285,24 @@ def test_ctypes_structs_match_the_c_header_layout(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_extract_cells_equals_the_reference_and_orients_the_interfaces():
+    """``extract_cells`` (the fluid part of a conjugate mesh) against digests of the reference's
+    own ``extract_cells`` (``tests/golden/extract_digests.json``): sub-mesh arrays, zones, face
+    and cell maps; the interface faces point out of the kept cells and the kept volume is the
+    fluid volume."""
+    import json
+
+    from gputest_b200.mesh.unstructured import compute_geometry, extract_cells
+    from tests.golden.mesh_cases import extract_digest, zoned_meshes
+
+    ref = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "extract_digests.json")))
+    for key, (m, keep) in zoned_meshes().items():
+        sub, fmap, cmap = extract_cells(m, keep)
+        assert extract_digest(sub, fmap, cmap) == ref[key], key
+        g, g0 = compute_geometry(sub), compute_geometry(m)
+        assert g.flipped_faces == 0
+        assert np.isclose(g.cell_volume.sum(), g0.cell_volume[keep].sum(), rtol=1e-13)
+        iface = [z for z in sub.boundary_zones() if z.name.startswith("interface-")]
+        assert len(iface) == 1 and iface[0].count > 0
