@@ -13,7 +13,9 @@ as fixtures; ``tests/test_oracle_golden.py`` re-checks the oracle against them.
 
 Scope: steady laminar flow (SIMPLE/SIMPLEC), energy with adiabatic/temperature/flux walls,
 upwind and bounded second-order convection, Green-Gauss or least-squares pressure force,
-uniform body force and per-cell momentum/energy sources, the divergence guard. Two
+uniform body force and per-cell momentum/energy sources, the divergence guard, and the
+k-omega SST model (``oracle/sst_oracle.py``: face viscosities with Spalding's wall law,
+transpose stress, turbulent energy diffusivity, the k and omega transport solves). Two
 features the reference lacks are added the way its test harness would add them:
 a per-cell Brinkman drag ``alpha V`` on the momentum diagonal, and a per-face boundary
 velocity profile written into ``ub_fixed`` (followed by ``initialize({})``).
@@ -233,6 +235,7 @@ class OracleFV:
         self.nb = Sb / np.sqrt(SSb)[:, None]
         self.db_t = db - np.einsum("fd,fd->f", db, self.nb)[:, None] * self.nb
         self.vol, self.xc, self.xfb = vol, xc, xfb
+        self.face_centre, self.face_area_vec = fc, Sall
         self.yb = np.abs(np.einsum("fd,fd->f", db, Sb)) / np.sqrt(SSb)
         self.wl, self.wlb, self.Ginv = wl, wlb, Ginv
         self.dP_f = xf - xc[P]
@@ -571,9 +574,10 @@ class OracleSimple:
     GUARD_FACTOR, GUARD_MIN_RELAX, GUARD_FALLBACK, GUARD_MIN_RELAX_U = 0.6, 0.1, True, 0.2
 
     def __init__(self, mesh, case, native=None, porosity=None, amg_theta=0.08):
-        for attr, off in (("turbulence", "laminar"), ("radiation", "off")):
-            if getattr(case, attr) != off:
-                raise NotImplementedError(f"{attr}={getattr(case, attr)!r} is outside the oracle's scope")
+        if case.turbulence not in ("laminar", "k-omega-sst"):
+            raise NotImplementedError(f"turbulence={case.turbulence!r} is outside the oracle's scope")
+        if case.radiation != "off":
+            raise NotImplementedError(f"radiation={case.radiation!r} is outside the oracle's scope")
         if case.unsteady or case.species or case.mrf or case.solids or case.periodic:
             raise NotImplementedError("transient, species, MRF, solids and periodic cases are outside the oracle's scope")
         self.case, self.mesh = case, mesh
@@ -603,6 +607,11 @@ class OracleSimple:
         self.Fb = self._boundary_flux_fixed(ub)
         self.mom_source = None
         self.energy_source = None
+        self.turb = None
+        if case.turbulence == "k-omega-sst":                                           # simple.py:115-117
+            from .sst_oracle import OracleSST
+
+            self.turb = OracleSST(self)
         self.guard_enabled = case.relax_p is None
         self._capture = None
         self._reset_guard()
@@ -617,12 +626,14 @@ class OracleSimple:
         pb = np.zeros(n)
         tk = np.zeros(n, dtype=np.int64)
         tv = np.zeros(n)
+        self.zone_specs = {}
         for z in self.mesh.boundary_zones():
             spec = case.boundaries.get(z.name)
             if spec is None:
                 spec = _Spec(FLUENT_TO_KIND.get(z.type, "wall"))
                 if spec.kind == "inlet":
                     spec.normal_speed = 1.0
+            self.zone_specs[z.name] = spec
             m = fv.bzone == z.id
             kind[m] = _KIND_CODE[spec.kind]
             if spec.kind in ("wall", "inlet"):
@@ -697,22 +708,30 @@ class OracleSimple:
         return flux * (self.m_inlet + self.m_pres)
 
     # ---- discretisation --------------------------------------------------------------------------
+    @staticmethod
+    def _split_gamma(gamma):
+        """A diffusivity as (interior-face, boundary-face) values; a scalar serves both
+        (``simple.py:333-338``)."""
+        return gamma if isinstance(gamma, tuple) else (gamma, gamma)
+
     def _coefficients(self, gamma, dirichlet):
         """``simple.py:340-353``."""
         fv, F, Fb = self.fv, self.F, self.Fb
-        D = gamma * fv.alpha
+        gf, gb = self._split_gamma(gamma)
+        D = gf * fv.alpha
         aPN = -(D + np.maximum(-F, 0.0))
         aNP = -(D + np.maximum(F, 0.0))
-        Db = gamma * fv.alpha_b * dirichlet
+        Db = gb * fv.alpha_b * dirichlet
         diag = fv.scatter(D + np.maximum(F, 0.0), D + np.maximum(-F, 0.0), Db + np.maximum(Fb, 0.0))
         return diag, aPN, aNP, Db
 
     def _rhs(self, gamma, phi, grad, phi_b, Db, extra=None, scheme=None):
         """``simple.py:355-374``."""
         fv, F, Fb = self.fv, self.F, self.Fb
+        gface, _ = self._split_gamma(gamma)
         rhs = fv.Cb @ ((Db + np.maximum(-Fb, 0.0)) * phi_b)
         gf = fv.face_interp_vec(grad)
-        rhs = rhs + fv.Cdiff @ (gamma * np.sum(gf * fv.Tvec, axis=1))
+        rhs = rhs + fv.Cdiff @ (gface * np.sum(gf * fv.Tvec, axis=1))
         if (scheme or self.case.scheme) == "second-order":
             P, N = fv.P, fv.N
             phP, phN = phi[P], phi[N]
@@ -768,13 +787,17 @@ class OracleSimple:
             src = src + fv.vol[:, None] * drive[None, :]
         if self.mom_source is not None:
             src = src + self.mom_source
+        gm = mu
+        if self.turb is not None:                                                      # simple.py:545-548
+            gm = self.turb.momentum_viscosity(U)
+            src = src + self.turb.transpose_stress(gU)
         res = {}
         Ustar = np.empty_like(U)
         au = self.relax_u
-        diag, aPN, aNP, Db = self._coefficients(mu, self.m_dirvel)
+        diag, aPN, aNP, Db = self._coefficients(gm, self.m_dirvel)
         if self.porosity is not None:  # implicit Brinkman drag alpha V (not in the reference)
             diag = diag + self.porosity * fv.vol
-        rhs_all = [self._rhs(mu, U[:, k], gU[k], ub[:, k], Db, src[:, k]) for k in range(dim)]
+        rhs_all = [self._rhs(gm, U[:, k], gU[k], ub[:, k], Db, src[:, k]) for k in range(dim)]
         A = fv.matrix(diag, aPN, aNP)
         num = [float(np.sum(np.abs(rhs_all[k] - A @ U[:, k]))) for k in range(dim)]     # simple.py:565-569
         den = [float(np.sum(np.abs(diag * U[:, k]))) for k in range(dim)]
@@ -835,6 +858,12 @@ class OracleSimple:
         if self.energy:
             res["energy"] = self._energy()
             cap["energy"] = self._energy_capture
+        if self.turb is not None:                                                      # simple.py:662-669
+            ubc = self._velocity_bvals(self.U, gU)
+            gUc = [fv.gradient(self.U[:, k], ubc[:, k]) for k in range(dim)]
+            k_old, w_old = self.turb.k, self.turb.w
+            res.update(self.turb.solve(gUc))
+            cap["turbulence"] = {"k": (k_old, self.turb.k), "omega": (w_old, self.turb.w)}
         self.iteration += 1
         self.step_count = self.iteration
         self.last_linear = {"momentum_iters": its, "pressure_iters": pinfo.iterations,
@@ -861,6 +890,8 @@ class OracleSimple:
         """``simple.py:778-813`` (laminar, no radiation)."""
         c, fv = self.case, self.fv
         gam = c.conductivity / c.cp
+        if self.turb is not None:
+            gam = self.turb.energy_diffusivity(gam)                                    # simple.py:781-782
         T = self.T
         TP = T[fv.Pb]
         fixed = self.tkind == T_FIXED
@@ -953,6 +984,8 @@ class OracleSimple:
         out["pressure"] = self.p.copy()
         if self.energy:
             out["temperature"] = self.T.copy()
+        if self.turb is not None:
+            out.update(self.turb.fields())
         return out
 
     def state_dict(self):
@@ -961,6 +994,8 @@ class OracleSimple:
               "iteration": self.iteration}
         if self.energy:
             st["T"] = self.T.copy()
+        if getattr(self, "turb", None) is not None:
+            st.update(self.turb.state())
         st["time"], st["time_step"] = 0.0, 0
         st["res_continuity_norm"] = self._res_max5.get("continuity", 0.0)
         return st
@@ -976,6 +1011,8 @@ class OracleSimple:
         self.iteration = int(st.get("iteration", 0))
         self._gp = self._gU = self._gT = None
         self._capture = None
+        if self.turb is not None:
+            self.turb.load(st)
         if float(st.get("res_continuity_norm", 0.0)) > 0:
             self._res_max5["continuity"] = float(st["res_continuity_norm"])
 
@@ -986,3 +1023,4 @@ class _Spec:
     def __init__(self, kind):
         self.kind, self.velocity, self.normal_speed, self.pressure = kind, None, None, 0.0
         self.thermal, self.value = "adiabatic", 0.0
+        self.turb_intensity = self.turb_viscosity_ratio = self.k = self.omega = None

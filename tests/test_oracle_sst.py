@@ -1,0 +1,62 @@
+"""The oracle's k-omega SST model (``oracle/sst_oracle.py`` driven by ``OracleSimple``) against
+the reference's own SST solver, through the fixtures of ``tests/golden/sst_fixtures.npz`` (made
+by ``tests/golden/make_sst_golden.py`` on the cases of ``tests/golden/sst_cases.py``): Spalding's
+u+, the wall distance, the inlet and initial turbulence values, and after a number of outer
+iterations every field, residual and linear-solver count, the momentum face viscosities and the
+transpose-stress source."""
+
+import os
+
+import numpy as np
+import pytest
+
+from gputest_b200.mesh.unstructured import cartesian_mesh_2d, extrude_to_3d
+from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase
+from oracle.simplec_oracle import OracleSimple
+from oracle.sst_oracle import spalding_uplus
+from tests.golden.sst_cases import RE_Y, SST_CASES
+
+GOLD = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sst_fixtures.npz"))
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _oracle(name):
+    mesh_fn, kw, n = SST_CASES[name]
+    bnd = {z: BoundarySpec(**spec) for z, spec in kw["boundaries"].items()}
+    return OracleSimple(mesh_fn(cartesian_mesh_2d, extrude_to_3d), UnstructuredCase(**{**kw, "boundaries": bnd})), n
+
+
+def test_spalding_uplus_equals_the_reference():
+    assert np.array_equal(GOLD["spalding|re_y"], RE_Y)
+    assert _rel(spalding_uplus(RE_Y), GOLD["spalding|uplus"]) <= 1e-15
+    up = spalding_uplus(RE_Y)
+    assert up[0] == 0.0
+    assert np.allclose(up[1:4], np.sqrt(RE_Y[1:4]), rtol=2e-3)  # sublayer: u+ = y+
+
+
+@pytest.mark.parametrize("name", sorted(SST_CASES))
+def test_oracle_sst_equals_the_reference(name):
+    o, n = _oracle(name)
+    p = f"sst|{name}|"
+    t = o.turb
+    assert np.array_equal(t.y, GOLD[p + "wall_distance"])
+    for key, ours in (("kb_in", t.kb_in), ("sb_in", t.sb_in), ("k0", t.k), ("w0", t.w)):
+        assert np.array_equal(ours, GOLD[p + key]), key
+    for _ in range(n):
+        o.step()
+    assert o.iteration == int(GOLD[p + "iterations"][0])
+    fields = o.fields()
+    for k in (k.split("|", 3)[3] for k in GOLD.files if k.startswith(p + "field|")):
+        assert _rel(fields[k], GOLD[p + "field|" + k]) <= 1e-10, k
+    for k, v in o.residuals()["scaled"].items():
+        assert v == pytest.approx(float(GOLD[p + "res|" + k][0]), rel=1e-8), k
+    lin = list(o.last_linear["momentum_iters"]) + [o.last_linear["pressure_iters"]]
+    assert lin == list(GOLD[p + "linear"])
+    gf, gb = t.momentum_viscosity(o.U)
+    assert _rel(gf, GOLD[p + "mu_face"]) <= 1e-10
+    assert _rel(gb, GOLD[p + "mu_bface"]) <= 1e-10
+    assert _rel(t.transpose_stress(o._gU), GOLD[p + "transpose_stress"]) <= 1e-9
