@@ -13,7 +13,7 @@ from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "csrc", "libb2simplec.so")
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 B2S_OK = 0
 _ERRORS = {-1: "invalid argument", -2: "kernel launch failed", -3: "work space too small", -4: "no usable CUDA device",
@@ -45,6 +45,13 @@ class FlowParams(ctypes.Structure):
     _fields_ = [("rho", F64), ("mu", F64), ("relax_u", F64), ("relax_p", F64), ("body", F64 * 3),
                 ("simplec", I32), ("second_order", I32), ("singular_p", I32), ("pad", I32),
                 ("relax_u_cell", P), ("relax_p_cell", P), ("simplec_cell", P)]
+
+
+class SST(ctypes.Structure):
+    """``b2s_sst``: constants and set-up arrays of the k-omega SST model."""
+    _fields_ = [(name, F64) for name in ("rho", "mu", "nu", "k_min", "w_min", "relax_k", "relax_w", "k_over_cp", "eb",
+                                         "cmu25", "g1", "g2")] + [("second_order", I32), ("pad_", I32)] + [
+        (name, P) for name in ("y", "y_wall", "yb", "kb_in", "wb_in")]
 
 
 class SolveInfo(ctypes.Structure):
@@ -125,6 +132,16 @@ _SIGS = {
                                    ctypes.c_int, ctypes.c_int, P, P, P, I64, P, P, P], ctypes.c_int),
     "b2s_pcg_groups_workspace_bytes": ([P], I64),
     "b2s_residual_vjp_d": ([P, P, F64, F64, F64, ctypes.c_int] + [P] * 18 + [P], ctypes.c_int),
+    # k-omega SST
+    "b2s_momentum_assemble_turb_d": ([P] * 21 + [P], ctypes.c_int),
+    "b2s_energy_assemble_turb_d": ([P, P, P, P, F64, F64, ctypes.c_int] + [P] * 12 + [P], ctypes.c_int),
+    "b2s_sst_part_blocks": ([P], ctypes.c_int),
+    "b2s_sst_momentum_terms_d": ([P] * 12 + [P], ctypes.c_int),
+    "b2s_sst_bvals_d": ([P] * 7 + [P], ctypes.c_int),
+    "b2s_sst_sources_d": ([P] * 7 + [P], ctypes.c_int),
+    "b2s_sst_transport_assemble_d": ([P, P, ctypes.c_int] + [P] * 11 + [P], ctypes.c_int),
+    "b2s_sst_transport_finish_d": ([P, P, ctypes.c_int] + [P] * 9 + [P], ctypes.c_int),
+    "b2s_sst_update_d": ([P] * 6 + [P], ctypes.c_int),
     "b2s_pcg_groups_mixed_d": ([P, P, P, P, P, P, P, I32, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, F64, P, I64,
                                 P, P, P], ctypes.c_int),
 }

@@ -14,44 +14,9 @@
 //
 // Bandwidth: each interior face is read by its two cells; with RCM-ordered cells the second
 // read falls inside a window that L2 (126 MB) holds, so DRAM sees each face once.
-#include "b2s_common.cuh"
+#include "b2s_fv.cuh"
 
 namespace b2s {
-
-// numpy.maximum(x, 0.0): NaN propagates, -0.0 stays -0.0.
-__device__ __forceinline__ double npmax0(double x) { return (x < 0.0) ? 0.0 : x; }
-__device__ __forceinline__ double npmin(double a, double b) { return (a <= b || a != a) ? a : b; }
-__device__ __forceinline__ double npmax(double a, double b) { return (a >= b || a != a) ? a : b; }
-
-// Visit the rows of Cdiff: the owned and neighbour faces of cell c merged by reference face
-// index; fn(face, +1/-1).
-template <class Fn>
-__device__ __forceinline__ void for_cdiff(const b2s_mesh& m, int c, Fn fn) {
-  int j = m.own_ptr[c], je = m.own_ptr[c + 1];
-  int k = m.nei_ptr[c], ke = m.nei_ptr[c + 1];
-  int kf = k < ke ? m.nei_face[k] : 0;
-  while (j < je || k < ke) {
-    bool own = (k >= ke) || (j < je && m.forig[j] < m.forig[kf]);
-    if (own) {
-      fn(j, true);
-      ++j;
-    } else {
-      fn(kf, false);
-      ++k;
-      if (k < ke) kf = m.nei_face[k];
-    }
-  }
-}
-
-// Cells of this block in a stage that writes one partial sum per block: a grid-stride range
-// of cells, or, on a tiled mesh (block-diagonal batches), exactly the cells of tile blockIdx.x.
-struct CellRange {
-  int c, end, step;
-};
-__device__ __forceinline__ CellRange cell_range(const b2s_mesh& m) {
-  if (m.tiles) return {m.tiles[blockIdx.x] + (int)threadIdx.x, m.tiles[blockIdx.x + 1], (int)blockDim.x};
-  return {(int)(blockIdx.x * blockDim.x + threadIdx.x), m.nc, (int)(gridDim.x * blockDim.x)};
-}
 
 // ------------------------------------------------------------------------------ face interp
 __global__ void face_interp_k(b2s_mesh m, int k, const double* __restrict__ phi, double* __restrict__ out) {
@@ -234,121 +199,16 @@ __global__ void flow_bvals_k(b2s_mesh m, b2s_bc bc, const double* __restrict__ U
   }
 }
 
-// ------------------------------------------------------------------------------ transport rows
-// One row of a convection-diffusion system (simple.py:340-374): coefficients, the CSR row,
-// and the right-hand side of NQ scalar fields that share the matrix.
-//   diag = (Cown(D + max(F,0)) + Cnei(D + max(-F,0))) + Cb(Db + max(Fb,0)),  D = gamma alpha
-//   aPN = -(D + max(-F,0)), aNP = -(D + max(F,0)),  Db = gamma alpha_b dirichlet
-//   rhs = Cb((Db + max(-Fb,0)) phib) + Cdiff(gamma gf.T) [- Cdiff(F (ho - up))] + extra
-template <int DIM, int NQ>
-struct RowOut {
-  double diag;     // a_P (before relaxation and extra diagonal terms)
-  double sumnb;    // scatter(-aPN, -aNP)
-  double rhs[NQ];  // without the extra source
-};
-
-template <int DIM, int NQ, class VT>
-__device__ __forceinline__ RowOut<DIM, NQ> transport_row(const b2s_mesh& m, int c, double gamma,
-                                                         const double* dirichlet, const double* F, const double* Fb,
-                                                         const double* phi, int64_t phi_stride,
-                                                         const double* grad, int64_t grad_stride,
-                                                         const double* phib, int64_t phib_stride, bool second,
-                                                         VT* val, bool write_offdiag) {
-  const int nc = m.nc, nf = m.nf, nb = m.nb;
-  RowOut<DIM, NQ> o;
-  double s_own = 0.0, s_nei = 0.0, s_b = 0.0, nb_own = 0.0, nb_nei = 0.0;
-  for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
-    const double D = gamma * m.alpha[f], Ff = F[f];
-    s_own += D + npmax0(Ff);
-    const double aPN = -(D + npmax0(-Ff));
-    nb_own += -aPN;
-    if (write_offdiag) val[m.slot_PN[f]] = aPN;
-  }
-  for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
-    const int f = m.nei_face[k];
-    const double D = gamma * m.alpha[f], Ff = F[f];
-    s_nei += D + npmax0(-Ff);
-    const double aNP = -(D + npmax0(Ff));
-    nb_nei += -aNP;
-    if (write_offdiag) val[m.slot_NP[f]] = aNP;
-  }
-  double rb[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) rb[q] = 0.0;
-  for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) {
-    const double Db = gamma * m.alpha_b[f] * dirichlet[f];
-    const double Fbf = Fb[f];
-    s_b += Db + npmax0(Fbf);
-    const double coef = Db + npmax0(-Fbf);
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) rb[q] += coef * phib[q * phib_stride + f];
-  }
-  o.diag = (s_own + s_nei) + s_b;
-  o.sumnb = nb_own + nb_nei;
-  // explicit non-orthogonal diffusion and deferred second-order correction over Cdiff rows
-  double rn[NQ], rh[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) rn[q] = rh[q] = 0.0;
-  for_cdiff(m, c, [&](int f, bool own) {
-    const int P = m.fP[f], N = m.fN[f];
-    const double w = m.w[f], w1 = 1.0 - w, Ff = F[f];
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      const double* g = grad + q * grad_stride;
-      double s = 0.0;
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) {
-        const double gf = w * g[(int64_t)a * nc + P] + w1 * g[(int64_t)a * nc + N];
-        const double t = gf * m.Tv[(int64_t)a * nf + f];
-        s = (a == 0) ? t : s + t;
-      }
-      const double v = gamma * s;
-      rn[q] += own ? v : -v;
-      if (second) {
-        const double* ph = phi + q * phi_stride;
-        const double phP = ph[P], phN = ph[N];
-        double hoP = 0.0, hoN = 0.0;
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-          const double tP = g[(int64_t)a * nc + P] * m.dPf[(int64_t)a * nf + f];
-          const double tN = g[(int64_t)a * nc + N] * m.dNf[(int64_t)a * nf + f];
-          hoP = (a == 0) ? tP : hoP + tP;
-          hoN = (a == 0) ? tN : hoN + tN;
-        }
-        hoP = phP + hoP;
-        hoN = phN + hoN;
-        const bool up = Ff >= 0.0;
-        const double lo = npmin(phP, phN), hi = npmax(phP, phN);
-        const double ho = npmin(npmax(up ? hoP : hoN, lo), hi);
-        const double dc = Ff * (ho - (up ? phP : phN));
-        rh[q] += own ? dc : -dc;
-      }
-    }
-  });
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    double r = rb[q] + rn[q];
-    if (second) r = r - rh[q];
-    o.rhs[q] = r;
-  }
-  return o;
-}
-
-// (A x)_c over the CSR row in stored order with a_cc = dval (scipy's csr_matvec order).
-__device__ __forceinline__ double row_apply(const b2s_mesh& m, const double* val, int c, double dval,
-                                            const double* x) {
-  const int sd = m.slot_diag[c];
-  double s = 0.0;
-  for (int j = m.rowptr[c]; j < m.rowptr[c + 1]; ++j) s += (j == sd ? dval : val[j]) * x[m.col[j]];
-  return s;
-}
 
 // ------------------------------------------------------------------------------ momentum
 // 2-D: at most 64 registers, so four 256-thread blocks fit per SM and a 131k-cell mesh runs in
 // one wave (80 registers gave 1.16 waves; measured 0.045 -> 0.033 ms); 3-D keeps the 128
 // registers it uses without a bound (two blocks per SM: a tighter bound's spills cost what the
 // occupancy gains).
-template <int DIM>
+// TURB: per-face viscosities mu_f [nf] / mu_b [nb] and a per-cell source tsrc [DIM][nc] from the
+// turbulence model (mu + mu_t, the wall-function viscosity on walls, the transpose stress;
+// simple.py:545-548); the laminar instantiation is the scalar-viscosity kernel unchanged.
+template <int DIM, bool TURB>
 __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Up,
                                     const double* __restrict__ gUp, const double* __restrict__ gp,
                                     const double* __restrict__ bUp, const double* __restrict__ F,
@@ -356,7 +216,9 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_
                                     const double* __restrict__ msrc, double* __restrict__ val,
                                     double* __restrict__ diag_out, double* __restrict__ inv_out,
                                     double* __restrict__ dP_out, double* __restrict__ b_out,
-                                    double* __restrict__ br_out, double* __restrict__ part) {
+                                    double* __restrict__ br_out, double* __restrict__ part,
+                                    const double* __restrict__ mu_f, const double* __restrict__ mu_b,
+                                    const double* __restrict__ tsrc) {
   __shared__ double red[(kThreads / 32 + 1) * 2 * DIM];
   const int nc = m.nc, nb = m.nb;
   double acc[2 * DIM];
@@ -367,8 +229,14 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_
     const int c = r_.c;
     const double au = prm.relax_u_cell ? prm.relax_u_cell[c] : prm.relax_u;
     const bool simplec = prm.simplec_cell ? prm.simplec_cell[c] != 0 : prm.simplec != 0;
-    RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
-                                                 (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
+    RowOut<DIM, DIM> o;
+    if constexpr (TURB)
+      o = transport_row_g<DIM, DIM>(m, c, FaceGamma{mu_f, mu_b}, bc.m_dirvel, F, Fb, Up + nc, nc,
+                                    gUp + (int64_t)DIM * nc, (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0,
+                                    val, true);
+    else
+      o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
+                                  (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
     double diag = o.diag;
     const double V = m.vol[c];
     if (por) diag = diag + por[c] * V;
@@ -388,6 +256,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_
       double src = -gp[(int64_t)k * nc + c] * V;
       if (drive) src = src + V * prm.body[k];
       if (msrc) src = src + msrc[(int64_t)k * nc + c];
+      if constexpr (TURB) src = src + tsrc[(int64_t)k * nc + c];
       const double rhs = o.rhs[k] + src;
       const double* u = Up + (int64_t)(1 + k) * nc;
       const double Au = row_apply(m, val, c, diag, u);
@@ -594,8 +463,10 @@ __global__ void energy_bvals_k(b2s_mesh m, b2s_bc bc, const double* __restrict__
   }
 }
 
-template <int DIM>
-__global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, double gamma, double cp, double aT, int second,
+// GT: ScalarGamma (k/cp) or FaceGamma (k/cp + mu_t/Pr_t per face from the turbulence model,
+// simple.py:781-782).
+template <int DIM, class GT>
+__global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, GT gamma, double cp, double aT, int second,
                                   const double* __restrict__ T, const double* __restrict__ gT,
                                   const double* __restrict__ Tb, const double* __restrict__ F,
                                   const double* __restrict__ Fb, const double* __restrict__ esrc,
@@ -606,7 +477,7 @@ __global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, double gamma, double cp
   double acc[2] = {0.0, 0.0};
   for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
     const int c = r_.c;
-    RowOut<DIM, 1> o = transport_row<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
+    RowOut<DIM, 1> o = transport_row_g<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
                                              second != 0, val, true);
     // q_in = Cb(flux tval |Sb| / cp) (+ source)
     double q = 0.0;
@@ -870,23 +741,49 @@ int b2s_flow_bvals_d(const b2s_mesh* m, const b2s_bc* bc, const double* Up, cons
   return B2S_OK;
 }
 
+}  // extern "C"
+
+template <bool TURB>
+static int momentum_assemble(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Up,
+                             const double* gUp, const double* gp, const double* bUp, const double* F,
+                             const double* Fb, const double* porosity, const double* msrc, double* val,
+                             double* diag, double* inv, double* dP, double* b, double* br, double* part,
+                             const double* mu_f, const double* mu_b, const double* tsrc, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !diag || !inv || !dP || !b ||
+      !br || !part || !(prm->relax_u > 0.0))
+    return B2S_ERR_ARG;
+  if (TURB && (!mu_f || (!mu_b && m->nb) || !tsrc)) return B2S_ERR_ARG;
+  unsigned g = part_grid_m(*m);
+  if (m->dim == 2)
+    momentum_assemble_k<2, TURB><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb,
+                                                                       porosity, msrc, val, diag, inv, dP, b, br,
+                                                                       part, mu_f, mu_b, tsrc);
+  else
+    momentum_assemble_k<3, TURB><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb,
+                                                                       porosity, msrc, val, diag, inv, dP, b, br,
+                                                                       part, mu_f, mu_b, tsrc);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+extern "C" {
+
 int b2s_momentum_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Up,
                             const double* gUp, const double* gp, const double* bUp, const double* F,
                             const double* Fb, const double* porosity, const double* msrc, double* val,
                             double* diag, double* inv, double* dP, double* b, double* br, double* part,
                             b2s_stream_t s) {
-  if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !diag || !inv || !dP || !b ||
-      !br || !part || !(prm->relax_u > 0.0))
-    return B2S_ERR_ARG;
-  unsigned g = part_grid_m(*m);
-  if (m->dim == 2)
-    momentum_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb, porosity,
-                                                                 msrc, val, diag, inv, dP, b, br, part);
-  else
-    momentum_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb, porosity,
-                                                                 msrc, val, diag, inv, dP, b, br, part);
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  return momentum_assemble<false>(m, bc, prm, Up, gUp, gp, bUp, F, Fb, porosity, msrc, val, diag, inv, dP, b, br,
+                                  part, nullptr, nullptr, nullptr, s);
+}
+
+int b2s_momentum_assemble_turb_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Up,
+                                 const double* gUp, const double* gp, const double* bUp, const double* F,
+                                 const double* Fb, const double* porosity, const double* msrc, const double* mu_f,
+                                 const double* mu_b, const double* tsrc, double* val, double* diag, double* inv,
+                                 double* dP, double* b, double* br, double* part, b2s_stream_t s) {
+  return momentum_assemble<true>(m, bc, prm, Up, gUp, gp, bUp, F, Fb, porosity, msrc, val, diag, inv, dP, b, br,
+                                 part, mu_f, mu_b, tsrc, s);
 }
 
 int b2s_pressure_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm, const double* Ustar,
@@ -950,22 +847,44 @@ int b2s_energy_bvals_d(const b2s_mesh* m, const b2s_bc* bc, const double* T, con
   return B2S_OK;
 }
 
-int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp, double relax_T,
-                          int second_order, const double* T, const double* gT, const double* Tb, const double* F,
-                          const double* Fb, const double* esrc, double* val, double* diag, double* inv, double* b,
-                          double* br, double* part, b2s_stream_t s) {
+}  // extern "C"
+
+template <class GT>
+static int energy_assemble(const b2s_mesh* m, const b2s_bc* bc, GT gamma, double cp, double relax_T,
+                           int second_order, const double* T, const double* gT, const double* Tb, const double* F,
+                           const double* Fb, const double* esrc, double* val, double* diag, double* inv, double* b,
+                           double* br, double* part, b2s_stream_t s) {
   if (!mesh_ok(m) || !bc || !T || !gT || (!Tb && m->nb) || !F || !Fb || !val || !diag || !inv || !b || !br ||
       !part || !(relax_T > 0.0) || !(cp != 0.0))
     return B2S_ERR_ARG;
   unsigned g = part_grid_m(*m);
   if (m->dim == 2)
-    energy_assemble_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT, Tb,
-                                                               F, Fb, esrc, val, diag, inv, b, br, part);
+    energy_assemble_k<2, GT><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT,
+                                                                   Tb, F, Fb, esrc, val, diag, inv, b, br, part);
   else
-    energy_assemble_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT, Tb,
-                                                               F, Fb, esrc, val, diag, inv, b, br, part);
+    energy_assemble_k<3, GT><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T, gT,
+                                                                   Tb, F, Fb, esrc, val, diag, inv, b, br, part);
   B2S_LAUNCH_CHECK();
   return B2S_OK;
+}
+
+extern "C" {
+
+int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp, double relax_T,
+                          int second_order, const double* T, const double* gT, const double* Tb, const double* F,
+                          const double* Fb, const double* esrc, double* val, double* diag, double* inv, double* b,
+                          double* br, double* part, b2s_stream_t s) {
+  return energy_assemble(m, bc, ScalarGamma{gamma}, cp, relax_T, second_order, T, gT, Tb, F, Fb, esrc, val, diag,
+                         inv, b, br, part, s);
+}
+
+int b2s_energy_assemble_turb_d(const b2s_mesh* m, const b2s_bc* bc, const double* gamma_f, const double* gamma_b,
+                               double cp, double relax_T, int second_order, const double* T, const double* gT,
+                               const double* Tb, const double* F, const double* Fb, const double* esrc, double* val,
+                               double* diag, double* inv, double* b, double* br, double* part, b2s_stream_t s) {
+  if (!gamma_f || (!gamma_b && m && m->nb)) return B2S_ERR_ARG;
+  return energy_assemble(m, bc, FaceGamma{gamma_f, gamma_b}, cp, relax_T, second_order, T, gT, Tb, F, Fb, esrc, val,
+                         diag, inv, b, br, part, s);
 }
 
 int b2s_momentum_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,

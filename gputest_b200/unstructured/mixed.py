@@ -34,6 +34,7 @@ class MixedSimpleSolver(SimpleSolver):
     """Drop-in ``SimpleSolver`` whose linear systems are stored and solved in float."""
 
     PRECISIONS = ("mixed", "fp32", "fp64")
+    TURBULENCE = ("laminar",)
     REFINE_PASSES = 8       # double refinement passes of the pressure-correction solve at most
     INNER_TOL_FLOOR = 1e-5  # smallest relative reduction asked of one float pass
 

@@ -22,15 +22,21 @@ brings back the residual sums and the linear-solver records:
   8. AMG-PCG of the pressure correction, one launch                b2s_pcg_amg_d
   9. flux, pressure and velocity corrections with grad(p'), fused  b2s_correct_d (+ mean removal)
  10. energy: boundary values, gradient, assembly, BiCGSTAB         b2s_energy_*_d
- 11. residual sums                                                 b2s_sum_partials_d
+ 11. k-omega SST: k and omega, mu_t (``turbulence.DeviceSST``)     b2s_sst_*_d
+ 12. residual sums                                                 b2s_sum_partials_d
+
+With the SST model, stage 4 takes per-face viscosities (mu + mu_t, Spalding's wall-function
+viscosity on walls) and the transpose-stress source from b2s_sst_momentum_terms_d, run between
+stages 3 and 4, and the energy equation the turbulent diffusivity k/cp + mu_t/Pr_t.
 
 Fields live on the device in the mesh's device numbering, component-major. The public
 attributes ``U``, ``p``, ``T``, ``F``, ``Fb`` and every report return host arrays in the
 reference's numbering. There is no CPU fallback: without a CUDA device the constructor
 raises.
 
-Not implemented (the constructor raises ``NotImplementedError``): turbulence, radiation,
-species, moving reference frames, solid zones, periodic pairs and transient runs.
+Not implemented (the constructor raises ``NotImplementedError``): the k-epsilon models,
+radiation, species, moving reference frames, solid zones, periodic pairs and transient runs
+(and the SST model in the mixed-precision and batched forms).
 Additions over the reference: ``set_porosity`` (implicit Brinkman drag alpha V on the momentum
 diagonal) and ``set_boundary_velocity`` (a per-face velocity profile on a wall or inlet zone).
 """
@@ -85,9 +91,9 @@ class DeviceBackend:
         torch.cuda.synchronize(self.torch_device)
 
 
-def _check_scope(case: UnstructuredCase, precisions=("fp64",)):
+def _check_scope(case: UnstructuredCase, precisions=("fp64",), turbulence=("laminar",)):
     unsupported = []
-    if case.turbulence != "laminar":
+    if case.turbulence not in turbulence:
         unsupported.append(f"turbulence={case.turbulence!r}")
     if case.radiation != "off":
         unsupported.append("radiation")
@@ -118,6 +124,7 @@ class SimpleSolver:
     GUARD_FALLBACK = True
     GUARD_MIN_RELAX_U = 0.2
     PRECISIONS = ("fp64",)
+    TURBULENCE = ("laminar", "k-omega-sst")
 
     def __init__(self, mesh: UnstructuredMesh, case: UnstructuredCase, backend=None, max_coarse: int = 150,
                  amg_theta: float = 0.08):
@@ -129,7 +136,7 @@ class SimpleSolver:
         (``amg.py:149-168``), far better conditioned on anisotropic 3-D meshes."""
         import torch
 
-        _check_scope(case, self.PRECISIONS)
+        _check_scope(case, self.PRECISIONS, self.TURBULENCE)
         self.case, self.mesh = case, mesh
         self.torch_device = _lib.require_device()
         self.be = DeviceBackend(self.torch_device)
@@ -174,8 +181,13 @@ class SimpleSolver:
         self.porosity = None
         self.mom_source = None
         self.energy_source = None
+        self.turb = None
         self._build_boundaries()
         self._allocate()
+        if case.turbulence == "k-omega-sst":
+            from .turbulence import DeviceSST
+
+            self.turb = DeviceSST(self)
         U0 = np.zeros((nc, dim))
         U0[:] = (list(case.init_velocity) + [0.0] * 3)[:dim]
         T0 = np.full(nc, float(case.init_T)) if self.energy else None
@@ -280,9 +292,14 @@ class SimpleSolver:
         self.Q_MOM, self.Q_CONT, self.Q_SUMP = 0, 2 * dim, 2 * dim + 1
         self.Q_SUMF, self.Q_SUMFB, self.Q_ENUM, self.Q_EDEN = 2 * dim + 2, 2 * dim + 3, 2 * dim + 4, 2 * dim + 5
         self.NQ = 2 * dim + 6
+        ninfo = dim + 2
+        if self.case.turbulence != "laminar":
+            # per field (k, omega): the blocks' maximum diagonal, then the two residual sums
+            self.Q_TMAX, self.Q_TRES = (self.NQ, self.NQ + 3), (self.NQ + 1, self.NQ + 4)
+            self.NQ += 6
+            ninfo += 2
         self.part = z(self.NQ * self.nblk)
         self.q_of = torch.arange(self.NQ, dtype=torch.int32, device=dev)
-        ninfo = dim + 2
         self.report = torch.zeros(self.NQ * 8 + ninfo * INFO_DTYPE.itemsize, dtype=torch.uint8, device=dev)
         # two pinned host copies of the report, each with the event that marks its copy done, so
         # that run() can enqueue the next iteration while the host reads this one's report
@@ -295,6 +312,7 @@ class SimpleSolver:
         self.info_mom = base
         self.info_p = base + dim * INFO_DTYPE.itemsize
         self.info_T = base + (dim + 1) * INFO_DTYPE.itemsize
+        self.info_turb = (base + (dim + 2) * INFO_DTYPE.itemsize, base + (dim + 3) * INFO_DTYPE.itemsize)
         wb = max(L.b2s_bicgstab_workspace_bytes(nc, dim), L.b2s_bicgstab_workspace_bytes(nc, 1))
         self.work_bicg = torch.empty(wb // 8 + 1, dtype=torch.float64, device=dev)
 
@@ -501,13 +519,25 @@ class SimpleSolver:
         self._mark("gradients")
         part = self.part
         pt = lambda q: part.data_ptr() + 8 * q * self.nblk  # noqa: E731
-        _lib.check(L.b2s_momentum_assemble_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(), gp.data_ptr(),
-                                             self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
-                                             None if self.porosity is None else self.porosity.data_ptr(),
-                                             None if self.mom_source is None else self.mom_source.data_ptr(),
-                                             self.val_A.data_ptr(), self.diag.data_ptr(), self.inv.data_ptr(),
-                                             self.dP.data_ptr(), self.bmom.data_ptr(), self.brmom.data_ptr(),
-                                             pt(self.Q_MOM), s), "b2s_momentum_assemble_d")
+        por = None if self.porosity is None else self.porosity.data_ptr()
+        msrc = None if self.mom_source is None else self.mom_source.data_ptr()
+        if self.turb is None:
+            _lib.check(L.b2s_momentum_assemble_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(),
+                                                 gp.data_ptr(), self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(), por,
+                                                 msrc, self.val_A.data_ptr(), self.diag.data_ptr(),
+                                                 self.inv.data_ptr(), self.dP.data_ptr(), self.bmom.data_ptr(),
+                                                 self.brmom.data_ptr(), pt(self.Q_MOM), s), "b2s_momentum_assemble_d")
+        else:
+            t = self.turb
+            self.kernel_launches += t.launch_momentum_terms(Up, self.gUp, old, s)
+            self._mark("turbulence_terms")
+            _lib.check(L.b2s_momentum_assemble_turb_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(),
+                                                      gp.data_ptr(), self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
+                                                      por, msrc, t.mu_f.data_ptr(), t.mu_b.data_ptr(),
+                                                      t.tsrc.data_ptr(), self.val_A.data_ptr(), self.diag.data_ptr(),
+                                                      self.inv.data_ptr(), self.dP.data_ptr(), self.bmom.data_ptr(),
+                                                      self.brmom.data_ptr(), pt(self.Q_MOM), s),
+                       "b2s_momentum_assemble_turb_d")
         self._mark("momentum_assembly")
         self.Ustar.copy_(Up[1:])
         _lib.check(L.b2s_bicgstab_jacobi_d(nc, dim, fv.rowptr.data_ptr(), fv.col.data_ptr(), self.val_A.data_ptr(),
@@ -542,6 +572,10 @@ class SimpleSolver:
             self._launch_energy(old, new, Fn, Fbn, s)
             self.kernel_launches += 4
             self._mark("energy")
+        if self.turb is not None:
+            self.kernel_launches += self.turb.launch_transport(old, new, Upn, Fn, Fbn, pt, self.Q_TMAX, self.Q_TRES,
+                                                               self.info_turb, s)
+            self._mark("turbulence")
         _lib.check(L.b2s_sum_partials_d(part.data_ptr(), self.nblk, self.NQ, self.NQ, self.q_of.data_ptr(),
                                         self.scal.data_ptr(), s), "b2s_sum_partials_d")
         self.kernel_launches += 1
@@ -559,13 +593,18 @@ class SimpleSolver:
                    "b2s_ls_gradient_d")
         self._lagT = True
         second = (c.scalar_scheme or c.scheme) == "second-order"
-        _lib.check(L.b2s_energy_assemble_d(m, bc, c.conductivity / c.cp, c.cp, c.relax_T, int(second), T.data_ptr(),
-                                           self.gT.data_ptr(), self.Tb.data_ptr(), Fn.data_ptr(), Fbn.data_ptr(),
-                                           None if self.energy_source is None else self.energy_source.data_ptr(),
-                                           self.val_T.data_ptr(), self.diagT.data_ptr(), self.invT.data_ptr(),
-                                           self.bT.data_ptr(), self.brT.data_ptr(),
-                                           self.part.data_ptr() + 8 * self.Q_ENUM * self.nblk, s),
-                   "b2s_energy_assemble_d")
+        esrc = None if self.energy_source is None else self.energy_source.data_ptr()
+        tail = (self.val_T.data_ptr(), self.diagT.data_ptr(), self.invT.data_ptr(), self.bT.data_ptr(),
+                self.brT.data_ptr(), self.part.data_ptr() + 8 * self.Q_ENUM * self.nblk, s)
+        if self.turb is None:
+            _lib.check(L.b2s_energy_assemble_d(m, bc, c.conductivity / c.cp, c.cp, c.relax_T, int(second), T.data_ptr(),
+                                               self.gT.data_ptr(), self.Tb.data_ptr(), Fn.data_ptr(), Fbn.data_ptr(),
+                                               esrc, *tail), "b2s_energy_assemble_d")
+        else:  # k/cp + mu_t/Pr_t per face (simple.py:781-782)
+            _lib.check(L.b2s_energy_assemble_turb_d(m, bc, self.turb.kT_f.data_ptr(), self.turb.kT_b.data_ptr(), c.cp,
+                                                    c.relax_T, int(second), T.data_ptr(), self.gT.data_ptr(),
+                                                    self.Tb.data_ptr(), Fn.data_ptr(), Fbn.data_ptr(), esrc, *tail),
+                       "b2s_energy_assemble_turb_d")
         Tn.copy_(T)
         _lib.check(L.b2s_bicgstab_jacobi_d(self.nc, 1, fv.rowptr.data_ptr(), fv.col.data_ptr(), self.val_T.data_ptr(),
                                            self.brT.data_ptr(), self.invT.data_ptr(), Tn.data_ptr(), 1e-3, 60, 1,
@@ -626,6 +665,8 @@ class SimpleSolver:
             out.append(self.gpf)
         if self.energy and getattr(self, "gT", None) is not None:
             out.append(self.gT)
+        if self.turb is not None:
+            out.append(self.turb.yplus)
         return out
 
     def _save_lagged(self):
@@ -687,6 +728,11 @@ class SimpleSolver:
             r, s_ = float(scal[self.Q_ENUM]), float(scal[self.Q_EDEN])
             res["energy"] = r / s_ if s_ > 0 else r
             cap["energy"] = {"info": infos[dim + 1], "alpha": c.relax_T}
+        if self.turb is not None:  # turbulence.py:297-300
+            for q, name in enumerate(("k", "omega")):
+                qn = self.Q_TRES[q]
+                res[name] = float(scal[qn]) / max(float(scal[qn + 1]), 1e-300)
+            cap["turbulence"] = {"k_info": infos[dim + 2], "omega_info": infos[dim + 3]}
         self.iteration += 1
         self.step_count = self.iteration
         self.last_linear = {"momentum_iters": [i.iterations for i in mom_info], "pressure_iters": p_info.iterations,
@@ -780,6 +826,8 @@ class SimpleSolver:
                 "iteration": self.iteration, "res_continuity_norm": self._res_max5.get("continuity", 0.0)}
         if self.energy:
             snap["T"] = self._T[c].clone()
+        if self.turb is not None:
+            snap["turb"] = self.turb.snapshot(c)
         return snap
 
     def _restore(self, snap):
@@ -791,6 +839,8 @@ class SimpleSolver:
         self._Fb[tgt].copy_(snap["Fb"])
         if self.energy and "T" in snap:
             self._T[tgt].copy_(snap["T"])
+        if self.turb is not None and "turb" in snap:
+            self.turb.restore(snap["turb"], tgt)
         self._cur = tgt
         self.iteration = int(snap.get("iteration", 0))
         self._lag = self._lagT = False
@@ -843,6 +893,8 @@ class SimpleSolver:
         st = {"U": self.U, "p": self.p, "F": self.F, "Fb": self.Fb, "iteration": self.iteration}
         if self.energy:
             st["T"] = self.T
+        if self.turb is not None:
+            st.update(self.turb.state(self._cur))
         st["time"], st["time_step"] = 0.0, 0
         st["res_continuity_norm"] = self._res_max5.get("continuity", 0.0)
         return st
@@ -862,8 +914,12 @@ class SimpleSolver:
             snap["Fb"][: h.n_bf] = fv.bfaces_to_device(st["Fb"])
         if self.energy and "T" in st:
             snap["T"] = fv.cells_to_device(np.asarray(st["T"], dtype=np.float64))
+        if self.turb is not None:
+            snap["turb"] = self.turb.snapshot(self._cur)
         self._capture = None
         self._restore(snap)
+        if self.turb is not None:
+            self.turb.load(st, self._cur)
 
     # ------------------------------------------------------------------ reports
     def residuals(self) -> dict:
@@ -899,6 +955,8 @@ class SimpleSolver:
         out["pressure"] = self.p
         if self.energy:
             out["temperature"] = self.T
+        if self.turb is not None:
+            out.update(self.turb.fields(self._cur))
         if names:
             out = {k: v for k, v in out.items() if k in names}
         return out
@@ -931,6 +989,8 @@ class SimpleSolver:
         h = self.fv.host
         pb = self._pressure_bvals_host()
         mu_b = np.full(pb.shape, float(self.case.viscosity))
+        if self.turb is not None:  # simple.py:900-904
+            mu_b = self.turb.wall_viscosity(self._Up[self._cur], self.gUp, self._cur)
         du = self.U[h.Pb] - self._ub_fixed_h
         du_t = du - np.einsum("fd,fd->f", du, h.nb)[:, None] * h.nb
         f_p = pb[:, None] * h.Sb

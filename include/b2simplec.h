@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define B2S_ABI_VERSION 3
+#define B2S_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define B2S_API __attribute__((visibility("default")))
@@ -202,6 +202,17 @@ B2S_API int b2s_momentum_assemble_d(const b2s_mesh* m, const b2s_bc* bc, const b
                             double* diag, double* inv, double* dP, double* b, double* br, double* part,
                             b2s_stream_t s);
 
+/* b2s_momentum_assemble_d with a viscosity per face and an extra per-cell source, as the
+ * turbulence model supplies them (simple.py:545-548): mu_f [nf] (mu + mu_t), mu_b [nb] (walls:
+ * the wall-function viscosity), tsrc [dim][nc] (the transpose stress, a cell total added after
+ * msrc). prm->mu is not used. */
+B2S_API int b2s_momentum_assemble_turb_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                         const double* Up, const double* gUp, const double* gp, const double* bUp,
+                                         const double* F, const double* Fb, const double* porosity,
+                                         const double* msrc, const double* mu_f, const double* mu_b,
+                                         const double* tsrc, double* val, double* diag, double* inv, double* dP,
+                                         double* b, double* br, double* part, b2s_stream_t s);
+
 /* Rhie-Chow predictor fluxes and the pressure-correction system (simple.py:583-623):
  *   in:  Ustar [dim][nc], p [nc], gp [dim][nc], dP [nc]
  *   out: Fst [nf], cf [nf], Fbst [nb], cb [nb], val [nnz] (A_p), rhs [nc] (= -m*),
@@ -237,6 +248,14 @@ B2S_API int b2s_energy_assemble_d(const b2s_mesh* m, const b2s_bc* bc, double ga
                           int second_order, const double* T, const double* gT, const double* Tb, const double* F,
                           const double* Fb, const double* esrc, double* val, double* diag, double* inv, double* b,
                           double* br, double* part, b2s_stream_t s);
+
+/* b2s_energy_assemble_d with the diffusivity per face: gamma_f [nf], gamma_b [nb] (k/cp + mu_t/Pr_t,
+ * walls k/cp; flowtrace/unstructured/turbulence.py:245-249). */
+B2S_API int b2s_energy_assemble_turb_d(const b2s_mesh* m, const b2s_bc* bc, const double* gamma_f,
+                                       const double* gamma_b, double cp, double relax_T, int second_order,
+                                       const double* T, const double* gT, const double* Tb, const double* F,
+                                       const double* Fb, const double* esrc, double* val, double* diag, double* inv,
+                                       double* b, double* br, double* part, b2s_stream_t s);
 
 /* Row residuals and scales of a system (flowtrace/unstructured/diagnostics.py:146-151):
  * r = b - A x, s = |b| + |A| |x|; with dval, row i's diagonal entry (slot_diag[i]) is dval[i]. */
@@ -478,6 +497,76 @@ B2S_API int b2s_residual_vjp_d(const b2s_mesh* m, const b2s_bc* bc, double rho, 
                                const double* lg, const double* lF, const double* lFb, double* work, double* oU,
                                double* op, double* og, double* oF, double* oFb, double* opor, double* oub,
                                b2s_stream_t s);
+
+/* ----------------------------------------------------------------------------------------- */
+/* k-omega SST (Menter, Kuntz & Langtry 2003; flowtrace/unstructured/turbulence.py:116-438).
+ * The model's state is k and omega ([2][nc]: k then omega) and mu_t [nc]; per outer iteration:
+ *   before the momentum assembly   b2s_sst_momentum_terms_d
+ *   after the energy equation      b2s_sst_bvals_d, b2s_ls_gradient_d (2 fields),
+ *                                  b2s_sst_sources_d, then for q = 0 (k) and q = 1 (omega):
+ *                                  b2s_sst_transport_assemble_d, b2s_sst_transport_finish_d and a
+ *                                  Jacobi-BiCGSTAB solve (tol 1e-3, 60 iterations, from the old
+ *                                  field), and b2s_sst_update_d. */
+typedef struct b2s_sst {
+  double rho, mu, nu;       /* density, molecular viscosity, mu / rho */
+  double k_min, w_min;      /* floors of k and omega */
+  double relax_k, relax_w;  /* under-relaxation of the two transport solves */
+  double k_over_cp;         /* energy: conductivity / cp (unused without energy) */
+  double eb;                /* exp(-kappa B) of Spalding's law (kappa 0.41, B 5.2) */
+  double cmu25;             /* Cmu^0.25 (Cmu 0.09) */
+  double g1, g2;            /* gamma_1,2 = beta_1,2 / beta* - sigma_w1,2 kappa^2 / sqrt(beta*) */
+  int32_t second_order;     /* bounded second-order convection of k and omega (else upwind) */
+  int32_t pad_;
+  const double* y;          /* [nc] wall distance (wall cells: normal distance to their wall face) */
+  const double* y_wall;     /* [nc] wall cells: smallest normal distance to one of their wall faces; +inf elsewhere */
+  const double* yb;         /* [nb] |db . n|, owner centre to face, normal */
+  const double* kb_in;      /* [nb] k where the face is fixed (inlets, inflow at openings) */
+  const double* wb_in;      /* [nb] omega there */
+} b2s_sst;
+
+/* Blocks (= partial sums) of the two SST transport passes; equals b2s_mesh_part_blocks. */
+B2S_API int b2s_sst_part_blocks(const b2s_mesh* m);
+
+/* Face viscosities and source of the momentum equations and the turbulent heat diffusivity
+ * (turbulence.py:235-261, 399-417) from U (Up = [p, U], [1+dim][nc]), its gradient
+ * (gUp [1+dim][dim][nc]) and mu_t: mu_f [nf], mu_b [nb] (walls: mu Re_y / u+^2 from Spalding's
+ * law), yplus [nb] (optional, 0 off walls), tsrc [dim][nc] = div(mu_t (grad U)^T), and, both or
+ * neither, kT_f [nf] / kT_b [nb] = k/cp + mu_t/Pr_t (walls k/cp). */
+B2S_API int b2s_sst_momentum_terms_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_sst* t, const double* Up,
+                                     const double* gUp, const double* mut, double* mu_f, double* mu_b,
+                                     double* yplus, double* tsrc, double* kT_f, double* kT_b, b2s_stream_t s);
+
+/* Boundary values of k and omega (KWb [2][nb]) and the mask of fixed faces (fixed [nb], 0/1):
+ * fixed at inlets and at open faces with inflow (Fb < 0), zero-gradient elsewhere. */
+B2S_API int b2s_sst_bvals_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_sst* t, const double* KW,
+                            const double* Fb, double* KWb, double* fixed, b2s_stream_t s);
+
+/* Per cell, from grad U (gU [dim][dim][nc]), k/omega, their gradients (gKW [2][dim][nc]) and mu_t:
+ * coef [8][nc] = (mu + sigma_k mu_t, mu + sigma_w mu_t, Sc_k, Sp_k, Sc_w, Sp_w, |S|, near-wall
+ * omega of wall cells). */
+B2S_API int b2s_sst_sources_d(const b2s_mesh* m, const b2s_sst* t, const double* gU, const double* KW,
+                              const double* gKW, const double* mut, double* coef, b2s_stream_t s);
+
+/* Transport system of field q (0 k, 1 omega): off-diagonals into val [nnz], the unrelaxed
+ * diagonal (+ Sp V) into diag [nc], the right-hand side (+ Sc V) into b [nc], each block's
+ * maximum diagonal into part_max [b2s_sst_part_blocks]. */
+B2S_API int b2s_sst_transport_assemble_d(const b2s_mesh* m, const b2s_sst* t, int q, const double* KW,
+                                         const double* KWb, const double* fixed, const double* gKW, const double* F,
+                                         const double* Fb, const double* coef, double* val, double* diag, double* b,
+                                         double* part_max, b2s_stream_t s);
+
+/* Completes the system of b2s_sst_transport_assemble_d: for omega the wall cells are pinned to
+ * coef[7] (diag and b += 1e10 max(diag) x (1, value)); the residual sums |b - A phi| and
+ * |diag phi| over the cells above the floor and not pinned go to part_res (2 quantities x
+ * blocks); val's diagonal, inv [nc] and br [nc] receive the relaxed system. */
+B2S_API int b2s_sst_transport_finish_d(const b2s_mesh* m, const b2s_sst* t, int q, const double* KW,
+                                       const double* coef, const double* part_max, double* val, double* diag,
+                                       double* b, double* inv, double* br, double* part_res, b2s_stream_t s);
+
+/* New state from the solves (KWn [2][nc]): k, omega floored into KW [2][nc], and
+ * mu_t = rho a1 k / max(a1 omega, |S| F2) into mut [nc]. */
+B2S_API int b2s_sst_update_d(const b2s_mesh* m, const b2s_sst* t, const double* KWn, const double* coef,
+                             double* KW, double* mut, b2s_stream_t s);
 
 #ifdef __cplusplus
 }

@@ -268,7 +268,7 @@ def test_ctypes_structs_match_the_c_header_layout(tmp_path):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     pairs = {"b2s_mesh": _lib.Mesh, "b2s_bc": _lib.BC, "b2s_flow_params": _lib.FlowParams,
              "b2s_solve_info": _lib.SolveInfo, "b2s_amg_level": _lib.AmgLevel, "b2s_amg": _lib.Amg,
-             "b2s_amg_f32": _lib.Amg32, "b2s_team_config": _lib.TeamConfig}
+             "b2s_amg_f32": _lib.Amg32, "b2s_team_config": _lib.TeamConfig, "b2s_sst": _lib.SST}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "b2simplec.h"', "int main(void) {"]
     for cname, py in pairs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')

@@ -60,3 +60,51 @@ def test_oracle_sst_equals_the_reference(name):
     assert _rel(gf, GOLD[p + "mu_face"]) <= 1e-10
     assert _rel(gb, GOLD[p + "mu_bface"]) <= 1e-10
     assert _rel(t.transpose_stress(o._gU), GOLD[p + "transpose_stress"]) <= 1e-9
+
+
+@pytest.mark.parametrize("name", sorted(SST_CASES))
+def test_product_sst_setup_equals_the_reference(name):
+    """The B200 path's host set-up of the SST model (wall distance, inflow and initial values;
+    ``gputest_b200.unstructured.turbulence.host_setup``) against the reference's."""
+    from gputest_b200.unstructured.fvmesh import HostFV
+    from gputest_b200.unstructured.turbulence import host_setup
+
+    o, _ = _oracle(name)
+    hs = host_setup(o.mesh, HostFV(o.mesh), o.bkind, o.zone_specs, o.ub_fixed, o.case)
+    p = f"sst|{name}|"
+    assert np.array_equal(hs["y"], GOLD[p + "wall_distance"])
+    assert np.array_equal(hs["kb_in"], GOLD[p + "kb_in"]) and np.array_equal(hs["wb_in"], GOLD[p + "sb_in"])
+    assert hs["k0"] == GOLD[p + "k0"][0] and hs["w0"] == GOLD[p + "w0"][0]
+    assert np.array_equal(np.isfinite(hs["y_wall"]), np.isin(np.arange(o.nc), o.turb.wall_cells))
+
+
+def test_sst_is_rejected_where_it_is_not_implemented():
+    """The mixed-precision and batched solvers do not carry the SST model: they refuse the case
+    before touching a device."""
+    from gputest_b200.unstructured.mixed import MixedSimpleSolver
+
+    mesh_fn, kw, _ = SST_CASES["chan2d"]
+    bnd = {z: BoundarySpec(**spec) for z, spec in kw["boundaries"].items()}
+    with pytest.raises(NotImplementedError, match="turbulence"):
+        MixedSimpleSolver(mesh_fn(cartesian_mesh_2d, extrude_to_3d),
+                          UnstructuredCase(**{**kw, "boundaries": bnd, "precision": "mixed"}))
+
+
+def test_energy_case_temperature_is_set_to_1e_4():
+    """On the triangulated channel with energy, the reference's temperature after 20 iterations is
+    fixed only to about 1e-4: perturbing mu_t by 1e-15 relative (below the roundoff of the
+    operations) changes the iteration count of an energy BiCGSTAB solve (tolerance 1e-3) and
+    moves the temperature by up to ~1e-4, while every other field moves by ~1e-13. The CUDA
+    parity test compares the temperature of this case at 2e-4 for that reason."""
+    worst, others = 0.0, 0.0
+    for seed in range(3):
+        o, n = _oracle("tri2d_energy")
+        o.turb.mut = o.turb.mut * (1 + 1e-15 * np.random.default_rng(seed).standard_normal(o.nc))
+        for _ in range(n):
+            o.step()
+        f = o.fields()
+        p = "sst|tri2d_energy|field|"
+        worst = max(worst, _rel(f["temperature"], GOLD[p + "temperature"]))
+        others = max(others, *(_rel(f[k], GOLD[p + k]) for k in ("x-velocity", "pressure", "turb-kinetic-energy")))
+    assert 1e-6 < worst < 2e-4
+    assert others < 1e-11
