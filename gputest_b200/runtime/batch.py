@@ -7,7 +7,8 @@ grouped, and every group of cases that can share one iteration - the same dimens
 settings ``BatchSimpleSolver`` requires them to share, no energy equation - is solved as
 block-diagonal batches of at most ``max_batch_cells`` cells (largest cases first) in one
 ``BatchSimpleSolver`` each (one set of launches per stage for all its cases). A case that cannot
-share (energy, a setting of its own, ``precision="fp64"``) is solved alone by ``SimpleSolver``.
+share (energy, a setting of its own, ``precision="fp64"``) is solved alone by ``SimpleSolver``, or
+by ``ConjugateSolver`` when it has solid zones.
 As in the reference, each case's boundaries start from its mesh's zone types
 (``default_boundaries``) with the job's overrides, a case that fails is reported with its
 error and does not stop the others, and every result names the device it ran on.
@@ -123,7 +124,7 @@ def run_batch(jobs: List[BatchJob], max_batch_cells: int = 4_000_000, precision:
     import torch
 
     from ..unstructured.batch import BatchSimpleSolver
-    from ..unstructured.simple import SimpleSolver
+    from ..unstructured.conjugate import make_solver
 
     t0 = time.perf_counter()
     plan = plan_batch(jobs, max_batch_cells, precision)
@@ -166,7 +167,7 @@ def run_batch(jobs: List[BatchJob], max_batch_cells: int = 4_000_000, precision:
         t1 = time.perf_counter()
         res = {"name": n, "mesh": job.mesh, "backend": "b200", "device": device, "error": None}
         try:
-            s = SimpleSolver(mesh, case)
+            s = make_solver(mesh, case)  # a conjugate solver for cases with solid zones (batch.py:74)
             s.run()
             res.update({"cells": mesh.n_cells, "iterations": s.iteration, "converged": bool(s.converged),
                         "solve_seconds": time.perf_counter() - t1, "residuals": s.residuals()["scaled"],

@@ -1,0 +1,116 @@
+"""The oracle's conjugate heat transfer (``oracle/conjugate_oracle.py``) against the reference's
+``ConjugateSolver``, through ``tests/golden/conjugate_fixtures.npz`` (made by
+``tests/golden/make_conjugate_golden.py`` on the cases of ``tests/golden/conjugate_cases.py``): a
+1-D composite wall of two solids around a fluid slab, a channel over a heated solid block, and a
+lid-driven triangulated cavity around a heated solid disc. Also the product's host set-up of the
+same solver (``gputest_b200.unstructured.conjugate.conjugate_setup``)."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from gputest_b200.unstructured.case import BoundarySpec, UnstructuredCase
+from oracle.conjugate_oracle import OracleConjugate
+from tests.golden.conjugate_cases import CONJUGATE_CASES
+
+GOLD = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "conjugate_fixtures.npz"))
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _case(name):
+    build, kw, n = CONJUGATE_CASES[name]
+    bnd = {z: BoundarySpec(**spec) for z, spec in kw["boundaries"].items()}
+    return build(), UnstructuredCase(**{**kw, "boundaries": bnd}), n
+
+
+@pytest.mark.parametrize("name", sorted(CONJUGATE_CASES))
+def test_oracle_conjugate_equals_the_reference(name):
+    mesh, case, n = _case(name)
+    o = OracleConjugate(mesh, case)
+    p = f"cht|{name}|"
+    gf, gb = o.face_gamma()
+    assert np.array_equal(gf, GOLD[p + "gamma_face"]) and np.array_equal(gb, GOLD[p + "gamma_bface"])
+    assert np.array_equal(o.q_cell, GOLD[p + "q_cell"]) and np.array_equal(o.cell_map, GOLD[p + "cell_map"])
+    for _ in range(n):
+        o.step()
+    assert o.iteration == int(GOLD[p + "iterations"][0])
+    f = o.fields()
+    for k in (k.split("|", 3)[3] for k in GOLD.files if k.startswith(p + "field|")):
+        assert _rel(f[k], GOLD[p + "field|" + k]) <= 1e-12, k
+    for k, v in o.residuals()["scaled"].items():
+        assert v == pytest.approx(float(GOLD[p + "res|" + k][0]), rel=1e-8, abs=1e-300), k
+    assert list(o.last_linear["momentum_iters"]) + [o.last_linear["pressure_iters"]] == list(GOLD[p + "linear"])
+    ref = json.loads(bytes(GOLD[p + "heat_flow"]).decode())
+    ours = o.heat_flow()
+    assert set(ours) == set(ref)
+    for k, v in ref.items():
+        assert ours[k] == pytest.approx(v, rel=1e-9, abs=1e-12), k
+
+
+def test_composite_wall_is_exact():
+    """The reference's own check (``tests/test_zones.py:92-105``): with harmonic face
+    conductivities the 1-D composite wall is solved exactly."""
+    mesh, case, _ = _case("composite")
+    o = OracleConjugate(mesh, case)
+    for _ in range(60):
+        o.step()
+    x, T = o.fv.xc[:, 0], o.fields()["temperature"]
+    q = 1 / 3.2
+    Te = np.where(x < 1, 1 - q * x / 5, np.where(x < 2, 1 - q / 5 - q * (x - 1), 1 - 1.2 * q - 2 * q * (x - 2)))
+    assert np.abs(T - Te).max() < 1e-10
+
+
+@pytest.mark.parametrize("name", sorted(CONJUGATE_CASES))
+def test_product_conjugate_setup_equals_the_reference(name):
+    """The B200 path's host set-up (``conjugate_setup``): harmonic face diffusivities, sources,
+    the fluid sub-mesh's cell map, the flux maps and the thermal boundary arrays."""
+    from gputest_b200.unstructured.conjugate import conjugate_setup
+
+    mesh, case, _ = _case(name)
+    hs = conjugate_setup(mesh, case)
+    p = f"cht|{name}|"
+    assert np.array_equal(hs["gamma_face"], GOLD[p + "gamma_face"])
+    assert np.array_equal(hs["gamma_bface"], GOLD[p + "gamma_bface"])
+    assert np.array_equal(hs["q_cell"], GOLD[p + "q_cell"]) and np.array_equal(hs["cell_map"], GOLD[p + "cell_map"])
+    o = OracleConjugate(mesh, case)
+    for k in ("if_dst", "bf_src", "bf_dst"):
+        assert np.array_equal(hs[k], getattr(o, "_" + k)), k
+    assert np.array_equal(hs["tkind"], o.tkind) and np.array_equal(hs["tval"], o.tval)
+    assert np.array_equal(hs["is_outlet"], o.is_outlet)
+    assert not hs["flow_case"].solids and not hs["flow_case"].energy
+
+
+def test_conjugate_setup_rejects_what_the_reference_rejects():
+    """``tests/test_zones.py:108-111``: a solid zone without a conductivity, and no energy."""
+    from gputest_b200.unstructured.conjugate import conjugate_setup
+
+    mesh, case, _ = _case("heated")
+    with pytest.raises(ValueError):
+        conjugate_setup(mesh, UnstructuredCase(energy=True))
+    with pytest.raises(ValueError):
+        conjugate_setup(mesh, UnstructuredCase(energy=False, solids=dict(case.solids)))
+
+
+def test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks():
+    """How far the reference's own temperature moves when the cell conductivities are perturbed by
+    1e-15 relative: below 1e-10 on the composite wall and the heated channel, ~1e-7 on the
+    triangulated cavity (an energy BiCGSTAB solve at tolerance 1e-4 changes its iteration count).
+    The CUDA test compares temperatures at 1e-8 and 1e-5 for that reason."""
+    worst = {}
+    for name in sorted(CONJUGATE_CASES):
+        for seed in range(2):
+            mesh, case, n = _case(name)
+            o = OracleConjugate(mesh, case)
+            o.gam_cell = o.gam_cell * (1 + 1e-15 * np.random.default_rng(seed).standard_normal(o.nc))
+            for _ in range(n):
+                o.step()
+            d = _rel(o.fields()["temperature"], GOLD[f"cht|{name}|field|temperature"])
+            worst[name] = max(worst.get(name, 0.0), d)
+    assert worst["composite"] < 1e-10 and worst["heated"] < 1e-10
+    assert worst["tri_disc"] < 1e-5
