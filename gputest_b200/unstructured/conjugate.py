@@ -34,7 +34,7 @@ from .case import FLUENT_TO_KIND, BoundarySpec, UnstructuredCase
 from .fvmesh import FVMesh, HostFV
 from .simple import T_FIXED, T_FLUX, SimpleSolver
 
-__all__ = ["ConjugateSolver", "conjugate_setup", "make_solver"]
+__all__ = ["ConjugateSolver", "conjugate_setup", "device_flux_maps", "make_solver"]
 
 
 def conjugate_setup(mesh: UnstructuredMesh, case: UnstructuredCase, hfv: HostFV = None, sub_hfv: HostFV = None) -> dict:
@@ -101,6 +101,15 @@ def conjugate_setup(mesh: UnstructuredMesh, case: UnstructuredCase, hfv: HostFV 
             "bf_src": bf_src, "bf_dst": bf_dst, "tkind": tk, "tval": tv, "is_outlet": out}
 
 
+def device_flux_maps(hs: dict, fv, sfv):
+    """Index maps from the fluid sub-mesh's device face order (``sfv``) to the full mesh's
+    (``fv``): interior face i of the fluid goes to full interior face ``if_dst[i]``; fluid
+    boundary face ``bf_src[k]`` to full boundary face ``bf_dst[k]`` (``hs`` from
+    ``conjugate_setup``)."""
+    full_if, full_bf, sub_bf = np.argsort(fv.face_ref), np.argsort(fv.bface_ref), np.argsort(sfv.bface_ref)
+    return full_if[hs["if_dst"][sfv.face_ref]], sub_bf[hs["bf_src"]], full_bf[hs["bf_dst"]]
+
+
 class ConjugateSolver:
     """Drop-in for ``flowtrace.unstructured.conjugate.ConjugateSolver`` on one B200."""
 
@@ -125,14 +134,8 @@ class ConjugateSolver:
         self.nc, self.dim = mesh.n_cells, mesh.dim
         self.energy = True
         sfv = self.flow.fv
-        # index maps: the fluid's device face order -> the full mesh's device face order
-        full_if = np.argsort(fv.face_ref)
-        full_bf = np.argsort(fv.bface_ref)
-        sub_bf = np.argsort(sfv.bface_ref)
         as_idx = lambda a: torch.as_tensor(np.asarray(a, dtype=np.int64), device=dev)  # noqa: E731
-        self._if_dst = as_idx(full_if[hs["if_dst"][sfv.face_ref]])
-        self._bf_src = as_idx(sub_bf[hs["bf_src"]])
-        self._bf_dst = as_idx(full_bf[hs["bf_dst"]])
+        self._if_dst, self._bf_src, self._bf_dst = (as_idx(a) for a in device_flux_maps(hs, fv, sfv))
         z = lambda *shape: torch.zeros(*shape, dtype=torch.float64, device=dev)  # noqa: E731
         nc, nf, nb, dim = fv.nc, max(fv.n_if, 1), max(fv.n_bf, 1), fv.dim
         one = lambda t, n=1: t if t.numel() else z(n)  # noqa: E731

@@ -114,3 +114,31 @@ def test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks():
             worst[name] = max(worst.get(name, 0.0), d)
     assert worst["composite"] < 1e-10 and worst["heated"] < 1e-10
     assert worst["tri_disc"] < 1e-5
+
+
+@pytest.mark.parametrize("name", sorted(CONJUGATE_CASES))
+def test_device_flux_maps_scatter_like_the_reference(name):
+    """The index maps ``ConjugateSolver`` builds (``device_flux_maps``) to move the fluid's face fluxes (in the fluid
+    sub-mesh's device face order) into the full mesh's device face order, applied on the host to
+    the device layouts (``FVMesh`` built on the CPU): in range, one-to-one, and equal after
+    conversion to the reference's order to the oracle's ``_full_fluxes`` (``conjugate.py:136-144``)."""
+    import torch
+
+    from gputest_b200.unstructured.conjugate import conjugate_setup, device_flux_maps
+    from gputest_b200.unstructured.fvmesh import FVMesh
+
+    mesh, case, _ = _case(name)
+    hs = conjugate_setup(mesh, case)
+    fv, sfv = FVMesh(mesh, torch.device("cpu")), FVMesh(hs["sub"], torch.device("cpu"))
+    if_dst, bf_src, bf_dst = device_flux_maps(hs, fv, sfv)
+    assert if_dst.min() >= 0 and if_dst.max() < fv.n_if and np.unique(if_dst).size == if_dst.size
+    assert bf_src.max() < sfv.n_bf and bf_dst.max() < fv.n_bf and np.unique(bf_dst).size == bf_dst.size
+    o = OracleConjugate(mesh, case)
+    rng = np.random.default_rng(0)
+    o.flow.F, o.flow.Fb = rng.standard_normal(o.flow.fv.n_if), rng.standard_normal(o.flow.fv.n_bf)
+    F_ref, Fb_ref = o._full_fluxes()
+    F_dev = np.zeros(fv.n_if)
+    F_dev[if_dst] = o.flow.F[sfv.face_ref]
+    Fb_dev = np.zeros(fv.n_bf)
+    Fb_dev[bf_dst] = o.flow.Fb[sfv.bface_ref][bf_src]
+    assert np.array_equal(F_dev, F_ref[fv.face_ref]) and np.array_equal(Fb_dev, Fb_ref[fv.bface_ref])
