@@ -15,9 +15,11 @@ from tests.golden.conjugate_cases import CONJUGATE_CASES
 
 pytestmark = pytest.mark.gpu
 GOLD = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "conjugate_fixtures.npz"))
-# the reference's own temperature on the triangulated cavity moves by ~1e-7 under 1e-15 relative
-# perturbations (test_oracle_conjugate.test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks)
+# the reference's own temperature on the triangulated cavity moves by ~1e-7, and its energy
+# residual by up to 1.5e-4, under 1e-15 relative perturbations of the conductivities
+# (test_oracle_conjugate.test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks)
 TEMPERATURE_TOL = {"composite": 1e-8, "heated": 1e-8, "tri_disc": 1e-5}
+ENERGY_RESIDUAL_TOL = {"composite": 1e-4, "heated": 1e-4, "tri_disc": 1e-3}
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -58,7 +60,7 @@ def test_cuda_conjugate_equals_the_reference(name):
         assert _err(f[k], GOLD[p + "field|" + k]) <= tol, k
     for k, v in s.residuals()["scaled"].items():
         g = float(GOLD[p + "res|" + k][0])
-        assert v == pytest.approx(g, rel=1e-4 if k == "energy" else 1e-5, abs=1e-13), k
+        assert v == pytest.approx(g, rel=ENERGY_RESIDUAL_TOL[name] if k == "energy" else 1e-5, abs=1e-13), k
     lin = list(s.last_linear["momentum_iters"]) + [s.last_linear["pressure_iters"]]
     gold = list(GOLD[p + "linear"])
     assert lin[:-1] == gold[:-1] and abs(lin[-1] - gold[-1]) <= 1

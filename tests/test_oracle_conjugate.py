@@ -100,9 +100,11 @@ def test_conjugate_setup_rejects_what_the_reference_rejects():
 def test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks():
     """How far the reference's own temperature moves when the cell conductivities are perturbed by
     1e-15 relative: below 1e-10 on the composite wall and the heated channel, ~1e-7 on the
-    triangulated cavity (an energy BiCGSTAB solve at tolerance 1e-4 changes its iteration count).
-    The CUDA test compares temperatures at 1e-8 and 1e-5 for that reason."""
-    worst = {}
+    triangulated cavity (an energy BiCGSTAB solve at tolerance 1e-4 changes its iteration count),
+    where the energy residual moves by up to ~1.5e-4. The CUDA test compares temperatures at 1e-8
+    and 1e-5 and that residual at 1e-3 for that reason."""
+    worst, res_worst = {}, 0.0
+    g = float(GOLD["cht|tri_disc|res|energy"][0])
     for name in sorted(CONJUGATE_CASES):
         for seed in range(2):
             mesh, case, n = _case(name)
@@ -112,8 +114,11 @@ def test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks():
                 o.step()
             d = _rel(o.fields()["temperature"], GOLD[f"cht|{name}|field|temperature"])
             worst[name] = max(worst.get(name, 0.0), d)
+            if name == "tri_disc":
+                res_worst = max(res_worst, abs(o.residuals()["scaled"]["energy"] / g - 1))
     assert worst["composite"] < 1e-10 and worst["heated"] < 1e-10
     assert worst["tri_disc"] < 1e-5
+    assert 1e-5 < res_worst < 1e-3
 
 
 @pytest.mark.parametrize("name", sorted(CONJUGATE_CASES))
