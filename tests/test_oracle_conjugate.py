@@ -101,10 +101,12 @@ def test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks():
     """How far the reference's own temperature moves when the cell conductivities are perturbed by
     1e-15 relative: below 1e-10 on the composite wall and the heated channel, ~1e-7 on the
     triangulated cavity (an energy BiCGSTAB solve at tolerance 1e-4 changes its iteration count),
-    where the energy residual moves by up to ~1.5e-4. The CUDA test compares temperatures at 1e-8
-    and 1e-5 and that residual at 1e-3 for that reason."""
-    worst, res_worst = {}, 0.0
+    where the energy residual moves by up to ~1.5e-4 and the heat flows by ~6e-6. The CUDA test
+    compares temperatures at 1e-8 and 1e-5, that residual at 1e-3 and those heat flows at 1e-4
+    for that reason."""
+    worst, res_worst, hf_worst = {}, 0.0, 0.0
     g = float(GOLD["cht|tri_disc|res|energy"][0])
+    hf_ref = json.loads(bytes(GOLD["cht|tri_disc|heat_flow"]).decode())
     for name in sorted(CONJUGATE_CASES):
         for seed in range(2):
             mesh, case, n = _case(name)
@@ -116,9 +118,12 @@ def test_conjugate_temperatures_are_set_to_what_the_gpu_test_asks():
             worst[name] = max(worst.get(name, 0.0), d)
             if name == "tri_disc":
                 res_worst = max(res_worst, abs(o.residuals()["scaled"]["energy"] / g - 1))
+                hf = o.heat_flow()
+                hf_worst = max(hf_worst, *(abs(hf[k] - v) / abs(v) for k, v in hf_ref.items() if v != 0))
     assert worst["composite"] < 1e-10 and worst["heated"] < 1e-10
     assert worst["tri_disc"] < 1e-5
     assert 1e-5 < res_worst < 1e-3
+    assert 1e-7 < hf_worst < 1e-4
 
 
 @pytest.mark.parametrize("name", sorted(CONJUGATE_CASES))
