@@ -81,6 +81,20 @@ def make_workload(name):
         desc = {"workload": "3-D duct 4x1x1, 128x64x64 hexes (524,288 cells), jitter 0.1h seed 1, parabolic inlet "
                             "Re 500, heated walls 5e3 W/m2, Pr 0.71; SA-AMG strength theta 0", "cells": mesh.n_cells}
         return mesh, case, desc, inlet, {"amg_theta": 0.0}
+    if name == "sst":
+        # turbulent channel, k-omega SST with Spalding wall viscosity; nodes clustered to both walls
+        eta = np.linspace(0.0, 1.0, 257)
+        ys = 0.5 * (1.0 + np.tanh(2.5 * (2.0 * eta - 1.0)) / np.tanh(2.5))
+        mesh = cartesian_mesh_2d(512, 256, 8.0, 1.0, names=("inlet", "outlet", "bottom", "top"),
+                                 types=("velocity-inlet", "pressure-outlet", "wall", "wall"), ys=ys)
+        case = UnstructuredCase(boundaries={"inlet": BoundarySpec("inlet", velocity=[1.0, 0.0]),
+                                            "outlet": BoundarySpec("outlet", pressure=0.0)},
+                                viscosity=1e-4, turbulence="k-omega-sst", scheme="second-order",
+                                max_iter=100000, tol=1e-6)
+        desc = {"workload": "turbulent channel 8x1, 512x256 quads (131,072 cells) clustered to the walls (tanh 2.5), "
+                            "Re_h 1e4, k-omega SST with Spalding wall viscosity, linear-upwind U, upwind k/omega, "
+                            "SA-AMG PCG", "cells": mesh.n_cells}
+        return mesh, case, desc, None, {}
     raise SystemExit(f"unknown config {name!r}")
 
 
