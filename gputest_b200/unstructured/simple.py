@@ -1,11 +1,12 @@
 """Pressure-based SIMPLE/SIMPLEC solver on unstructured meshes, on one B200.
 
 Drop-in for ``flowtrace.unstructured.simple.SimpleSolver`` (``flowtrace/unstructured/
-simple.py:71-1072``) on its steady laminar path: same constructor, ``step()``, ``finished``,
-``converged``, ``residuals()``, ``diagnostics()``, ``fields()``, ``state_dict()`` /
-``load_state()``, ``initialize()``, ``set_sources()``, ``describe()``, ``mass_balance()``,
-``wall_forces()``, ``heat_flow()``, ``cell_centres()``, ``last_linear``, ``guard_events``,
-the relaxation attributes and the divergence guard, with the same algorithm.
+simple.py:71-1072``) on its steady path, laminar or with the k-omega SST model: same
+constructor, ``step()``, ``finished``, ``converged``, ``residuals()``, ``diagnostics()``,
+``fields()``, ``state_dict()`` / ``load_state()``, ``initialize()``, ``set_sources()``,
+``describe()``, ``mass_balance()``, ``wall_forces()``, ``wall_report()``, ``wall_profile()``,
+``heat_flow()``, ``cell_centres()``, ``last_linear``, ``guard_events``, the relaxation
+attributes and the divergence guard, with the same algorithm.
 
 One outer iteration is a fixed sequence of CUDA stages from ``libb2simplec.so`` on the
 current stream, with no host synchronisation until its end, where one device->host copy
@@ -984,13 +985,74 @@ class SimpleSolver:
             pP = pP + np.sum(gp[h.Pb] * h.db, axis=1)
         return self.m_pres_h * self._pb_fixed_h + (1.0 - self.m_pres_h) * pP
 
+    def _wall_viscosity_host(self) -> np.ndarray:
+        """Boundary-face viscosity of the momentum equations, reference numbering: mu, or with the
+        SST model mu + mu_t and on walls the wall-function value (``simple.py:900-904``)."""
+        if self.turb is not None:
+            return self.turb.wall_viscosity(self._Up[self._cur], self.gUp, self._cur)
+        return np.full(self.fv.host.n_bf, float(self.case.viscosity))
+
+    def _wall_shear_host(self):
+        """Wall shear stress vector per boundary face, mu_w (u_P - u_w)_t / y_b, and (u_P - u_w)_t."""
+        h = self.fv.host
+        rel = self.U[h.Pb] - self._ub_fixed_h
+        rel_t = rel - np.sum(rel * h.nb, axis=1)[:, None] * h.nb
+        return self._wall_viscosity_host()[:, None] * rel_t / h.yb[:, None], rel_t
+
+    def wall_report(self) -> dict:
+        """Per wall zone: area, pressure/viscous/total force, Cd and Cl (``case.ref_velocity``,
+        ``case.ref_area``), area-weighted and maximum y+, mean skin friction and, with energy, the
+        conducted heat flow (``simple.py:906-950``; no radiation on this path)."""
+        h, c = self.fv.host, self.case
+        rho, mu = c.density, c.viscosity
+        tau_vec, _ = self._wall_shear_host()
+        tau = np.sqrt(np.sum(tau_vec * tau_vec, axis=1))
+        yplus = h.yb * np.sqrt(tau / rho) * rho / mu
+        forces = self.wall_forces()
+        qconv = None
+        if self.energy:
+            TP = self.T[h.Pb]
+            Tw = np.where(self.tkind_h == T_FIXED, self._tval_h, TP)
+            qconv = (c.conductivity * h.alpha_b * (Tw - TP) * (self.tkind_h == T_FIXED)
+                     + np.where(self.tkind_h == T_FLUX, self._tval_h * h.Sb_mag, 0.0))
+        qdyn = 0.5 * rho * c.ref_velocity ** 2
+        out = {}
+        for z in self.mesh.boundary_zones():
+            if z.name not in forces:
+                continue
+            m = h.bzone == z.id
+            A = h.Sb_mag[m]
+            f = forces[z.name]
+            Ft = np.asarray(f["total"])
+            rep = {"area": float(A.sum()), "force_pressure": f["pressure"], "force_viscous": f["viscous"],
+                   "force_total": f["total"], "cd": float(Ft[0] / (qdyn * c.ref_area)),
+                   "cl": float(Ft[1] / (qdyn * c.ref_area)),
+                   "yplus_avg": float((yplus[m] * A).sum() / A.sum()), "yplus_max": float(yplus[m].max()),
+                   "cf_avg": float((tau[m] * A).sum() / A.sum() / qdyn)}
+            if qconv is not None:
+                rep["heat_flow_conv"] = float(qconv[m].sum())
+            out[z.name] = rep
+        return out
+
+    def wall_profile(self, zone: str) -> dict:
+        """Face-wise x, y, Cf, Cp and y+ on one wall zone, sorted by x (``simple.py:952-968``)."""
+        h, c = self.fv.host, self.case
+        m = h.bzone == self.mesh.zone_by_name(zone).id
+        rho, mu = c.density, c.viscosity
+        _, rel_t = self._wall_shear_host()
+        tau = self._wall_viscosity_host() * np.sqrt(np.sum(rel_t * rel_t, axis=1)) / h.yb
+        qdyn = 0.5 * rho * c.ref_velocity ** 2
+        xfb = h.xfb[m]
+        order = np.argsort(xfb[:, 0])
+        return {"x": xfb[order, 0], "y": xfb[order, 1], "cf": tau[m][order] / qdyn,
+                "cp": self._pressure_bvals_host()[m][order] / qdyn,
+                "yplus": (h.yb * np.sqrt(tau / rho) * rho / mu)[m][order]}
+
     def wall_forces(self) -> dict:
         """Pressure and viscous force on every wall zone (``simple.py:970-1001``)."""
         h = self.fv.host
         pb = self._pressure_bvals_host()
-        mu_b = np.full(pb.shape, float(self.case.viscosity))
-        if self.turb is not None:  # simple.py:900-904
-            mu_b = self.turb.wall_viscosity(self._Up[self._cur], self.gUp, self._cur)
+        mu_b = self._wall_viscosity_host()
         du = self.U[h.Pb] - self._ub_fixed_h
         du_t = du - np.einsum("fd,fd->f", du, h.nb)[:, None] * h.nb
         f_p = pb[:, None] * h.Sb

@@ -988,6 +988,84 @@ class OracleSimple:
             out.update(self.turb.fields())
         return out
 
+    def _wall_viscosity(self):
+        """Boundary-face viscosity of the momentum equation (``simple.py:900-904``)."""
+        if self.turb is not None:
+            return self.turb.momentum_viscosity(self.U)[1]
+        return np.full(self.fv.n_bf, float(self.case.viscosity))
+
+    def wall_forces(self):
+        """Pressure and viscous force on every wall zone (``simple.py:970-1001``)."""
+        fv = self.fv
+        pb = self._pressure_bvals(self.p, self._gp)
+        mu_b = self._wall_viscosity()
+        du = self.U[fv.Pb] - self.ub_fixed
+        du_t = du - np.einsum("fd,fd->f", du, fv.nb)[:, None] * fv.nb
+        f_p = pb[:, None] * fv.Sb
+        f_v = (mu_b * fv.alpha_b)[:, None] * du_t
+        out = {}
+        for z in self.mesh.boundary_zones():
+            m = (fv.bzone == z.id) & (self.bkind == WALL)
+            if m.any():
+                fp, fvis = f_p[m].sum(axis=0), f_v[m].sum(axis=0)
+                out[z.name] = {"pressure": fp.tolist(), "viscous": fvis.tolist(), "total": (fp + fvis).tolist()}
+        return out
+
+    def _wall_shear(self):
+        """Wall shear stress vector per boundary face, mu_w (u_P - u_w)_t / y_b."""
+        fv = self.fv
+        rel = self.U[fv.Pb] - self.ub_fixed
+        rel_t = rel - np.sum(rel * fv.nb, axis=1)[:, None] * fv.nb
+        return self._wall_viscosity()[:, None] * rel_t / fv.yb[:, None], rel_t
+
+    def wall_report(self):
+        """Per wall zone: area, forces, Cd/Cl, y+, skin friction, conducted heat
+        (``simple.py:906-950``, no radiation)."""
+        fv, c = self.fv, self.case
+        rho, mu = c.density, c.viscosity
+        tau_vec, _ = self._wall_shear()
+        tau = np.sqrt(np.sum(tau_vec * tau_vec, axis=1))
+        yplus = fv.yb * np.sqrt(tau / rho) * rho / mu
+        forces = self.wall_forces()
+        qconv = None
+        if self.energy:
+            Tw = np.where(self.tkind == T_FIXED, self.tval, self.T[fv.Pb])
+            qconv = (c.conductivity * fv.alpha_b * (Tw - self.T[fv.Pb]) * (self.tkind == T_FIXED)
+                     + np.where(self.tkind == T_FLUX, self.tval * fv.Sb_mag, 0.0))
+        qdyn = 0.5 * rho * c.ref_velocity ** 2
+        out = {}
+        for z in self.mesh.boundary_zones():
+            if z.name not in forces:
+                continue
+            m = fv.bzone == z.id
+            A = fv.Sb_mag[m]
+            f = forces[z.name]
+            Ft = np.asarray(f["total"])
+            rep = {"area": float(A.sum()), "force_pressure": f["pressure"], "force_viscous": f["viscous"],
+                   "force_total": f["total"], "cd": float(Ft[0] / (qdyn * c.ref_area)),
+                   "cl": float(Ft[1] / (qdyn * c.ref_area)),
+                   "yplus_avg": float((yplus[m] * A).sum() / A.sum()), "yplus_max": float(yplus[m].max()),
+                   "cf_avg": float((tau[m] * A).sum() / A.sum() / qdyn)}
+            if qconv is not None:
+                rep["heat_flow_conv"] = float(qconv[m].sum())
+            out[z.name] = rep
+        return out
+
+    def wall_profile(self, zone):
+        """Face-wise x, y, Cf, Cp, y+ on one wall zone, sorted by x (``simple.py:952-968``)."""
+        fv, c = self.fv, self.case
+        z = self.mesh.zone_by_name(zone)
+        m = fv.bzone == z.id
+        rho, mu = c.density, c.viscosity
+        _, rel_t = self._wall_shear()
+        tau = self._wall_viscosity() * np.sqrt(np.sum(rel_t * rel_t, axis=1)) / fv.yb
+        qdyn = 0.5 * rho * c.ref_velocity ** 2
+        xfb = fv.xfb[m]
+        order = np.argsort(xfb[:, 0])
+        return {"x": xfb[order, 0], "y": xfb[order, 1], "cf": tau[m][order] / qdyn,
+                "cp": self._pressure_bvals(self.p, self._gp)[m][order] / qdyn,
+                "yplus": (fv.yb * np.sqrt(tau / rho) * rho / mu)[m][order]}
+
     def state_dict(self):
         """``simple.py:1033-1046``."""
         st = {"U": self.U.copy(), "p": self.p.copy(), "F": self.F.copy(), "Fb": self.Fb.copy(),
