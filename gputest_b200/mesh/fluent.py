@@ -386,8 +386,9 @@ _FLUENT_BC = {v: k for k, v in BC_CODES.items()}
 
 def write_fluent_mesh(mesh: UnstructuredMesh, path: str, binary: bool = False, title: str = "b2s") -> None:
     """Write ``mesh`` as a Fluent mesh file (ASCII sections, or binary node and face sections);
-    ``read_fluent_mesh`` of the file gives back the same arrays and zones. Face zones must be
-    contiguous ranges of faces (as the generators and ``sort_faces_by_zone`` leave them)."""
+    ``read_fluent_mesh`` of the file gives back the same arrays and zones. Face and cell zones
+    must be contiguous ranges (as the generators, ``sort_faces_by_zone`` and ``set_cell_zone``
+    leave them); otherwise ValueError."""
     dim, nn, nc, nf = mesh.dim, mesh.n_nodes, mesh.n_cells, mesh.n_faces
     counts = np.diff(mesh.face_ptr)
     fnodes = mesh.face_nodes.copy()
@@ -405,6 +406,10 @@ def write_fluent_mesh(mesh: UnstructuredMesh, path: str, binary: bool = False, t
         out.append(b"))\n")
     out.append(f"(12 (0 1 {nc:x} 0))\n".encode())
     for z in sorted(mesh.cell_zones(), key=lambda z: z.first):
+        if z.last < z.first or not np.all(mesh.cell_zone[z.first:z.last + 1] == z.id) or \
+                np.count_nonzero(mesh.cell_zone == z.id) != z.last - z.first + 1:
+            raise ValueError(f"cell zone {z.name!r} is not a contiguous range of cells (set_cell_zone renumbers "
+                             "cells so that it is)")
         out.append(f"(12 ({z.id:x} {z.first + 1:x} {z.last + 1:x} 1 0))\n".encode())
     out.append(f"(13 (0 1 {nf:x} 0))\n".encode())
     for z in sorted(mesh.face_zones(), key=lambda z: z.first):

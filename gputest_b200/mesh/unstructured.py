@@ -470,6 +470,38 @@ def extrude_to_3d(mesh2d: UnstructuredMesh, nz: int, lz: float,
     return sort_faces_by_zone(m)
 
 
+def set_cell_zone(mesh: UnstructuredMesh, where, name: str, type: str = "fluid") -> UnstructuredMesh:
+    """A new mesh with the cells whose centres satisfy ``where(xc)`` in a new cell zone ``name``
+    (id: the largest zone id + 1) of Fluent type ``type`` (``flowtrace/mesh/unstructured.py:611-644``).
+    Cells are renumbered by a stable sort on their zone id, so that every cell zone is a
+    contiguous range of cells (as Fluent files store them); zones left without cells are
+    dropped. Raises ValueError when no cell matches."""
+    sel = np.asarray(where(compute_geometry(mesh).cell_centre), dtype=bool)
+    if not sel.any():
+        raise ValueError("no cell matches the zone condition")
+    zid = max(mesh.zones) + 1
+    cz = np.where(sel, zid, mesh.cell_zone)
+    zones = dict(mesh.zones)
+    zones[zid] = Zone(zid, name, type, "cell")
+    old_of_new = np.argsort(cz, kind="stable")
+    new_of_old = np.empty_like(old_of_new)
+    new_of_old[old_of_new] = np.arange(old_of_new.size)
+    cz = cz[old_of_new]
+    present = set(np.unique(cz).tolist())
+    out = {}
+    for k, z in zones.items():
+        if z.kind != "cell":
+            out[k] = z
+        elif k in present:
+            idx = np.flatnonzero(cz == k)
+            out[k] = Zone(z.id, z.name, z.type, "cell", int(idx[0]), int(idx[-1]))
+    nei = np.where(mesh.neighbour >= 0, new_of_old[np.maximum(mesh.neighbour, 0)], -1)
+    return UnstructuredMesh(dim=mesh.dim, nodes=mesh.nodes, face_ptr=mesh.face_ptr, face_nodes=mesh.face_nodes,
+                            owner=new_of_old[mesh.owner], neighbour=nei, face_zone=mesh.face_zone,
+                            n_cells=mesh.n_cells, cell_zone=cz, zones=out, name=mesh.name,
+                            periodic=list(mesh.periodic))
+
+
 def extract_cells(mesh: UnstructuredMesh, keep, interface_type: str = "wall"):
     """The sub-mesh of the cells where ``keep`` is True (``flowtrace/mesh/unstructured.py:714-779``):
     the fluid part of a conjugate heat-transfer mesh. Faces between a kept and a dropped cell

@@ -40,3 +40,19 @@ def extract_digest(sub, fmap, cmap) -> dict:
     out["cell_map"] = hashlib.sha256(np.ascontiguousarray(cmap, dtype=np.int64).tobytes()).hexdigest()
     out["name"] = sub.name
     return out
+
+
+def cell_zone_cases(cartesian_mesh_2d, extrude_to_3d, set_cell_zone):
+    """Meshes built with ``set_cell_zone`` (once or twice) from generated meshes; the generators
+    and ``set_cell_zone`` are passed in, so that the reference's and this package's build them."""
+    m1 = cartesian_mesh_2d(30, 3, 3.0, 1.0)
+    m1 = set_cell_zone(m1, lambda x: x[:, 0] < 1.0, "a", "solid")
+    m1 = set_cell_zone(m1, lambda x: x[:, 0] > 2.0, "b", "solid")
+    return {
+        "quad_lower_half": set_cell_zone(cartesian_mesh_2d(8, 6), lambda x: x[:, 1] < 0.5, "solid", "solid"),
+        "tri_disc": set_cell_zone(cartesian_mesh_2d(12, 12, triangulate=True, jitter=0.1, seed=4),
+                                  lambda x: (x[:, 0] - 0.5) ** 2 + (x[:, 1] - 0.5) ** 2 < 0.09, "heater", "solid"),
+        "hex_slab": set_cell_zone(extrude_to_3d(cartesian_mesh_2d(5, 4, jitter=0.1, seed=2), 3, 1.0),
+                                  lambda x: x[:, 0] < 0.45, "wall-block", "solid"),
+        "composite_two_zones": m1,
+    }

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from gputest_b200.mesh.fluent import FluentMeshError, read_fluent_mesh, write_fluent_mesh
+from gputest_b200.mesh.unstructured import cartesian_mesh_2d
 from tests.golden.fluent_cases import ARRAYS, digest, generated_cases, generated_meshes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -82,3 +83,23 @@ def test_a_mesh_read_from_a_file_solves_like_the_mesh_it_was_written_from(tmp_pa
     b.run()
     for k, v in b.fields().items():
         assert np.array_equal(a.fields()[k], v), k
+
+
+def test_set_cell_zone_equals_the_reference_and_round_trips_through_a_file(tmp_path):
+    """``set_cell_zone`` against digests of the reference's (``tests/golden/cellzone_digests.json``,
+    made by ``tests/golden/make_cellzone_golden.py``); its meshes (contiguous cell zones) write and
+    read back unchanged, while a mesh whose cell zone is not contiguous is refused by the writer."""
+    from gputest_b200.mesh.unstructured import extrude_to_3d, set_cell_zone
+    from tests.golden.mesh_cases import cell_zone_cases, with_solid_zone
+
+    ref = json.load(open(os.path.join(HERE, "golden", "cellzone_digests.json")))
+    cases = cell_zone_cases(cartesian_mesh_2d, extrude_to_3d, set_cell_zone)
+    assert set(cases) == set(ref)
+    for key, m in cases.items():
+        assert digest(m) == ref[key], key
+        p = tmp_path / f"{key}.msh"
+        write_fluent_mesh(m, str(p))
+        assert digest(read_fluent_mesh(str(p))) == ref[key], key
+    scattered, _ = with_solid_zone(cartesian_mesh_2d(8, 6), lambda x: x[:, 1] < 0.5)
+    with pytest.raises(ValueError, match="contiguous"):
+        write_fluent_mesh(scattered, str(tmp_path / "bad.msh"))

@@ -67,3 +67,24 @@ def test_run_batch_solves_each_case_like_the_case_alone(tmp_path):
         got = np.load(r["npz"])
         for k, v in s.fields().items():
             assert float(np.abs(got[k] - v).max()) <= 1e-6 * max(float(np.abs(v).max()), 1e-300), (n, k)
+
+
+def test_a_case_with_a_solid_zone_is_planned_alone(tmp_path):
+    """A mesh file with a solid cell zone (``set_cell_zone``) and the solid's conductivity in the
+    case: read back with its zones, planned to run alone (``run_batch`` hands it to
+    ``make_solver``, which builds a ``ConjugateSolver``), beside a batch of plain cases."""
+    from gputest_b200.mesh.unstructured import set_cell_zone
+    from gputest_b200.runtime.batch import _prepare
+
+    m = cartesian_mesh_2d(30, 10, 4.0, 1.25, names=("inlet", "outlet", "bottom", "top"),
+                          types=("velocity-inlet", "pressure-outlet", "wall", "wall"), y0=-0.25)
+    m = set_cell_zone(m, lambda x: x[:, 1] < 0.0, "heater", "solid")
+    path = str(tmp_path / "heated.msh")
+    write_fluent_mesh(m, path)
+    job = BatchJob("heated", path, {"energy": True, "conductivity": 0.05, "viscosity": 0.05,
+                                    "solids": {"heater": {"conductivity": 2.0, "source": 4.0}},
+                                    "boundaries": {"inlet": {"kind": "inlet", "normal_speed": 1.0}}})
+    mesh, case = _prepare(job)
+    assert any(z.type == "solid" for z in mesh.cell_zones()) and case.solids
+    plan = plan_batch(_jobs(tmp_path)[:3] + [job])
+    assert plan["single"] == ["heated"] and plan["batches"] == [["cav_a", "chan", "cav_b"]]
