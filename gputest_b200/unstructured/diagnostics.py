@@ -194,6 +194,13 @@ def evaluate(solver) -> dict:
             lo = torch.minimum(lo, torch.where(fixed, tval, inf).min())
         sc.add("dT|ref", hi - lo)
         health["temperature"] = T_new
+    turb = getattr(solver, "turb", None)
+    tnames = ("k", "omega") if turb is not None and "turbulence" in cap else ()
+    for q, tname in enumerate(tnames):  # diagnostics.py:287-290
+        t_old, t_new = turb._KW[old][q], turb._KW[new][q]
+        sc.add(f"d{tname}|num", (t_new - t_old).abs().max())
+        sc.add(f"d{tname}|ref", t_new.abs().max())
+        health[tname] = t_new
     for hname, arr in health.items():
         sc.add(f"health|{hname}", (~torch.isfinite(arr)).sum().double())
     vals = sc.fetch()
@@ -250,6 +257,8 @@ def evaluate(solver) -> dict:
     if ecap is not None:
         change["temperature"] = None if rolled else ratio(vals["dT|num"], vals["dT|ref"])
         change["temperature_reference"] = vals["dT|ref"]
+    for tname in tnames:
+        change[tname] = None if rolled else ratio(vals[f"d{tname}|num"], vals[f"d{tname}|ref"])
     out["field_change"] = change
     nonfinite = {hname: int(vals[f"health|{hname}"]) for hname in health}
     out["health"] = {"finite": not any(nonfinite.values()), "nonfinite_values": nonfinite}

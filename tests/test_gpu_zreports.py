@@ -43,3 +43,19 @@ def test_cuda_wall_reports_equal_the_reference(name):
     for k, v in s.wall_profile(zone).items():
         g = GOLD[f"rep|{name}|profile|" + k]
         assert np.abs(v - g).max() <= 1e-7 * np.abs(g).max(), k
+
+
+def test_cuda_sst_diagnostics_report_k_and_omega():
+    """As the reference's ``tests/test_diagnostics.py:227-234``: with the SST model the
+    diagnostics' field changes include k and omega, and their health counts are reported."""
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    build, kw, _, _ = REPORT_CASES["sst_chan2d"]
+    bnd = {z: BoundarySpec(**spec) for z, spec in kw["boundaries"].items()}
+    s = SimpleSolver(build(cartesian_mesh_2d, extrude_to_3d), UnstructuredCase(**{**kw, "boundaries": bnd}))
+    for _ in range(5):
+        s.step()
+    d = s.diagnostics()
+    ch = d["field_change"]
+    assert ch["k"] is not None and ch["omega"] is not None and 0 <= ch["k"] < 1e3
+    assert d["health"]["finite"] and {"k", "omega"} <= set(d["health"]["nonfinite_values"])
