@@ -287,6 +287,12 @@ def stage_bytes(solver, stage, step_info):
         cells = nc * 8 * (d + d * d + d + 1) + nc * 8 * (3 + 2 * d) + nc * 4 * 2  # U, gU, gp, vol; outputs; slot_diag, bptr
         bnd = nb * 8 * (3 + d) + nb * 4
         return faces + cells + bnd + csr + nnz * 8  # CSR read for the residual, values written
+    if stage == "turbulence_terms":  # b2s_sst_momentum_terms_d: face viscosities, wall law, transpose stress
+        energy = getattr(solver, "energy", False)
+        faces = face_topo + nf * 8 * (1 + d) + nf * 8 * (2 if energy else 1)  # w, S; mu_f (+ kT_f) out
+        cells = nc * 8 * (1 + d + d * d) + nc * 8 * d + (nc + 1) * 4  # mu_t, U, grad U; tsrc out; bptr
+        bnd = nb * 8 * (1 + 1 + 2 * d) + nb * 8 * (3 if energy else 2)  # m_wall, yb, ub, n; mu_b, y+ (+ kT_b)
+        return faces + cells + bnd
     if stage == "pressure_assembly":
         faces = face_topo + nf * 8 * (3 + 2 * d) + nf * 8 * 2 + nf * 4 * 2  # w, alpha, S, d; Fst, cf out; slots
         cells = nc * 8 * (d + 1 + d + 1) + nc * 8 * 2 + nnz * 8
