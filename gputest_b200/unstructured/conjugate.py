@@ -15,8 +15,9 @@ scattered into the full mesh's face order by index maps built once. What runs on
 set-up (``conjugate_setup``: solid zones, the sub-mesh, conductivities, sources, the face maps)
 and the reports.
 
-Laminar only: with a turbulence model the face diffusivities change every iteration
-(k/cp + mu_t/Pr_t in the fluid), which this solver does not implement.
+With the k-omega SST model the fluid cells' diffusivity is k/cp + mu_t/Pr_t, so the face
+diffusivities are rebuilt on the device every iteration from the flow's mu_t
+(``harmonic_face_gamma``).
 """
 
 from __future__ import annotations
@@ -34,7 +35,17 @@ from .case import FLUENT_TO_KIND, BoundarySpec, UnstructuredCase
 from .fvmesh import FVMesh, HostFV
 from .simple import T_FIXED, T_FLUX, SimpleSolver
 
-__all__ = ["ConjugateSolver", "conjugate_setup", "device_flux_maps", "make_solver"]
+__all__ = ["ConjugateSolver", "conjugate_setup", "device_flux_maps", "harmonic_face_gamma", "make_solver"]
+
+PR_T = 0.85  # turbulent Prandtl number of the energy equation (flowtrace/unstructured/turbulence.py:59)
+
+
+def harmonic_face_gamma(g, w, fP, fN, bP):
+    """Face diffusivities from the cell diffusivities ``g`` (``conjugate.py:146-159``): inside,
+    1 / ((1 - w) / g_P + w / g_N), the owner side holding (1 - w) of the distance; on boundary
+    faces the owner's value. Tensors on any device (index tensors of dtype long)."""
+    gP, gN = g[fP], g[fN]
+    return 1.0 / ((1.0 - w) / gP + w / gN), g[bP]
 
 
 def conjugate_setup(mesh: UnstructuredMesh, case: UnstructuredCase, hfv: HostFV = None, sub_hfv: HostFV = None) -> dict:
@@ -118,9 +129,6 @@ class ConjugateSolver:
     def __init__(self, mesh: UnstructuredMesh, case: UnstructuredCase, backend=None, **flow_kwargs):
         import torch
 
-        if case.turbulence != "laminar":
-            raise NotImplementedError("conjugate heat transfer with a turbulence model is not implemented on the "
-                                      "B200 path")
         self.case, self.mesh = case, mesh
         hfv = HostFV(mesh)
         hs = conjugate_setup(mesh, case, hfv=hfv)
@@ -163,6 +171,13 @@ class ConjugateSolver:
                       "pb_fixed": zb, "m_tfix": bfd(tk == T_FIXED), "m_tflux": bfd(tk == T_FLUX),
                       "m_out": bfd(hs["is_outlet"]), "tval": bfd(hs["tval"])}
         self.cbc = _lib.BC(**{k: v.data_ptr() for k, v in self._bc_t.items()})
+        self._turb_idx = None
+        if self.flow.turb is not None:  # mu_t / Pr_t joins the fluid cells' diffusivity every iteration
+            self._turb_idx = as_idx(fv.iperm[hs["cell_map"][sfv.perm]])  # fluid device cell -> full device cell
+            self._gam_cell = fv.cells_to_device(hs["gam_cell"])
+            self._mut_full = z(nc)
+            self._face_idx = (fv.t["fP"].long(), fv.t["fN"].long(), fv.t["bP"].long())
+            self._update_gamma()
         self._lagT = False
         self._res_energy = 1.0
         self.last_linear = {}
@@ -170,6 +185,14 @@ class ConjugateSolver:
         self.kernel_launches = 0
 
     # ------------------------------------------------------------------ the energy equation
+    def _update_gamma(self):
+        """Face diffusivities with the flow's current mu_t (``conjugate.py:146-159``)."""
+        fl, fv = self.flow, self.fv
+        self._mut_full.index_copy_(0, self._turb_idx, fl.turb._mut[fl._cur])
+        gf, gb = harmonic_face_gamma(self._gam_cell + self._mut_full / PR_T, fv.t["w"], *self._face_idx)
+        self.gamma_f[: gf.numel()].copy_(gf)
+        self.gamma_b[: gb.numel()].copy_(gb)
+
     def _full_fluxes(self):
         """The fluid's current mass fluxes on the full mesh's faces, zero on solid faces
         (``conjugate.py:136-144``)."""
@@ -189,6 +212,8 @@ class ConjugateSolver:
         s = _lib.stream_ptr()
         m, bc = fv.cmesh_ref, ctypes.byref(self.cbc)
         self._full_fluxes()
+        if self._turb_idx is not None:
+            self._update_gamma()
         _lib.check(L.b2s_energy_bvals_d(m, bc, self.T.data_ptr(), self.gT.data_ptr() if self._lagT else None,
                                         self.Fb.data_ptr(), self.Tb.data_ptr(), s), "b2s_energy_bvals_d")
         _lib.check(L.b2s_ls_gradient_d(m, 1, self.T.data_ptr(), self.Tb.data_ptr(), self.gT.data_ptr(), s),
@@ -306,7 +331,9 @@ class ConjugateSolver:
         cond = g * h.alpha_b * (Tb - TP) * (tk == T_FIXED) + np.where(tk == T_FLUX, tv * h.Sb_mag, 0.0)
         q = cond - c.cp * Fb * Tb
         res = {z.name: float(q[h.bzone == z.id].sum()) for z in self.mesh.boundary_zones()}
-        gf = self._gamma_face_h * c.cp
+        if self._turb_idx is not None:
+            self._update_gamma()
+        gf = (fv.faces_to_host(self.gamma_f[: h.n_if]) if self._turb_idx is not None else self._gamma_face_h) * c.cp
         sP, sN = self.solid[h.P], self.solid[h.N]
         iface = sP != sN
         flux = gf * h.alpha * (T[h.N] - T[h.P])

@@ -35,7 +35,7 @@ class _EnergyOps:
 
 
 class OracleConjugate:
-    """``ConjugateSolver`` (``conjugate.py:46-318``), laminar."""
+    """``ConjugateSolver`` (``conjugate.py:46-318``), laminar or with the k-omega SST model."""
 
     def __init__(self, mesh, case):
         from gputest_b200.mesh.unstructured import extract_cells
@@ -120,10 +120,14 @@ class OracleConjugate:
         return F, Fb
 
     def face_gamma(self):
-        """Harmonic mean of the two cells' diffusivities, weighted by the distances to the face
-        (``conjugate.py:146-159``, laminar)."""
+        """Harmonic mean of the two cells' diffusivities, weighted by the distances to the face;
+        with the SST model the fluid cells add mu_t / Pr_t (``conjugate.py:146-159``)."""
         fv = self.fv
-        g = self.gam_cell
+        g = self.gam_cell.copy()
+        if self.flow.turb is not None:
+            from .sst_oracle import PR_T
+
+            g[self.cell_map] += self.flow.turb.mut / PR_T
         gP, gN = g[fv.P], g[fv.N]
         w = fv.w
         return 1.0 / ((1.0 - w) / gP + w / gN), g[fv.Pb]

@@ -47,6 +47,12 @@ CONJUGATE_CASES = {
                     boundaries={"inlet": {"kind": "inlet", "normal_speed": 1.0, "value": 0.0},
                                 "outlet": {"kind": "outlet"}},
                     max_iter=300, tol=0.0, pressure_tol=1e-9), 30),
+    "heated_sst": (_heated,
+                   dict(energy=True, conductivity=0.002, viscosity=2e-3, turbulence="k-omega-sst",
+                        solids={"heater": {"conductivity": 2.0, "source": 4.0}},
+                        boundaries={"inlet": {"kind": "inlet", "normal_speed": 1.0, "value": 0.0},
+                                    "outlet": {"kind": "outlet"}},
+                        max_iter=300, tol=0.0, pressure_tol=1e-9), 20),
     "tri_disc": (_tri_disc,
                  dict(energy=True, conductivity=0.02, viscosity=0.01,
                       solids={"heater": {"conductivity": 3.0, "source": 2.0}},
