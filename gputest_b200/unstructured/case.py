@@ -1,9 +1,10 @@
 """Case and boundary-condition objects of the unstructured SIMPLEC solver.
 
 Same fields, defaults and validation as ``flowtrace/unstructured/case.py:9-188`` so that a
-case written for the reference runs here unchanged. Fields of models that this solver does
-not implement (turbulence, radiation, species, MRF, solids, periodic pairs, transient) are
-kept so such cases still parse; ``SimpleSolver`` rejects them with ``NotImplementedError``.
+case written for the reference runs here unchanged. The k-omega SST model and solid zones (through
+``conjugate.make_solver``) are implemented; fields of the models that are not (the k-epsilon
+models, radiation, species, MRF, periodic pairs, transient) are kept so such cases still parse,
+and ``SimpleSolver`` rejects them with ``NotImplementedError``.
 """
 
 from __future__ import annotations
