@@ -134,6 +134,8 @@ _SIGS = {
     "b2s_residual_vjp_d": ([P, P, F64, F64, F64, ctypes.c_int] + [P] * 18 + [P], ctypes.c_int),
     # k-omega SST
     "b2s_momentum_assemble_turb_d": ([P] * 21 + [P], ctypes.c_int),
+    "b2s_momentum_assemble_mixed_turb_d": ([P] * 19 + [P], ctypes.c_int),
+    "b2s_energy_assemble_mixed_turb_d": ([P, P, P, P, F64, F64, ctypes.c_int] + [P] * 10 + [P], ctypes.c_int),
     "b2s_energy_assemble_turb_d": ([P, P, P, P, F64, F64, ctypes.c_int] + [P] * 12 + [P], ctypes.c_int),
     "b2s_sst_part_blocks": ([P], ctypes.c_int),
     "b2s_sst_momentum_terms_d": ([P] * 12 + [P], ctypes.c_int),

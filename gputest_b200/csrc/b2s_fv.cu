@@ -507,38 +507,47 @@ __global__ void energy_assemble_k(b2s_mesh m, b2s_bc bc, GT gamma, double cp, do
 
 // sum_nb a_nb phi_nb of row c for NQ fields: upwind + diffusion off-diagonals recomputed from
 // the face data the row assembly has just read (simple.py:340-353).
-template <int NQ>
-__device__ __forceinline__ void offdiag_apply(const b2s_mesh& m, int c, double gamma, const double* F,
-                                              const double* phi, int64_t phi_stride, double (&out)[NQ]) {
+template <int NQ, class GT>
+__device__ __forceinline__ void offdiag_apply_g(const b2s_mesh& m, int c, const GT& gam, const double* F,
+                                                const double* phi, int64_t phi_stride, double (&out)[NQ]) {
 #pragma unroll
   for (int q = 0; q < NQ; ++q) out[q] = 0.0;
   for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) {
-    const double aPN = -(gamma * m.alpha[f] + npmax0(-F[f]));
+    const double aPN = -(gam.in(f) * m.alpha[f] + npmax0(-F[f]));
     const int N = m.fN[f];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) out[q] += aPN * phi[q * phi_stride + N];
   }
   for (int k = m.nei_ptr[c]; k < m.nei_ptr[c + 1]; ++k) {
     const int f = m.nei_face[k];
-    const double aNP = -(gamma * m.alpha[f] + npmax0(F[f]));
+    const double aNP = -(gam.in(f) * m.alpha[f] + npmax0(F[f]));
     const int P = m.fP[f];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) out[q] += aNP * phi[q * phi_stride + P];
   }
 }
 
+template <int NQ>
+__device__ __forceinline__ void offdiag_apply(const b2s_mesh& m, int c, double gamma, const double* F,
+                                              const double* phi, int64_t phi_stride, double (&out)[NQ]) {
+  offdiag_apply_g<NQ>(m, c, ScalarGamma{gamma}, F, phi, phi_stride, out);
+}
+
 // 2-D: at most 64 registers, so four 256-thread blocks fit per SM and a 131k-cell mesh runs in
 // one wave (80 registers gave 1.16 waves; measured 0.045 -> 0.033 ms); 3-D keeps the 128
 // registers it uses without a bound (two blocks per SM: a tighter bound's spills cost what the
 // occupancy gains).
-template <int DIM>
+// TURB: per-face viscosities and the transpose-stress source, as momentum_assemble_k<DIM, true>.
+template <int DIM, bool TURB>
 __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_mixed_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Up,
                                           const double* __restrict__ gUp, const double* __restrict__ gp,
                                           const double* __restrict__ bUp, const double* __restrict__ F,
                                           const double* __restrict__ Fb, const double* __restrict__ por,
                                           const double* __restrict__ msrc, float* __restrict__ val,
                                           float* __restrict__ inv_out, double* __restrict__ dP_out,
-                                          float* __restrict__ r_out, double* __restrict__ part) {
+                                          float* __restrict__ r_out, double* __restrict__ part,
+                                          const double* __restrict__ mu_f, const double* __restrict__ mu_b,
+                                          const double* __restrict__ tsrc) {
   __shared__ double red[(kThreads / 32 + 1) * 2 * DIM];
   const int nc = m.nc, nb = m.nb;
   double acc[2 * DIM];
@@ -549,8 +558,14 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_
     const int c = r_.c;
     const double au = prm.relax_u_cell ? prm.relax_u_cell[c] : prm.relax_u;
     const bool simplec = prm.simplec_cell ? prm.simplec_cell[c] != 0 : prm.simplec != 0;
-    RowOut<DIM, DIM> o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
-                                                 (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
+    RowOut<DIM, DIM> o;
+    if constexpr (TURB)
+      o = transport_row_g<DIM, DIM>(m, c, FaceGamma{mu_f, mu_b}, bc.m_dirvel, F, Fb, Up + nc, nc,
+                                    gUp + (int64_t)DIM * nc, (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0,
+                                    val, true);
+    else
+      o = transport_row<DIM, DIM>(m, c, prm.mu, bc.m_dirvel, F, Fb, Up + nc, nc, gUp + (int64_t)DIM * nc,
+                                  (int64_t)DIM * nc, bUp + nb, nb, prm.second_order != 0, val, true);
     double diag = o.diag;
     const double V = m.vol[c];
     if (por) diag = diag + por[c] * V;
@@ -564,12 +579,14 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_
     }
     dP_out[c] = V / denom;
     double anb[DIM];
-    offdiag_apply<DIM>(m, c, prm.mu, F, Up + nc, nc, anb);
+    if constexpr (TURB) offdiag_apply_g<DIM>(m, c, FaceGamma{mu_f, mu_b}, F, Up + nc, nc, anb);
+    else offdiag_apply<DIM>(m, c, prm.mu, F, Up + nc, nc, anb);
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
       double src = -gp[(int64_t)k * nc + c] * V;
       if (drive) src = src + V * prm.body[k];
       if (msrc) src = src + msrc[(int64_t)k * nc + c];
+      if constexpr (TURB) src = src + tsrc[(int64_t)k * nc + c];
       const double rhs = o.rhs[k] + src;
       const double uc = Up[(int64_t)(1 + k) * nc + c];
       const double r = rhs - (diag * uc + anb[k]);
@@ -581,8 +598,8 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_
   block_partials<2 * DIM>(acc, red, part);
 }
 
-template <int DIM>
-__global__ void energy_assemble_mixed_k(b2s_mesh m, b2s_bc bc, double gamma, double cp, double aT, int second,
+template <int DIM, class GT>
+__global__ void energy_assemble_mixed_k(b2s_mesh m, b2s_bc bc, GT gamma, double cp, double aT, int second,
                                         const double* __restrict__ T, const double* __restrict__ gT,
                                         const double* __restrict__ Tb, const double* __restrict__ F,
                                         const double* __restrict__ Fb, const double* __restrict__ esrc,
@@ -593,7 +610,7 @@ __global__ void energy_assemble_mixed_k(b2s_mesh m, b2s_bc bc, double gamma, dou
   double acc[2] = {0.0, 0.0};
   for (CellRange r_ = cell_range(m); r_.c < r_.end; r_.c += r_.step) {
     const int c = r_.c;
-    RowOut<DIM, 1> o = transport_row<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
+    RowOut<DIM, 1> o = transport_row_g<DIM, 1>(m, c, gamma, bc.m_tfix, F, Fb, T, nc, gT, (int64_t)DIM * nc, Tb, nb,
                                              second != 0, val, true);
     double q = 0.0;
     for (int f = m.bptr[c]; f < m.bptr[c + 1]; ++f) q += bc.m_tflux[f] * bc.tval[f] * m.Sb_mag[f] / cp;
@@ -601,7 +618,7 @@ __global__ void energy_assemble_mixed_k(b2s_mesh m, b2s_bc bc, double gamma, dou
     const double rhs = o.rhs[0] + q;
     const double diag = o.diag;
     double anb[1];
-    offdiag_apply<1>(m, c, gamma, F, T, nc, anb);
+    offdiag_apply_g<1>(m, c, gamma, F, T, nc, anb);
     const double Tc = T[c];
     const double r = rhs - (diag * Tc + anb[0]);
     acc[0] += fabs(r);
@@ -887,22 +904,47 @@ int b2s_energy_assemble_turb_d(const b2s_mesh* m, const b2s_bc* bc, const double
                          diag, inv, b, br, part, s);
 }
 
+}  // extern "C"
+
+template <bool TURB>
+static int momentum_assemble_mixed(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                   const double* Up, const double* gUp, const double* gp, const double* bUp,
+                                   const double* F, const double* Fb, const double* porosity, const double* msrc,
+                                   float* val, float* inv, double* dP, float* r, double* part, const double* mu_f,
+                                   const double* mu_b, const double* tsrc, b2s_stream_t s) {
+  if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !inv || !dP || !r || !part ||
+      !(prm->relax_u > 0.0))
+    return B2S_ERR_ARG;
+  if (TURB && (!mu_f || (!mu_b && m->nb) || !tsrc)) return B2S_ERR_ARG;
+  unsigned g = part_grid_m(*m);
+  if (m->dim == 2)
+    momentum_assemble_mixed_k<2, TURB><<<g, kThreads, 0, (cudaStream_t)s>>>(
+        *m, *bc, *prm, Up, gUp, gp, bUp, F, Fb, porosity, msrc, val, inv, dP, r, part, mu_f, mu_b, tsrc);
+  else
+    momentum_assemble_mixed_k<3, TURB><<<g, kThreads, 0, (cudaStream_t)s>>>(
+        *m, *bc, *prm, Up, gUp, gp, bUp, F, Fb, porosity, msrc, val, inv, dP, r, part, mu_f, mu_b, tsrc);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+extern "C" {
+
 int b2s_momentum_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
                                   const double* Up, const double* gUp, const double* gp, const double* bUp,
                                   const double* F, const double* Fb, const double* porosity, const double* msrc,
                                   float* val, float* inv, double* dP, float* r, double* part, b2s_stream_t s) {
-  if (!mesh_ok(m) || !bc || !prm || !Up || !gUp || !gp || !bUp || !F || !Fb || !val || !inv || !dP || !r || !part ||
-      !(prm->relax_u > 0.0))
-    return B2S_ERR_ARG;
-  unsigned g = part_grid_m(*m);
-  if (m->dim == 2)
-    momentum_assemble_mixed_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb,
-                                                                       porosity, msrc, val, inv, dP, r, part);
-  else
-    momentum_assemble_mixed_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, *prm, Up, gUp, gp, bUp, F, Fb,
-                                                                       porosity, msrc, val, inv, dP, r, part);
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  return momentum_assemble_mixed<false>(m, bc, prm, Up, gUp, gp, bUp, F, Fb, porosity, msrc, val, inv, dP, r, part,
+                                        nullptr, nullptr, nullptr, s);
+}
+
+int b2s_momentum_assemble_mixed_turb_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                       const double* Up, const double* gUp, const double* gp, const double* bUp,
+                                       const double* F, const double* Fb, const double* porosity,
+                                       const double* msrc, const double* mu_f, const double* mu_b,
+                                       const double* tsrc, float* val, float* inv, double* dP, float* r,
+                                       double* part, b2s_stream_t s) {
+  return momentum_assemble_mixed<true>(m, bc, prm, Up, gUp, gp, bUp, F, Fb, porosity, msrc, val, inv, dP, r, part,
+                                       mu_f, mu_b, tsrc, s);
 }
 
 int b2s_pressure_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
@@ -923,22 +965,45 @@ int b2s_pressure_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, const b2s
   return B2S_OK;
 }
 
-int b2s_energy_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp, double relax_T,
-                                int second_order, const double* T, const double* gT, const double* Tb,
-                                const double* F, const double* Fb, const double* esrc, float* val, float* inv,
-                                float* r, double* part, b2s_stream_t s) {
+}  // extern "C"
+
+template <class GT>
+static int energy_assemble_mixed(const b2s_mesh* m, const b2s_bc* bc, GT gamma, double cp, double relax_T,
+                                 int second_order, const double* T, const double* gT, const double* Tb,
+                                 const double* F, const double* Fb, const double* esrc, float* val, float* inv,
+                                 float* r, double* part, b2s_stream_t s) {
   if (!mesh_ok(m) || !bc || !T || !gT || (!Tb && m->nb) || !F || !Fb || !val || !inv || !r || !part ||
       !(relax_T > 0.0) || !(cp != 0.0))
     return B2S_ERR_ARG;
   unsigned g = part_grid_m(*m);
   if (m->dim == 2)
-    energy_assemble_mixed_k<2><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T,
-                                                                     gT, Tb, F, Fb, esrc, val, inv, r, part);
+    energy_assemble_mixed_k<2, GT><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order,
+                                                                         T, gT, Tb, F, Fb, esrc, val, inv, r, part);
   else
-    energy_assemble_mixed_k<3><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order, T,
-                                                                     gT, Tb, F, Fb, esrc, val, inv, r, part);
+    energy_assemble_mixed_k<3, GT><<<g, kThreads, 0, (cudaStream_t)s>>>(*m, *bc, gamma, cp, relax_T, second_order,
+                                                                         T, gT, Tb, F, Fb, esrc, val, inv, r, part);
   B2S_LAUNCH_CHECK();
   return B2S_OK;
+}
+
+extern "C" {
+
+int b2s_energy_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp, double relax_T,
+                                int second_order, const double* T, const double* gT, const double* Tb,
+                                const double* F, const double* Fb, const double* esrc, float* val, float* inv,
+                                float* r, double* part, b2s_stream_t s) {
+  return energy_assemble_mixed(m, bc, ScalarGamma{gamma}, cp, relax_T, second_order, T, gT, Tb, F, Fb, esrc, val, inv,
+                               r, part, s);
+}
+
+int b2s_energy_assemble_mixed_turb_d(const b2s_mesh* m, const b2s_bc* bc, const double* gamma_f,
+                                     const double* gamma_b, double cp, double relax_T, int second_order,
+                                     const double* T, const double* gT, const double* Tb, const double* F,
+                                     const double* Fb, const double* esrc, float* val, float* inv, float* r,
+                                     double* part, b2s_stream_t s) {
+  if (!gamma_f || (!gamma_b && m && m->nb)) return B2S_ERR_ARG;
+  return energy_assemble_mixed(m, bc, FaceGamma{gamma_f, gamma_b}, cp, relax_T, second_order, T, gT, Tb, F, Fb, esrc,
+                               val, inv, r, part, s);
 }
 
 int b2s_row_residuals_d(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,

@@ -63,6 +63,8 @@ def _union_case(cases: Sequence[UnstructuredCase], meshes: Sequence[Unstructured
 class BatchSimpleSolver(MixedSimpleSolver):
     """Many independent cases (list of meshes and cases of one dimension) solved together."""
 
+    TURBULENCE = ("laminar",)
+
     # team shapes of the per-case Krylov solves (``b2s_team_config``: blocks per cluster, threads
     # per block, rows-per-warp switch), one per solve; ``autotune`` picks among TEAM_CANDIDATES on
     # the batch itself

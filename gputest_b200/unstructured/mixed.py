@@ -34,7 +34,7 @@ class MixedSimpleSolver(SimpleSolver):
     """Drop-in ``SimpleSolver`` whose linear systems are stored and solved in float."""
 
     PRECISIONS = ("mixed", "fp32", "fp64")
-    TURBULENCE = ("laminar",)
+    TURBULENCE = ("laminar", "k-omega-sst")  # the SST stages themselves stay in double
     REFINE_PASSES = 8       # double refinement passes of the pressure-correction solve at most
     INNER_TOL_FLOOR = 1e-5  # smallest relative reduction asked of one float pass
 
@@ -92,13 +92,23 @@ class MixedSimpleSolver(SimpleSolver):
         self._mark("gradients")
         part = self.part
         pt = lambda q: part.data_ptr() + 8 * q * self.nblk  # noqa: E731
-        _lib.check(L.b2s_momentum_assemble_mixed_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(),
-                                                   gp.data_ptr(), self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
-                                                   None if self.porosity is None else self.porosity.data_ptr(),
-                                                   None if self.mom_source is None else self.mom_source.data_ptr(),
-                                                   self.val_A32.data_ptr(), self.inv32.data_ptr(), self.dP.data_ptr(),
-                                                   self.r32.data_ptr(), pt(self.Q_MOM), s),
-                   "b2s_momentum_assemble_mixed_d")
+        por = None if self.porosity is None else self.porosity.data_ptr()
+        msrc = None if self.mom_source is None else self.mom_source.data_ptr()
+        tail = (self.val_A32.data_ptr(), self.inv32.data_ptr(), self.dP.data_ptr(), self.r32.data_ptr(),
+                pt(self.Q_MOM), s)
+        if self.turb is None:
+            _lib.check(L.b2s_momentum_assemble_mixed_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(),
+                                                       gp.data_ptr(), self.bUp.data_ptr(), F.data_ptr(), Fb.data_ptr(),
+                                                       por, msrc, *tail), "b2s_momentum_assemble_mixed_d")
+        else:
+            t = self.turb
+            self.kernel_launches += t.launch_momentum_terms(Up, self.gUp, old, s)
+            self._mark("turbulence_terms")
+            _lib.check(L.b2s_momentum_assemble_mixed_turb_d(self._m_mom, bc, pr, Up.data_ptr(), self.gUp.data_ptr(),
+                                                            gp.data_ptr(), self.bUp.data_ptr(), F.data_ptr(),
+                                                            Fb.data_ptr(), por, msrc, t.mu_f.data_ptr(),
+                                                            t.mu_b.data_ptr(), t.tsrc.data_ptr(), *tail),
+                       "b2s_momentum_assemble_mixed_turb_d")
         self._mark("momentum_assembly")
         # U* = U + dU, dU from A_r dU = b - A U (float, from zero)
         _lib.check(L.b2s_bicgstab_jacobi_f32_d(nc, dim, fv.rowptr.data_ptr(), fv.col.data_ptr(),
@@ -137,6 +147,10 @@ class MixedSimpleSolver(SimpleSolver):
             self._launch_energy(old, new, Fn, Fbn, s)
             self.kernel_launches += 4
             self._mark("energy")
+        if self.turb is not None:
+            self.kernel_launches += self.turb.launch_transport(old, new, Upn, Fn, Fbn, pt, self.Q_TMAX, self.Q_TRES,
+                                                               self.info_turb, s)
+            self._mark("turbulence")
         _lib.check(L.b2s_sum_partials_d(part.data_ptr(), self.nblk, self.NQ, self.NQ, self.q_of.data_ptr(),
                                         self.scal.data_ptr(), s), "b2s_sum_partials_d")
         self.kernel_launches += 1
@@ -153,13 +167,20 @@ class MixedSimpleSolver(SimpleSolver):
                    "b2s_ls_gradient_d")
         self._lagT = True
         second = (c.scalar_scheme or c.scheme) == "second-order"
-        _lib.check(L.b2s_energy_assemble_mixed_d(m, bc, c.conductivity / c.cp, c.cp, c.relax_T, int(second),
-                                                 T.data_ptr(), self.gT.data_ptr(), self.Tb.data_ptr(), Fn.data_ptr(),
-                                                 Fbn.data_ptr(),
-                                                 None if self.energy_source is None else self.energy_source.data_ptr(),
-                                                 self.val_T32.data_ptr(), self.invT32.data_ptr(), self.rT32.data_ptr(),
-                                                 self.part.data_ptr() + 8 * self.Q_ENUM * self.nblk, s),
-                   "b2s_energy_assemble_mixed_d")
+        esrc = None if self.energy_source is None else self.energy_source.data_ptr()
+        tail = (self.val_T32.data_ptr(), self.invT32.data_ptr(), self.rT32.data_ptr(),
+                self.part.data_ptr() + 8 * self.Q_ENUM * self.nblk, s)
+        if self.turb is None:
+            _lib.check(L.b2s_energy_assemble_mixed_d(m, bc, c.conductivity / c.cp, c.cp, c.relax_T, int(second),
+                                                     T.data_ptr(), self.gT.data_ptr(), self.Tb.data_ptr(),
+                                                     Fn.data_ptr(), Fbn.data_ptr(), esrc, *tail),
+                       "b2s_energy_assemble_mixed_d")
+        else:  # k/cp + mu_t/Pr_t per face (simple.py:781-782)
+            _lib.check(L.b2s_energy_assemble_mixed_turb_d(m, bc, self.turb.kT_f.data_ptr(), self.turb.kT_b.data_ptr(),
+                                                          c.cp, c.relax_T, int(second), T.data_ptr(),
+                                                          self.gT.data_ptr(), self.Tb.data_ptr(), Fn.data_ptr(),
+                                                          Fbn.data_ptr(), esrc, *tail),
+                       "b2s_energy_assemble_mixed_turb_d")
         _lib.check(L.b2s_bicgstab_jacobi_f32_d(self.nc, 1, fv.rowptr.data_ptr(), fv.col.data_ptr(),
                                                self.val_T32.data_ptr(), self.rT32.data_ptr(), self.invT32.data_ptr(),
                                                self.dT32.data_ptr(), 1e-3, 60, 1, 1, Tn.data_ptr(), T.data_ptr(),

@@ -388,11 +388,27 @@ B2S_API int b2s_pressure_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, c
                                           double* Fst, double* cf, double* Fbst, double* cb, float* val, double* rhs,
                                           double* part, b2s_stream_t s);
 
+/* b2s_momentum_assemble_mixed_d with the turbulence model's face viscosities and transpose-stress
+ * source (as b2s_momentum_assemble_turb_d). */
+B2S_API int b2s_momentum_assemble_mixed_turb_d(const b2s_mesh* m, const b2s_bc* bc, const b2s_flow_params* prm,
+                                               const double* Up, const double* gUp, const double* gp,
+                                               const double* bUp, const double* F, const double* Fb,
+                                               const double* porosity, const double* msrc, const double* mu_f,
+                                               const double* mu_b, const double* tsrc, float* val, float* inv,
+                                               double* dP, float* r, double* part, b2s_stream_t s);
+
 /* Energy assembly of b2s_energy_assemble_d in the form of b2s_momentum_assemble_mixed_d. */
 B2S_API int b2s_energy_assemble_mixed_d(const b2s_mesh* m, const b2s_bc* bc, double gamma, double cp,
                                         double relax_T, int second_order, const double* T, const double* gT,
                                         const double* Tb, const double* F, const double* Fb, const double* esrc,
                                         float* val, float* inv, float* r, double* part, b2s_stream_t s);
+
+/* b2s_energy_assemble_mixed_d with the diffusivity per face (as b2s_energy_assemble_turb_d). */
+B2S_API int b2s_energy_assemble_mixed_turb_d(const b2s_mesh* m, const b2s_bc* bc, const double* gamma_f,
+                                             const double* gamma_b, double cp, double relax_T, int second_order,
+                                             const double* T, const double* gT, const double* Tb, const double* F,
+                                             const double* Fb, const double* esrc, float* val, float* inv, float* r,
+                                             double* part, b2s_stream_t s);
 
 /* Jacobi-BiCGSTAB of b2s_bicgstab_jacobi_d with float matrix values and vectors (reductions in
  * double). zero_x0 starts from x = 0 without reading x; out64/base64 (both or neither, [nrhs][n])

@@ -79,15 +79,17 @@ def test_product_sst_setup_equals_the_reference(name):
 
 
 def test_sst_is_rejected_where_it_is_not_implemented():
-    """The mixed-precision and batched solvers do not carry the SST model: they refuse the case
-    before touching a device."""
+    """The batched solver does not carry the SST model: it refuses the case before touching a
+    device (the mixed-precision solver carries it, its SST stages in double)."""
+    from gputest_b200.unstructured.batch import BatchSimpleSolver
     from gputest_b200.unstructured.mixed import MixedSimpleSolver
 
+    assert "k-omega-sst" in MixedSimpleSolver.TURBULENCE
     mesh_fn, kw, _ = SST_CASES["chan2d"]
     bnd = {z: BoundarySpec(**spec) for z, spec in kw["boundaries"].items()}
+    case = UnstructuredCase(**{**kw, "boundaries": bnd, "precision": "mixed"})
     with pytest.raises(NotImplementedError, match="turbulence"):
-        MixedSimpleSolver(mesh_fn(cartesian_mesh_2d, extrude_to_3d),
-                          UnstructuredCase(**{**kw, "boundaries": bnd, "precision": "mixed"}))
+        BatchSimpleSolver([mesh_fn(cartesian_mesh_2d, extrude_to_3d)] * 2, [case, case])
 
 
 def test_energy_case_temperature_is_set_to_1e_4():
