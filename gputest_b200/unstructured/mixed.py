@@ -15,7 +15,10 @@ the linear algebra moved to float where the fixed point does not depend on it:
   is applied to it; the AMG hierarchy is rebuilt in double and copied to float, its coarsest
   level is solved with the double inverse;
 * gradients, fluxes, boundary values, the corrections, the continuity imbalance and every norm
-  stay double, and so do the fields.
+  stay double, and so do the fields;
+* with the k-omega SST model, the float momentum and energy rows take the model's per-face
+  viscosities and transpose-stress source, and the model's own stages (k, omega, mu_t) run in
+  double as in ``SimpleSolver``.
 
 The converged fields therefore agree with the double path's to the tolerance of the outer
 convergence test, not to the float rounding of the systems. ``diagnostics()`` and

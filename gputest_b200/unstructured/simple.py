@@ -36,8 +36,8 @@ reference's numbering. There is no CPU fallback: without a CUDA device the const
 raises.
 
 Not implemented (the constructor raises ``NotImplementedError``): the k-epsilon models,
-radiation, species, moving reference frames, solid zones, periodic pairs and transient runs
-(and the SST model in the mixed-precision and batched forms).
+radiation, species, moving reference frames, periodic pairs and transient runs (and the SST
+model in the batched form). Cases with solid zones go to ``conjugate.make_solver``.
 Additions over the reference: ``set_porosity`` (implicit Brinkman drag alpha V on the momentum
 diagonal) and ``set_boundary_velocity`` (a per-face velocity profile on a wall or inlet zone).
 """
