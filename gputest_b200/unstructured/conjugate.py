@@ -48,7 +48,8 @@ def harmonic_face_gamma(g, w, fP, fN, bP):
     return 1.0 / ((1.0 - w) / gP + w / gN), g[bP]
 
 
-def conjugate_setup(mesh: UnstructuredMesh, case: UnstructuredCase, hfv: HostFV = None, sub_hfv: HostFV = None) -> dict:
+def conjugate_setup(mesh: UnstructuredMesh, case: UnstructuredCase, hfv: HostFV = None,
+                    sub_hfv: HostFV = None) -> dict:
     """Host set-up of a conjugate case, in the reference's numbering (``conjugate.py:47-134``):
     the solid mask, the fluid sub-mesh with its face and cell maps, the flow case (no solids, no
     energy equation, interfaces as walls), the diffusivity k/cp per cell, the source per cell
@@ -133,7 +134,8 @@ class ConjugateSolver:
         hfv = HostFV(mesh)
         hs = conjugate_setup(mesh, case, hfv=hfv)
         self.solid, self.cell_map = hs["solid"], hs["cell_map"]
-        self.gam_cell, self.tkind_h, self.tval_h, self.is_outlet_h = hs["gam_cell"], hs["tkind"], hs["tval"], hs["is_outlet"]
+        self.gam_cell, self.tkind_h = hs["gam_cell"], hs["tkind"]
+        self.tval_h, self.is_outlet_h = hs["tval"], hs["is_outlet"]
         self._gamma_face_h, self._q_cell_h = hs["gamma_face"], hs["q_cell"]
         self.flow = SimpleSolver(hs["sub"], hs["flow_case"], **flow_kwargs)
         self.flow.external_energy = True  # no divergence guard under a conjugate solver (simple.py:733)
