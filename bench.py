@@ -406,6 +406,23 @@ def max_over_ranks(ms: float, world: int, device=None) -> float:
 
 
 # ---------------------------------------------------------------------------------- batched sweep
+def deal_cases(cells, world):
+    """Greedy cells-balanced deal of independent cases to ``world`` ranks: largest case first,
+    each to the rank with the fewest cells so far (ties to the lowest rank). Returns, per rank,
+    its case indices in increasing order. Every case goes to exactly one rank; the spread of
+    the ranks' cell totals is at most the largest case's cell count."""
+    import numpy as np
+
+    order = np.argsort([-int(c) for c in cells], kind="stable")
+    load = np.zeros(world)
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = int(np.argmin(load))
+        load[r] += int(cells[i])
+        out[r].append(int(i))
+    return [sorted(o) for o in out]
+
+
 def run_batch(args, rank, world):
     """The batched sweep (``--config c4``): all cases as one ``BatchSimpleSolver`` (the timed arm)
     against the same cases solved one at a time by ``MixedSimpleSolver`` (same arithmetic), on a
@@ -419,15 +436,7 @@ def run_batch(args, rank, world):
     from gputest_b200.unstructured.mixed import MixedSimpleSolver
 
     meshes, cases, kinds = make_batch_workload(args.batch_cases)
-    order = np.argsort([-m.n_cells for m in meshes], kind="stable")
-    load = np.zeros(world)
-    mine = []
-    for i in order:  # greedy cells-balanced deal
-        r = int(np.argmin(load))
-        load[r] += meshes[i].n_cells
-        if r == rank:
-            mine.append(int(i))
-    mine.sort()
+    mine = deal_cases([m.n_cells for m in meshes], world)[rank]
     meshes, cases, kinds = [meshes[i] for i in mine], [cases[i] for i in mine], [kinds[i] for i in mine]
     ncell = int(sum(m.n_cells for m in meshes))
     K, W = args.steps, max(args.warmup, 3)

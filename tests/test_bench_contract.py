@@ -1,5 +1,6 @@
 """bench.py's contract on CPU: the reference arm prints one JSON line with the required keys,
-and the replica timing takes the maximum over ranks (world size 2, gloo)."""
+the replica timing takes the maximum over ranks, and the batched sweep's cases are dealt to
+ranks without overlap or loss (world size 2, gloo)."""
 
 import json
 import os
@@ -39,22 +40,61 @@ def _worker(rank, port, q):
     dist.destroy_process_group()
 
 
-def test_replica_time_is_the_max_over_two_gloo_ranks():
+def _free_port():
     import socket
-
-    import torch.multiprocessing as mp
 
     with socket.socket() as sck:
         sck.bind(("127.0.0.1", 0))
-        port = sck.getsockname()[1]
+        return sck.getsockname()[1]
+
+
+def _run_ranks(target, world=2):
+    import torch.multiprocessing as mp
+
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=target, args=(r, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
-        p.join(120)
+        p.join(300)
         assert p.exitcode == 0
-    got = dict(q.get(timeout=10) for _ in range(2))
+    return dict(q.get(timeout=10) for _ in range(world))
+
+
+def test_replica_time_is_the_max_over_two_gloo_ranks():
+    got = _run_ranks(_worker)
     assert got == {0: 15.0, 1: 15.0}
     assert pytest.approx(15.0) == got[0]
+
+
+def _deal_worker(rank, port, q):
+    import torch.distributed as dist
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=2)
+    meshes, _, _ = bench.make_batch_workload(256)
+    cells = [m.n_cells for m in meshes]
+    mine = bench.deal_cases(cells, 2)[rank]
+    shares = [None, None]
+    dist.all_gather_object(shares, mine)  # each rank learns the other's share through the group
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, (shares, cells)))
+
+
+def test_batch_cases_dealt_to_two_gloo_ranks_are_disjoint_complete_and_balanced():
+    """The batched sweep's 256 cases dealt to two ranks (greedy, largest first): each rank's
+    share, gathered over the process group, is the same on both ranks; the shares are disjoint,
+    cover every case, and their cell totals differ by at most the largest case."""
+    got = _run_ranks(_deal_worker)
+    (s0, cells), (s1, _) = got[0], got[1]
+    assert s0 == s1
+    a, b = set(s0[0]), set(s0[1])
+    assert not (a & b) and a | b == set(range(256)) and len(s0[0]) + len(s0[1]) == 256
+    la, lb = sum(cells[i] for i in a), sum(cells[i] for i in b)
+    assert abs(la - lb) <= max(cells)
+    assert min(len(a), len(b)) > 64  # both ranks get a real share of the sweep
