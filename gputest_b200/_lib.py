@@ -110,6 +110,8 @@ _SIGS = {
     "b2s_amg_strength_changes_d": ([P, F64, P, P], ctypes.c_int),
     "b2s_row_residuals_d": ([I32, P, P, P, P, P, P, P, P, P, P], ctypes.c_int),
     "b2s_flux_balance_d": ([P, P, P, P, P, P], ctypes.c_int),
+    "b2s_matrix_properties_workspace_bytes": ([], I64),
+    "b2s_matrix_properties_d": ([P, P, P, I64, P, P], ctypes.c_int),
     "b2s_bicgstab_jacobi_noalloc_d": ([I32, ctypes.c_int, P, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, P, P],
                                       ctypes.c_int),
     # mixed precision

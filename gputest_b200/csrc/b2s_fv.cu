@@ -671,6 +671,65 @@ __global__ void flux_balance_k(b2s_mesh m, const double* __restrict__ F, const d
   }
 }
 
+// Properties of a cell-cell matrix on the mesh pattern that decide whether CG applies
+// (flowtrace/unstructured/diagnostics.py:384-412, restated from the definitions): per row the
+// diagonal and the sum of |off-diagonal| in stored order, per owned face the pair
+// (a_PN, a_NP), which is the whole off-diagonal pattern (every off-diagonal entry belongs to
+// one face, no pair repeats). Per block: max |a|, max |a_PN - a_NP|, max off-diagonal entry,
+// min (a_ii - sum_j |a_ij|) / max(|a_ii|, 1e-300), min a_ii; NaN propagates through every max
+// and min. Max and min are exact, so the result does not depend on the order.
+__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || b != b) ? NAN : fmax(a, b); }
+__device__ __forceinline__ double nan_min(double a, double b) { return (a != a || b != b) ? NAN : fmin(a, b); }
+
+constexpr int kPropQ = 5;
+constexpr int kPropBlocks = 1024;
+
+__global__ void matrix_properties_k(b2s_mesh m, const double* __restrict__ val, double* __restrict__ part) {
+  __shared__ double red[kPropQ][kThreads / 32];
+  double q[kPropQ] = {0.0, 0.0, -INFINITY, INFINITY, INFINITY};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < m.nc; c += gridDim.x * blockDim.x) {
+    double dg = 0.0, off = 0.0;
+    for (int j = m.rowptr[c]; j < m.rowptr[c + 1]; ++j) {
+      const double a = val[j];
+      q[0] = nan_max(q[0], fabs(a));
+      if (m.col[j] == c) {
+        dg = a;
+      } else {
+        off += fabs(a);
+        q[2] = nan_max(q[2], a);
+      }
+    }
+    q[3] = nan_min(q[3], (dg - off) / fmax(fabs(dg), 1e-300));
+    q[4] = nan_min(q[4], dg);
+    for (int f = m.own_ptr[c]; f < m.own_ptr[c + 1]; ++f) q[1] = nan_max(q[1], fabs(val[m.slot_PN[f]] - val[m.slot_NP[f]]));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kPropQ; ++k) {
+    double v = q[k];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, v, o);
+      v = (k >= 3) ? nan_min(v, u) : nan_max(v, u);
+    }
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kPropQ) {
+    const int k = threadIdx.x;
+    double v = red[k][0];
+    for (int w = 1; w < kThreads / 32; ++w) v = (k >= 3) ? nan_min(v, red[k][w]) : nan_max(v, red[k][w]);
+    part[k * kPropBlocks + blockIdx.x] = v;
+  }
+}
+
+__global__ void matrix_properties_finish_k(int nblk, const double* __restrict__ part, double* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= kPropQ) return;
+  double v = part[k * kPropBlocks];
+  for (int b = 1; b < nblk; ++b) v = (k >= 3) ? nan_min(v, part[k * kPropBlocks + b]) : nan_max(v, part[k * kPropBlocks + b]);
+  out[k] = v;
+}
+
 }  // namespace b2s
 
 using namespace b2s;
@@ -1019,6 +1078,20 @@ int b2s_flux_balance_d(const b2s_mesh* m, const double* F, const double* Fb, dou
                        b2s_stream_t s) {
   if (!mesh_ok(m) || !F || !Fb || !mass || !through) return B2S_ERR_ARG;
   flux_balance_k<<<grid_for(m->nc), kThreads, 0, (cudaStream_t)s>>>(*m, F, Fb, mass, through);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int64_t b2s_matrix_properties_workspace_bytes(void) { return (int64_t)kPropQ * kPropBlocks * (int64_t)sizeof(double); }
+
+int b2s_matrix_properties_d(const b2s_mesh* m, const double* val, double* work, int64_t work_bytes, double* out,
+                            b2s_stream_t s) {
+  if (!mesh_ok(m) || m->nc <= 0 || !val || !work || !out) return B2S_ERR_ARG;
+  if (work_bytes < b2s_matrix_properties_workspace_bytes()) return B2S_ERR_WORKSPACE;
+  const unsigned g = grid_for(m->nc) < (unsigned)kPropBlocks ? grid_for(m->nc) : (unsigned)kPropBlocks;
+  matrix_properties_k<<<g, kThreads, 0, (cudaStream_t)s>>>(*m, val, work);
+  B2S_LAUNCH_CHECK();
+  matrix_properties_finish_k<<<1, 32, 0, (cudaStream_t)s>>>((int)g, work, out);
   B2S_LAUNCH_CHECK();
   return B2S_OK;
 }

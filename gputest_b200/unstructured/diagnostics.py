@@ -5,8 +5,9 @@ The report of ``flowtrace/unstructured/diagnostics.py`` (``evaluate`` :214-359, 
 conventions (Oettli-Prager componentwise backward errors with Higham's gamma_K row exclusion,
 true linear reductions, local and global continuity, field change, non-finite counts). The
 row residuals and cell flux balances are computed on the device by ``b2s_row_residuals_d`` and
-``b2s_flux_balance_d`` from the systems the iteration left on the device; all scalars are
-reduced on the device and reach the host in one transfer. Cell indices in the report (worst
+``b2s_flux_balance_d`` from the systems the iteration left on the device, and the pressure
+matrix's CG conditions by ``b2s_matrix_properties_d``; all scalars are reduced on the device
+and reach the host in one transfer. Cell indices in the report (worst
 cells) are in the reference's numbering.
 """
 
@@ -285,23 +286,34 @@ def summary(d: dict) -> dict:
 
 
 def pressure_matrix_properties(solver) -> Optional[dict]:
-    """Conditions for CG on the latest pressure-correction matrix (``diagnostics.py:384-412``):
-    symmetry, non-positive off-diagonals, weak diagonal dominance. One host transfer."""
-    import scipy.sparse as sp
+    """Whether preconditioned CG applies to the latest pressure-correction matrix, with the keys
+    of ``flowtrace/unstructured/diagnostics.py:384-412``: it is a symmetric M-matrix (positive
+    semi-definite; singular up to a constant when no boundary fixes the pressure) when
+
+    * |A - A^T| is at most 64 u max|A| (u the unit round-off): on the mesh pattern every
+      off-diagonal pair is one face's (a_PN, a_NP), so this is the largest |a_PN - a_NP|;
+    * no off-diagonal entry exceeds 64 u max|A|;
+    * every diagonal entry is positive and every row weakly diagonally dominant: the margin
+      (a_ii - sum_{j != i} |a_ij|) / |a_ii| is at least -64 u.
+
+    One device pass over the matrix (``b2s_matrix_properties_d``: exact maxima and minima over
+    rows and faces) and a read of five numbers; None before the first iteration."""
+    import torch
 
     if getattr(solver, "_capture", None) is None:
         return None
-    A = sp.csr_matrix(solver.fv.matrix_to_host(solver.val_P), dtype=np.float64)
-    scale = float(abs(A).max()) or 1.0
-    asym = float(abs(A - A.T).max()) / scale if A.nnz else 0.0
-    diag = A.diagonal()
-    off = A - sp.diags(diag)
-    off_row_abs = np.asarray(abs(off).sum(axis=1)).ravel()
-    margin = (diag - off_row_abs) / np.maximum(np.abs(diag), 1e-300)
+    L, fv = _lib.lib(), solver.fv
+    work = torch.empty(int(L.b2s_matrix_properties_workspace_bytes()) // 8, dtype=torch.float64, device=fv.device)
+    res = torch.empty(5, dtype=torch.float64, device=fv.device)
+    _lib.check(L.b2s_matrix_properties_d(fv.cmesh_ref, solver.val_P.data_ptr(), work.data_ptr(), work.numel() * 8,
+                                         res.data_ptr(), _lib.stream_ptr()), "b2s_matrix_properties_d")
+    amax, asym_abs, off_max, margin, dmin = (float(v) for v in res.cpu().numpy())
+    scale = amax or 1.0
+    asym = asym_abs / scale if fv.nnz else 0.0
     tol = 64 * unit_roundoff(np.float64)
     out = {"symmetric": asym <= tol, "max_relative_asymmetry": asym,
-           "offdiagonal_nonpositive": bool(off.data.max() <= tol * scale) if off.nnz else True,
-           "weakly_diagonally_dominant": bool(margin.min() >= -tol) and bool((diag > 0).all()),
-           "min_dominance_margin": float(margin.min()), "singular": bool(getattr(solver, "singular_p", False))}
+           "offdiagonal_nonpositive": bool(off_max <= tol * scale) if fv.n_if else True,
+           "weakly_diagonally_dominant": bool(margin >= -tol) and bool(dmin > 0),
+           "min_dominance_margin": margin, "singular": bool(getattr(solver, "singular_p", False))}
     out["cg_applicable"] = out["symmetric"] and out["offdiagonal_nonpositive"] and out["weakly_diagonally_dominant"]
     return out

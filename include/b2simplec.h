@@ -265,6 +265,15 @@ B2S_API int b2s_row_residuals_d(int32_t n, const int32_t* rowptr, const int32_t*
 /* Cell mass imbalance (net outflow) and throughflow sum |F| of face fluxes (diagnostics.py:253-257). */
 B2S_API int b2s_flux_balance_d(const b2s_mesh* m, const double* F, const double* Fb, double* mass, double* through,
                                b2s_stream_t s);
+/* Properties of a cell-cell matrix on the mesh's CSR pattern that decide whether CG applies
+ * (replaces the host check of flowtrace/unstructured/diagnostics.py:384-412):
+ * out[0] = max |a_ij|, out[1] = max over faces |a_PN - a_NP| (the largest entry of |A - A^T|),
+ * out[2] = the largest off-diagonal entry, out[3] = min over rows (a_ii - sum_j!=i |a_ij|) /
+ * max(|a_ii|, 1e-300), out[4] = min a_ii. NaN entries make the affected outputs NaN. work holds
+ * b2s_matrix_properties_workspace_bytes() bytes; out is device memory (5 doubles). */
+B2S_API int64_t b2s_matrix_properties_workspace_bytes(void);
+B2S_API int b2s_matrix_properties_d(const b2s_mesh* m, const double* val, double* work, int64_t work_bytes,
+                                    double* out, b2s_stream_t s);
 
 /* ----------------------------------------------------------------------------------------- */
 /* Smoothed-aggregation AMG (flowtrace/linalg/amg.py:80-146) with aggregates and sparsity

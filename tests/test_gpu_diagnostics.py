@@ -172,6 +172,22 @@ def test_diagnostics_converge_towards_zero():
         assert late[k] < 1e-3 * early[k]
 
 
+def _host_matrix_properties(A):
+    """The definitions of ``flowtrace/unstructured/diagnostics.py:384-412`` evaluated with SciPy
+    on a host copy of the matrix (the checker of the device pass)."""
+    import scipy.sparse as sp
+
+    A = sp.csr_matrix(A)
+    scale = float(abs(A).max()) or 1.0
+    diag = A.diagonal()
+    off = (A - sp.diags(diag)).tocsr()
+    off.eliminate_zeros()
+    rowsum = np.asarray(abs(off).sum(axis=1)).ravel()
+    return {"asym": float(abs(A - A.T).max()) / scale, "off_max": float(off.data.max()) if off.nnz else -np.inf,
+            "margin": float(((diag - rowsum) / np.maximum(np.abs(diag), 1e-300)).min()), "scale": scale,
+            "dmin": float(diag.min())}
+
+
 def test_pressure_matrix_meets_the_conditions_for_cg():
     s = _cavity(n=10)
     assert D.pressure_matrix_properties(s) is None
@@ -181,3 +197,26 @@ def test_pressure_matrix_meets_the_conditions_for_cg():
     d = _run(_duct(energy=False), 3)
     pm = D.pressure_matrix_properties(d)
     assert pm["cg_applicable"] and not pm["singular"] and pm["min_dominance_margin"] >= -64 * D.unit_roundoff(np.float64)
+    for solver in (s, d):
+        pm = D.pressure_matrix_properties(solver)
+        h = _host_matrix_properties(solver.fv.matrix_to_host(solver.val_P))
+        assert pm["max_relative_asymmetry"] == h["asym"]
+        assert pm["min_dominance_margin"] == pytest.approx(h["margin"], rel=1e-12, abs=1e-15)
+        assert pm["offdiagonal_nonpositive"] == (h["off_max"] <= 64 * D.unit_roundoff(np.float64) * h["scale"])
+
+
+def test_pressure_matrix_properties_flag_a_planted_asymmetry_and_a_positive_offdiagonal():
+    """Entries planted in a copy of the matrix on the host side: the device pass reports what the
+    host definitions give."""
+    s = _cavity(n=10)
+    _run(s, 3)
+    fv = s.fv
+    j = int(fv.t["slot_PN"][5])
+    s.val_P[j] = s.val_P[j] * 0.5  # a_PN != a_NP on one face
+    pm = D.pressure_matrix_properties(s)
+    h = _host_matrix_properties(fv.matrix_to_host(s.val_P))
+    assert not pm["symmetric"] and pm["max_relative_asymmetry"] == pytest.approx(h["asym"], rel=1e-15)
+    assert not pm["cg_applicable"]
+    s.val_P[j] = abs(float(s.val_P[j])) + 1.0  # a positive off-diagonal entry
+    pm = D.pressure_matrix_properties(s)
+    assert not pm["offdiagonal_nonpositive"]
