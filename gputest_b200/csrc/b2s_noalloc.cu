@@ -9,12 +9,16 @@
 // caller; this entry point takes the same inputs and outputs without one.
 //
 // The scratch is a file-scope __device__ array sized for B2S_NOALLOC_MAX_UNKNOWNS unknowns
-// (n * nrhs); every GPU that loads the library holds it until the process exits. In host code
-// the array's name is only a host-side stand-in, so its device address is looked up with
-// cudaGetSymbolAddress, once per device, with that device current, on the first call on that
-// device (make that first call before any stream capture). Every call on a device shares the
-// one array, so calls that overlap on the GPU (concurrent streams, or several host threads)
-// race on it: serialise them. The solve initialises every scratch value it reads before reading
+// (n * nrhs): 11 vectors of 131,072 doubles plus 2 x 1184 x 9 doubles of block partials,
+// 11,704,832 bytes, which every GPU that loads the library holds until the process exits. In
+// host code the array's name is only a host-side stand-in, so its device address is looked up
+// with cudaGetSymbolAddress with the device current, on the first call in each CUDA context of a
+// device (the primary context that the runtime and torch use, or a context the caller made with
+// the driver API): the address is kept per device together with the id of the context it was
+// looked up in, and looked up again when the current context differs (after a
+// cudaDeviceReset, for instance). Make the first call on a device before any stream capture.
+// Every call on a device shares the one array, so calls that overlap on the GPU (concurrent
+// streams, or several host threads) race on it: serialise them. The solve initialises every scratch value it reads before reading
 // it (r, r_hat, u, p, v and w are set in its first phase, the rest are written before use), so the
 // contents left by the previous call do not matter.
 #include <mutex>
@@ -31,6 +35,35 @@ __device__ __align__(256) double g_bicgstab_scratch[kScratchDoubles];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // id of the context each address belongs to
+
+// The id of the current CUDA context (cuCtxGetCurrent + cuCtxGetId, reached through the
+// runtime's driver entry points so the library does not link the driver library itself).
+// 0 when either call is unavailable: the address is then looked up on every call.
+typedef int (*ctx_get_current_fn)(void**);
+typedef int (*ctx_get_id_fn)(void*, unsigned long long*);
+
+unsigned long long current_context_id() {
+  static ctx_get_current_fn get_current = nullptr;
+  static ctx_get_id_fn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (ctx_get_current_fn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (ctx_get_id_fn)f;
+    looked_up = true;
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 }  // namespace
 
@@ -45,10 +78,13 @@ extern "C" int b2s_bicgstab_jacobi_noalloc_d(int32_t n, int nrhs, const int32_t*
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_addr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
+      // the lookup also makes the device's primary context current when no context is yet
       void* addr = nullptr;
       if (cudaGetSymbolAddress(&addr, g_bicgstab_scratch) != cudaSuccess || !addr) return B2S_ERR_DEVICE;
       g_scratch_addr[dev] = (double*)addr;
+      g_scratch_ctx[dev] = current_context_id();
     }
     scratch = g_scratch_addr[dev];
   }

@@ -153,10 +153,11 @@ B2S_API int b2s_bicgstab_jacobi_d(int32_t n, int nrhs, const int32_t* rowptr, co
  * reaches the solver only through this C ABI and owns no CUDA allocator, or one whose device
  * memory is fully handed out before the solve): no work argument; the work space is a static
  * device array inside the library, sized for n * nrhs <= B2S_NOALLOC_MAX_UNKNOWNS (larger
- * problems return B2S_ERR_TOO_LARGE), held by every GPU that loads the library until exit. The
- * first call on a device looks the array's device address up (make it before any stream
- * capture); calls that overlap on the GPU share the array and race. No counterpart in the
- * reference, whose ft_bicgstab_jacobi always takes its work array from the caller. */
+ * problems return B2S_ERR_TOO_LARGE): 11,704,832 bytes, held by every GPU that loads the
+ * library until exit. The first call in each CUDA context of a device looks the array's device
+ * address up in that context (make it before any stream capture); calls that overlap on the
+ * GPU share the array and race. No counterpart in the reference, whose ft_bicgstab_jacobi
+ * always takes its work array from the caller. */
 #define B2S_NOALLOC_MAX_UNKNOWNS 131072
 B2S_API int b2s_bicgstab_jacobi_noalloc_d(int32_t n, int nrhs, const int32_t* rowptr, const int32_t* col,
                                           const double* val, const double* b, const double* inv_diag, double* x,

@@ -16,13 +16,13 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _system(seed, nrhs):
+def _system(seed, nrhs, mesh=None):
     import torch
 
     from gputest_b200.mesh.unstructured import cartesian_mesh_2d
     from gputest_b200.unstructured.fvmesh import FVMesh
 
-    mesh = cartesian_mesh_2d(24, 24, triangulate=True, warp=0.05)
+    mesh = mesh if mesh is not None else cartesian_mesh_2d(24, 24, triangulate=True, warp=0.05)
     fv = FVMesh(mesh)
     rng = np.random.default_rng(seed)
     d = 4 + rng.random(fv.nc)
@@ -76,6 +76,29 @@ def test_noalloc_bicgstab_equals_the_allocating_entry_point_on_consecutive_calls
         assert rel < 1e-12, rel
 
 
+def test_noalloc_single_system_and_exactly_at_capacity():
+    """One right-hand side, then n * nrhs exactly at the capacity (65,536 cells x 2), where the
+    static array's vectors and its block partials are packed tightest; both against the
+    allocating entry point."""
+    import torch
+
+    from gputest_b200.mesh.unstructured import cartesian_mesh_2d
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    cases = ((13, 1, 1e-8, 200, None), (14, 2, 1e-3, 60, cartesian_mesh_2d(256, 256, jitter=0.1, seed=4)))
+    for seed, nrhs, tol, maxiter, mesh in cases:
+        fv, val, B, X0, inv = _system(seed, nrhs, mesh)
+        assert mesh is None or fv.nc * nrhs == 131072
+        xa, ia = _solve(fv, val, B, X0, inv, tol, maxiter, noalloc=False)
+        xn, inn = _solve(fv, val, B, X0, inv, tol, maxiter, noalloc=True)
+        for a, b in zip(ia, inn):
+            assert (a.iterations, a.converged) == (b.iterations, b.converged)
+            assert abs(a.residual - b.residual) <= 1e-10 * max(a.residual, 1e-300)
+        rel = float((xn - xa).abs().max() / xa.abs().max().clamp_min(1e-300))
+        assert rel < 1e-12, rel
+
+
 def test_noalloc_rejects_sizes_beyond_its_capacity():
     import torch
 
@@ -87,3 +110,7 @@ def test_noalloc_rejects_sizes_beyond_its_capacity():
     # n * nrhs above the capacity is refused before any pointer is used or any kernel launched
     rc = L.b2s_bicgstab_jacobi_noalloc_d(131072, 2, None, None, None, None, None, None, 0.1, 30, 1, None, None)
     assert rc == -5
+    rc = L.b2s_bicgstab_jacobi_noalloc_d(131073, 1, None, None, None, None, None, None, 0.1, 30, 1, None, None)
+    assert rc == -5
+    rc = L.b2s_bicgstab_jacobi_noalloc_d(43691, 3, None, None, None, None, None, None, 0.1, 30, 1, None, None)
+    assert rc == -5  # 131,073 unknowns over three systems
