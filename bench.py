@@ -326,35 +326,73 @@ def stage_bytes(solver, stage, step_info):
     return None
 
 
-def sample_clocks(out_path):
-    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
-    try:
-        fh = open(out_path, "w")
-        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
-                                stdout=fh, stderr=subprocess.DEVNULL), fh
-    except Exception:
-        return None, None
+def _smi_target(dev_index):
+    """The nvidia-smi id of torch device ``dev_index``: its entry of CUDA_VISIBLE_DEVICES (an
+    index or a UUID) when that is set, else the index itself."""
+    vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    return vis[dev_index] if dev_index < len(vis) else str(dev_index)
 
 
-def parse_clocks(path, dev_index):
-    sm, mx, reasons = [], None, set()
-    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-    try:
-        for line in open(path):
+class ClockSampler:
+    """nvidia-smi samples of the SM clock, the power draw, the utilisation and the throttle
+    reasons of one GPU every 100 ms, from ``start()`` to ``stop()``, into a temporary file."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, dev_index):
+        import tempfile
+
+        self.target = _smi_target(dev_index)
+        fd, self.path = tempfile.mkstemp(prefix="b2s_clocks_", suffix=".csv")
+        os.close(fd)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.target, f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def stop(self):
+        """Stop sampling; the median SM clock over the samples taken under load (utilisation
+        above 0), the maximum clock and every throttle reason seen active."""
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        self.fh.close()
+        sm, loaded, mx, reasons = [], [], None, set()
+        for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9 or f[0] != str(dev_index):
+            if len(f) < 8:
                 continue
-            sm.append(float(f[1]))
-            mx = float(f[2])
-            for n, v in zip(names, f[5:9]):
+            try:
+                clk, mx = float(f[0]), float(f[1])
+            except ValueError:
+                continue
+            sm.append(clk)
+            try:
+                if float(f[3]) > 0:
+                    loaded.append(clk)
+            except ValueError:
+                pass
+            for n, v in zip(self.NAMES, f[4:8]):
                 if v.lower() == "active":
                     reasons.add(n)
-    except Exception:
-        pass
-    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-            "samples": len(sm)}
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
+        use = loaded or sm
+        return {"sm_mhz": statistics.median(use) if use else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm), "samples_under_load": len(loaded)}
 
 
 # ---------------------------------------------------------------------------------- CPU reference
@@ -504,7 +542,7 @@ def run_batch(args, rank, world):
     if args.converge:
         cc = [__import__("copy").deepcopy(c) for c in cases]
         for c in cc:
-            c.max_iter = args.converge_max_iter
+            c.max_iter = args.batch_converge_max_iter
         bc = BatchSimpleSolver(meshes, cc)
         c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         c0.record()
@@ -547,23 +585,24 @@ def batch_cpu_reference(args):
     ref = {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "iterations": 1, "seconds": seq_ms / 1e3,
            "sample": f"{len(sample)} of {len(meshes)} cases, one after another, >= 3 s each after 1 warm-up "
                      "iteration; per-iteration time interpolated over the cell count of every case"}
-    desc = {"workload": f"batched sweep: {len(meshes)} 2-D cavity/channel cases, 1k-64k cells log-uniform, jitter "
+    return ref, batch_desc(args)
+
+
+def batch_desc(args):
+    """Workload description of the whole batched sweep (every case, whatever the rank count)."""
+    meshes, _, _ = make_batch_workload(args.batch_cases)
+    ncell = sum(m.n_cells for m in meshes)
+    return {"workload": f"batched sweep: {len(meshes)} 2-D cavity/channel cases, 1k-64k cells log-uniform, jitter "
                         f"0.15h, Re 100-2000, seed 2 ({ncell:,} cells)", "cells": ncell}
-    return ref, desc
 
 
 def main_batch(args, rank, world, dev):
     import torch
 
-    smi, smi_fh = (sample_clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
-                   if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else sample_clocks(f"/tmp/clocks_rank{rank}.csv"))
+    smi = ClockSampler(dev).start()
     t_e2e = time.perf_counter()
     r = run_batch(args, rank, world)
-    if smi is not None:
-        smi.terminate()
-        smi.wait()
-        smi_fh.close()
-    clocks = parse_clocks(smi_fh.name, dev) if smi is not None else None
+    clocks = smi.stop()
     bs, K = r["solver"], args.steps
     torch.cuda.synchronize()
     f = bs.fields()
@@ -595,10 +634,9 @@ def main_batch(args, rank, world, dev):
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": r["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 systems, f64 residuals", "data": "synthetic",
-            "config": {"workload": f"batched sweep: {r['ncase']} 2-D cavity/channel cases, 1k-64k cells log-uniform, "
-                                   f"jitter 0.15h, Re 100-2000, seed 2 ({r['ncell']:,} cells on rank 0)",
-                       "cases": r["kinds"], "precision": "mixed", "l2": "flushed between timed steps (512 MiB write)",
-                       "parallelism": f"cases dealt to {world} ranks" if world > 1 else "single GPU"},
+            "config": workload_config(batch_desc(args)), "cases": r["kinds"], "cells_rank0": r["ncell"],
+            "precision": "mixed", "l2": "flushed between timed steps (512 MiB write)",
+            "parallelism": f"cases dealt to {world} ranks" if world > 1 else "single GPU",
             "one_at_a_time": {"value": r["one_at_a_time"], "unit": UNIT, "ratio": r["value"] / world / r["one_at_a_time"],
                               "sample": f"{len(r['sample'])} cases timed alone with MixedSimpleSolver "
                                         f"({K} steps each), per-step time interpolated over the cell count"},
@@ -627,10 +665,13 @@ def main():
                     help="fp64: the drop-in SimpleSolver; mixed: MixedSimpleSolver (float systems, double residuals)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--converge", action="store_true", help="also run to the 1e-6 residual and report it")
+    ap.add_argument("--converge", action="store_true", help="c4: also run the batch to the 1e-6 residual")
+    ap.add_argument("--no-converge", action="store_true", help="skip the to-convergence runs (FP64 and mixed)")
+    ap.add_argument("--no-c3", action="store_true", help="c2: skip the 524,288-cell duct block (FP64 vs mixed)")
     ap.add_argument("--batch-cases", type=int, default=256, help="c4: cases in the sweep")
     ap.add_argument("--batch-sample", type=int, default=24, help="c4: cases timed one at a time")
-    ap.add_argument("--converge-max-iter", type=int, default=6000, help="c4: outer-iteration cap of --converge")
+    ap.add_argument("--converge-max-iter", type=int, default=40000, help="outer-iteration cap of the to-convergence runs")
+    ap.add_argument("--batch-converge-max-iter", type=int, default=6000, help="c4: outer-iteration cap of --converge")
     ap.add_argument("--fd-dirs", type=int, default=16, help="c5: random finite-difference directions")
     ap.add_argument("--adj-grid", default="512x128", help="c5: channel grid nx x ny")
     ap.add_argument("--probe-grid", default="256x128x128", help="probe: duct grid nx x ny x nz")
@@ -653,7 +694,7 @@ def main():
         line = {"metric": METRIC, "value": ref["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": ref["iterations"],
                 "warmup": args.warmup, "ms_per_step": 1e3 * ref["seconds"] / ref["iterations"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": dict(desc, parallelism="host cores"), "impl": "reference",
+                "config": workload_config(desc), "parallelism": "host cores", "impl": "reference",
                 "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": ref["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -720,6 +761,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    smi = ClockSampler(dev).start()  # over every GPU phase below: warm-up to the last solve
     # ---- device-timed run
     run_case = __import__("copy").deepcopy(case)
     run_case.tol = 0.0  # K steps regardless of convergence
@@ -732,8 +774,6 @@ def main():
     launches0 = s.kernel_launches
     ev = []
     infos = []
-    smi, smi_fh = (sample_clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
-                   if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else sample_clocks(f"/tmp/clocks_rank{rank}.csv"))
 
     def before():  # L2 flush between timed iterations, outside their events
         flush.zero_()
@@ -746,10 +786,6 @@ def main():
     barrier()
     s.run(max_steps=K, hooks=(before, after, lambda: infos.append(dict(s.last_linear))))
     barrier()
-    if smi is not None:
-        smi.terminate()
-        smi.wait()
-        smi_fh.close()
     launches = s.kernel_launches - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
     graphs = bool(s.use_graphs and s._graphs)
@@ -765,7 +801,6 @@ def main():
     torch.cuda.synchronize()
     total_ms = max_over_ranks(sum(step_ms), world, "cuda")
     value = world * nc * K / (total_ms / 1e3)
-    clocks = parse_clocks(smi_fh.name if smi_fh is not None else "", dev) if smi is not None else None
 
     # ---- roofline of the dominant stage (stage events over the timed region)
     peaks = {}
@@ -788,14 +823,17 @@ def main():
                 "traffic": traffic, "algorithmic_bytes_per_launch": byts / K,
                 "kernel_timing": "CUDA events between stages over K stage-by-stage steps right after the timed region",
                 "stage_ms_per_step": {k: v / K for k, v in sorted(times.items(), key=lambda kv: -kv[1])}}
+    del s
 
     # ---- end to end through the public API, from host data
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
+    t_host = time.perf_counter()
     s2 = mk(run_case)
     if inlet is not None:
         inlet(s2)
+    setup_s = time.perf_counter() - t_host
     s2.run(max_steps=W + K)
     f = s2.fields()
     e1.record()
@@ -806,22 +844,26 @@ def main():
     d2h = s2.report.numel() * (W + K) + sum(v.nbytes for v in f.values())
     e2e = {"value": world * nc * (W + K) / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d / (W + K),
            "d2h_bytes_per_step": d2h / (W + K), "includes": "solver construction from the host mesh, W+K steps, "
-           "fields() read back"}
+           "fields() read back", "setup_seconds": setup_s, "seconds": e2e_ms / 1e3}
+    del s2
 
+    # ---- the metric's "to 1e-6" half: fresh solvers run to the 1e-6 scaled residual
     converge = None
-    if args.converge:
+    if not args.no_converge and args.config in ("c1", "c2", "c3", "sst"):
         barrier()
-        s3 = mk(case)
-        if inlet is not None:
-            inlet(s3)
-        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        c0.record()
-        s3.run()
-        c1.record()
-        torch.cuda.synchronize()
-        ms = c0.elapsed_time(c1)
-        converge = {"converged": bool(s3.converged), "iterations": s3.iteration, "seconds": ms / 1e3,
-                    "value": nc * s3.iteration / (ms / 1e3), "residuals": s3.residuals()["scaled"]}
+        converge = {"fp64": solve_to_convergence(SimpleSolver, mesh, case, inlet, skw, args.converge_max_iter)}
+        if args.config != "sst":
+            converge["mixed"] = solve_to_convergence(MixedSimpleSolver, mesh, case, inlet, skw, args.converge_max_iter)
+            converge["mixed_over_fp64"] = mixed_over_fp64(converge["fp64"], converge["mixed"])
+        for v in converge.values():
+            v.pop("fields", None)
+
+    # ---- the metric's "vs plain FP64 GPU path" half on the 524,288-cell duct
+    c3 = None
+    if args.config == "c2" and not args.no_c3:
+        barrier()
+        c3 = c3_block(args)
+    clocks = smi.stop()
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -839,11 +881,79 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 systems, f64 residuals", "data": "synthetic",
-            "config": dict(desc, precision=args.precision, l2="flushed between timed steps (512 MiB write)",
-                           parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+            "config": workload_config(desc), "precision": args.precision,
+            "l2": "flushed between timed steps (512 MiB write)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-            "linear_iterations_last": infos[K - 1], "cuda_graphs": graphs, "to_convergence": converge}
+            "linear_iterations_last": infos[K - 1], "cuda_graphs": graphs, "to_convergence": converge, "c3": c3}
     print(json.dumps(line), flush=True)
+
+
+def workload_config(desc):
+    """The ``config`` object of both arms: the workload and its size, nothing arm-specific."""
+    return {"workload": desc["workload"], "cells": desc["cells"]}
+
+
+def solve_to_convergence(Solver, mesh, case, inlet, skw, max_iter):
+    """A fresh solver from the host mesh run to the case's tolerance (1e-6 scaled residual) with
+    ``run()``; seconds by CUDA events around ``run()`` (set-up excluded, reported apart)."""
+    import copy
+
+    import torch
+
+    c = copy.deepcopy(case)
+    c.max_iter = int(max_iter)
+    t0 = time.perf_counter()
+    s = Solver(mesh, c, **skw)
+    if inlet is not None:
+        inlet(s)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    s.run()
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    out = {"converged": bool(s.converged), "iterations": int(s.iteration), "seconds": sec,
+           "value": mesh.n_cells * s.iteration / sec, "ms_per_step": 1e3 * sec / max(s.iteration, 1),
+           "setup_seconds": setup_s, "tol": float(c.tol),
+           "residuals": {k: float(v) for k, v in s.residuals()["scaled"].items()},
+           "amg_setups": int(s.amg_setups), "fields": s.fields()}
+    del s
+    torch.cuda.empty_cache()
+    return out
+
+
+def mixed_over_fp64(a, b):
+    """Mixed over FP64: cell-iterations/s ratio, seconds-to-convergence ratio and the largest
+    relative field difference of the two converged runs (max |mixed - fp64| / max |fp64|)."""
+    import numpy as np
+
+    diff = {}
+    for k, v in a["fields"].items():
+        if k in b["fields"]:
+            ref = np.asarray(v)
+            diff[k] = float(np.abs(np.asarray(b["fields"][k]) - ref).max() / max(np.abs(ref).max(), 1e-300))
+    return {"cell_iters_per_s_ratio": b["value"] / a["value"], "time_to_tol_ratio": a["seconds"] / b["seconds"],
+            "iterations": [a["iterations"], b["iterations"]], "field_max_rel_diff": diff}
+
+
+def c3_block(args):
+    """The 524,288-cell heated duct: FP64 ``SimpleSolver`` and ``MixedSimpleSolver`` from fresh
+    solvers to the 1e-6 scaled residual; seconds, cell-iterations/s, their ratio and the
+    converged fields' difference."""
+    from gputest_b200.unstructured.mixed import MixedSimpleSolver
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    mesh, case, desc, inlet, skw = make_workload("c3")
+    a = solve_to_convergence(SimpleSolver, mesh, case, inlet, skw, args.converge_max_iter)
+    b = solve_to_convergence(MixedSimpleSolver, mesh, case, inlet, skw, args.converge_max_iter)
+    out = {"workload": desc["workload"], "cells": desc["cells"], "fp64": a, "mixed": b,
+           "mixed_over_fp64": mixed_over_fp64(a, b)}
+    a.pop("fields")
+    b.pop("fields")
+    return out
 
 
 if __name__ == "__main__":

@@ -1,0 +1,210 @@
+"""Parity at the benchmark configurations, at full size (the reference's ``tests/test_gpu_real.py:
+92-107`` and ``tests/test_native.py:79-103`` are the models).
+
+* C2, the 131,072-triangle Re 1000 cavity, with the reference's AMG (``max_coarse=300``,
+  re-aggregation): 40 iterations iterate by iterate against the oracle running the reference's
+  own C++ kernels.
+* C3, the 524,288-cell heated duct (strength threshold 0): 3 iterations iterate by iterate.
+* The benchmarked configuration (``max_coarse=150``, aggregates fixed at the first set-up):
+  C1 converged against the oracle's converged solution; C2 and C3 (FP64 and mixed precision)
+  converged to the 1e-6 scaled residual, then checked to be fixed points of the reference's
+  iteration: one oracle iteration started from the device's converged state (fields and lagged
+  gradients) evaluates the reference's residuals there, which equal the device's own and stay
+  below the tolerance. The oracle cannot run these cases to convergence in a test (about 20,000
+  iterations of 0.2 s on C2); the fixed-point test is size independent.
+* C3, FP64 and mixed precision both converged to 1e-10: fields within 1e-6 of each other.
+
+The file is named to be collected after the other device tests.
+"""
+
+import copy
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+def _workload(name):
+    import bench
+
+    return bench.make_workload(name)
+
+
+def _oracle(mesh, case, amg_theta=0.08, inlet=False):
+    """The oracle driving the reference's own C++/OpenMP kernels (``oracle/_ref``) when they are
+    built, the NumPy restatement otherwise; with the duct's parabolic inlet when asked."""
+    from oracle.simplec_oracle import OracleSimple, load_native
+
+    o = OracleSimple(mesh, copy.deepcopy(case), native=load_native(), amg_theta=amg_theta)
+    if inlet:
+        z = mesh.zone_by_name("inlet")
+        fc = o.fv.xfb[o.fv.bzone == z.id]
+        u = 36.0 * fc[:, 1] * (1 - fc[:, 1]) * fc[:, 2] * (1 - fc[:, 2])
+        ub = o.ub_fixed.copy()
+        ub[o.fv.bzone == z.id] = np.stack([u, 0 * u, 0 * u], axis=1)
+        o.ub_fixed = ub
+        o.initialize({})
+    return o
+
+
+def _fields_close(fs, fo, tol):
+    for k, v in fo.items():
+        if k in fs and k != "viscosity-turb":
+            assert _rel(fs[k], v) < tol, (k, _rel(fs[k], v))
+
+
+# ------------------------------------------------------------------------- iterate by iterate
+def test_c2_full_size_iterates_equal_the_oracle_with_the_reference_amg():
+    """C2 at full size, 40 iterations: fields within 1e-8, momentum iteration counts equal at
+    every iteration, pressure iteration counts within one."""
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    mesh, case, _, _, skw = _workload("c2")
+    case = copy.deepcopy(case)
+    case.tol, case.max_iter, case.pressure_tol = 0.0, 40, 1e-9
+    s = SimpleSolver(mesh, case, max_coarse=300, **skw)
+    s.reaggregate = True  # the reference re-aggregates at every rebuild
+    o = _oracle(mesh, case)
+    for _ in range(40):
+        s.step()
+        o.step()
+        assert s.last_linear["momentum_iters"] == o.last_linear["momentum_iters"], o.iteration
+        assert abs(s.last_linear["pressure_iters"] - o.last_linear["pressure_iters"]) <= 1, o.iteration
+    _fields_close(s.fields(), o.fields(), 1e-8)
+    for k, v in o.residuals()["scaled"].items():
+        assert s.residuals()["scaled"][k] == pytest.approx(v, rel=1e-6), k
+
+
+def test_c3_full_size_iterates_equal_the_oracle():
+    """The 524,288-cell duct with energy, 3 iterations: fields within 1e-9, every linear
+    iteration count equal."""
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    mesh, case, _, inlet, skw = _workload("c3")
+    case = copy.deepcopy(case)
+    case.tol, case.max_iter = 0.0, 3
+    s = SimpleSolver(mesh, case, max_coarse=300, **skw)
+    s.reaggregate = True
+    inlet(s)
+    o = _oracle(mesh, case, amg_theta=skw["amg_theta"], inlet=True)
+    for _ in range(3):
+        s.step()
+        o.step()
+        assert s.last_linear["momentum_iters"] == o.last_linear["momentum_iters"], o.iteration
+        assert s.last_linear["pressure_iters"] == o.last_linear["pressure_iters"], o.iteration
+    _fields_close(s.fields(), o.fields(), 1e-9)
+
+
+# ------------------------------------------------------------------------- the benched configuration
+def test_c1_benched_configuration_converges_to_the_oracle_solution():
+    """C1 (64 x 64 cavity, Re 100, upwind, PCG 1e-8) with the benchmarked AMG: to the 1e-6 scaled
+    residual in the oracle's number of outer iterations (within 5%), and, both run on to 1e-10,
+    the oracle's converged fields within 1e-8."""
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    mesh, case, _, _, _ = _workload("c1")
+    case = copy.deepcopy(case)
+    case.max_iter = 5000
+    s = SimpleSolver(mesh, case)  # max_coarse 150, fixed aggregates: the benched default
+    o = _oracle(mesh, case)
+    s.run()
+    while not o.finished:
+        o.step()
+    assert s.converged and o.converged
+    assert abs(s.iteration - o.iteration) <= 0.05 * o.iteration, (s.iteration, o.iteration)
+    for solver in (s, o):
+        solver.case.tol = 1e-10
+        solver.converged = False
+    s.run()
+    while not o.finished:
+        o.step()
+    assert s.converged and o.converged
+    _fields_close(s.fields(), o.fields(), 1e-8)
+
+
+def _gradients_to_oracle(s, o):
+    """The device's lagged gradients (the ones its next iteration reconstructs boundary values
+    from) into the oracle, in the reference's numbering."""
+    fv, dim = s.fv, s.dim
+    gp = s.gpf if s.case.pressure_gradient == "green-gauss" else s.gUp[0]
+    o._gp = fv.cells_to_host(gp)
+    o._gU = [fv.cells_to_host(s.gUp[1 + k]) for k in range(dim)]
+    if s.energy and getattr(s, "gT", None) is not None:
+        o._gT = fv.cells_to_host(s.gT)
+
+
+def _fixed_point_check(s, o, tol, rel_equal):
+    """One more device iteration and one oracle iteration from the same converged state: the
+    reference's residuals there stay below 2 x tol; with ``rel_equal`` they also equal the
+    device's to that relative tolerance, and the two updated states agree to 1e-5."""
+    st = s.state_dict()
+    o.load_state(st)
+    _gradients_to_oracle(s, o)
+    s.converged = False
+    s.case.max_iter = s.iteration + 1
+    s.step()
+    o.case.tol, o.case.max_iter = 0.0, o.iteration + 1
+    o.step()
+    ro, rs = o.residuals()["scaled"], s.residuals()["scaled"]
+    assert max(ro.values()) < 2 * tol, ro
+    if rel_equal is not None:
+        for k, v in ro.items():
+            assert rs[k] == pytest.approx(v, rel=rel_equal), (k, rs[k], v)
+        _fields_close(s.fields(), o.fields(), 1e-5)
+    return ro
+
+
+def test_c2_benched_configuration_converged_state_is_a_fixed_point_of_the_oracle():
+    """C2 at full size with the benchmarked AMG, run to the 1e-6 scaled residual (about 20,000
+    outer iterations); the reference's iteration, started from that state, finds the same
+    residuals (relative 1e-5) below the tolerance."""
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    mesh, case, _, _, skw = _workload("c2")
+    case = copy.deepcopy(case)
+    case.max_iter = 60000
+    s = SimpleSolver(mesh, case, **skw)
+    s.run()
+    assert s.converged, (s.iteration, s.residuals()["scaled"])
+    _fixed_point_check(s, _oracle(mesh, case), case.tol, 1e-5)
+
+
+def test_c3_fp64_and_mixed_converged_states_are_fixed_points_and_agree_at_1e_10():
+    """The 524,288-cell duct, FP64 and mixed precision with the benchmarked AMG: each converged
+    to 1e-6 is a fixed point of the reference's FP64 iteration at that tolerance (for FP64 the
+    reference's residuals equal the device's); both run on to 1e-10 give fields within 1e-6 of
+    each other."""
+    from gputest_b200.unstructured.mixed import MixedSimpleSolver
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    mesh, case, _, inlet, skw = _workload("c3")
+    fields = {}
+    for name, Solver, rel_equal in (("fp64", SimpleSolver, 1e-5), ("mixed", MixedSimpleSolver, None)):
+        c = copy.deepcopy(case)
+        c.max_iter = 20000
+        s = Solver(mesh, c, **skw)
+        inlet(s)
+        s.run()
+        assert s.converged, (name, s.iteration, s.residuals()["scaled"])
+        _fixed_point_check(s, _oracle(mesh, c, amg_theta=skw["amg_theta"], inlet=True), c.tol, rel_equal)
+        s.case.tol, s.case.max_iter = 1e-10, s.iteration + 5000
+        s.converged = False
+        s.run()
+        assert s.converged, (name, s.iteration, s.residuals()["scaled"])
+        fields[name] = s.fields()
+        del s
+    for k, v in fields["fp64"].items():
+        assert _rel(fields["mixed"][k], v) <= 1e-6, (k, _rel(fields["mixed"][k], v))
