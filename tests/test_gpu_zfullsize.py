@@ -4,7 +4,8 @@
 * C2, the 131,072-triangle Re 1000 cavity, with the reference's AMG (``max_coarse=300``,
   re-aggregation): 40 iterations iterate by iterate against the oracle running the reference's
   own C++ kernels.
-* C3, the 524,288-cell heated duct (strength threshold 0): 3 iterations iterate by iterate.
+* C3, the 524,288-cell heated duct (strength threshold 0): 3 iterations iterate by iterate
+  (the temperature against the reference's own round-off sensitivity, see the test).
 * The benchmarked configuration (``max_coarse=150``, aggregates fixed at the first set-up):
   C1 converged against the oracle's converged solution; C2 and C3 (FP64 and mixed precision)
   converged to the 1e-6 scaled residual, then checked to be fixed points of the reference's
@@ -89,8 +90,15 @@ def test_c2_full_size_iterates_equal_the_oracle_with_the_reference_amg():
 
 
 def test_c3_full_size_iterates_equal_the_oracle():
-    """The 524,288-cell duct with energy, 3 iterations: fields within 1e-9, every linear
-    iteration count equal."""
+    """The 524,288-cell duct with energy, 3 iterations: velocity and pressure within 1e-9, every
+    momentum and pressure iteration count equal, each iteration's energy matrix (and the first
+    iteration's right-hand side, before the temperatures differ) within 1e-8 of the oracle's per
+    entry, the energy solve's iteration count equal. The temperature itself is compared against the reference's own round-off
+    sensitivity: the energy Jacobi-BiCGSTAB stops at its 60-iteration cap far from its 1e-3
+    tolerance (relative residual ~0.04), where its iterate is chaotic - the oracle's temperature
+    moves by tens of percent when the conductivity is perturbed by 1e-15 relative (measured by a
+    second oracle run here) - so the device's temperature may differ from the oracle's by as
+    much as the oracle differs from itself under that perturbation."""
     from gputest_b200.unstructured.simple import SimpleSolver
 
     mesh, case, _, inlet, skw = _workload("c3")
@@ -100,12 +108,26 @@ def test_c3_full_size_iterates_equal_the_oracle():
     s.reaggregate = True
     inlet(s)
     o = _oracle(mesh, case, amg_theta=skw["amg_theta"], inlet=True)
+    perturbed = copy.deepcopy(case)
+    perturbed.conductivity = case.conductivity * (1.0 + 1e-15)
+    o2 = _oracle(mesh, perturbed, amg_theta=skw["amg_theta"], inlet=True)
     for _ in range(3):
         s.step()
         o.step()
+        o2.step()
         assert s.last_linear["momentum_iters"] == o.last_linear["momentum_iters"], o.iteration
         assert s.last_linear["pressure_iters"] == o.last_linear["pressure_iters"], o.iteration
-    _fields_close(s.fields(), o.fields(), 1e-9)
+        es, eo = s.captured_systems()["energy"], o._capture["energy"]
+        Ao = getattr(eo["A"], "csr", eo["A"])
+        assert abs(es["A"] - Ao).max() <= 1e-8 * abs(Ao).max(), o.iteration
+        if o.iteration == 1:  # later right-hand sides carry the deferred correction of T
+            assert _rel(es["b"], eo["b"]) <= 1e-8
+        assert es["info"].iterations == eo["info"].iterations, o.iteration
+    fs, fo, fo2 = s.fields(), o.fields(), o2.fields()
+    _fields_close({k: v for k, v in fs.items() if k != "temperature"}, fo, 1e-9)
+    own = _rel(fo2["temperature"], fo["temperature"])  # the reference's own round-off sensitivity
+    assert own > 1e-6  # the energy solve is in its chaotic regime (else the bound below would be loose)
+    assert _rel(fs["temperature"], fo["temperature"]) <= own, (_rel(fs["temperature"], fo["temperature"]), own)
 
 
 # ------------------------------------------------------------------------- the benched configuration
