@@ -104,6 +104,7 @@ _SIGS = {
     "b2s_amg_workspace_bytes": ([P], I64),
     "b2s_amg_rebuild_d": ([P, P, I64, P], ctypes.c_int),
     "b2s_pcg_workspace_bytes": ([P], I64),
+    "b2s_pcg_set_launch": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "b2s_pcg_amg_d": ([P, I32, P, P, P, P, P, F64, ctypes.c_int, ctypes.c_int, P, I64, P, P], ctypes.c_int),
     "b2s_amg_vcycle_d": ([P, P, P, P, I64, P], ctypes.c_int),
     "b2s_host_aggregate": ([I64, P, P, P], I64),

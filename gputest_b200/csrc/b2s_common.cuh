@@ -77,11 +77,21 @@ __device__ __forceinline__ void block_partials(const double (&v)[NQ], double* sm
 }
 
 // Fixed-order total of quantity q over nb block partials (quantity-major layout), by one warp.
+// Each lane adds its partials b = lane, lane + 32, ... in that order; they are loaded eight at a
+// time as one straight-line block, so a lane's loads are in flight together instead of one
+// after another (the totals follow a grid barrier, on the critical path of every reduction).
 __device__ __forceinline__ double warp_total(const double* part, int nb, int nq, int q) {
   const int lane = threadIdx.x & 31;
   const double* pq = part + (int64_t)q * nb;
   double s = 0.0;
-  for (int b = lane; b < nb; b += 32) s += pq[b];
+  for (int b = lane; b < nb; b += 32 * 8) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = (b + 32 * u < nb) ? pq[b + 32 * u] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (b + 32 * u < nb) s += v[u];
+  }
   (void)nq;
   return warp_sum(s);
 }
@@ -99,6 +109,14 @@ __device__ __forceinline__ void grid_totals(const double* part, int nb, int nq, 
 }
 
 __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
+
+// Load of data that no thread writes while the kernel runs (matrix values, index arrays,
+// Jacobi inverses): through the read-only data path, whose lines stay cached on the SM across
+// the grid barriers of a cooperative kernel. Never for a vector the kernel writes.
+template <class T>
+__device__ __forceinline__ T ldro(const T* p) {
+  return __ldg(p);
+}
 
 }  // namespace b2s
 

@@ -9,6 +9,8 @@
 // in the same order, so all blocks take identical branches, and every loop is bounded by
 // maxiter. Partial sums alternate between two buffers so that a block writing the next
 // reduction never overtakes a block still reading the previous one.
+#include <mutex>
+
 #include "b2s_common.cuh"
 
 namespace b2s {
@@ -49,20 +51,21 @@ __device__ __forceinline__ void grid_reduce(cg::grid_group& grid, const double (
 constexpr int kRowUnroll = 8;
 
 // Rows [0, n) of a grid phase, one thread per row: emit(i, s) with s[k] the sum over row i's
-// entries j of entry(j, k). Each row's first kRowUnroll entries are issued as one straight-line
+// entries j of entry(j, k). A row's entries are issued kRowUnroll at a time as one straight-line
 // block so that their loads are in flight together; the sums keep the entries' stored order.
 template <int NR, class Entry, class Emit>
 __device__ __forceinline__ void walk_rows_nr(int n, int gt, int gs, const int32_t* __restrict__ rowptr, Entry entry,
                                              Emit emit) {
   for (int i = gt; i < n; i += gs) {
-    const int ja = rowptr[i], jae = rowptr[i + 1];
+    const int ja = ldro(rowptr + i), jae = ldro(rowptr + i + 1);
     double sa[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) sa[k] = 0.0;
+    for (int j = ja; j < jae; j += kRowUnroll) {
 #pragma unroll
-    for (int k = 0; k < kRowUnroll; ++k)
-      if (ja + k < jae) entry(ja + k, sa);
-    for (int j = ja + kRowUnroll; j < jae; ++j) entry(j, sa);
+      for (int k = 0; k < kRowUnroll; ++k)
+        if (j + k < jae) entry(j + k, sa);
+    }
     emit(i, sa);
   }
 }
@@ -139,15 +142,15 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
 #pragma unroll
     for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
     for (int i = gt; i < n; i += gs) {
-      const int j0 = a.rowptr[i], j1 = a.rowptr[i + 1];
-      const double iv = inv[i];
+      const int j0 = ldro(a.rowptr + i), j1 = ldro(a.rowptr + i + 1);
+      const double iv = ldro(inv + i);
       double ax[NR];
 #pragma unroll
       for (int k = 0; k < NR; ++k) ax[k] = 0.0;
       if (!a.zero_x0) {
         for (int j = j0; j < j1; ++j) {
-          const double av = a.val[j];
-          const int c = a.col[j];
+          const double av = ldro(a.val + j);
+          const int c = ldro(a.col + j);
 #pragma unroll
           for (int k = 0; k < NR; ++k) ax[k] += av * x[k][c];
         }
@@ -221,15 +224,15 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
         walk_rows_nr<NR>(
             n, gt, gs, a.rowptr,
             [&](int j, double (&sv)[NR]) {
-              const double aij = a.val[j];
-              const int c = a.col[j];
+              const double aij = ldro(a.val + j);
+              const int c = ldro(a.col + j);
 #pragma unroll
               for (int k = 0; k < NR; ++k)
                 if (st[k] == ACTIVE) sv[k] += aij * ((double)u[k][c] + beta[k] * w[k][c]);
             },
             [&](int i, const double (&av_)[NR]) {
               xupd(i);
-              const double iv = inv[i];
+              const double iv = ldro(inv + i);
 #pragma unroll
               for (int k = 0; k < NR; ++k)
                 if (st[k] == ACTIVE) {
@@ -271,8 +274,8 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
       walk_rows_nr<NR>(
           n, gt, gs, a.rowptr,
           [&](int j, double (&sv)[NR]) {
-            const double aij = a.val[j];
-            const int c = a.col[j];
+            const double aij = ldro(a.val + j);
+            const int c = ldro(a.col + j);
 #pragma unroll
             for (int k = 0; k < NR; ++k)
               if (st[k] == ACTIVE) sv[k] += aij * ((double)u[k][c] - alpha[k] * z[k][c]);
@@ -425,6 +428,8 @@ struct PcgArgsT {
   double* part1;
   VBufT<T> lv[B2S_AMG_MAX_LEVELS];
   b2s_solve_info* info;
+  int csize;    // blocks per thread-block cluster of the launch (0: no clusters)
+  int sub_nnz;  // largest level (entries) run on the subset of the grid (first cluster or block 0)
 };
 using PcgArgs = PcgArgsT<double>;
 
@@ -458,9 +463,11 @@ struct Rows {
 };
 
 // The rows [0, n) of a phase: emit(i, sum over row i's entries j of entry(j)). With one lane per
-// row and more rows than lanes, two rows are walked together, the first kRowUnroll entries of
-// both in one straight-line block, so that both rows' loads are in flight at once; each row's
-// sum keeps the entries' stored order, and every lane emits its rows in increasing order.
+// row and more rows than lanes, two rows are walked together, kRowUnroll entries of both at a
+// time in one straight-line block, so that both rows' loads are in flight at once. Otherwise a
+// lane takes kRowUnroll of its row's entries (every g-th) at a time the same way. Each row's
+// sum keeps the entries' stored order per lane (then the group's xor tree), and every lane
+// emits its rows in increasing order.
 template <class Entry, class Emit>
 __device__ __forceinline__ void walk_rows(const Rows& R, int n, const int32_t* __restrict__ rowptr, Entry entry,
                                           Emit emit) {
@@ -469,21 +476,23 @@ __device__ __forceinline__ void walk_rows(const Rows& R, int n, const int32_t* _
       const int ia = i0 + R.sub, ib = ia + R.stride;
       int ja = 0, jae = 0, jb = 0, jbe = 0;
       if (ia < n) {
-        ja = rowptr[ia];
-        jae = rowptr[ia + 1];
+        ja = ldro(rowptr + ia);
+        jae = ldro(rowptr + ia + 1);
       }
       if (ib < n) {
-        jb = rowptr[ib];
-        jbe = rowptr[ib + 1];
+        jb = ldro(rowptr + ib);
+        jbe = ldro(rowptr + ib + 1);
       }
       double sa = 0.0, sb = 0.0;
+      while (ja < jae || jb < jbe) {
 #pragma unroll
-      for (int k = 0; k < kRowUnroll; ++k) {
-        if (ja + k < jae) sa += entry(ja + k);
-        if (jb + k < jbe) sb += entry(jb + k);
+        for (int k = 0; k < kRowUnroll; ++k) {
+          if (ja + k < jae) sa += entry(ja + k);
+          if (jb + k < jbe) sb += entry(jb + k);
+        }
+        ja += kRowUnroll;
+        jb += kRowUnroll;
       }
-      for (int j = ja + kRowUnroll; j < jae; ++j) sa += entry(j);
-      for (int j = jb + kRowUnroll; j < jbe; ++j) sb += entry(j);
       if (ia < n) emit(ia, sa);
       if (ib < n) emit(ib, sb);
     }
@@ -492,8 +501,14 @@ __device__ __forceinline__ void walk_rows(const Rows& R, int n, const int32_t* _
       const int i = i0 + R.sub;
       const bool act = i < n;
       double s = 0.0;
-      if (act)
-        for (int j = rowptr[i] + R.lane; j < rowptr[i + 1]; j += R.g) s += entry(j);
+      if (act) {
+        const int je = ldro(rowptr + i + 1);
+        for (int j = ldro(rowptr + i) + R.lane; j < je; j += kRowUnroll * R.g) {
+#pragma unroll
+          for (int k = 0; k < kRowUnroll; ++k)
+            if (j + k * R.g < je) s += entry(j + k * R.g);
+        }
+      }
       s = R.total(s);
       if (act && R.writer()) emit(i, s);
     }
@@ -506,35 +521,51 @@ __device__ __forceinline__ void jacobi_step(const b2s_amg_level& L, const LvVals
                                             const T* x, T* y, int gt, int gs) {
   const Rows R(L.n, L.nnz, gt, gs);
   auto emit = [&](int i, double s) {
-    const double wd = w * V.dinv[i];
+    const double wd = w * ldro(V.dinv + i);
     const double xi = x ? (double)x[i] : wd * b[i];
     y[i] = xi + wd * (b[i] - s);
   };
   if (x) {
-    walk_rows(R, L.n, L.rowptr, [&](int j) { return (double)V.val[j] * x[L.col[j]]; }, emit);
+    walk_rows(R, L.n, L.rowptr, [&](int j) { return (double)ldro(V.val + j) * x[ldro(L.col + j)]; }, emit);
   } else {
     walk_rows(R, L.n, L.rowptr, [&](int j) {
-      const int c = L.col[j];
-      return (double)V.val[j] * ((w * V.dinv[c]) * b[c]);
+      const int c = ldro(L.col + j);
+      return (double)ldro(V.val + j) * ((w * ldro(V.dinv + c)) * b[c]);
     }, emit);
   }
 }
 
 // Barrier of a V-cycle phase: the whole grid for the large levels, block 0 alone for the tail.
+// kGrid: every block; kBlock: block 0 alone (block barriers); kCluster: the blocks of the
+// launch's first thread-block cluster (cluster barriers, which also order the cluster's global
+// memory accesses).
+enum { kGrid = 0, kBlock = 1, kCluster = 2 };
 struct Phase {
   cg::grid_group* grid;
-  bool tail;
+  int kind;
   int t, n;  // this thread's index and the number of threads in the phase
   __device__ __forceinline__ void sync() const {
-    if (tail) __syncthreads();
+    if (kind == kBlock) __syncthreads();
+    else if (kind == kCluster) cg::this_cluster().sync();
     else grid->sync();
   }
 };
 
-// Down-leg of level l (amg.py:135-139): pre-smoothing (the first two sweeps fused: the first
-// sweep's x = w D^-1 b is evaluated on the fly), residual, restriction to the next level.
+// The first sweep from x = 0, x1 = w D^-1 b (amg.py:135), of level l's row i, stored by the
+// phase that produces row i of b (the PCG residual update for level 0, the restriction for the
+// coarser levels) into the level's y buffer, so that the pre-smoothing phase gathers one value
+// per matrix entry instead of two. Same arithmetic as evaluating it on the fly.
 template <class T>
-__device__ __forceinline__ T* vdown(const PcgArgsT<T>& a, int l, const T* b, const Phase& ph) {
+__device__ __forceinline__ void store_first_sweep(const PcgArgsT<T>& a, int l, int i, T bi) {
+  a.lv[l].y[i] = (T)((a.h.omega * (double)ldro(a.lvv[l].dinv + i)) * (double)bi);
+}
+
+// Down-leg of level l (amg.py:135-139): pre-smoothing, residual, restriction to the next level.
+// The first two sweeps are one phase: with pre, the first sweep x1 = w D^-1 b is already in the
+// level's y buffer (store_first_sweep); otherwise it is evaluated on the fly for each neighbour.
+// The restriction also stores the next level's first sweep.
+template <class T>
+__device__ __forceinline__ T* vdown(const PcgArgsT<T>& a, int l, const T* b, const Phase& ph, bool pre) {
   const b2s_amg& h = a.h;
   const b2s_amg_level& lv = h.levels[l];
   const LvVals<T>& V = a.lvv[l];
@@ -544,9 +575,9 @@ __device__ __forceinline__ T* vdown(const PcgArgsT<T>& a, int l, const T* b, con
   T* Y = a.lv[l].y;
   T* c = X;
   if (h.sweeps <= 1) {
-    for (int i = ph.t; i < lv.n; i += ph.n) X[i] = (w * V.dinv[i]) * b[i];
+    for (int i = ph.t; i < lv.n; i += ph.n) X[i] = (w * ldro(V.dinv + i)) * b[i];
   } else {
-    jacobi_step(lv, V, w, b, (const T*)nullptr, X, ph.t, ph.n);
+    jacobi_step(lv, V, w, b, pre ? (const T*)Y : (const T*)nullptr, X, ph.t, ph.n);
     T* o = Y;
     for (int sw = 2; sw < h.sweeps; ++sw) {
       ph.sync();
@@ -559,11 +590,17 @@ __device__ __forceinline__ T* vdown(const PcgArgsT<T>& a, int l, const T* b, con
   ph.sync();
   T* Rv = a.lv[l].r;
   walk_rows(Rows(lv.n, lv.nnz, ph.t, ph.n), lv.n, lv.rowptr,
-            [&](int j) { return (double)V.val[j] * c[lv.col[j]]; }, [&](int i, double s) { Rv[i] = b[i] - s; });
+            [&](int j) { return (double)ldro(V.val + j) * c[ldro(lv.col + j)]; },
+            [&](int i, double s) { Rv[i] = b[i] - s; });
   ph.sync();
   T* bn = (l + 1 < L) ? a.lv[l + 1].b : a.cb;
+  const bool pre_next = l + 1 < L && h.sweeps >= 2;
   walk_rows(Rows(lv.nc, lv.p_nnz, ph.t, ph.n), lv.nc, lv.r_rowptr,
-            [&](int j) { return (double)V.r_val[j] * Rv[lv.r_col[j]]; }, [&](int I, double s) { bn[I] = s; });
+            [&](int j) { return (double)ldro(V.r_val + j) * Rv[ldro(lv.r_col + j)]; },
+            [&](int I, double s) {
+              bn[I] = s;
+              if (pre_next) store_first_sweep(a, l + 1, I, (T)s);
+            });
   ph.sync();
   return c;
 }
@@ -582,7 +619,7 @@ __device__ __forceinline__ T* vup(const PcgArgsT<T>& a, int l, const T* b, T* c,
   const bool want = stats != nullptr;
   double acc[3] = {0.0, 0.0, 0.0};
   walk_rows(Rows(lv.n, lv.p_nnz, ph.t, ph.n), lv.n, lv.p_rowptr,
-            [&](int j) { return (double)V.p_val[j] * xc[lv.p_col[j]]; },
+            [&](int j) { return (double)ldro(V.p_val + j) * xc[ldro(lv.p_col + j)]; },
             [&](int i, double s) {
               const double zi = c[i] + s;
               c[i] = zi;
@@ -596,9 +633,9 @@ __device__ __forceinline__ T* vup(const PcgArgsT<T>& a, int l, const T* b, T* c,
   for (int sw = 0; sw < h.sweeps; ++sw) {
     ph.sync();
     const bool last = sw + 1 == h.sweeps;
-    walk_rows(R, lv.n, lv.rowptr, [&](int j) { return (double)V.val[j] * c[lv.col[j]]; },
+    walk_rows(R, lv.n, lv.rowptr, [&](int j) { return (double)ldro(V.val + j) * c[ldro(lv.col + j)]; },
               [&](int i, double s) {
-                const double zi = c[i] + (w * V.dinv[i]) * (b[i] - s);
+                const double zi = c[i] + (w * ldro(V.dinv + i)) * (b[i] - s);
                 o[i] = zi;
                 if (want && last) {
                   acc[0] += zi;
@@ -627,7 +664,11 @@ __device__ __forceinline__ void vcoarse(const PcgArgsT<T>& a, const T* cb, const
   for (int I = ph.t >> 5; I < nc; I += ph.n >> 5) {
     const double* row = a.h.coarse_inv + (int64_t)I * nc;
     double s = 0.0;
-    for (int J = lane; J < nc; J += 32) s += row[J] * cb[J];
+    for (int J = lane; J < nc; J += 32 * kRowUnroll) {
+#pragma unroll
+      for (int k = 0; k < kRowUnroll; ++k)
+        if (J + 32 * k < nc) s += ldro(row + J + 32 * k) * cb[J + 32 * k];
+    }
     s = warp_sum(s);
     if (lane == 0) a.cx[I] = s;
   }
@@ -644,47 +685,57 @@ __device__ __forceinline__ T* tail_result(const PcgArgsT<T>& a, int l) {
   return ((down + sw) & 1) ? a.lv[l].y : a.lv[l].x;
 }
 
-// Levels of at most kTailRows rows (no more rows than one block has threads) and kTailNnz
-// entries, and the coarse solve, run in block 0 with block barriers while the other blocks wait
-// at the next grid barrier: below that size a level is latency-bound and a grid barrier costs
-// more than it saves.
-constexpr int kTailRows = kCoopThreads;
-constexpr int kTailNnz = 16384;
+// The small end of the hierarchy runs on a subset of the grid while the other blocks wait at
+// the next grid barrier. A phase costs about a barrier (grid ~1.3 us, cluster ~0.35 us, block
+// ~0.05 us on B200) plus its gathers, which an SM issues at roughly one scattered cache line per
+// cycle: a level of E entries is worth moving from the 148 SMs to a subset of S SMs when
+// E (1/S - 1/148) / 2 ns is below the barrier time saved. The subset is the launch's first
+// thread-block cluster when the launch is made of clusters (PcgArgsT::csize > 0), else block 0;
+// it takes every level (and the coarse solve) with at most PcgArgsT::sub_nnz entries (matrix,
+// prolongation; coarse_n^2 for the coarse solve) and at most 4 rows per thread.
+constexpr int kSubRowsPerThread = 4;
 
-// z = M r: the V-cycle of flowtrace/linalg/amg.py:130-142. Returns the buffer holding z. With
+// z = M r: the V-cycle of flowtrace/linalg/amg.py:130-142. Returns the buffer holding z. pre0:
+// the caller stored level 0's first sweep from rhs0 (store_first_sweep) when it wrote rhs0. With
 // stats != nullptr, when level 0 runs on the whole grid, stats[0..2] receive sum z, sum r z and
 // sum r (r = rhs0) and *have_stats is set; otherwise the caller reduces them itself.
 template <class T>
-__device__ T* vcycle(cg::grid_group& grid, const PcgArgsT<T>& a, const T* rhs0, int gt, int gs,
+__device__ T* vcycle(cg::grid_group& grid, const PcgArgsT<T>& a, const T* rhs0, bool pre0, int gt, int gs,
                      double* red = nullptr, double* stats = nullptr, int pb = 0, bool* have_stats = nullptr) {
   const b2s_amg& h = a.h;
   const int L = h.nlevels;
   T* cur[B2S_AMG_MAX_LEVELS];
   const T* cb = (L == 0) ? rhs0 : a.cb;
-  int Lg = L;  // levels from Lg on (all small) run in block 0; the others on the whole grid
-  while (Lg > 0 && h.levels[Lg - 1].n <= kTailRows && h.levels[Lg - 1].nnz <= kTailNnz &&
-         h.levels[Lg - 1].p_nnz <= kTailNnz)
+  const bool cl = a.csize > 0;
+  const int64_t sub_rows = (int64_t)(cl ? a.csize : 1) * blockDim.x * kSubRowsPerThread;
+  const int64_t sub_nnz = a.sub_nnz;
+  int Lg = L;  // levels from Lg on (all small) run on the subset; the others on the whole grid
+  while (Lg > 0 && h.levels[Lg - 1].n <= sub_rows && h.levels[Lg - 1].nnz <= sub_nnz &&
+         h.levels[Lg - 1].p_nnz <= sub_nnz)
     --Lg;
-  const Phase gph = {&grid, false, gt, gs};
-  const Phase tph = {&grid, true, (int)threadIdx.x, (int)blockDim.x};
-  for (int l = 0; l < Lg; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, gph);
-  if (Lg == L && h.coarse_n > kTailRows) {
+  const bool sub_coarse = (int64_t)h.coarse_n * h.coarse_n <= sub_nnz;
+  const Phase gph = {&grid, kGrid, gt, gs};
+  const Phase sph = cl ? Phase{&grid, kCluster, (int)(blockIdx.x * blockDim.x + threadIdx.x), a.csize * (int)blockDim.x}
+                       : Phase{&grid, kBlock, (int)threadIdx.x, (int)blockDim.x};
+  const bool in_sub = cl ? (int)blockIdx.x < a.csize : blockIdx.x == 0;
+  for (int l = 0; l < Lg; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, gph, l > 0 || pre0);
+  if (Lg == L && !sub_coarse) {
     vcoarse(a, cb, gph);
   } else {
-    if (blockIdx.x == 0) {
-      for (int l = Lg; l < L; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, tph);
-      vcoarse(a, cb, tph);
+    if (in_sub) {
+      for (int l = Lg; l < L; ++l) cur[l] = vdown(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, sph, l > 0 || pre0);
+      vcoarse(a, cb, sph);
       for (int l = L - 1; l >= Lg; --l)
         cur[l] = vup(a, l, (l == 0) ? rhs0 : (const T*)a.lv[l].b, cur[l], (const T*)((l + 1 < L) ? cur[l + 1] : a.cx),
-                     tph, (const T*)nullptr, nullptr, nullptr, 0);
+                     sph, (const T*)nullptr, nullptr, nullptr, 0);
     }
     grid.sync();
   }
   for (int l = Lg - 1; l >= 0; --l) {
     const T* xc;
     if (l + 1 < L) {
-      // the next level's solution: every block tracks it on the grid levels; for the first tail
-      // level (run by block 0 alone) every block names it from the sweep parity
+      // the next level's solution: every block tracks it on the grid levels; for the first level
+      // run by the subset every block names it from the sweep parity
       if (l + 1 < Lg) xc = cur[l + 1];
       else xc = tail_result(a, l + 1);
     } else {
@@ -717,6 +768,7 @@ __device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const 
   const int n = a.n;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   double* part[2] = {a.part0, a.part1};
+  const bool pre0 = a.h.nlevels > 0 && a.h.sweeps >= 2;  // level 0's first sweep stored with r
   T* r = a.r;
   T* q = a.q;
   T* pbuf[2] = {a.p, a.p2};
@@ -729,6 +781,7 @@ __device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const 
       const double bi = bvec[i];
       x[i] = 0.0;
       r[i] = bi;
+      if (pre0 && !a.project) store_first_sweep(a, 0, i, (T)bi);
       acc[0] += bi * bi;
       acc[1] += bi;
     }
@@ -742,6 +795,7 @@ __device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const 
       for (int i = gt; i < n; i += gs) {
         const double ri = r[i] - mean;
         r[i] = ri;
+        if (pre0) store_first_sweep(a, 0, i, (T)ri);
         acc2[0] += ri * ri;
       }
       __syncthreads();
@@ -766,7 +820,7 @@ __device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const 
   auto precondition = [&]() {
     __syncthreads();
     bool have = false;
-    z = vcycle(grid, a, (const T*)r, gt, gs, red, stats, pb, &have);
+    z = vcycle(grid, a, (const T*)r, pre0, gt, gs, red, stats, pb, &have);
     double sz, srz, sr;
     if (have) {
       pb ^= 1;
@@ -803,9 +857,9 @@ __device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const 
       walk_rows_nr<1>(
           n, gt, gs, a.rowptr,
           [&](int j, double (&sv)[1]) {
-            const int c = a.col[j];
+            const int c = ldro(a.col + j);
             const double pj = first ? z[c] - zm : (z[c] - zm) + beta * po[c];
-            sv[0] += a.val[j] * pj;
+            sv[0] += ldro(a.val + j) * pj;
           },
           [&](int i, const double (&sv)[1]) {
             const double pi = first ? z[i] - zm : (z[i] - zm) + beta * po[i];
@@ -833,6 +887,7 @@ __device__ CgOutcome pcg_core(cg::grid_group& grid, const PcgArgsT<T>& a, const 
         x[i] = x[i] + alpha * pn[i];
         const double ri = r[i] - alpha * q[i];
         r[i] = ri;
+        if (pre0) store_first_sweep(a, 0, i, (T)ri);
         acc[0] += ri * ri;
       }
       grid_reduce<2>(grid, acc, red, part[pb], tot);
@@ -1012,6 +1067,102 @@ static int coop_grid(K kernel, int* grid_out) {
   return B2S_OK;
 }
 
+// Cooperative launches of the AMG-PCG kernels as thread-block clusters of g_pcg_cluster blocks
+// (the small end of each V-cycle then runs on the first cluster with cluster barriers). The
+// grid is every cluster that co-resides on the device, which leaves a few SMs idle when the
+// cluster size does not divide the SMs of a GPC; a launch is made with clusters only when that
+// grid still covers three quarters of the SMs, and falls back to a plain cooperative launch
+// (csize = 0) when the cluster launch is refused.
+static int g_pcg_cluster = 0;
+static int g_sub_nnz[2] = {4096, 32768};  // without / with clusters
+
+static int coop_cluster_grid(const void* kernel, int C, int* grid_out) {
+  struct Entry {
+    const void* kernel;
+    int dev, C, grid;
+  };
+  static Entry cache[32];
+  static int ncache = 0;
+  static std::mutex mu;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return B2S_ERR_DEVICE;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (int i = 0; i < ncache; ++i)
+      if (cache[i].kernel == kernel && cache[i].dev == dev && cache[i].C == C) {
+        *grid_out = cache[i].grid;
+        return cache[i].grid > 0 ? B2S_OK : B2S_ERR_DEVICE;
+      }
+  }
+  if (C > 8) cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeCooperative;
+  attr[1].val.cooperative = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)C, 1, 1);
+  cfg.blockDim = dim3(kCoopThreads, 1, 1);
+  cfg.attrs = attr;
+  cfg.numAttrs = 2;
+  int ncl = 0, g = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, kernel, &cfg) == cudaSuccess && ncl > 0) {
+    g = ncl * C;
+    if (g > kMaxCoopBlocks) g = kMaxCoopBlocks - kMaxCoopBlocks % C;
+  } else {
+    cudaGetLastError();
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (ncache < 32) cache[ncache++] = {kernel, dev, C, g};
+  *grid_out = g;
+  return g > 0 ? B2S_OK : B2S_ERR_DEVICE;
+}
+
+// Launch an AMG-PCG kernel whose argument block is *args_block; its csize and sub_nnz fields
+// (at *csize, *sub_nnz) are set to the launch shape used.
+template <class K>
+static int launch_pcg_kernel(K kernel, void* args_block, int* csize, int* sub_nnz, b2s_stream_t s) {
+  void* args[] = {args_block};
+  const int C = g_pcg_cluster;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return B2S_ERR_DEVICE;
+  int g = 0;
+  if (C > 1 && coop_cluster_grid((const void*)kernel, C, &g) == B2S_OK && 4 * g >= 3 * sms) {
+    *csize = C;
+    *sub_nnz = g_sub_nnz[1];
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeCooperative;
+    attr[1].val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)g, 1, 1);
+    cfg.blockDim = dim3(kCoopThreads, 1, 1);
+    cfg.stream = (cudaStream_t)s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    if (cudaLaunchKernelExC(&cfg, (const void*)kernel, args) == cudaSuccess) {
+      B2S_LAUNCH_CHECK();
+      return B2S_OK;
+    }
+    cudaGetLastError();  // a refused launch configuration: launch without clusters
+  }
+  *csize = 0;
+  *sub_nnz = g_sub_nnz[0];
+  int rc;
+  if ((rc = coop_grid(kernel, &g)) != B2S_OK) return rc;
+  if (cudaLaunchCooperativeKernel((void*)kernel, g, kCoopThreads, args, 0, (cudaStream_t)s) != cudaSuccess)
+    return B2S_ERR_LAUNCH;
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
 template <class T>
 static T* pcg_layout(const b2s_amg* h, T* w, PcgArgsT<T>& a) {
   const int64_t n = h->nlevels ? h->levels[0].n : h->coarse_n;
@@ -1060,6 +1211,16 @@ static int launch_bicgstab(BicgArgsT<T>& a, int nrhs, b2s_stream_t s) {
 using namespace b2s;
 
 extern "C" {
+
+int b2s_pcg_set_launch(int cluster_blocks, int sub_entries) {
+  if (cluster_blocks != 0 && cluster_blocks != 2 && cluster_blocks != 4 && cluster_blocks != 8 &&
+      cluster_blocks != 16)
+    return B2S_ERR_ARG;
+  if (sub_entries < 0) return B2S_ERR_ARG;
+  g_pcg_cluster = cluster_blocks;
+  g_sub_nnz[cluster_blocks > 0 ? 1 : 0] = sub_entries;
+  return B2S_OK;
+}
 
 int b2s_spmv_d(int32_t n, int k, const int32_t* rowptr, const int32_t* col, const double* val, const double* x,
                double* y, b2s_stream_t s) {
@@ -1186,13 +1347,7 @@ int b2s_pcg_amg_d(const b2s_amg* h, int32_t n, const int32_t* rowptr, const int3
   a.project = project ? 1 : 0;
   a.info = info;
   pcg_layout(h, (double*)work, a);
-  void* args[] = {&a};
-  int g = 0, rc;
-  if ((rc = coop_grid(pcg_amg_coop_k, &g)) != B2S_OK) return rc;
-  if (cudaLaunchCooperativeKernel((void*)pcg_amg_coop_k, g, kCoopThreads, args, 0, (cudaStream_t)s) != cudaSuccess)
-    return B2S_ERR_LAUNCH;
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  return launch_pcg_kernel(pcg_amg_coop_k, &a, &a.csize, &a.sub_nnz, s);
 }
 
 static bool amg32_ok(const b2s_amg* h, const b2s_amg_f32* h32) {
@@ -1252,13 +1407,7 @@ int b2s_pcg_amg_mixed_d(const b2s_amg* h, const b2s_amg_f32* h32, const b2s_mesh
   M.maxiter = maxiter;
   M.maxpass = maxpass;
   M.min_inner_tol = min_inner_tol;
-  void* args[] = {&M};
-  int g = 0, rc;
-  if ((rc = coop_grid(pcg_mixed_coop_k, &g)) != B2S_OK) return rc;
-  if (cudaLaunchCooperativeKernel((void*)pcg_mixed_coop_k, g, kCoopThreads, args, 0, (cudaStream_t)s) != cudaSuccess)
-    return B2S_ERR_LAUNCH;
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  return launch_pcg_kernel(pcg_mixed_coop_k, &M, &M.a.csize, &M.a.sub_nnz, s);
 }
 
 }  // extern "C"
@@ -1267,7 +1416,7 @@ namespace b2s {
 __global__ void __launch_bounds__(kCoopThreads) vcycle_coop_k(PcgArgs a) {
   cg::grid_group grid = cg::this_grid();
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
-  const double* z = vcycle(grid, a, a.b, gt, gs);
+  const double* z = vcycle(grid, a, a.b, false, gt, gs);
   const int n = a.h.nlevels ? a.h.levels[0].n : a.h.coarse_n;
   for (int i = gt; i < n; i += gs) a.x[i] = z[i];
 }
@@ -1290,11 +1439,5 @@ extern "C" int b2s_amg_vcycle_d(const b2s_amg* h, const double* b, double* x, vo
   a.project = 0;
   a.info = nullptr;
   pcg_layout(h, (double*)work, a);
-  void* args[] = {&a};
-  int g = 0, rc;
-  if ((rc = coop_grid(vcycle_coop_k, &g)) != B2S_OK) return rc;
-  if (cudaLaunchCooperativeKernel((void*)vcycle_coop_k, g, kCoopThreads, args, 0, (cudaStream_t)s) != cudaSuccess)
-    return B2S_ERR_LAUNCH;
-  B2S_LAUNCH_CHECK();
-  return B2S_OK;
+  return launch_pcg_kernel(vcycle_coop_k, &a, &a.csize, &a.sub_nnz, s);
 }

@@ -358,6 +358,16 @@ B2S_API int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, 
  * rebuilds. project != 0 removes the mean from the residual and the preconditioned residual
  * (singular pure-Neumann systems). x starts at zero. */
 B2S_API int64_t b2s_pcg_workspace_bytes(const b2s_amg* h);
+/* Launch shape of the AMG-PCG and V-cycle kernels (b2s_pcg_amg_d, b2s_pcg_amg_mixed_d,
+ * b2s_amg_vcycle_d), for all later launches: cooperative launches made of thread-block clusters
+ * of cluster_blocks blocks (2, 4, 8 or 16; 0: no clusters, the default), and the size below
+ * which a level of the V-cycle runs on a subset of the grid instead of all of it: levels (and the
+ * coarse solve) of at most sub_entries matrix entries run on the first cluster with cluster
+ * barriers, or without clusters on block 0 with block barriers (defaults 32768 and 4096). Results
+ * agree up to round-off (how many lanes share a row depends on the phase's thread count).
+ * Returns B2S_OK or B2S_ERR_ARG. No counterpart in the reference (launch parameters of this
+ * implementation). */
+B2S_API int b2s_pcg_set_launch(int cluster_blocks, int sub_entries);
 B2S_API int b2s_pcg_amg_d(const b2s_amg* h, int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,
                           const double* b, double* x, double tol, int maxiter, int project, void* work,
                           int64_t work_bytes, b2s_solve_info* info, b2s_stream_t s);
