@@ -111,8 +111,8 @@ __device__ __forceinline__ void grid_totals(const double* part, int nb, int nq, 
 __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
 
 // Load of data that no thread writes while the kernel runs (matrix values, index arrays,
-// Jacobi inverses): through the read-only data path, whose lines stay cached on the SM across
-// the grid barriers of a cooperative kernel. Never for a vector the kernel writes.
+// Jacobi inverses) through the read-only data path. Used by the AMG-PCG, where it measured
+// faster on the 524k duct; never for a vector the kernel writes.
 template <class T>
 __device__ __forceinline__ T ldro(const T* p) {
   return __ldg(p);

@@ -57,7 +57,7 @@ template <int NR, class Entry, class Emit>
 __device__ __forceinline__ void walk_rows_nr(int n, int gt, int gs, const int32_t* __restrict__ rowptr, Entry entry,
                                              Emit emit) {
   for (int i = gt; i < n; i += gs) {
-    const int ja = ldro(rowptr + i), jae = ldro(rowptr + i + 1);
+    const int ja = rowptr[i], jae = rowptr[i + 1];
     double sa[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) sa[k] = 0.0;
@@ -142,15 +142,15 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
 #pragma unroll
     for (int q = 0; q < 3 * NR; ++q) acc[q] = 0.0;
     for (int i = gt; i < n; i += gs) {
-      const int j0 = ldro(a.rowptr + i), j1 = ldro(a.rowptr + i + 1);
-      const double iv = ldro(inv + i);
+      const int j0 = a.rowptr[i], j1 = a.rowptr[i + 1];
+      const double iv = inv[i];
       double ax[NR];
 #pragma unroll
       for (int k = 0; k < NR; ++k) ax[k] = 0.0;
       if (!a.zero_x0) {
         for (int j = j0; j < j1; ++j) {
-          const double av = ldro(a.val + j);
-          const int c = ldro(a.col + j);
+          const double av = a.val[j];
+          const int c = a.col[j];
 #pragma unroll
           for (int k = 0; k < NR; ++k) ax[k] += av * x[k][c];
         }
@@ -224,15 +224,15 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
         walk_rows_nr<NR>(
             n, gt, gs, a.rowptr,
             [&](int j, double (&sv)[NR]) {
-              const double aij = ldro(a.val + j);
-              const int c = ldro(a.col + j);
+              const double aij = a.val[j];
+              const int c = a.col[j];
 #pragma unroll
               for (int k = 0; k < NR; ++k)
                 if (st[k] == ACTIVE) sv[k] += aij * ((double)u[k][c] + beta[k] * w[k][c]);
             },
             [&](int i, const double (&av_)[NR]) {
               xupd(i);
-              const double iv = ldro(inv + i);
+              const double iv = inv[i];
 #pragma unroll
               for (int k = 0; k < NR; ++k)
                 if (st[k] == ACTIVE) {
@@ -274,8 +274,8 @@ __global__ void __launch_bounds__(kCoopThreads) bicgstab_coop_k(BicgArgsT<T> a) 
       walk_rows_nr<NR>(
           n, gt, gs, a.rowptr,
           [&](int j, double (&sv)[NR]) {
-            const double aij = ldro(a.val + j);
-            const int c = ldro(a.col + j);
+            const double aij = a.val[j];
+            const int c = a.col[j];
 #pragma unroll
             for (int k = 0; k < NR; ++k)
               if (st[k] == ACTIVE) sv[k] += aij * ((double)u[k][c] - alpha[k] * z[k][c]);
