@@ -704,6 +704,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--converge", action="store_true", help="c4: also run the batch to the 1e-6 residual")
+    ap.add_argument("--no-amg-setup", action="store_true",
+                    help="skip the AMG set-up block (device vs host set-up, re-aggregation policy)")
     ap.add_argument("--no-converge", action="store_true", help="skip the to-convergence runs (FP64 and mixed)")
     ap.add_argument("--no-c3", action="store_true", help="c2: skip the 524,288-cell duct block (FP64 vs mixed)")
     ap.add_argument("--batch-cases", type=int, default=256, help="c4: cases in the sweep")
@@ -896,6 +898,12 @@ def main():
         for v in converge.values():
             v.pop("fields", None)
 
+    # ---- the AMG set-up: device against host, and the reference's re-aggregation policy
+    amg_setup = None
+    if not args.no_amg_setup and args.config in ("c1", "c2", "c3"):
+        barrier()
+        amg_setup = amg_setup_block(mesh, case, inlet, skw, steps=100 if args.config != "c3" else 30)
+
     # ---- the metric's "vs plain FP64 GPU path" half on the 524,288-cell duct
     c3 = None
     if args.config == "c2" and not args.no_c3:
@@ -923,8 +931,74 @@ def main():
             "l2": "flushed between timed steps (512 MiB write)",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-            "linear_iterations_last": infos[K - 1], "cuda_graphs": graphs, "to_convergence": converge, "c3": c3}
+            "linear_iterations_last": infos[K - 1], "cuda_graphs": graphs, "to_convergence": converge, "c3": c3,
+            "amg_setup": amg_setup}
     print(json.dumps(line), flush=True)
+
+
+def amg_setup_block(mesh, case, inlet, skw, steps):
+    """The hierarchy's set-up from the pressure-correction matrix of the third iteration: on the
+    device (``AMGHierarchy.on_device``, median of 3) and on the host (SciPy + the C++ greedy,
+    then the device rebuild), whether both give the same aggregates; then fresh solvers timed
+    over ``steps`` iterations after 12, with the first set-up's aggregates kept (the default) and
+    with the reference's policy (``reaggregate``: a device set-up from the first level whose
+    strength graph changed, at every rebuild where one did)."""
+    import statistics
+
+    import torch
+
+    from gputest_b200.linalg.amg import AMGHierarchy
+    from gputest_b200.unstructured.simple import SimpleSolver
+
+    c = __import__("copy").deepcopy(case)
+    c.tol = 0.0
+    s = SimpleSolver(mesh, c, **skw)
+    if inlet:
+        inlet(s)
+    for _ in range(3):
+        s.step()
+    fv = s.fv
+    perm = torch.as_tensor(fv.perm, device="cuda")
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t0
+
+    dev_s, hd = [], None
+    for _ in range(3):
+        hd, dt = timed(lambda: AMGHierarchy.on_device(perm, fv.rowptr, fv.col, fv.t["slot_diag"], s.val_P,
+                                                      singular=s.singular_p, max_coarse=s.max_coarse,
+                                                      theta=s.amg_theta))
+        dev_s.append(dt)
+
+    def host():
+        h = AMGHierarchy(fv.matrix_to_host(s.val_P), fv.perm, fv.rowptr, fv.col, fv.t["slot_diag"], s.val_P,
+                         fv.slot_ref, singular=s.singular_p, max_coarse=s.max_coarse, theta=s.amg_theta)
+        h.rebuild()
+        return h
+
+    hh, host_s = timed(host)
+    same = hd.sizes == hh.sizes and all(torch.equal(hd._keep[2 * l]["agg"], hh._keep[2 * l]["agg"])
+                                        for l in range(hh.n_levels - 1))
+    sizes = list(hd.sizes)
+    del s, hd, hh
+    runs = {}
+    for name, reagg in (("fixed", False), ("reaggregate", True)):
+        s = SimpleSolver(mesh, c, **skw)
+        if inlet:
+            inlet(s)
+        s.reaggregate = reagg
+        for _ in range(12):
+            s.step()
+        n0 = s.amg_setups
+        _, dt = timed(lambda: s.run(max_steps=steps))
+        runs[name] = {"ms_per_step": dt / steps * 1e3, "setups": s.amg_setups - n0}
+        del s
+    return {"device_ms": statistics.median(dev_s) * 1e3, "host_ms": host_s * 1e3, "same_aggregates": bool(same),
+            "level_sizes": sizes, "steps": steps, **runs}
 
 
 def workload_config(desc):

@@ -454,57 +454,46 @@ int64_t b2s_amg_workspace_bytes(const b2s_amg* h) {
   return (int64_t)sizeof(double) * (2 * nmax + 4 * (int64_t)kMaxCoopBlocks + dense);
 }
 
-int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s) {
-  if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || h->coarse_n < 1 ||
-      (h->ngroups == 0 && h->coarse_n > 1024) || !work || !h->coarse_inv || !h->coarse_rowptr || !h->coarse_col ||
-      !h->coarse_val || (h->ngroups > 0 && (!h->coarse_group_ptr || !h->coarse_inv_off || !h->group_singular)))
+}  // extern "C"
+
+namespace {
+// Numeric rebuild of one level from its matrix values: D^-1, rho, P, R, W = A P and the next
+// level's values A_c = R W on the pattern (crow, ccol).
+int rebuild_level(const b2s_amg_level& L, int ngroups, const int32_t* next_group_ptr, const int32_t* crow,
+                  const int32_t* ccol, double* cval, double* xa, double* xb, double* part0, double* part1, int g,
+                  cudaStream_t st) {
+  if (!L.diag_slot || !L.agg || !L.tval || !L.x0 || !L.p_col || !L.p_val || !L.r_col || !L.r_from_p || !L.r_val ||
+      !L.w_rowptr || !L.w_col || !L.w_val || !L.rho || !crow || !ccol || !cval)
     return B2S_ERR_ARG;
-  if (work_bytes < b2s_amg_workspace_bytes(h)) return B2S_ERR_WORKSPACE;
-  cudaStream_t st = (cudaStream_t)s;
-  int64_t nmax = 0;
-  for (int l = 0; l < h->nlevels; ++l) nmax = h->levels[l].n > nmax ? h->levels[l].n : nmax;
-  double* xa = (double*)work;
-  double* xb = xa + nmax;
-  double* part0 = xb + nmax;
-  double* part1 = part0 + 2 * (int64_t)kMaxCoopBlocks;
-  double* dense = part1 + 2 * (int64_t)kMaxCoopBlocks;
-  int g = 0, rc;
-  if ((rc = power_grid(&g)) != B2S_OK) return rc;
-  for (int l = 0; l < h->nlevels; ++l) {
-    b2s_amg_level L = h->levels[l];
-    if (!L.diag_slot || !L.agg || !L.tval || !L.x0 || !L.p_col || !L.p_val || !L.r_col || !L.r_from_p ||
-        !L.r_val || !L.w_rowptr || !L.w_col || !L.w_val || !L.rho)
-      return B2S_ERR_ARG;
-    dinv_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
-    B2S_LAUNCH_CHECK();
-    if (h->ngroups > 0) {
-      if (!L.group_ptr) return B2S_ERR_ARG;
-      const int32_t* next = (l + 1 < h->nlevels) ? h->levels[l + 1].group_ptr : h->coarse_group_ptr;
-      power_groups_k<<<(unsigned)h->ngroups, kCoopThreads, 0, st>>>(L, next, xa, xb);
-    } else if (L.n <= kPowerBlockRows) {
-      power_block_k<<<1, kCoopThreads, 0, st>>>(L, xa, xb);
-    } else {
-      void* args[] = {&L, &xa, &xb, &part0, &part1};  // xa, xb: the two power-iteration buffers
-      if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
-        return B2S_ERR_LAUNCH;
-    }
-    const bool terms = L.p_tptr && L.p_tj && L.w_tptr && L.w_tj && L.w_te;
-    if (terms) pvals_terms_k<<<grid_for(L.n), kThreads, 0, st>>>(L, h->ngroups);
-    else pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L, h->ngroups);
-    rvals_k<<<grid_for(L.p_nnz), kThreads, 0, st>>>(L);
-    if (terms) wvals_terms_k<<<grid_for(L.w_nnz), kThreads, 0, st>>>(L);
-    else wvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
-    B2S_LAUNCH_CHECK();
-    const bool last = l + 1 == h->nlevels;
-    const int32_t* crow = last ? h->coarse_rowptr : h->levels[l + 1].rowptr;
-    const int32_t* ccol = last ? h->coarse_col : h->levels[l + 1].col;
-    double* cval = last ? h->coarse_val : h->levels[l + 1].val;
-    if (terms && L.c_tptr && L.c_te && L.c_ts && L.c_nnz > 0)
-      acvals_terms_k<<<grid_for(L.c_nnz), kThreads, 0, st>>>(L, cval);
-    else
-      acvals_k<<<(unsigned)cdiv(L.nc, kGalWarps), kGalWarps * 32, 0, st>>>(L, crow, ccol, cval);
-    B2S_LAUNCH_CHECK();
+  dinv_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+  B2S_LAUNCH_CHECK();
+  if (ngroups > 0) {
+    if (!L.group_ptr || !next_group_ptr) return B2S_ERR_ARG;
+    power_groups_k<<<(unsigned)ngroups, kCoopThreads, 0, st>>>(L, next_group_ptr, xa, xb);
+  } else if (L.n <= kPowerBlockRows) {
+    power_block_k<<<1, kCoopThreads, 0, st>>>(L, xa, xb);
+  } else {
+    b2s_amg_level Lc = L;
+    void* args[] = {&Lc, &xa, &xb, &part0, &part1};  // xa, xb: the two power-iteration buffers
+    if (cudaLaunchCooperativeKernel((void*)power_coop_k, g, kCoopThreads, args, 0, st) != cudaSuccess)
+      return B2S_ERR_LAUNCH;
   }
+  const bool terms = L.p_tptr && L.p_tj && L.w_tptr && L.w_tj && L.w_te;
+  if (terms) pvals_terms_k<<<grid_for(L.n), kThreads, 0, st>>>(L, ngroups);
+  else pvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L, ngroups);
+  rvals_k<<<grid_for(L.p_nnz), kThreads, 0, st>>>(L);
+  if (terms) wvals_terms_k<<<grid_for(L.w_nnz), kThreads, 0, st>>>(L);
+  else wvals_k<<<grid_for(L.n), kThreads, 0, st>>>(L);
+  B2S_LAUNCH_CHECK();
+  if (terms && L.c_tptr && L.c_te && L.c_ts && L.c_nnz > 0)
+    acvals_terms_k<<<grid_for(L.c_nnz), kThreads, 0, st>>>(L, cval);
+  else
+    acvals_k<<<(unsigned)cdiv(L.nc, kGalWarps), kGalWarps * 32, 0, st>>>(L, crow, ccol, cval);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int coarse_inverse(const b2s_amg* h, double* dense, cudaStream_t st) {
   if (h->ngroups > 0) {  // one dense block per case, each at most kSmemCoarse rows (checked at set-up)
     const size_t gsm = (size_t)kSmemCoarse * kSmemCoarse * sizeof(double);
     if (cudaFuncSetAttribute(coarse_inverse_groups_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm) !=
@@ -528,6 +517,68 @@ int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stre
   return B2S_OK;
 }
 
+bool hierarchy_ok(const b2s_amg* h) {
+  return h && h->nlevels >= 0 && h->nlevels <= B2S_AMG_MAX_LEVELS && h->coarse_n >= 1 &&
+         !(h->ngroups == 0 && h->coarse_n > 1024) && h->coarse_inv && h->coarse_rowptr && h->coarse_col &&
+         h->coarse_val && !(h->ngroups > 0 && (!h->coarse_group_ptr || !h->coarse_inv_off || !h->group_singular));
+}
+}  // namespace
+
+extern "C" {
+
+int b2s_amg_rebuild_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s) {
+  if (!hierarchy_ok(h) || !work) return B2S_ERR_ARG;
+  if (work_bytes < b2s_amg_workspace_bytes(h)) return B2S_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)s;
+  int64_t nmax = 0;
+  for (int l = 0; l < h->nlevels; ++l) nmax = h->levels[l].n > nmax ? h->levels[l].n : nmax;
+  double* xa = (double*)work;
+  double* xb = xa + nmax;
+  double* part0 = xb + nmax;
+  double* part1 = part0 + 2 * (int64_t)kMaxCoopBlocks;
+  double* dense = part1 + 2 * (int64_t)kMaxCoopBlocks;
+  int g = 0, rc;
+  if ((rc = power_grid(&g)) != B2S_OK) return rc;
+  for (int l = 0; l < h->nlevels; ++l) {
+    const bool last = l + 1 == h->nlevels;
+    const int32_t* next_gp = last ? h->coarse_group_ptr : h->levels[l + 1].group_ptr;
+    const int32_t* crow = last ? h->coarse_rowptr : h->levels[l + 1].rowptr;
+    const int32_t* ccol = last ? h->coarse_col : h->levels[l + 1].col;
+    double* cval = last ? h->coarse_val : h->levels[l + 1].val;
+    if ((rc = rebuild_level(h->levels[l], h->ngroups, next_gp, crow, ccol, cval, xa, xb, part0, part1, g, st)) !=
+        B2S_OK)
+      return rc;
+  }
+  return coarse_inverse(h, dense, st);
+}
+
+int64_t b2s_amg_level_workspace_bytes(const b2s_amg_level* L) {
+  if (!L || L->n < 1) return -1;
+  return (int64_t)sizeof(double) * (2 * (int64_t)L->n + 4 * (int64_t)kMaxCoopBlocks);
+}
+
+int b2s_amg_level_rebuild_d(const b2s_amg_level* L, const int32_t* crow, const int32_t* ccol, double* cval,
+                            void* work, int64_t work_bytes, b2s_stream_t s) {
+  if (!L || L->n < 1 || !work) return B2S_ERR_ARG;
+  if (work_bytes < b2s_amg_level_workspace_bytes(L)) return B2S_ERR_WORKSPACE;
+  double* xa = (double*)work;
+  double* xb = xa + L->n;
+  double* part0 = xb + L->n;
+  double* part1 = part0 + 2 * (int64_t)kMaxCoopBlocks;
+  int g = 0, rc;
+  if ((rc = power_grid(&g)) != B2S_OK) return rc;
+  return rebuild_level(*L, 0, nullptr, crow, ccol, cval, xa, xb, part0, part1, g, (cudaStream_t)s);
+}
+
+int b2s_amg_coarse_inverse_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s) {
+  if (!hierarchy_ok(h) || !work) return B2S_ERR_ARG;
+  if (work_bytes < b2s_amg_workspace_bytes(h)) return B2S_ERR_WORKSPACE;
+  int64_t nmax = 0;
+  for (int l = 0; l < h->nlevels; ++l) nmax = h->levels[l].n > nmax ? h->levels[l].n : nmax;
+  double* dense = (double*)work + 2 * nmax + 4 * (int64_t)kMaxCoopBlocks;
+  return coarse_inverse(h, dense, (cudaStream_t)s);
+}
+
 int b2s_amg_strength_changes_d(const b2s_amg* h, double theta, int32_t* count, b2s_stream_t s) {
   if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || !count) return B2S_ERR_ARG;
   cudaStream_t st = (cudaStream_t)s;
@@ -536,6 +587,20 @@ int b2s_amg_strength_changes_d(const b2s_amg* h, double theta, int32_t* count, b
     const b2s_amg_level& L = h->levels[l];
     if (!L.strong || !L.diag_slot) return B2S_ERR_ARG;
     strength_changes_k<<<grid_for(L.n), kThreads, 0, st>>>(L, theta, count);
+    B2S_LAUNCH_CHECK();
+  }
+  return B2S_OK;
+}
+
+int b2s_amg_level_strength_changes_d(const b2s_amg* h, double theta, int32_t* counts, b2s_stream_t s) {
+  if (!h || h->nlevels < 0 || h->nlevels > B2S_AMG_MAX_LEVELS || (h->nlevels > 0 && !counts)) return B2S_ERR_ARG;
+  if (h->nlevels == 0) return B2S_OK;
+  cudaStream_t st = (cudaStream_t)s;
+  if (cudaMemsetAsync(counts, 0, sizeof(int32_t) * h->nlevels, st) != cudaSuccess) return B2S_ERR_LAUNCH;
+  for (int l = 0; l < h->nlevels; ++l) {
+    const b2s_amg_level& L = h->levels[l];
+    if (!L.strong || !L.diag_slot) return B2S_ERR_ARG;
+    strength_changes_k<<<grid_for(L.n), kThreads, 0, st>>>(L, theta, counts + l);
     B2S_LAUNCH_CHECK();
   }
   return B2S_OK;

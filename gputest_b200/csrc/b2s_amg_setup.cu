@@ -1,0 +1,431 @@
+// Device set-up of the SA-AMG hierarchy: strength of connection, transposed entry slots and the
+// greedy three-pass aggregation of flowtrace/linalg/amg.py:25-57, reproduced exactly.
+//
+// The reference's aggregation visits the nodes one after another in index order (the "priority"
+// here: the reference numbering on level 0, the aggregate numbering below):
+//   pass 1: a node becomes a root when it and all its strong neighbours S(i) are still free; the
+//           root takes S(i) into its aggregate;
+//   pass 2: a node left free joins the aggregate of its first strong neighbour (column order)
+//           that already has one;
+//   pass 3: nodes still free become aggregates of their own.
+// Pass 1 is a lexicographically-first independent set: at its turn a node i is free with a
+// free neighbourhood exactly when no earlier root r is in conflict with it, where r conflicts
+// with i when i is in S(r), r is in S(i), or S(i) and S(r) share a node. So i is a root iff
+// every conflicting node of lower priority is decided "not a root". The kernel below decides
+// every node as soon as that holds, by dataflow: thread t owns the nodes of priority t, t + T,
+// ... (T threads, all resident through a cooperative launch), visits them in increasing
+// priority, and polls the decisions of the node's lower-priority conflicts until it can
+// decide. The undecided node of lowest priority can always decide, and its owner is working
+// on it, so the kernel finishes in as many dependent steps as the longest chain of decisions;
+// every poll loop is bounded and a run that exhausts it reports an error instead of waiting.
+// Roots are numbered in priority order (a scan), exactly as the reference's counter; every
+// other node finds its root (at most one root has it in its S), and pass 2's choice - the
+// lowest-priority strong neighbour that is aggregated at that point, i.e. aggregated in pass 1
+// or left over with a lower priority - is resolved by following those links down in priority.
+#include "b2s_common.cuh"
+
+namespace b2s {
+
+constexpr int32_t kUndecided = 0, kRoot = 1, kNotRoot = 2;
+constexpr int kScanTile = 1024;
+
+__device__ __forceinline__ int32_t ld_relaxed(const int32_t* p) {
+  int32_t v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(int32_t* p, int32_t v) {
+  asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// strong[e] = 1 where |a_e| >= theta sqrt(|a_ii a_jj|), j = col[e] != i (amg.py:60-66, the same
+// operations in the same order).
+__global__ void strength_k(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                           const double* __restrict__ val, const int32_t* __restrict__ diag_slot, double theta,
+                           uint8_t* __restrict__ strong) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double di = fabs(val[diag_slot[i]]);
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+      const int c = col[e];
+      uint8_t s = 0;
+      if (c != i) s = fabs(val[e]) >= theta * sqrt(di * fabs(val[diag_slot[c]])) ? 1 : 0;
+      strong[e] = s;
+    }
+  }
+}
+
+// tslot[e] = the slot of (col[e], i) for every entry e = (i, col[e]) of a structurally symmetric
+// pattern; a missing transpose is counted in *missing and its slot set to e itself.
+__global__ void transpose_slots_k(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                  int sorted, int32_t* __restrict__ tslot, int32_t* __restrict__ missing) {
+  int bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+      const int c = col[e];
+      int lo = rowptr[c], hi = rowptr[c + 1], found = -1;
+      if (c == i) {
+        found = e;
+      } else if (sorted) {
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (col[mid] < i) lo = mid + 1;
+          else hi = mid;
+        }
+        if (lo < rowptr[c + 1] && col[lo] == i) found = lo;
+      } else {
+        for (int q = lo; q < hi; ++q)
+          if (col[q] == i) {
+            found = q;
+            break;
+          }
+      }
+      if (found < 0) {
+        ++bad;
+        found = e;
+      }
+      tslot[e] = found;
+    }
+  }
+  if (bad) atomicAdd(missing, bad);
+}
+
+struct AggGraph {
+  int n;
+  const int32_t* rowptr;
+  const int32_t* col;
+  const uint8_t* strong;  // strong[e]: col[e] in S(row)
+  const int32_t* tslot;   // strong[tslot[e]]: row in S(col[e])
+  const int32_t* prio;    // [n] priority (visiting order) of every node
+  const int32_t* rank_node;  // [n] node of every priority
+};
+
+// The lower-priority conflicts of node i, in a fixed order: j in row i with i in S(j) or j in
+// S(i); then, for every j in S(i), the nodes r with j in S(r) (they would have taken j). A node
+// may appear more than once. count only (out == nullptr) or write them to out.
+__device__ int node_conflicts(const AggGraph& g, int i, int32_t* out) {
+  const int p = g.prio[i];
+  int c = 0;
+  for (int e = g.rowptr[i]; e < g.rowptr[i + 1]; ++e) {
+    const int j = g.col[e];
+    if (j == i) continue;
+    const bool sij = g.strong[e] != 0;
+    if ((sij || g.strong[g.tslot[e]] != 0) && g.prio[j] < p) {
+      if (out) out[c] = j;
+      ++c;
+    }
+    if (!sij) continue;
+    for (int e2 = g.rowptr[j]; e2 < g.rowptr[j + 1]; ++e2) {
+      const int r = g.col[e2];
+      if (r == i || r == j || g.strong[g.tslot[e2]] == 0 || g.prio[r] >= p) continue;
+      if (out) out[c] = r;
+      ++c;
+    }
+  }
+  return c;
+}
+
+__global__ void conflict_counts_k(AggGraph g, int32_t* cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x)
+    cnt[i] = node_conflicts(g, i, nullptr);
+}
+
+// Writes the lists at their scanned offsets when they fit the capacity (else error 3).
+__global__ void conflict_lists_k(AggGraph g, const int32_t* __restrict__ off, const int32_t* __restrict__ total,
+                                 int64_t capacity, int32_t* lists, int32_t* err) {
+  if ((int64_t)*total > capacity) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(err, 3);
+    return;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x)
+    node_conflicts(g, i, lists + off[i]);
+}
+
+// Decides node i (pass 1) from its conflict list [k0, k1): kNotRoot as soon as one of them is a
+// root, kRoot once all are decided "not a root"; -1 when the poll budget ran out or another
+// thread reported an error. A poll reads the list from the first entry found undecided on (the
+// ones before it are decided "not a root" and stay so); the list is read-only (cached), the
+// decisions are relaxed loads at device scope, issued together.
+__device__ int decide_node(const int32_t* __restrict__ lists, int k0, int k1, const int32_t* status, int64_t limit,
+                           int64_t& polls, const int32_t* err) {
+  for (;;) {
+    int first = -1;
+    for (int k = k0; k < k1; ++k) {
+      const int32_t s = ld_relaxed(status + __ldg(lists + k));
+      if (s == kRoot) return kNotRoot;
+      if (s == kUndecided && first < 0) first = k;
+    }
+    if (first < 0) return kRoot;
+    if (++polls > limit) return -1;
+    if ((polls & 63) == 0 && ld_relaxed(err) != 0) return -1;
+    k0 = first;
+    __nanosleep(64);
+  }
+}
+
+__global__ void __launch_bounds__(kCoopThreads) aggregate_roots_k(AggGraph g, const int32_t* lists,
+                                                                  const int32_t* off, int32_t* status, int64_t limit,
+                                                                  int32_t* err) {
+  if (ld_relaxed(err) != 0) return;
+  const int T = gridDim.x * blockDim.x;
+  int64_t polls = 0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += T) {
+    const int i = g.rank_node[p];
+    const int d = decide_node(lists, off[i], off[i + 1], status, limit, polls, err);
+    if (d < 0) {
+      atomicExch(err, 1);
+      return;
+    }
+    st_relaxed(status + i, d);
+  }
+}
+
+// ------------------------------------------------------------------ exclusive scan of int32 flags
+// Three launches: tile sums, a one-block scan of the tile sums, the scan of every tile.
+__device__ __forceinline__ int block_excl_scan(int v, int* sm, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < nw ? sm[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) sm[lane] = w;
+  }
+  __syncthreads();
+  const int before = (warp > 0 ? sm[warp - 1] : 0) + x - v;
+  if (total) *total = sm[nw - 1];
+  __syncthreads();
+  return before;
+}
+
+__global__ void __launch_bounds__(kScanTile) tile_sums_k(int n, const int32_t* __restrict__ flag, int32_t* tsum) {
+  __shared__ int sm[32];
+  const int i = blockIdx.x * kScanTile + threadIdx.x;
+  int tot = 0;
+  block_excl_scan(i < n ? flag[i] : 0, sm, &tot);
+  if (threadIdx.x == 0) tsum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanTile) tile_offsets_k(int ntiles, int32_t* tsum, int32_t* total) {
+  __shared__ int sm[32];
+  int carry = 0;
+  for (int b = 0; b < ntiles; b += kScanTile) {
+    const int i = b + threadIdx.x;
+    const int v = i < ntiles ? tsum[i] : 0;
+    int tot = 0;
+    const int ex = block_excl_scan(v, sm, &tot);
+    if (i < ntiles) tsum[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kScanTile) tile_scan_k(int n, const int32_t* __restrict__ flag,
+                                                         const int32_t* __restrict__ toff, int32_t* out) {
+  __shared__ int sm[32];
+  const int i = blockIdx.x * kScanTile + threadIdx.x;
+  const int ex = block_excl_scan(i < n ? flag[i] : 0, sm, nullptr);
+  if (i < n) out[i] = toff[blockIdx.x] + ex;
+}
+
+// ------------------------------------------------------------------ numbering and passes 2 and 3
+// flag[p] = 1 where the node of priority p is a root
+__global__ void root_flags_k(AggGraph g, const int32_t* __restrict__ status, int32_t* flag) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x)
+    flag[p] = status[g.rank_node[p]] == kRoot ? 1 : 0;
+}
+
+// Pass 1's aggregates: a root's number is its rank among the roots (rid, by priority); any other
+// node takes the number of the root r with the node in S(r), if there is one; else -1.
+__global__ void assign_pass1_k(AggGraph g, const int32_t* __restrict__ status, const int32_t* __restrict__ rid,
+                               int32_t* agg) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    int a = -1;
+    if (status[i] == kRoot) {
+      a = rid[g.prio[i]];
+    } else {
+      for (int e = g.rowptr[i]; e < g.rowptr[i + 1]; ++e) {
+        const int r = g.col[e];
+        if (r != i && g.strong[g.tslot[e]] && status[r] == kRoot) {
+          a = rid[g.prio[r]];
+          break;
+        }
+      }
+    }
+    agg[i] = a;
+  }
+}
+
+// Pass 2 links: a node left over joins its lowest-priority strong neighbour that is aggregated
+// when its turn comes - aggregated in pass 1, or left over with a lower priority (joined before
+// it). link[i] = that neighbour, -1 when none (pass 3), i itself for nodes of pass 1.
+__global__ void pass2_links_k(AggGraph g, const int32_t* __restrict__ agg1, int32_t* link) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    if (agg1[i] >= 0) {
+      link[i] = i;
+      continue;
+    }
+    const int pi = g.prio[i];
+    int best = -1, bp = 0x7fffffff;
+    for (int e = g.rowptr[i]; e < g.rowptr[i + 1]; ++e) {
+      const int j = g.col[e];
+      if (j == i || !g.strong[e]) continue;
+      const int pj = g.prio[j];
+      if ((agg1[j] >= 0 || pj < pi) && pj < bp) best = j, bp = pj;
+    }
+    link[i] = best;
+  }
+}
+
+// Resolves the links (each step strictly lower in priority, so every chain ends at a node of
+// pass 1 or at one without a link); flag[p] = 1 for the nodes of pass 3.
+__global__ void pass2_resolve_k(AggGraph g, const int32_t* __restrict__ agg1, const int32_t* __restrict__ link,
+                                int32_t* agg, int32_t* flag, int32_t* err) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    int x = i, a = agg1[i];
+    for (int step = 0; a < 0 && step <= g.n; ++step) {
+      const int j = link[x];
+      if (j < 0) break;
+      x = j;
+      a = agg1[x];
+    }
+    if (a < 0 && link[x] >= 0) atomicExch(err, 2);  // a chain longer than n: not possible
+    agg[i] = a;
+    flag[g.prio[i]] = a < 0 ? 1 : 0;
+  }
+}
+
+// Pass 3: the nodes still without an aggregate, numbered after the others in priority order.
+__global__ void pass3_k(AggGraph g, const int32_t* __restrict__ off, const int32_t* __restrict__ na1,
+                        int32_t* agg) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x)
+    if (agg[i] < 0) agg[i] = *na1 + off[g.prio[i]];
+}
+
+__global__ void aggregate_total_k(int32_t* info) { info[0] = info[2] + info[3]; }
+
+__global__ void aggregate_sizes_k(int n, const int32_t* __restrict__ agg, int32_t* cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) atomicAdd(cnt + agg[i], 1);
+}
+
+}  // namespace b2s
+
+using namespace b2s;
+
+namespace {
+int coop_grid(const void* kernel, int threads, int* grid) {
+  int dev = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return B2S_ERR_DEVICE;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return B2S_ERR_DEVICE;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess || per <= 0)
+    return B2S_ERR_DEVICE;
+  *grid = sms * per;
+  return B2S_OK;
+}
+
+int scan_flags(int n, const int32_t* flag, int32_t* out, int32_t* tsum, int32_t* total, cudaStream_t st) {
+  const int tiles = (int)cdiv(n, kScanTile);
+  tile_sums_k<<<tiles, kScanTile, 0, st>>>(n, flag, tsum);
+  tile_offsets_k<<<1, kScanTile, 0, st>>>(tiles, tsum, total);
+  tile_scan_k<<<tiles, kScanTile, 0, st>>>(n, flag, tsum, out);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int b2s_amg_strength_d(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,
+                       const int32_t* diag_slot, double theta, uint8_t* strong, b2s_stream_t s) {
+  if (n < 0 || (n > 0 && (!rowptr || !col || !val || !diag_slot || !strong))) return B2S_ERR_ARG;
+  if (n == 0) return B2S_OK;
+  strength_k<<<grid_for(n), kThreads, 0, (cudaStream_t)s>>>(n, rowptr, col, val, diag_slot, theta, strong);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_csr_transpose_slots_d(int32_t n, const int32_t* rowptr, const int32_t* col, int32_t sorted, int32_t* tslot,
+                              int32_t* missing, b2s_stream_t s) {
+  if (n < 0 || !missing || (n > 0 && (!rowptr || !col || !tslot))) return B2S_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  if (cudaMemsetAsync(missing, 0, sizeof(int32_t), st) != cudaSuccess) return B2S_ERR_LAUNCH;
+  if (n == 0) return B2S_OK;
+  transpose_slots_k<<<grid_for(n), kThreads, 0, st>>>(n, rowptr, col, sorted != 0, tslot, missing);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int64_t b2s_amg_aggregate_workspace_bytes(int32_t n, int64_t capacity) {
+  if (n < 0 || capacity < 0) return -1;
+  const int64_t tiles = cdiv(n > 0 ? n : 1, kScanTile);
+  return (int64_t)sizeof(int32_t) * (5 * (int64_t)n + tiles + 9 + capacity);
+}
+
+int b2s_amg_aggregate_d(int32_t n, const int32_t* rowptr, const int32_t* col, const uint8_t* strong,
+                        const int32_t* tslot, const int32_t* prio, const int32_t* rank_node, int32_t* agg,
+                        int32_t* counts, int32_t* info, void* work, int64_t work_bytes, b2s_stream_t s) {
+  if (n < 1 || !rowptr || !col || !strong || !tslot || !prio || !rank_node || !agg || !counts || !info || !work)
+    return B2S_ERR_ARG;
+  const int64_t tiles = cdiv(n, kScanTile);
+  const int64_t fixed = (int64_t)sizeof(int32_t) * (5 * (int64_t)n + tiles + 9);
+  if (work_bytes < fixed) return B2S_ERR_WORKSPACE;
+  int64_t capacity = (work_bytes - fixed) / (int64_t)sizeof(int32_t);
+  cudaStream_t st = (cudaStream_t)s;
+  int32_t* status = (int32_t*)work;
+  int32_t* flag = status + n;
+  int32_t* ids = flag + n;
+  int32_t* link = ids + n;
+  int32_t* off = link + n;  // [n + 1] offsets of the conflict lists
+  int32_t* tsum = off + n + 1;
+  int32_t* lists = tsum + tiles + 8;
+  // info: [0] aggregates, [1] error (1: poll budget exhausted, 2: broken link chain, 3: conflict
+  //       lists above the work space's capacity), [2] aggregates of passes 1-2, [3] nodes of pass 3
+  if (cudaMemsetAsync(info, 0, 4 * sizeof(int32_t), st) != cudaSuccess) return B2S_ERR_LAUNCH;
+  if (cudaMemsetAsync(status, 0, (size_t)n * sizeof(int32_t), st) != cudaSuccess) return B2S_ERR_LAUNCH;
+  AggGraph g{n, rowptr, col, strong, tslot, prio, rank_node};
+  int32_t* err = info + 1;
+  int rc;
+  const unsigned gn = grid_for(n);
+  conflict_counts_k<<<gn, kThreads, 0, st>>>(g, flag);
+  B2S_LAUNCH_CHECK();
+  if ((rc = scan_flags(n, flag, off, tsum, off + n, st)) != B2S_OK) return rc;
+  conflict_lists_k<<<gn, kThreads, 0, st>>>(g, off, off + n, capacity, lists, err);
+  B2S_LAUNCH_CHECK();
+  int grid = 0;
+  if ((rc = coop_grid((const void*)aggregate_roots_k, kCoopThreads, &grid)) != B2S_OK) return rc;
+  int64_t limit = 1 << 22;  // polls of one thread, ~0.3 s of waiting: far above any chain
+  const int32_t* lists_c = lists;
+  const int32_t* off_c = off;
+  void* args[] = {&g, &lists_c, &off_c, &status, &limit, &err};
+  if (cudaLaunchCooperativeKernel((const void*)aggregate_roots_k, grid, kCoopThreads, args, 0, st) != cudaSuccess)
+    return B2S_ERR_LAUNCH;
+  root_flags_k<<<gn, kThreads, 0, st>>>(g, status, flag);
+  B2S_LAUNCH_CHECK();
+  if ((rc = scan_flags(n, flag, ids, tsum, info + 2, st)) != B2S_OK) return rc;
+  assign_pass1_k<<<gn, kThreads, 0, st>>>(g, status, ids, agg);
+  pass2_links_k<<<gn, kThreads, 0, st>>>(g, agg, link);
+  // agg holds pass 1's numbers; resolve into status (free now), then number pass 3 into agg
+  pass2_resolve_k<<<gn, kThreads, 0, st>>>(g, agg, link, status, flag, err);
+  B2S_LAUNCH_CHECK();
+  if ((rc = scan_flags(n, flag, ids, tsum, info + 3, st)) != B2S_OK) return rc;
+  if (cudaMemcpyAsync(agg, status, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return B2S_ERR_LAUNCH;
+  pass3_k<<<gn, kThreads, 0, st>>>(g, ids, info + 2, agg);
+  aggregate_total_k<<<1, 1, 0, st>>>(info);
+  B2S_LAUNCH_CHECK();
+  if (cudaMemsetAsync(counts, 0, (size_t)n * sizeof(int32_t), st) != cudaSuccess) return B2S_ERR_LAUNCH;
+  aggregate_sizes_k<<<gn, kThreads, 0, st>>>(n, agg, counts);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+}  // extern "C"

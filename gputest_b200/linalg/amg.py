@@ -1,20 +1,24 @@
 """Smoothed-aggregation AMG hierarchy for the pressure-correction solve on B200.
 
-Set-up follows ``flowtrace/linalg/amg.py:80-117`` once, on the host, on the first matrix it
-is given: strength of connection (theta = 0.08), greedy three-pass aggregation (the C++ helper
-``b2s_host_aggregate``), and the resulting sparsity patterns of P = (I - w D^-1 A) T,
-W = A P and A_c = P^T W, level by level. From then on the aggregates and patterns are fixed
-and every numeric quantity is rebuilt on the device by ``rebuild()`` (``b2s_amg_rebuild_d``):
-D^-1, the spectral radius by 15 power iterations from the reference's start vector
-(``default_rng(0)``, ``amg.py:69-77``), P, R = P^T, the Galerkin products and the inverse of
-the coarsest matrix. The V-cycle (2+2 damped-Jacobi sweeps, w = 0.8) runs inside the PCG
-kernel.
+The set-up is the reference's (``flowtrace/linalg/amg.py:80-117``): strength of connection,
+the greedy three-pass aggregation, P = (I - 4/(3 rho) D^-1 A) T, W = A P and A_c = P^T W,
+level by level. ``AMGHierarchy.on_device`` does it on the device: strength flags and the
+aggregation in CUDA (``b2s_amg_strength_d``, ``b2s_amg_aggregate_d``, which reproduces the
+sequential greedy exactly), the patterns and term lists of the products from sorted distinct
+keys (``product_patterns``), and each level's numeric rebuild, whose Galerkin product gives the
+next level's values. ``AMGHierarchy(...)`` is the same set-up on the host (SciPy, the C++ helper
+``b2s_host_aggregate``); batches of independent cases use it. Afterwards every numeric quantity
+is rebuilt on the device by ``rebuild()`` (``b2s_amg_rebuild_d``): D^-1, the spectral radius by
+15 power iterations from the reference's start vector (``default_rng(0)``, ``amg.py:69-77``),
+P, R = P^T, the Galerkin products and the inverse of the coarsest matrix. The V-cycle (2+2
+damped-Jacobi sweeps, w = 0.8) runs inside the PCG kernel.
 
-Difference from the reference, by design: the reference re-aggregates at every rebuild. Here
-the aggregates of the first build are kept; the strength graph they come from is recomputed
-by ``strength_changed()`` so a caller can detect when it would differ. ``max_coarse``
-defaults to 150 (the reference's 300) so that the coarsest matrix is inverted in one block's
-shared memory; 300 reproduces the reference's hierarchy exactly.
+The reference re-aggregates at every rebuild. Callers choose: keep the first set-up's
+aggregates (the solvers' default), or re-aggregate when ``first_strength_change()`` reports a
+level whose strength graph changed, resuming the device set-up at that level
+(``on_device(prev=..., start=...)``) - the reference's hierarchy at every rebuild.
+``max_coarse`` defaults to 150 (the reference's 300) so that the coarsest matrix is inverted in
+one block's shared memory; 300 reproduces the reference's hierarchy exactly.
 """
 
 from __future__ import annotations
@@ -148,6 +152,166 @@ def term_lists(rp, cl, agg, na, Pp, Wp, Cp, r_col, r_rowptr, cap=TERM_CAP, devic
     ptr, order = _slot_lists(sc, Cp.nnz)
     out["c_tptr"], out["c_te"], out["c_ts"] = i32(ptr), i32(q[order]), i32(s_[order])
     return out
+
+
+def _sorted_ptr(sorted_rows, nrows):
+    """CSR offsets of nrows rows from the (ascending) row of every entry, without a host sync."""
+    import torch
+
+    return torch.searchsorted(sorted_rows, torch.arange(nrows + 1, device=sorted_rows.device))
+
+
+def _unique_pattern(keys, nrows, ncols):
+    """CSR pattern of the distinct row * ncols + col keys: (indptr, indices, sorted keys), int64."""
+    import torch
+
+    u = torch.unique(keys, sorted=True)
+    return _sorted_ptr(u // ncols, nrows), u % ncols, u
+
+
+def _grouped(slot, nslot):
+    """``_slot_lists`` without a host sync: stable grouping of terms by output slot."""
+    import torch
+
+    srt = torch.sort(slot, stable=True)
+    return _sorted_ptr(srt.values, nslot), srt.indices
+
+
+def _expand_sized(ptr, idx, total):
+    """``_expand`` with its output size known (no host sync)."""
+    import torch
+
+    lens = ptr[idx + 1] - ptr[idx]
+    src = torch.repeat_interleave(torch.arange(idx.numel(), device=idx.device), lens, output_size=total)
+    start = torch.repeat_interleave(ptr[idx] - (torch.cumsum(lens, 0) - lens), lens, output_size=total)
+    return src, start + torch.arange(total, device=idx.device)
+
+
+def _rows_of(ptr, nnz):
+    import torch
+
+    n = ptr.numel() - 1
+    return torch.repeat_interleave(torch.arange(n, device=ptr.device), ptr[1:] - ptr[:-1], output_size=nnz)
+
+
+def product_patterns(rp, cl, agg, na, cap=TERM_CAP):
+    """Patterns of P = A T, W = A P, A_c = P^T W and R = P^T for the aggregates ``agg`` (``na`` of
+    them) of the level whose CSR in stored order is (rp, cl) (int64 torch tensors on one device),
+    with the term lists of ``term_lists``, computed from sorted distinct keys instead of SciPy
+    products: every structure the device set-up needs, on the tensors' device (four host
+    synchronisations: the sizes of the products). Returns a dict of int64 tensors (patterns:
+    p_ptr/p_idx, w_ptr/w_idx, c_ptr/c_idx, r_rowptr/r_col/r_from_p) and int32 term lists (None
+    where a list would exceed ``cap`` terms)."""
+    import torch
+
+    dev = rp.device
+    n, nnz = rp.numel() - 1, cl.numel()
+    rows = _rows_of(rp, nnz)
+    i32 = lambda t: t.to(torch.int32).contiguous()  # noqa: E731
+    out = {}
+    # P: A entry j of row i -> (i, agg[col j])
+    kp = rows * na + agg[cl]
+    p_ptr, p_idx, p_keys = _unique_pattern(kp, n, na)
+    p_nnz = p_idx.numel()
+    out.update(p_ptr=p_ptr, p_idx=p_idx)
+    ptr, order = _grouped(torch.searchsorted(p_keys, kp), p_nnz)
+    out["p_tptr"], out["p_tj"] = i32(ptr), i32(order)
+    # W: (A entry j of row i, P entry e of row col j) -> (i, col e), generated j-major
+    lens = p_ptr[cl + 1] - p_ptr[cl]
+    w_terms = int(lens.sum())
+    jj, e = _expand_sized(p_ptr, cl, w_terms)
+    kw = rows[jj] * na + p_idx[e]
+    w_ptr, w_idx, w_keys = _unique_pattern(kw, n, na)
+    out.update(w_ptr=w_ptr, w_idx=w_idx)
+    if w_terms <= cap:
+        ptr, order = _grouped(torch.searchsorted(w_keys, kw), w_idx.numel())
+        out["w_tptr"], out["w_tj"], out["w_te"] = i32(ptr), i32(jj[order]), i32(e[order])
+    else:
+        out["w_tptr"] = out["w_tj"] = out["w_te"] = None
+    del jj, e, kw
+    # R = P^T: P entries by (column, row)
+    prow = _rows_of(p_ptr, p_nnz)
+    r_from_p = torch.argsort(p_idx * n + prow)
+    out.update(r_rowptr=_sorted_ptr(p_idx[r_from_p], na), r_col=prow[r_from_p], r_from_p=r_from_p)
+    # A_c: (R entry q of coarse row I, W entry s of row r_col[q]) -> (I, col s), generated q-major
+    qrow = _rows_of(out["r_rowptr"], p_nnz)
+    rc = out["r_col"]
+    c_terms = int((w_ptr[rc + 1] - w_ptr[rc]).sum())
+    q, s_ = _expand_sized(w_ptr, rc, c_terms)
+    kc = qrow[q] * na + w_idx[s_]
+    c_ptr, c_idx, c_keys = _unique_pattern(kc, na, na)
+    out.update(c_ptr=c_ptr, c_idx=c_idx, c_keys=c_keys)
+    if c_terms <= cap and out["w_tptr"] is not None:
+        ptr, order = _grouped(torch.searchsorted(c_keys, kc), c_idx.numel())
+        out["c_tptr"], out["c_te"], out["c_ts"] = i32(ptr), i32(q[order]), i32(s_[order])
+    else:
+        out["c_tptr"] = out["c_te"] = out["c_ts"] = None
+    return out
+
+
+def device_strength(rowptr, col, val, diag_slot, theta, stream=None):
+    """Strong flags of every stored entry (``b2s_amg_strength_d``): uint8 tensor [nnz]."""
+    import torch
+
+    n = rowptr.numel() - 1
+    strong = torch.empty(col.numel(), dtype=torch.uint8, device=col.device)
+    _lib.check(_lib.lib().b2s_amg_strength_d(n, rowptr.data_ptr(), col.data_ptr(), val.data_ptr(),
+                                             diag_slot.data_ptr(), float(theta), strong.data_ptr(),
+                                             _lib.stream_ptr(stream)), "b2s_amg_strength_d")
+    return strong
+
+
+def device_transpose_slots(rowptr, col, sorted_cols, stream=None):
+    """Slot of every entry's transpose (``b2s_csr_transpose_slots_d``) and the device count of
+    entries without one (int32 tensors)."""
+    import torch
+
+    n = rowptr.numel() - 1
+    tslot = torch.empty(col.numel(), dtype=torch.int32, device=col.device)
+    missing = torch.zeros(1, dtype=torch.int32, device=col.device)
+    _lib.check(_lib.lib().b2s_csr_transpose_slots_d(n, rowptr.data_ptr(), col.data_ptr(), int(bool(sorted_cols)),
+                                                    tslot.data_ptr(), missing.data_ptr(), _lib.stream_ptr(stream)),
+               "b2s_csr_transpose_slots_d")
+    return tslot, missing
+
+
+def device_aggregate(rowptr, col, strong, tslot, prio, rank_node, stream=None):
+    """The reference's greedy aggregation on the device (``b2s_amg_aggregate_d``), nodes visited
+    in the order ``prio``: (agg int32 [n], counts int32 [n], info int32 [4]) on the device;
+    info[0] is the number of aggregates, info[1] an error code."""
+    import torch
+
+    n = rowptr.numel() - 1
+    dev = col.device
+    L = _lib.lib()
+    rl = (rowptr[1:] - rowptr[:-1]).to(torch.int64)
+    capacity = int(col.numel() + int((rl * rl).sum()))  # bounds every node's conflict list
+    wb = L.b2s_amg_aggregate_workspace_bytes(n, capacity)
+    if wb < 0:
+        raise RuntimeError("invalid aggregation size")
+    work = torch.empty(wb // 4 + 1, dtype=torch.int32, device=dev)
+    agg = torch.empty(n, dtype=torch.int32, device=dev)
+    counts = torch.empty(n, dtype=torch.int32, device=dev)
+    info = torch.zeros(4, dtype=torch.int32, device=dev)
+    _lib.check(L.b2s_amg_aggregate_d(n, rowptr.data_ptr(), col.data_ptr(), strong.data_ptr(), tslot.data_ptr(),
+                                     prio.data_ptr(), rank_node.data_ptr(), agg.data_ptr(), counts.data_ptr(),
+                                     info.data_ptr(), work.data_ptr(), work.numel() * 4, _lib.stream_ptr(stream)),
+               "b2s_amg_aggregate_d")
+    return agg, counts, info
+
+
+_START_VECTORS = {}
+
+
+def _start_vector(n, dev):
+    """The reference's power-iteration start vector (``default_rng(0)``, ``amg.py:69-77``) of
+    length n, on the device (cached: a re-aggregated hierarchy reuses the sizes it had)."""
+    import torch
+
+    key = (int(n), str(dev))
+    if key not in _START_VECTORS:
+        _START_VECTORS[key] = torch.as_tensor(np.random.default_rng(0).standard_normal(n), device=dev)
+    return _START_VECTORS[key]
 
 
 class AMGHierarchy:
@@ -338,7 +502,175 @@ class AMGHierarchy:
         h.coarse_n = nc
         h.coarse_rowptr, h.coarse_col = level_rowptr.data_ptr(), level_col.data_ptr()
         h.coarse_val, h.coarse_inv = level_val.data_ptr(), self.coarse_inv.data_ptr()
-        self.cref = ctypes.byref(h)
+        self._finish(dev)
+
+    @classmethod
+    def on_device(cls, perm, rowptr, col, diag_slot, val, singular=False, theta=0.08, max_coarse=150, max_levels=20,
+                  sweeps=2, omega=0.8, stream=None, prev=None, start=0):
+        """The set-up of ``flowtrace/linalg/amg.py:88-117`` done on the device, level by level:
+        strength (``b2s_amg_strength_d``), the greedy aggregation in the reference's visiting
+        order (``b2s_amg_aggregate_d``: the reference numbering ``perm`` on level 0, the aggregate
+        numbering below), the patterns and term lists of P, W, R and A_c from sorted distinct keys
+        (``product_patterns``), and the level's numeric rebuild (``b2s_amg_level_rebuild_d``),
+        whose Galerkin product gives the next level's values and so its strength graph. Same
+        aggregates, patterns and term lists as the host set-up; no host copy of the matrix. A
+        single case only (no ``groups``). ``perm`` maps device rows to reference rows (numpy or
+        a device tensor).
+
+        Re-aggregation (``prev``, ``start``): ``prev`` is a hierarchy of the same level-0 pattern
+        just rebuilt from the current matrix, whose levels below ``start`` kept their strength
+        graphs - so the reference would build the same aggregates there. Those levels are shared
+        with it and the set-up resumes at level ``start`` from its current values."""
+        import torch
+
+        self = cls.__new__(cls)
+        dev = val.device
+        L = _lib.lib()
+        sp_ = _lib.stream_ptr(stream)
+        self.singular, self.sweeps, self.omega, self.theta = bool(singular), int(sweeps), float(omega), theta
+        self._keep, self.sizes = [], []
+        h = self.c = _lib.Amg()
+        h.singular, h.sweeps, h.omega = int(self.singular), self.sweeps, self.omega
+        self.src_val, self.src_val32 = val, None
+        n0 = rowptr.numel() - 1
+        self.rowptr0, self.col0, self.n0 = rowptr, col, n0
+        i32 = lambda t: t.to(torch.int32).contiguous()  # noqa: E731
+        start = int(start) if prev is not None else 0
+        if start > 0:
+            if start >= prev.n_levels:
+                raise ValueError("start beyond the previous hierarchy's levels")
+            self.val0 = prev.val0  # the shared level 0 keeps the previous rebuild's values
+            for l in range(start):
+                h.levels[l] = prev.c.levels[l]
+                self._keep += prev._keep[2 * l:2 * l + 2]
+                self.sizes.append(prev.sizes[l])
+            nxt = prev._keep[2 * start - 1]
+            lv_rp, lv_cl, lv_val, lv_diag = nxt["rowptr"], nxt["col"], nxt["val"], nxt["diag"]
+            lv_rp64 = nxt.get("rowptr64", None)
+            lv_rp64 = lv_rp.to(torch.int64) if lv_rp64 is None else lv_rp64
+            lv_cl64 = nxt.get("col64", None)
+            lv_cl64 = lv_cl.to(torch.int64) if lv_cl64 is None else lv_cl64
+            n = prev.sizes[start]
+            prio = rank_node = torch.arange(n, dtype=torch.int32, device=dev)
+            x0_src = _start_vector(n, dev)
+            sorted_cols = True
+        else:
+            self.val0 = torch.empty_like(val)
+            self.val0.copy_(val)
+            perm_t = torch.as_tensor(np.asarray(perm, dtype=np.int64) if not torch.is_tensor(perm) else perm,
+                                     device=dev).to(torch.int64)
+            prio = i32(perm_t)
+            rank_node = torch.empty(n0, dtype=torch.int32, device=dev)
+            rank_node[perm_t] = torch.arange(n0, dtype=torch.int32, device=dev)
+            lv_rp, lv_cl, lv_val, lv_diag = rowptr, col, self.val0, diag_slot
+            lv_rp64, lv_cl64 = rowptr.to(torch.int64), col.to(torch.int64)
+            x0_src = _start_vector(n0, dev)[perm_t]
+            sorted_cols = False  # level 0's columns are in the reference's order, not the device's
+            n = n0
+        nlev = start
+        while n > max_coarse and nlev < max_levels - 1:
+            strong = device_strength(lv_rp, lv_cl, lv_val, lv_diag, theta, stream)
+            tslot, missing = device_transpose_slots(lv_rp, lv_cl, sorted_cols, stream)
+            agg, counts, info = device_aggregate(lv_rp, lv_cl, strong, tslot, prio, rank_node, stream)
+            ih = torch.cat([info, missing]).cpu()  # the level's read-back: aggregates and errors
+            if int(ih[4]) != 0:
+                raise RuntimeError("AMG set-up: the level's pattern is not structurally symmetric")
+            if int(ih[1]) != 0:
+                raise RuntimeError(f"device aggregation failed (code {int(ih[1])})")
+            na = int(ih[0])
+            if na >= n * 0.9:
+                break
+            pat = product_patterns(lv_rp64, lv_cl64, agg.to(torch.int64), na)
+            Lv = h.levels[nlev]
+            Lv.n, Lv.nnz, Lv.nc = n, lv_cl.numel(), na
+            Lv.p_nnz, Lv.w_nnz = pat["p_idx"].numel(), pat["w_idx"].numel()
+            c_nnz = pat["c_idx"].numel()
+            Lv.c_nnz = c_nnz if pat["c_tptr"] is not None else 0
+            bufs = {
+                "rowptr": lv_rp, "col": lv_cl, "val": lv_val, "diag_slot": lv_diag,
+                "dinv": torch.empty(n, dtype=torch.float64, device=dev), "agg": agg,
+                "tval": 1.0 / torch.sqrt(counts[:na].to(torch.float64)), "x0": x0_src.contiguous(),
+                "p_rowptr": i32(pat["p_ptr"]), "p_col": i32(pat["p_idx"]),
+                "p_val": torch.empty(Lv.p_nnz, dtype=torch.float64, device=dev),
+                "r_rowptr": i32(pat["r_rowptr"]), "r_col": i32(pat["r_col"]), "r_from_p": i32(pat["r_from_p"]),
+                "r_val": torch.empty(Lv.p_nnz, dtype=torch.float64, device=dev),
+                "w_rowptr": i32(pat["w_ptr"]), "w_col": i32(pat["w_idx"]),
+                "w_val": torch.empty(Lv.w_nnz, dtype=torch.float64, device=dev),
+                "rho": torch.zeros(1, dtype=torch.float64, device=dev), "strong": strong,
+            }
+            for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te", "c_ts"):
+                if pat[k] is not None:
+                    bufs[k] = pat[k]
+            for k, v in bufs.items():
+                setattr(Lv, k, v.data_ptr())
+            self._keep.append(bufs)
+            self.sizes.append(n)
+            # the next level: A_c on its pattern, from this level's numeric rebuild; its diagonal
+            # is in the pattern (a_ii p_iI^2 contributes to entry (I, I) of P^T A P)
+            c_rp, c_cl = i32(pat["c_ptr"]), i32(pat["c_idx"])
+            c_val = torch.empty(c_nnz, dtype=torch.float64, device=dev)
+            wl = L.b2s_amg_level_workspace_bytes(ctypes.byref(Lv))
+            work = torch.empty(max(wl, 8) // 8 + 1, dtype=torch.float64, device=dev)
+            _lib.check(L.b2s_amg_level_rebuild_d(ctypes.byref(Lv), c_rp.data_ptr(), c_cl.data_ptr(), c_val.data_ptr(),
+                                                 work.data_ptr(), work.numel() * 8, sp_), "b2s_amg_level_rebuild_d")
+            ar = torch.arange(na, device=dev)
+            lv_diag = i32(torch.searchsorted(pat["c_keys"], ar * na + ar))
+            lv_rp, lv_cl, lv_val = c_rp, c_cl, c_val
+            lv_rp64, lv_cl64 = pat["c_ptr"], pat["c_idx"]
+            self._keep.append({"rowptr": lv_rp, "col": lv_cl, "val": lv_val, "diag": lv_diag, "work": work,
+                               "rowptr64": lv_rp64, "col64": lv_cl64})
+            prio = rank_node = ar.to(torch.int32)
+            x0_src = _start_vector(na, dev)
+            sorted_cols = True
+            n = na
+            nlev += 1
+        h.nlevels = nlev
+        self.n_levels = nlev + 1
+        self.coarse_n = n
+        self.sizes.append(n)
+        self.coarse_val = lv_val
+        self.coarse_inv = torch.empty((n, n), dtype=torch.float64, device=dev)
+        self.ngroups = 0
+        h.coarse_n = n
+        h.coarse_rowptr, h.coarse_col = lv_rp.data_ptr(), lv_cl.data_ptr()
+        h.coarse_val, h.coarse_inv = lv_val.data_ptr(), self.coarse_inv.data_ptr()
+        self._keep.append({"coarse_rowptr": lv_rp, "coarse_col": lv_cl})
+        self._finish(dev)
+        _lib.check(L.b2s_amg_coarse_inverse_d(self.cref, self.work_rebuild.data_ptr(), self.work_rebuild.numel() * 8,
+                                              sp_), "b2s_amg_coarse_inverse_d")
+        return self
+
+    def first_strength_change(self, stream=None) -> int:
+        """The first level whose strength graph, with the current level matrices, differs from the
+        set-up's (the reference would aggregate it differently), or -1. Synchronises the stream."""
+        import torch
+
+        nl = max(self.c.nlevels, 1)
+        if self._level_counts is None or self._level_counts.numel() < nl:
+            self._level_counts = torch.zeros(nl, dtype=torch.int32, device=self._count.device)
+            self._level_counts_host = torch.zeros(nl, dtype=torch.int32)
+            if self._count.device.type == "cuda":
+                self._level_counts_host = self._level_counts_host.pin_memory()
+        if self.c.nlevels == 0:
+            return -1
+        _lib.check(_lib.lib().b2s_amg_level_strength_changes_d(self.cref, self.theta, self._level_counts.data_ptr(),
+                                                               _lib.stream_ptr(stream)),
+                   "b2s_amg_level_strength_changes_d")
+        self._level_counts_host.copy_(self._level_counts, non_blocking=True)
+        (stream or torch.cuda.current_stream()).synchronize()
+        changed = np.flatnonzero(self._level_counts_host.numpy()[: self.c.nlevels])
+        return int(changed[0]) if changed.size else -1
+
+    def to_f32(self, stream=None):
+        """Refresh the float copies of the level values (mixed precision) without a rebuild."""
+        if self.src_val32 is not None:
+            _lib.check(_lib.lib().b2s_amg_to_f32_d(self.cref, self.c32ref, _lib.stream_ptr(stream)), "b2s_amg_to_f32_d")
+
+    def _finish(self, dev):
+        """Workspaces and the strength-change counter of a complete hierarchy."""
+        import torch
+
+        self.cref = ctypes.byref(self.c)
         L = _lib.lib()
         wb = L.b2s_amg_workspace_bytes(self.cref)
         pb = L.b2s_pcg_workspace_bytes(self.cref)
@@ -347,6 +679,7 @@ class AMGHierarchy:
         self.work_rebuild = torch.empty(max(wb, 8) // 8 + 1, dtype=torch.float64, device=dev)
         self.work_pcg = torch.empty(max(pb, 8) // 8 + 1, dtype=torch.float64, device=dev)
         self._count = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._level_counts = None
         self._count_host = torch.zeros(1, dtype=torch.int32)
         if dev.type == "cuda":
             self._count_host = self._count_host.pin_memory()

@@ -169,7 +169,9 @@ class BatchSimpleSolver(MixedSimpleSolver):
         for g in range(ng):
             self._set_case_relax(g)
 
-    def _setup_amg(self):
+    def _setup_amg(self, start=0):
+        """Host set-up of the batch hierarchy (aggregates numbered case by case; never
+        re-aggregated, so ``start`` is always 0)."""
         import torch
 
         torch.cuda.current_stream().synchronize()
@@ -181,6 +183,7 @@ class BatchSimpleSolver(MixedSimpleSolver):
                                  theta=self.amg_theta, groups=self._cell_groups,
                                  group_singular=self.case_singular.astype(np.int32))
         self.amg_setups += 1
+        self._amg_fresh = False
         self._amg.enable_mixed(self.val_P32)
 
     def _params(self):

@@ -56,14 +56,13 @@ class MixedSimpleSolver(SimpleSolver):
         wb = max(L.b2s_bicgstab_f32_workspace_bytes(nc, dim), L.b2s_bicgstab_f32_workspace_bytes(nc, 1))
         self.work_bicg32 = torch.empty(wb // 8 + 1, dtype=torch.float64, device=dev)
 
-    def _setup_amg(self):
-        """Host set-up from the widened float pressure matrix; the V-cycle then reads float copies."""
-        import torch
-
-        torch.cuda.current_stream().synchronize()
+    def _setup_amg(self, start=0):
+        """Set-up from the widened float pressure matrix; the V-cycle then reads float copies."""
         self.val_P.copy_(self.val_P32)
-        super()._setup_amg()
+        super()._setup_amg(start)
         self._amg.enable_mixed(self.val_P32)
+        if self._amg_fresh:
+            self._amg.to_f32()
 
     def _launch(self, amg_ready=False):
         L, fv = _lib.lib(), self.fv

@@ -160,12 +160,14 @@ class SimpleSolver:
         self.amg_setups = 0
         # False: aggregates fixed at the first set-up, every numeric quantity rebuilt on the device
         # (no host work after the first iteration). True: the reference's behaviour (it
-        # re-aggregates at every rebuild) - the host set-up is redone whenever the strength graph
-        # of some level changed (a device check), a host round trip of the pressure matrix each
-        # time. Fixed aggregates give a preconditioner the reference never builds; on strongly
-        # varying coefficients (Brinkman porosity) that can stall the outer iteration, so
-        # porous problems (``adjoint.PorousChannel``) turn re-aggregation on.
+        # re-aggregates at every rebuild) - the device set-up is redone whenever the strength
+        # graph of some level changed (a device check; unchanged graphs give the same
+        # aggregates). Fixed aggregates give a preconditioner the reference never builds; on
+        # strongly varying coefficients (Brinkman porosity) that can stall the outer iteration,
+        # so porous problems (``adjoint.PorousChannel``) turn re-aggregation on.
         self.reaggregate = False
+        self.host_amg_setup = False  # True: the host set-up (SciPy) instead of the device set-up
+        self._perm_dev = None
         self.max_coarse = int(max_coarse)
         self.amg_theta = float(amg_theta)
         self.last_linear = {}
@@ -441,35 +443,57 @@ class SimpleSolver:
     def finished(self) -> bool:
         return self.converged or self.iteration >= self.case.max_iter
 
-    def _setup_amg(self):
-        """Host set-up of the hierarchy from the current pressure-correction matrix."""
+    def _setup_amg(self, start=0):
+        """Set-up of the hierarchy from the current pressure-correction matrix, on the device
+        (``AMGHierarchy.on_device``: the reference's aggregation and patterns without a host copy
+        of the matrix; from level ``start`` on when re-aggregating, the levels above it shared
+        with the current hierarchy); ``host_amg_setup`` selects the host set-up instead. Sets
+        ``_amg_fresh``: every numeric quantity already computed from the current matrix."""
         import torch
 
-        torch.cuda.current_stream().synchronize()
         # captured iterations reference the old hierarchy's buffers, which are freed with it
         self._graphs.clear()
-        A_host = self.fv.matrix_to_host(self.val_P)
-        self._amg = AMGHierarchy(A_host, self.fv.perm, self.fv.rowptr, self.fv.col, self.fv.t["slot_diag"],
-                                 self.val_P, self.fv.slot_ref, singular=self.singular_p, max_coarse=self.max_coarse,
-                                 theta=self.amg_theta)
+        if self.host_amg_setup:
+            torch.cuda.current_stream().synchronize()
+            A_host = self.fv.matrix_to_host(self.val_P)
+            self._amg = AMGHierarchy(A_host, self.fv.perm, self.fv.rowptr, self.fv.col, self.fv.t["slot_diag"],
+                                     self.val_P, self.fv.slot_ref, singular=self.singular_p,
+                                     max_coarse=self.max_coarse, theta=self.amg_theta)
+            self._amg_fresh = False
+        else:
+            if self._perm_dev is None:
+                self._perm_dev = torch.as_tensor(self.fv.perm, dtype=torch.int64, device=self.val_P.device)
+            self._amg = AMGHierarchy.on_device(self._perm_dev, self.fv.rowptr, self.fv.col, self.fv.t["slot_diag"],
+                                               self.val_P, singular=self.singular_p, max_coarse=self.max_coarse,
+                                               theta=self.amg_theta, prev=self._amg if start > 0 else None,
+                                               start=start)
+            self._amg_fresh = True
         self.amg_setups += 1
 
     def _ensure_amg(self, s):
         """Rebuild policy of ``simple.py:624-628``: a new preconditioner every ``amg_rebuild``
-        iterations. The numeric rebuild runs on the device; when the strength graph of some
-        level changed since the set-up (the reference would aggregate differently) the set-up
-        is redone from the current matrix, so the hierarchy is always the reference's."""
+        iterations. The numeric rebuild runs on the device; with ``reaggregate``, when the
+        strength graph of some level changed since the set-up (the reference would aggregate
+        differently) the set-up is redone from that level on, so the hierarchy is always the
+        reference's."""
+        levels = lambda: self._amg.n_levels - 1  # noqa: E731
         if self._amg is None:
             self._setup_amg()
-            self._amg_age = 10 ** 9
-        if self._amg_age >= self.amg_rebuild:
-            self._amg.rebuild()
-            self.kernel_launches += 6 * (self._amg.n_levels - 1) + 1
-            if self.reaggregate and self._amg.strength_changed():
-                self.kernel_launches += self._amg.n_levels - 1
-                self._setup_amg()
+            if not self._amg_fresh:
                 self._amg.rebuild()
-                self.kernel_launches += 6 * (self._amg.n_levels - 1) + 1
+            self.kernel_launches += 6 * levels() + 1
+            self._amg_age = 0
+        elif self._amg_age >= self.amg_rebuild:
+            self._amg.rebuild()
+            self.kernel_launches += 6 * levels() + 1
+            if self.reaggregate:
+                first = self._amg.first_strength_change()
+                self.kernel_launches += levels()
+                if first >= 0:
+                    self._setup_amg(start=first)
+                    if not self._amg_fresh:
+                        self._amg.rebuild()
+                    self.kernel_launches += 6 * levels() + 1
             self._amg_age = 0
         self._amg_age += 1
 

@@ -377,6 +377,8 @@ B2S_API int b2s_pcg_amg_d(const b2s_amg* h, int32_t n, const int32_t* rowptr, co
  * reference re-aggregates at every rebuild, so a non-zero count means its aggregates changed.
  * *count (device int) is overwritten. */
 B2S_API int b2s_amg_strength_changes_d(const b2s_amg* h, double theta, int32_t* count, b2s_stream_t s);
+/* The same count per level: counts[l] (device ints, [nlevels]) for level l. */
+B2S_API int b2s_amg_level_strength_changes_d(const b2s_amg* h, double theta, int32_t* counts, b2s_stream_t s);
 
 /* Apply one V-cycle: x = M b (for tests of the preconditioner). */
 B2S_API int b2s_amg_vcycle_d(const b2s_amg* h, const double* b, double* x, void* work, int64_t work_bytes, b2s_stream_t s);
@@ -385,6 +387,47 @@ B2S_API int b2s_amg_vcycle_d(const b2s_amg* h, const double* b, double* x, void*
  * strength graph given as HOST CSR arrays; agg[n] (host) receives each node's aggregate and
  * the return value is the number of aggregates (-1 on invalid arguments). */
 B2S_API int64_t b2s_host_aggregate(int64_t n, const int64_t* indptr, const int64_t* indices, int64_t* agg);
+
+/* Device set-up of the hierarchy, level by level (replaces the host set-up of
+ * flowtrace/linalg/amg.py:88-117 when the hierarchy is re-aggregated on the device).
+ *
+ * b2s_amg_strength_d: strong[e] = 1 where |a_e| >= theta sqrt(|a_ii a_jj|), col[e] != i
+ * (amg.py:60-66), for every stored entry of the CSR matrix (rowptr, col, val) of n rows.
+ *
+ * b2s_csr_transpose_slots_d: for a structurally symmetric pattern, tslot[e] = the slot of the
+ * transposed entry (col[e], row of e); sorted != 0 when every row's columns ascend (binary
+ * search), else rows are scanned. *missing (device int) counts entries without a transpose
+ * (their tslot is e itself).
+ *
+ * b2s_amg_aggregate_d: the greedy three-pass aggregation of amg.py:25-57 on the strength graph
+ * S(i) = {col[e] : e in row i, strong[e]}, visiting nodes in the order prio (a permutation of
+ * 0..n-1; rank_node its inverse), exactly the reference's result when prio is the reference's
+ * numbering and each row's strong columns are that numbering's columns. agg[n] receives the
+ * aggregates (numbered as the reference numbers them), counts[n] the size of each aggregate
+ * (entries >= the number of aggregates are 0), info[4] (device ints): [0] the number of
+ * aggregates, [1] an error code (0; 1: a poll limit of the pass-1 kernel ran out; 2: an
+ * inconsistent pass-2 chain; 3: the conflict lists exceed the work space), [2] the aggregates of
+ * pass 1, [3] the nodes of pass 3. The work space holds the nodes' conflict lists: at most
+ * capacity = nnz + sum over rows of (row length)^2 entries always suffices
+ * (b2s_amg_aggregate_workspace_bytes(n, capacity)). The pass-1 kernel is a cooperative launch
+ * whose threads wait on each other's decisions with bounded polls.
+ *
+ * b2s_amg_level_rebuild_d: the numeric rebuild of one (single-case) level from its matrix
+ * values (D^-1, rho, P, R, W) writing the next level's values cval on the pattern (crow, ccol);
+ * b2s_amg_coarse_inverse_d: the coarse inverse of a complete hierarchy (its workspace is
+ * b2s_amg_workspace_bytes). b2s_amg_rebuild_d is these applied to every level in turn. */
+B2S_API int b2s_amg_strength_d(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val,
+                               const int32_t* diag_slot, double theta, uint8_t* strong, b2s_stream_t s);
+B2S_API int b2s_csr_transpose_slots_d(int32_t n, const int32_t* rowptr, const int32_t* col, int32_t sorted,
+                                      int32_t* tslot, int32_t* missing, b2s_stream_t s);
+B2S_API int64_t b2s_amg_aggregate_workspace_bytes(int32_t n, int64_t capacity);
+B2S_API int b2s_amg_aggregate_d(int32_t n, const int32_t* rowptr, const int32_t* col, const uint8_t* strong,
+                                const int32_t* tslot, const int32_t* prio, const int32_t* rank_node, int32_t* agg,
+                                int32_t* counts, int32_t* info, void* work, int64_t work_bytes, b2s_stream_t s);
+B2S_API int64_t b2s_amg_level_workspace_bytes(const b2s_amg_level* L);
+B2S_API int b2s_amg_level_rebuild_d(const b2s_amg_level* L, const int32_t* crow, const int32_t* ccol, double* cval,
+                                    void* work, int64_t work_bytes, b2s_stream_t s);
+B2S_API int b2s_amg_coarse_inverse_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s);
 
 /* ----------------------------------------------------------------------------------------- */
 /* Mixed precision. No counterpart in the reference (its path is FP64 throughout): the linear    */
