@@ -865,7 +865,14 @@ def main():
                 "stage_ms_per_step": {k: v / K for k, v in sorted(times.items(), key=lambda kv: -kv[1])}}
     del s
 
-    # ---- end to end through the public API, from host data
+    # ---- end to end through the public API, from host data (after one untimed pass of the same
+    # calls, as the timed steps follow warm-up steps)
+    s2 = mk(run_case)
+    if inlet is not None:
+        inlet(s2)
+    s2.run(max_steps=2)
+    s2.fields()
+    del s2
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -879,12 +886,11 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
-    h2d = sum(v.numel() * v.element_size() for v in s2.fv.t.values()) + sum(
-        v.numel() * v.element_size() for v in s2._bc_t.values())
+    h2d = s2.fv.h2d_bytes + sum(v.numel() * v.element_size() for v in s2._bc_t.values()) + (1 + s2.dim) * nc * 8
     d2h = s2.report.numel() * (W + K) + sum(v.nbytes for v in f.values())
     e2e = {"value": world * nc * (W + K) / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d / (W + K),
            "d2h_bytes_per_step": d2h / (W + K), "includes": "solver construction from the host mesh, W+K steps, "
-           "fields() read back", "setup_seconds": setup_s, "seconds": e2e_ms / 1e3}
+           "fields() read back; after one untimed pass of the same calls", "setup_seconds": setup_s, "seconds": e2e_ms / 1e3}
     del s2
 
     # ---- the metric's "to 1e-6" half: fresh solvers run to the 1e-6 scaled residual

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 INCLUDE = os.path.join(ROOT, "include")
-SOURCES = ["b2s_fv.cu", "b2s_krylov.cu", "b2s_amg.cu", "b2s_amg_setup.cu", "b2s_batch.cu", "b2s_adjoint.cu", "b2s_noalloc.cu", "b2s_sst.cu"]
+SOURCES = ["b2s_setup.cu", "b2s_fv.cu", "b2s_krylov.cu", "b2s_amg.cu", "b2s_amg_setup.cu", "b2s_batch.cu", "b2s_adjoint.cu", "b2s_noalloc.cu", "b2s_sst.cu"]
 HEADERS = ["b2s_common.cuh", "b2s_fv.cuh"]
 LIB = os.path.join(HERE, "libb2simplec.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -124,25 +124,159 @@ class FVMesh:
     """Device layout of a mesh (see the module docstring). ``device`` defaults to the current
     CUDA device; there is no CPU variant."""
 
-    def __init__(self, mesh: UnstructuredMesh, device=None, reorder: bool = True, groups=None):
+    def __init__(self, mesh: UnstructuredMesh, device=None, reorder: bool = True, groups=None,
+                 device_setup: bool = True):
         """``groups`` (one label per cell, optional): cells of one group are kept contiguous in the
         device order, groups in increasing label order (the reverse Cuthill-McKee order within
-        each) - the layout of a block-diagonal batch of independent cases."""
+        each) - the layout of a block-diagonal batch of independent cases. ``device_setup``: the
+        geometry, face quantities, least-squares matrices, CSR pattern and layout are computed on
+        the device (``b2s_setup.cu``) from the raw mesh; False computes them on the host
+        (``HostFV``) and uploads them. Both give the same arrays (the least-squares inverses to
+        rounding); ``host`` is available either way (built on first use in the device set-up)."""
+        self.device = device if device is not None else _lib.require_device()
+        if mesh.periodic:
+            raise NotImplementedError("periodic meshes are not supported by the B200 SIMPLEC path")
+        self.mesh = mesh
+        self._host = None
+        self._geometry = None
+        dev = self.device
+        if device_setup and getattr(dev, "type", str(dev)) == "cuda":
+            ref = self._reference_arrays_on_device(mesh)
+        else:
+            ref = self._reference_arrays_from_host(mesh)
+        self._layout(ref, reorder, groups)
+
+    @property
+    def host(self) -> HostFV:
+        """The reference's FV quantities on the host (``HostFV``), built on first use."""
+        if self._host is None:
+            self._host = HostFV(self.mesh)
+        return self._host
+
+    @property
+    def geometry(self):
+        return self.host.geometry
+
+    def _reference_arrays_from_host(self, mesh):
+        """The FV quantities in the reference's numbering, from ``HostFV`` (host, then uploaded)."""
         import torch
 
-        self.device = device if device is not None else _lib.require_device()
-        h = self.host = HostFV(mesh)
-        self.mesh = mesh
-        self.dim, self.nc, self.n_if, self.n_bf, self.nnz = h.dim, h.nc, h.n_if, h.n_bf, h.nnz
-        self.non_orthogonality_deg = h.non_orthogonality_deg
-        self.geometry = h.geometry
-        nc, nf, nb, dim = h.nc, h.n_if, h.n_bf, h.dim
-        if max(nc, nf, nb, h.nnz) >= 2 ** 31 - 1:
-            raise ValueError("mesh too large for 32-bit indices")
-        # ---- cell order: reverse Cuthill-McKee of the cell adjacency
+        h = self._host = HostFV(mesh)
+        dev = self.device
+        T = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)  # noqa: E731
+        self.h2d_bytes = 8 * sum(np.asarray(a).size for a in (h.w, h.alpha, h.wl, h.S, h.d, h.Tvec, h.dxm, h.dP_f,
+                                                              h.dN_f, h.alpha_b, h.wlb, h.Sb_mag, h.Sb, h.db, h.nb,
+                                                              h.db_t, h.vol, h.Ginv))
+        return {"dim": h.dim, "nc": h.nc, "P": h.P, "N": h.N, "Pb": h.Pb, "bzone": h.bzone,
+                "non_orthogonality_deg": h.non_orthogonality_deg,
+                "w": T(h.w), "alpha": T(h.alpha), "wl": T(h.wl), "S": T(h.S), "d": T(h.d), "Tv": T(h.Tvec),
+                "dxm": T(h.dxm), "dPf": T(h.dP_f), "dNf": T(h.dN_f), "alpha_b": T(h.alpha_b), "wlb": T(h.wlb),
+                "Sb_mag": T(h.Sb_mag), "Sb": T(h.Sb), "db": T(h.db), "nbv": T(h.nb), "dbt": T(h.db_t),
+                "vol": T(h.vol), "Ginv": T(h.Ginv)}
+
+    def _reference_arrays_on_device(self, mesh):
+        """The FV quantities in the reference's numbering, computed on the device from the raw
+        mesh (nodes, face-node lists, owner, neighbour): ``b2s_face_geometry_d``,
+        ``b2s_cell_geometry_d``, ``b2s_fv_faces_d`` and ``b2s_ls_matrices_d``, with the per-cell
+        face lists in the reference's face order (stable sorts)."""
+        import torch
+
+        dev = self.device
+        L = _lib.lib()
+        sp_ = _lib.stream_ptr()
+        dim, nc = mesh.dim, mesh.n_cells
+        owner = np.asarray(mesh.owner, dtype=np.int64)
+        neighbour = np.asarray(mesh.neighbour, dtype=np.int64)
+        nf_all = owner.size
+        interior = neighbour >= 0
+        if_idx = np.flatnonzero(interior)
+        bf_idx = np.flatnonzero(~interior)
+        P, N, Pb = owner[if_idx], neighbour[if_idx], owner[bf_idx]
+        if np.any(P == N):
+            raise ValueError("a face connects a cell to itself")
+        n_if, n_bf = if_idx.size, bf_idx.size
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
+        f64 = lambda *sh: torch.empty(*sh, dtype=torch.float64, device=dev)  # noqa: E731
+        X = torch.as_tensor(np.ascontiguousarray(mesh.nodes, dtype=np.float64), device=dev)
+        fptr, fnodes = i32(mesh.face_ptr), i32(mesh.face_nodes)
+        own_t, nei_t = i32(owner), i32(neighbour)
+        if_t, bf_t, P_t, N_t, Pb_t = i32(if_idx), i32(bf_idx), i32(P), i32(N), i32(Pb)
+        self.h2d_bytes = sum(a.numel() * a.element_size() for a in (X, fptr, fnodes, own_t, nei_t, if_t, bf_t, P_t,
+                                                                     N_t, Pb_t))
+        ar = torch.arange(nc + 1, device=dev)
+
+        def lists(keys):
+            """Entries grouped by key (stable: increasing position within a key) and offsets."""
+            srt = torch.sort(keys, stable=True)
+            return torch.searchsorted(srt.values, ar).to(torch.int32), srt.indices.to(torch.int32)
+
+        own_ptr, own = lists(own_t)  # every face a cell owns, increasing face index
+        nei_ptr, nei_i = lists(N_t)  # interior faces by neighbour, increasing index
+        nei = if_t[nei_i.long()].contiguous()
+        pi_ptr, pi = lists(P_t)  # interior faces (interior index) by owner
+        pb_ptr, pb = lists(Pb_t)  # boundary faces (boundary index) by owner
+        fc, S = f64(nf_all, dim), f64(nf_all, dim)
+        cnt = torch.zeros(8, dtype=torch.int32, device=dev)
+        _lib.check(L.b2s_face_geometry_d(dim, nf_all, X.data_ptr(), fptr.data_ptr(), fnodes.data_ptr(), fc.data_ptr(),
+                                         S.data_ptr(), cnt.data_ptr(), sp_), "b2s_face_geometry_d")
+        ca, vol, xc = f64(nc, dim), f64(nc), f64(nc, dim)
+        _lib.check(L.b2s_cell_geometry_d(dim, nc, nf_all, own_t.data_ptr(), nei_t.data_ptr(), own_ptr.data_ptr(),
+                                         own.data_ptr(), nei_ptr.data_ptr(), nei.data_ptr(), fc.data_ptr(), S.data_ptr(),
+                                         ca.data_ptr(), vol.data_ptr(), xc.data_ptr(), cnt[1:].data_ptr(), sp_),
+                   "b2s_cell_geometry_d")
+        o = {k: f64(n_if, dim) for k in ("d", "Tv", "dPf", "dNf", "dxm")}
+        o.update({k: f64(max(n_if, 1)) for k in ("w", "alpha", "wl")})
+        o.update({k: f64(n_bf, dim) for k in ("db", "nbv", "dbt")})
+        o.update({k: f64(max(n_bf, 1)) for k in ("alpha_b", "wlb", "Sb_mag", "yb")})
+        cmin = f64(1)
+        _lib.check(L.b2s_fv_faces_d(dim, n_if, if_t.data_ptr(), P_t.data_ptr(), N_t.data_ptr(), n_bf, bf_t.data_ptr(),
+                                    Pb_t.data_ptr(), xc.data_ptr(), fc.data_ptr(), S.data_ptr(),
+                                    *[o[k].data_ptr() for k in ("d", "w", "alpha", "wl", "Tv", "dPf", "dNf", "dxm",
+                                                                "db", "alpha_b", "wlb", "Sb_mag", "nbv", "dbt", "yb")],
+                                    cmin.data_ptr(), sp_), "b2s_fv_faces_d")
+        G, Ginv = f64(nc, dim, dim), f64(nc, dim, dim)
+        flag = torch.empty(nc, dtype=torch.int32, device=dev)
+        _lib.check(L.b2s_ls_matrices_d(dim, nc, pi_ptr.data_ptr(), pi.data_ptr(), nei_ptr.data_ptr(), nei_i.data_ptr(),
+                                       pb_ptr.data_ptr(), pb.data_ptr(), o["d"].data_ptr(), o["wl"].data_ptr(),
+                                       o["db"].data_ptr(), o["wlb"].data_ptr(), G.data_ptr(), Ginv.data_ptr(),
+                                       flag.data_ptr(), sp_), "b2s_ls_matrices_d")
+        nflag = flag.sum(dtype=torch.int32).reshape(1)
+        chk = torch.cat([cnt[:3], nflag]).cpu().numpy()  # bad faces, flipped, non-positive volumes, singular G
+        if chk[0]:
+            raise ValueError("2-D meshes must have 2-node faces" if dim == 2 else "a face has fewer than 3 or more "
+                             "than 32 nodes")
+        if chk[2]:
+            raise ValueError(f"{int(chk[2])} cells have non-positive volume")
+        if chk[3]:  # singular least-squares matrices: the pseudo-inverse, as the reference
+            bad = torch.nonzero(flag).flatten()
+            Ginv[bad] = torch.as_tensor(np.linalg.pinv(G[bad].cpu().numpy()), device=dev)
+        cm = float(cmin.item()) if n_if else 1.0
+        self.flipped_faces = int(chk[1])
+        Sif, Sbf = S[if_t.long()], S[bf_t.long()]
+        return {"dim": dim, "nc": nc, "P": P, "N": N, "Pb": Pb, "bzone": np.asarray(mesh.face_zone)[bf_idx],
+                "non_orthogonality_deg": float(np.degrees(np.arccos(cm))) if n_if else 0.0,
+                "w": o["w"][:n_if], "alpha": o["alpha"][:n_if], "wl": o["wl"][:n_if], "S": Sif, "d": o["d"],
+                "Tv": o["Tv"], "dxm": o["dxm"], "dPf": o["dPf"], "dNf": o["dNf"], "alpha_b": o["alpha_b"][:n_bf],
+                "wlb": o["wlb"][:n_bf], "Sb_mag": o["Sb_mag"][:n_bf], "Sb": Sbf, "db": o["db"], "nbv": o["nbv"],
+                "dbt": o["dbt"], "vol": vol, "Ginv": Ginv, "xc": xc, "yb": o["yb"][:n_bf]}
+
+    def _layout(self, r, reorder, groups):
+        """The device layout (module docstring) of reference-numbered quantities ``r``: the cell
+        order, the face orders, the CSR pattern and its slot maps, SoA device tensors."""
+        import torch
+
+        dev = self.device
+        dim, nc = r["dim"], r["nc"]
+        P, N, Pb = r["P"], r["N"], r["Pb"]
+        nf, nb = P.size, Pb.size
+        self.dim, self.nc, self.n_if, self.n_bf = dim, nc, nf, nb
+        self.non_orthogonality_deg = r["non_orthogonality_deg"]
+        self.bzone = r["bzone"]
+        self._ref = r
+        # ---- cell order (host): reverse Cuthill-McKee of the cell adjacency
         if reorder and nf:
-            adj = sp.csr_matrix((np.ones(2 * nf, dtype=np.int8), (np.concatenate([h.P, h.N]),
-                                                                   np.concatenate([h.N, h.P]))), shape=(nc, nc))
+            adj = sp.csr_matrix((np.ones(2 * nf, dtype=np.int8), (np.concatenate([P, N]), np.concatenate([N, P]))),
+                                shape=(nc, nc))
             perm = np.asarray(reverse_cuthill_mckee(adj, symmetric_mode=True), dtype=np.int64)
         else:
             perm = np.arange(nc, dtype=np.int64)
@@ -152,60 +286,92 @@ class FVMesh:
         iperm = np.empty(nc, dtype=np.int64)
         iperm[perm] = np.arange(nc)
         self.perm, self.iperm = perm, iperm  # device -> reference, reference -> device
-        # ---- interior faces by (device owner, reference index)
-        Pn, Nn = iperm[h.P], iperm[h.N]
-        forder = np.lexsort((np.arange(nf), Pn))
-        self.face_ref = forder  # device face -> reference interior face
+        L64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=dev)  # noqa: E731
+        perm_t, iperm_t, P_t, N_t, Pb_t = L64(perm), L64(iperm), L64(P), L64(N), L64(Pb)
+        self.h2d_bytes += 8 * (2 * nc + 2 * nf + nb)
+        ar = torch.arange(nc + 1, device=dev)
+        # ---- interior faces by (device owner, reference index); faces by neighbour
+        Pn, Nn = iperm_t[P_t], iperm_t[N_t]
+        forder = torch.sort(Pn, stable=True).indices
         fP, fN = Pn[forder], Nn[forder]
-        own_ptr = np.concatenate([[0], np.cumsum(np.bincount(fP, minlength=nc))])
-        norder = np.lexsort((forder, fN))  # device faces grouped by neighbour, by reference index
-        nei_ptr = np.concatenate([[0], np.cumsum(np.bincount(fN, minlength=nc))])
+        own_ptr = torch.searchsorted(fP, ar)
+        norder = torch.argsort(fN * max(nf, 1) + forder)
+        nei_ptr = torch.searchsorted(fN[norder], ar)
         # ---- boundary faces by (device owner, reference index)
-        bPn = iperm[h.Pb]
-        border = np.lexsort((np.arange(nb), bPn))
-        self.bface_ref = border  # device boundary face -> reference boundary face
+        bPn = iperm_t[Pb_t]
+        border = torch.sort(bPn, stable=True).indices
         bP = bPn[border]
-        bptr = np.concatenate([[0], np.cumsum(np.bincount(bP, minlength=nc))])
-        # ---- CSR rows in device order, each keeping the reference's column order
-        rl = np.diff(h.indptr)
-        rowptr = np.concatenate([[0], np.cumsum(rl[perm])])
-        src = np.repeat(h.indptr[:-1][perm] - rowptr[:-1], rl[perm]) + np.arange(h.nnz)  # device slot -> ref slot
-        col = iperm[h.indices[src]]
-        slot_new = np.empty(h.nnz, dtype=np.int64)
-        slot_new[src] = np.arange(h.nnz)  # reference slot -> device slot
-        self.slot_ref = src
-        self.duplicate_pairs = h.duplicate_pairs
-        if h.duplicate_pairs:
+        bptr = torch.searchsorted(bP, ar)
+        # ---- the CSR pattern in the reference's numbering, then its rows in device order
+        dg = torch.arange(nc, device=dev)
+        keys = torch.unique(torch.cat([dg * nc + dg, P_t * nc + N_t, N_t * nc + P_t]), sorted=True)
+        nnz = keys.numel()
+        r_indptr = torch.searchsorted(keys // nc, ar)
+        r_indices = keys % nc
+        slot_diag = torch.searchsorted(keys, dg * nc + dg)
+        slot_PN = torch.searchsorted(keys, P_t * nc + N_t)
+        slot_NP = torch.searchsorted(keys, N_t * nc + P_t)
+        rl = r_indptr[1:] - r_indptr[:-1]
+        rlp = rl[perm_t]
+        rowptr = torch.zeros(nc + 1, dtype=torch.int64, device=dev)
+        rowptr[1:] = torch.cumsum(rlp, 0)
+        src = torch.repeat_interleave(r_indptr[:-1][perm_t] - rowptr[:-1], rlp, output_size=nnz) + torch.arange(
+            nnz, device=dev)  # device slot -> reference slot
+        col = iperm_t[r_indices[src]]
+        slot_new = torch.empty(nnz, dtype=torch.int64, device=dev)
+        slot_new[src] = torch.arange(nnz, device=dev)  # reference slot -> device slot
+        per_cell = (torch.bincount(P_t, minlength=nc) + torch.bincount(N_t, minlength=nc)
+                    + torch.bincount(Pb_t, minlength=nc))
+        spn = torch.sort(slot_PN).values
+        dup = (spn[1:] == spn[:-1]).any() if nf > 1 else torch.zeros((), dtype=torch.bool, device=dev)
+        stats = torch.stack([rl.max() if nc else torch.zeros((), dtype=torch.int64, device=dev),
+                             per_cell.max() if nc else torch.zeros((), dtype=torch.int64, device=dev),
+                             dup.to(torch.int64)]).cpu().numpy()
+        self.nnz = int(nnz)
+        if max(nc, nf, nb, self.nnz) >= 2 ** 31 - 1:
+            raise ValueError("mesh too large for 32-bit indices")
+        self.duplicate_pairs = bool(stats[2])
+        if self.duplicate_pairs:
             raise NotImplementedError("meshes with two faces joining the same pair of cells are not supported")
+        self._ref_csr = (r_indptr, r_indices)
+        self.face_ref = forder.cpu().numpy()  # device face -> reference interior face
+        self.bface_ref = border.cpu().numpy()  # device boundary face -> reference boundary face
+        self.slot_ref = src.cpu().numpy()
         # ---- device tensors
-        dev = self.device
-        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
-        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
-        soa = lambda a: f64(np.ascontiguousarray(np.asarray(a).T))  # (n, k) -> [k][n]  # noqa: E731
+        i32 = lambda t: t.to(torch.int32).contiguous()  # noqa: E731
+        soa = lambda t: t.t().contiguous()  # (n, k) -> [k][n]  # noqa: E731
         t = self.t = {}
         t["fP"], t["fN"], t["forig"] = i32(fP), i32(fN), i32(forder)
         t["own_ptr"], t["nei_ptr"], t["nei_face"] = i32(own_ptr), i32(nei_ptr), i32(norder)
         t["bP"], t["bptr"] = i32(bP), i32(bptr)
-        t["w"], t["alpha"], t["wl"] = f64(h.w[forder]), f64(h.alpha[forder]), f64(h.wl[forder])
-        for name, arr in (("S", h.S), ("d", h.d), ("Tv", h.Tvec), ("dxm", h.dxm), ("dPf", h.dP_f), ("dNf", h.dN_f)):
-            t[name] = soa(arr[forder])
-        t["alpha_b"], t["wlb"], t["Sb_mag"] = f64(h.alpha_b[border]), f64(h.wlb[border]), f64(h.Sb_mag[border])
-        for name, arr in (("Sb", h.Sb), ("db", h.db), ("nbv", h.nb), ("dbt", h.db_t)):
-            t[name] = soa(arr[border])
-        t["vol"] = f64(h.vol[perm])
-        t["Ginv"] = f64(np.ascontiguousarray(h.Ginv[perm].reshape(nc, dim * dim).T))
+        t["w"], t["alpha"], t["wl"] = r["w"][forder].contiguous(), r["alpha"][forder].contiguous(), r["wl"][forder].contiguous()
+        for name in ("S", "d", "Tv", "dxm", "dPf", "dNf"):
+            t[name] = soa(r[name][forder])
+        for name in ("alpha_b", "wlb", "Sb_mag"):
+            t[name] = r[name][border].contiguous()
+        for name in ("Sb", "db", "nbv", "dbt"):
+            t[name] = soa(r[name][border])
+        t["vol"] = r["vol"][perm_t].contiguous()
+        t["Ginv"] = r["Ginv"][perm_t].reshape(nc, dim * dim).t().contiguous()
         t["rowptr"], t["col"] = i32(rowptr), i32(col)
-        t["slot_diag"] = i32(slot_new[h.slot_diag[perm]])
-        t["slot_PN"] = i32(slot_new[h.slot_PN[forder]])
-        t["slot_NP"] = i32(slot_new[h.slot_NP[forder]])
+        t["slot_diag"] = i32(slot_new[slot_diag[perm_t]])
+        t["slot_PN"] = i32(slot_new[slot_PN[forder]])
+        t["slot_NP"] = i32(slot_new[slot_NP[forder]])
+        for k, v in list(t.items()):
+            if v.numel() == 0:  # a mesh without interior or boundary faces: keep valid pointers
+                t[k] = torch.zeros(1, dtype=v.dtype, device=dev)
         self.vol = t["vol"]
         self.rowptr, self.col = t["rowptr"], t["col"]
-        self.cmesh = _lib.Mesh(nc=nc, nf=nf, nb=nb, dim=dim, nnz=h.nnz,
+        self.cmesh = _lib.Mesh(nc=nc, nf=nf, nb=nb, dim=dim, nnz=self.nnz,
                                **{k: v.data_ptr() for k, v in t.items()})
         self.cmesh_ref = ctypes.byref(self.cmesh)
-        self.row_terms_max = int(rl.max()) + 1 if nc else 1
-        per_cell = np.bincount(h.P, minlength=nc) + np.bincount(h.N, minlength=nc) + np.bincount(h.Pb, minlength=nc)
-        self.cell_faces_max = int(per_cell.max()) if nc else 1
+        self.row_terms_max = int(stats[0]) + 1 if nc else 1
+        self.cell_faces_max = int(stats[1]) if nc else 1
+
+    def boundary_normals_host(self):
+        """Unit outward normals of the boundary faces, (nb, dim), reference order."""
+        nbv = self._ref["nbv"]
+        return nbv.detach().cpu().numpy() if hasattr(nbv, "detach") else np.asarray(nbv)
 
     # ---- conversions between the reference's and the device's numbering ------------------------------
     def cells_to_device(self, a):
@@ -263,11 +429,14 @@ class FVMesh:
 
     def matrix_to_host(self, val):
         """CSR values of a device matrix -> SciPy CSR in the reference's numbering."""
-        h = self.host
+        if not hasattr(self, "_ref_csr_host"):
+            ip, ix = self._ref_csr
+            self._ref_csr_host = (ip.cpu().numpy(), ix.cpu().numpy())
+        indptr, indices = self._ref_csr_host
         v = val.detach().double().cpu().numpy()
-        data = np.empty(h.nnz)
+        data = np.empty(self.nnz)
         data[self.slot_ref] = v
-        return sp.csr_matrix((data, h.indices, h.indptr), shape=(h.nc, h.nc))
+        return sp.csr_matrix((data, indices, indptr), shape=(self.nc, self.nc))
 
     # ---- operators (device in, device out), mirroring flowtrace.unstructured.fvmesh.FVMesh ------------
     def _stream(self):

@@ -208,8 +208,8 @@ class SimpleSolver:
     def _build_boundaries(self):
         """Boundary kinds, fixed values and masks (``flowtrace/unstructured/simple.py:185-240``)."""
         fv, case, dim = self.fv, self.case, self.dim
-        h = fv.host
-        n = h.n_bf
+        n = fv.n_bf
+        normals = None
         kind = np.zeros(n, dtype=np.int64)
         ub = np.zeros((n, dim))
         pb = np.zeros(n)
@@ -223,7 +223,7 @@ class SimpleSolver:
                 if spec.kind == "inlet":
                     spec.normal_speed = 1.0
             self.zone_specs[z.name] = spec
-            m = h.bzone == z.id
+            m = fv.bzone == z.id
             if spec.kind == "periodic" or z.type in ("periodic", "periodic-shadow"):
                 if m.any():
                     raise ValueError(f"zone {z.name!r} is periodic but not paired")
@@ -235,7 +235,9 @@ class SimpleSolver:
                 if spec.velocity is not None:
                     ub[m] = (list(spec.velocity) + [0.0, 0.0, 0.0])[:dim]
                 elif spec.normal_speed is not None:
-                    ub[m] = -spec.normal_speed * h.nb[m]
+                    if normals is None:
+                        normals = fv.boundary_normals_host()
+                    ub[m] = -spec.normal_speed * normals[m]
             pb[m] = spec.pressure
             if spec.kind == "wall":
                 tk[m] = {"adiabatic": T_ADIABATIC, "temperature": T_FIXED, "flux": T_FLUX}[spec.thermal]
@@ -321,37 +323,46 @@ class SimpleSolver:
 
     def _set_fields_host(self, U, p, T):
         """Fields from host arrays (reference numbering); face fluxes rebuilt from U
-        (``flowtrace/unstructured/simple.py:110-112,157-159``)."""
+        (``flowtrace/unstructured/simple.py:110-112,157-159``) on the device, with the
+        reference's operations in its order: F = rho sum_k (w U_P + (1 - w) U_N)_k S_k,
+        Fb = rho sum_k ub_k Sb_k on inlets and outlets, ub the velocity boundary values
+        (fixed on walls and inlets, the tangential part of U_P on symmetry planes, U_P on
+        outlets)."""
         import torch
 
-        fv, h = self.fv, self.fv.host
+        fv = self.fv
         c = self._cur
         self._Up[c][0].copy_(fv.cells_to_device(p))
         self._Up[c][1:].copy_(fv.cells_to_device(U))
         if self.energy and T is not None:
             self._T[c].copy_(fv.cells_to_device(T))
-        Uf = h.w[:, None] * U[h.P] + (1.0 - h.w)[:, None] * U[h.N]
-        F = self.case.density * np.sum(Uf * h.S, axis=1)
-        ub = self._velocity_bvals_host(U)
-        Fb = self._boundary_flux_fixed_host(ub)
-        if h.n_if:
-            self._F[c][: h.n_if].copy_(fv.faces_to_device(F))
-        if h.n_bf:
-            self._Fb[c][: h.n_bf].copy_(fv.bfaces_to_device(Fb))
+        Ud = self._Up[c][1:]
+        t, rho, dim = fv.t, self.case.density, self.dim
+        if fv.n_if:
+            w, fP, fN = t["w"], t["fP"].long(), t["fN"].long()
+            acc = None
+            for k in range(dim):
+                uf = w * Ud[k][fP] + (1.0 - w) * Ud[k][fN]
+                term = uf * t["S"][k]
+                acc = term if acc is None else acc + term
+            self._F[c][: fv.n_if].copy_(rho * acc)
+        if fv.n_bf:
+            bc, bP = self._bc_t, t["bP"].long()
+            UP = [Ud[k][bP] for k in range(dim)]
+            nb = t["nbv"]
+            un = None
+            for k in range(dim):
+                term = UP[k] * nb[k]
+                un = term if un is None else un + term
+            fixed = bc["m_wall"] + bc["m_inlet"]
+            flux = None
+            for k in range(dim):
+                ubk = (fixed * bc["ub_fixed"][k] + bc["m_sym"] * (UP[k] - un * nb[k])) + bc["m_pres"] * UP[k]
+                term = ubk * t["Sb"][k]
+                flux = term if flux is None else flux + term
+            self._Fb[c][: fv.n_bf].copy_((rho * flux) * (bc["m_inlet"] + bc["m_pres"]))
         self._lag = self._lagT = False
         torch.cuda.current_stream().synchronize()
-
-    def _velocity_bvals_host(self, U):
-        h = self.fv.host
-        UP = U[h.Pb]
-        un = np.sum(UP * h.nb, axis=1)
-        sym = UP - un[:, None] * h.nb
-        fixed = (self.m_wall_h + self.m_inlet_h)[:, None]
-        return fixed * self._ub_fixed_h + self.m_sym_h[:, None] * sym + self.m_pres_h[:, None] * UP
-
-    def _boundary_flux_fixed_host(self, ub):
-        flux = self.case.density * np.sum(ub * self.fv.host.Sb, axis=1)
-        return flux * (self.m_inlet_h + self.m_pres_h)
 
     # ------------------------------------------------------------------ public state
     @property

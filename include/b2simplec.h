@@ -109,6 +109,44 @@ B2S_API int b2s_abi_version(void);
 /* Number of multiprocessors of the current device (0 without a device). */
 B2S_API int b2s_device_sm_count(void);
 
+/* Device set-up of the finite-volume data from the raw mesh, in the reference's numbering and
+ * operation order (replaces the host set-up of flowtrace/mesh/unstructured.py:171-261 and
+ * flowtrace/unstructured/fvmesh.py:61-230). Points and vectors are row-major [n][dim].
+ *
+ * b2s_face_geometry_d: face centres fc and area vectors S of nf faces (face_ptr/face_nodes: the
+ * nodes of face f are face_nodes[face_ptr[f] .. face_ptr[f+1]-1]); *bad counts faces with a
+ * node count the dimension does not allow (2-D: 2; 3-D: 3..32).
+ *
+ * b2s_cell_geometry_d: cell volumes and centroids by the pyramid decomposition about the mean
+ * of the face centres (ca), after turning every S to point away from its owner; own_ptr/own:
+ * the faces each cell owns, nei_ptr/nei: the interior faces whose neighbour it is, each list in
+ * increasing face index. counts[2]: faces turned, cells of non-positive volume.
+ *
+ * b2s_fv_faces_d: the interior-face quantities (if_idx: the interior faces in increasing index,
+ * P/N their cells) d, w, alpha, wl = 1/|d|^2, T = S - alpha d, dPf, dNf, dxm, and the
+ * boundary-face quantities (bf_idx, Pb) db, alpha_b, wlb, |Sb|, unit normal, tangential part of
+ * db and wall distance |db.Sb|/|Sb|; *cos_min the smallest cosine between S and d.
+ *
+ * b2s_ls_matrices_d: the least-squares matrices G (the cell's interior faces as owner, as
+ * neighbour and its boundary faces, summed family by family) and their inverses (LU with
+ * partial pivoting); flag[c] = 1 where G is singular (|det| <= 1e-300) or the inverse not
+ * finite: the caller substitutes the pseudo-inverse there, as the reference does. */
+B2S_API int b2s_face_geometry_d(int32_t dim, int32_t nf, const double* nodes, const int32_t* face_ptr,
+                                const int32_t* face_nodes, double* fc, double* S, int32_t* bad, b2s_stream_t s);
+B2S_API int b2s_cell_geometry_d(int32_t dim, int32_t nc, int32_t nf, const int32_t* owner, const int32_t* neighbour,
+                                const int32_t* own_ptr, const int32_t* own, const int32_t* nei_ptr, const int32_t* nei,
+                                const double* fc, double* S, double* ca, double* vol, double* xc, int32_t* counts,
+                                b2s_stream_t s);
+B2S_API int b2s_fv_faces_d(int32_t dim, int32_t n_if, const int32_t* if_idx, const int32_t* P, const int32_t* N,
+                           int32_t n_bf, const int32_t* bf_idx, const int32_t* Pb, const double* xc, const double* fc,
+                           const double* S, double* d, double* w, double* alpha, double* wl, double* Tv, double* dPf,
+                           double* dNf, double* dxm, double* db, double* alpha_b, double* wlb, double* Sb_mag,
+                           double* nb, double* db_t, double* yb, double* cos_min, b2s_stream_t s);
+B2S_API int b2s_ls_matrices_d(int32_t dim, int32_t nc, const int32_t* pi_ptr, const int32_t* pi,
+                              const int32_t* ni_ptr, const int32_t* ni, const int32_t* pb_ptr, const int32_t* pb,
+                              const double* d, const double* wl, const double* db, const double* wlb, double* G,
+                              double* Ginv, int32_t* flag, b2s_stream_t s);
+
 /* out[c][f] = w[f] phi[c][P] + (1 - w[f]) phi[c][N] for k components.
  * Replaces ft_face_interp (flowtrace/native/fvm_kernels.h:34-36). */
 B2S_API int b2s_face_interp_d(const b2s_mesh* m, int k, const double* phi, double* out, b2s_stream_t s);
