@@ -102,6 +102,8 @@ _SIGS = {
     "b2s_energy_bvals_d": ([P, P, P, P, P, P, P], ctypes.c_int),
     "b2s_energy_assemble_d": ([P, P, F64, F64, F64, ctypes.c_int] + [P] * 12 + [P], ctypes.c_int),
     "b2s_face_geometry_d": ([I32, I32, P, P, P, P, P, P, P], ctypes.c_int),
+    "b2s_host_geometry": ([I32, I32, I32, P, P, P, P, P, I32, P, P, P, P, P], ctypes.c_int),
+    "b2s_host_face_geometry": ([I32, I32, P, P, P, P, P], ctypes.c_int),
     "b2s_cell_geometry_d": ([I32, I32, I32] + [P] * 12 + [P], ctypes.c_int),
     "b2s_fv_faces_d": ([I32, I32, P, P, P, I32, P, P] + [P] * 19 + [P], ctypes.c_int),
     "b2s_ls_matrices_d": ([I32, I32] + [P] * 13 + [P], ctypes.c_int),

@@ -11,32 +11,34 @@
 // cell-centric kernels below walk a cell's face lists in that order: own[] holds the faces a
 // cell owns (interior and boundary, increasing index), nei[] the interior faces whose
 // neighbour it is. Arrays of points and vectors are row-major [n][dim], as in NumPy.
+#include <vector>
+
 #include "b2s_common.cuh"
 
 namespace b2s {
 
+#define B2S_HD __host__ __device__ __forceinline__
+
 // The per-row dot product of np.einsum("fd,fd->f", a, b) as NumPy evaluates it: a0 b0 + a1 b1
 // in 2-D, (a0 b0 + a2 b2) + a1 b1 in 3-D (its two-lane accumulation; checked against NumPy).
 template <int D>
-__device__ __forceinline__ double edot(const double* a, const double* b) {
+B2S_HD double edot(const double* a, const double* b) {
   if (D == 2) return a[0] * b[0] + a[1] * b[1];
   return (a[0] * b[0] + a[2] * b[2]) + a[1] * b[1];
 }
 
 // NumPy's sum of a short contiguous row (pairwise summation: sequential below 9 terms, eight
 // interleaved partial sums above).
-__device__ double numpy_row_sum(const double* a, int n) {
+B2S_HD double numpy_row_sum(const double* a, int n) {
   if (n < 8) {
     double s = 0.0;
     for (int i = 0; i < n; ++i) s += a[i];
     return s;
   }
   double r[8];
-#pragma unroll
   for (int j = 0; j < 8; ++j) r[j] = a[j];
   int i = 8;
   for (; i + 8 <= n; i += 8)
-#pragma unroll
     for (int j = 0; j < 8; ++j) r[j] += a[i + j];
   double s = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
   for (; i < n; ++i) s += a[i];
@@ -45,135 +47,162 @@ __device__ double numpy_row_sum(const double* a, int n) {
 
 constexpr int kMaxFaceNodes = 32;
 
-// Face centres and area vectors (unstructured.py:171-212). 2-D: the segment midpoint and
-// S = (e_y, -e_x). 3-D: the k-node face fanned into triangles about the node mean.
+// The geometry of one face, one cell, ... as functions of the item index, shared by the device
+// kernels (one thread per item) and the host loop of b2s_host_geometry.
+
+// Face centre and area vector of face f (unstructured.py:171-212). 2-D: the segment midpoint
+// and S = (e_y, -e_x). 3-D: the k-node face fanned into triangles about the node mean, the
+// centre the triangle centroids weighted by their areas projected on S. False when the face's
+// node count is not allowed (2-D: 2; 3-D: 3..32).
 template <int D>
-__global__ void face_geometry_k(int nf, const double* __restrict__ X, const int32_t* __restrict__ fptr,
-                                const int32_t* __restrict__ fnodes, double* __restrict__ fc, double* __restrict__ S,
-                                int32_t* __restrict__ bad) {
-  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
-    const int p0 = fptr[f], k = fptr[f + 1] - p0;
-    if (D == 2) {
-      if (k != 2) {
-        atomicAdd(bad, 1);
-        continue;
-      }
-      const double* a = X + 2 * (int64_t)fnodes[p0];
-      const double* b = X + 2 * (int64_t)fnodes[p0 + 1];
-      fc[2 * (int64_t)f] = 0.5 * (a[0] + b[0]);
-      fc[2 * (int64_t)f + 1] = 0.5 * (a[1] + b[1]);
-      const double ex = b[0] - a[0], ey = b[1] - a[1];
-      S[2 * (int64_t)f] = ey;
-      S[2 * (int64_t)f + 1] = -ex;
-    } else {
-      if (k < 3 || k > kMaxFaceNodes) {
-        atomicAdd(bad, 1);
-        continue;
-      }
-      double mean[3] = {0.0, 0.0, 0.0};
-      for (int j = 0; j < k; ++j) {
-        const double* p = X + 3 * (int64_t)fnodes[p0 + j];
-        mean[0] = j ? mean[0] + p[0] : p[0];
-        mean[1] = j ? mean[1] + p[1] : p[1];
-        mean[2] = j ? mean[2] + p[2] : p[2];
-      }
-      mean[0] /= (double)k;
-      mean[1] /= (double)k;
-      mean[2] /= (double)k;
-      double tri[kMaxFaceNodes][3];
-      double Sk[3];
-      for (int j = 0; j < k; ++j) {
-        const double* p = X + 3 * (int64_t)fnodes[p0 + j];
-        const double* q = X + 3 * (int64_t)fnodes[p0 + (j + 1) % k];
-        const double a0 = p[0] - mean[0], a1 = p[1] - mean[1], a2 = p[2] - mean[2];
-        const double b0 = q[0] - mean[0], b1 = q[1] - mean[1], b2 = q[2] - mean[2];
-        tri[j][0] = 0.5 * (a1 * b2 - a2 * b1);
-        tri[j][1] = 0.5 * (a2 * b0 - a0 * b2);
-        tri[j][2] = 0.5 * (a0 * b1 - a1 * b0);
-        for (int c = 0; c < 3; ++c) Sk[c] = j ? Sk[c] + tri[j][c] : tri[j][c];
-      }
-      const double nrm = sqrt(((0.0 + Sk[0] * Sk[0]) + Sk[1] * Sk[1]) + Sk[2] * Sk[2]);
-      const double den = fmax(nrm, 1e-300);
-      const double u[3] = {Sk[0] / den, Sk[1] / den, Sk[2] / den};
-      double wt[kMaxFaceNodes];
-      double acc[3] = {0.0, 0.0, 0.0};
-      for (int j = 0; j < k; ++j) {
-        const double* p = X + 3 * (int64_t)fnodes[p0 + j];
-        const double* q = X + 3 * (int64_t)fnodes[p0 + (j + 1) % k];
-        wt[j] = edot<3>(tri[j], u);
-        for (int c = 0; c < 3; ++c) {
-          const double cen = ((mean[c] + p[c]) + q[c]) / 3.0;
-          const double t = wt[j] * cen;
-          acc[c] = j ? acc[c] + t : t;
-        }
-      }
-      double wsum = numpy_row_sum(wt, k);
-      if (!(fabs(wsum) > 0.0)) wsum = 1.0;
-      for (int c = 0; c < 3; ++c) {
-        fc[3 * (int64_t)f + c] = acc[c] / wsum;
-        S[3 * (int64_t)f + c] = Sk[c];
-      }
+B2S_HD bool face_geometry(int64_t f, const double* X, const int32_t* fptr, const int32_t* fnodes, double* fc,
+                          double* S) {
+  const int p0 = fptr[f], k = fptr[f + 1] - p0;
+  if (D == 2) {
+    if (k != 2) return false;
+    const double* a = X + 2 * (int64_t)fnodes[p0];
+    const double* b = X + 2 * (int64_t)fnodes[p0 + 1];
+    fc[2 * f] = 0.5 * (a[0] + b[0]);
+    fc[2 * f + 1] = 0.5 * (a[1] + b[1]);
+    const double ex = b[0] - a[0], ey = b[1] - a[1];
+    S[2 * f] = ey;
+    S[2 * f + 1] = -ex;
+    return true;
+  }
+  if (k < 3 || k > kMaxFaceNodes) return false;
+  double mean[3];
+  for (int j = 0; j < k; ++j) {
+    const double* p = X + 3 * (int64_t)fnodes[p0 + j];
+    for (int c = 0; c < 3; ++c) mean[c] = j ? mean[c] + p[c] : p[c];
+  }
+  for (int c = 0; c < 3; ++c) mean[c] /= (double)k;
+  double tri[kMaxFaceNodes][3], Sk[3];
+  for (int j = 0; j < k; ++j) {
+    const double* p = X + 3 * (int64_t)fnodes[p0 + j];
+    const double* q = X + 3 * (int64_t)fnodes[p0 + (j + 1) % k];
+    const double a0 = p[0] - mean[0], a1 = p[1] - mean[1], a2 = p[2] - mean[2];
+    const double b0 = q[0] - mean[0], b1 = q[1] - mean[1], b2 = q[2] - mean[2];
+    tri[j][0] = 0.5 * (a1 * b2 - a2 * b1);
+    tri[j][1] = 0.5 * (a2 * b0 - a0 * b2);
+    tri[j][2] = 0.5 * (a0 * b1 - a1 * b0);
+    for (int c = 0; c < 3; ++c) Sk[c] = j ? Sk[c] + tri[j][c] : tri[j][c];
+  }
+  const double den = fmax(sqrt((Sk[0] * Sk[0] + Sk[1] * Sk[1]) + Sk[2] * Sk[2]), 1e-300);
+  const double u[3] = {Sk[0] / den, Sk[1] / den, Sk[2] / den};
+  double wt[kMaxFaceNodes], acc[3];
+  for (int j = 0; j < k; ++j) {
+    const double* p = X + 3 * (int64_t)fnodes[p0 + j];
+    const double* q = X + 3 * (int64_t)fnodes[p0 + (j + 1) % k];
+    wt[j] = edot<3>(tri[j], u);
+    for (int c = 0; c < 3; ++c) {
+      const double t = wt[j] * (((mean[c] + p[c]) + q[c]) / 3.0);
+      acc[c] = j ? acc[c] + t : t;
     }
   }
-}
-
-// Approximate centres: the mean of the face centres (owned faces, then neighbour faces).
-template <int D>
-__global__ void centre_estimate_k(int nc, const int32_t* __restrict__ own_ptr, const int32_t* __restrict__ own,
-                                  const int32_t* __restrict__ nei_ptr, const int32_t* __restrict__ nei,
-                                  const double* __restrict__ fc, double* __restrict__ ca) {
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-    double so[D], sn[D];
-#pragma unroll
-    for (int a = 0; a < D; ++a) so[a] = sn[a] = 0.0;
-    for (int q = own_ptr[c]; q < own_ptr[c + 1]; ++q)
-#pragma unroll
-      for (int a = 0; a < D; ++a) so[a] += fc[D * (int64_t)own[q] + a];
-    for (int q = nei_ptr[c]; q < nei_ptr[c + 1]; ++q)
-#pragma unroll
-      for (int a = 0; a < D; ++a) sn[a] += fc[D * (int64_t)nei[q] + a];
-    const int cnt = (own_ptr[c + 1] - own_ptr[c]) + (nei_ptr[c + 1] - nei_ptr[c]);
-    const double den = (double)(cnt > 1 ? cnt : 1);
-#pragma unroll
-    for (int a = 0; a < D; ++a) ca[D * (int64_t)c + a] = (so[a] + sn[a]) / den;
+  double wsum = numpy_row_sum(wt, k);
+  if (!(fabs(wsum) > 0.0)) wsum = 1.0;
+  for (int c = 0; c < 3; ++c) {
+    fc[3 * f + c] = acc[c] / wsum;
+    S[3 * f + c] = Sk[c];
   }
+  return true;
 }
 
-// Orientation repair: S points from the owner to the neighbour (to the face, on the boundary).
+// Approximate centre of cell c: the mean of its face centres (owned faces, then neighbour faces).
 template <int D>
-__global__ void orient_k(int nf, const int32_t* __restrict__ owner, const int32_t* __restrict__ neighbour,
-                         const double* __restrict__ fc, const double* __restrict__ ca, double* __restrict__ S,
-                         int32_t* __restrict__ flipped) {
-  int local = 0;
-  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
-    const int o = owner[f], n = neighbour[f];
-    double ref[D];
-#pragma unroll
-    for (int a = 0; a < D; ++a)
-      ref[a] = n >= 0 ? ca[D * (int64_t)n + a] - ca[D * (int64_t)o + a] : fc[D * (int64_t)f + a] - ca[D * (int64_t)o + a];
-    if (edot<D>(S + D * (int64_t)f, ref) < 0.0) {
-#pragma unroll
-      for (int a = 0; a < D; ++a) S[D * (int64_t)f + a] *= -1.0;
-      ++local;
-    }
-  }
-  if (local) atomicAdd(flipped, local);
+B2S_HD void centre_estimate(int64_t c, const int32_t* own_ptr, const int32_t* own, const int32_t* nei_ptr,
+                            const int32_t* nei, const double* fc, double* ca) {
+  double so[D], sn[D];
+  for (int a = 0; a < D; ++a) so[a] = sn[a] = 0.0;
+  for (int q = own_ptr[c]; q < own_ptr[c + 1]; ++q)
+    for (int a = 0; a < D; ++a) so[a] += fc[D * (int64_t)own[q] + a];
+  for (int q = nei_ptr[c]; q < nei_ptr[c + 1]; ++q)
+    for (int a = 0; a < D; ++a) sn[a] += fc[D * (int64_t)nei[q] + a];
+  const int cnt = (own_ptr[c + 1] - own_ptr[c]) + (nei_ptr[c + 1] - nei_ptr[c]);
+  const double den = (double)(cnt > 1 ? cnt : 1);
+  for (int a = 0; a < D; ++a) ca[D * c + a] = (so[a] + sn[a]) / den;
 }
 
-// Pyramid volumes and centroids: the owned faces' pyramids, then the neighbour faces'.
+// Orientation repair of face f: S must point from the owner towards the neighbour (towards the
+// face, on the boundary). True when S was turned.
 template <int D>
-__device__ __forceinline__ void pyramid(const double* fcf, const double* Sf, double sign, const double* cac,
-                                        double& v, double (&vc)[D]) {
+B2S_HD bool orient(int64_t f, const int32_t* owner, const int32_t* neighbour, const double* fc, const double* ca,
+                   double* S) {
+  const int o = owner[f], n = neighbour[f];
+  double ref[D];
+  for (int a = 0; a < D; ++a)
+    ref[a] = n >= 0 ? ca[D * (int64_t)n + a] - ca[D * (int64_t)o + a] : fc[D * f + a] - ca[D * (int64_t)o + a];
+  if (!(edot<D>(S + D * f, ref) < 0.0)) return false;
+  for (int a = 0; a < D; ++a) S[D * f + a] *= -1.0;
+  return true;
+}
+
+// The pyramid of a face over the cell's approximate centre: volume v and v times its centroid.
+template <int D>
+B2S_HD void pyramid(const double* fcf, const double* Sf, double sign, const double* cac, double& v, double* vc) {
   double h[D], ss[D];
-#pragma unroll
   for (int a = 0; a < D; ++a) {
     h[a] = fcf[a] - cac[a];
     ss[a] = Sf[a] * sign;
   }
   v = edot<D>(ss, h) / (double)D;
   const double frac = D == 2 ? 2.0 / 3.0 : 0.75;
-#pragma unroll
   for (int a = 0; a < D; ++a) vc[a] = v * (cac[a] + frac * h[a]);
+}
+
+// Volume and centroid of cell c from its pyramids: owned faces, then neighbour faces. False
+// when the volume is not positive.
+template <int D>
+B2S_HD bool cell_volume(int64_t c, const int32_t* own_ptr, const int32_t* own, const int32_t* nei_ptr,
+                        const int32_t* nei, const double* fc, const double* S, const double* ca, double* vol,
+                        double* xc) {
+  const double* cac = ca + D * c;
+  double vo = 0.0, vn = 0.0, mo[D], mn[D], v, vc[D];
+  for (int a = 0; a < D; ++a) mo[a] = mn[a] = 0.0;
+  for (int q = own_ptr[c]; q < own_ptr[c + 1]; ++q) {
+    const int64_t f = own[q];
+    pyramid<D>(fc + D * f, S + D * f, 1.0, cac, v, vc);
+    vo += v;
+    for (int a = 0; a < D; ++a) mo[a] += vc[a];
+  }
+  for (int q = nei_ptr[c]; q < nei_ptr[c + 1]; ++q) {
+    const int64_t f = nei[q];
+    pyramid<D>(fc + D * f, S + D * f, -1.0, cac, v, vc);
+    vn += v;
+    for (int a = 0; a < D; ++a) mn[a] += vc[a];
+  }
+  const double V = vo + vn;
+  vol[c] = V;
+  for (int a = 0; a < D; ++a) xc[D * c + a] = (mo[a] + mn[a]) / V;
+  return V > 0.0;
+}
+
+template <int D>
+__global__ void face_geometry_k(int nf, const double* __restrict__ X, const int32_t* __restrict__ fptr,
+                                const int32_t* __restrict__ fnodes, double* __restrict__ fc, double* __restrict__ S,
+                                int32_t* __restrict__ bad) {
+  int local = 0;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x)
+    local += face_geometry<D>(f, X, fptr, fnodes, fc, S) ? 0 : 1;
+  if (local) atomicAdd(bad, local);
+}
+
+template <int D>
+__global__ void centre_estimate_k(int nc, const int32_t* __restrict__ own_ptr, const int32_t* __restrict__ own,
+                                  const int32_t* __restrict__ nei_ptr, const int32_t* __restrict__ nei,
+                                  const double* __restrict__ fc, double* __restrict__ ca) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    centre_estimate<D>(c, own_ptr, own, nei_ptr, nei, fc, ca);
+}
+
+template <int D>
+__global__ void orient_k(int nf, const int32_t* __restrict__ owner, const int32_t* __restrict__ neighbour,
+                         const double* __restrict__ fc, const double* __restrict__ ca, double* __restrict__ S,
+                         int32_t* __restrict__ flipped) {
+  int local = 0;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x)
+    local += orient<D>(f, owner, neighbour, fc, ca, S) ? 1 : 0;
+  if (local) atomicAdd(flipped, local);
 }
 
 template <int D>
@@ -183,33 +212,8 @@ __global__ void cell_volumes_k(int nc, const int32_t* __restrict__ own_ptr, cons
                                const double* __restrict__ ca, double* __restrict__ vol, double* __restrict__ xc,
                                int32_t* __restrict__ nonpos) {
   int local = 0;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-    const double* cac = ca + D * (int64_t)c;
-    double vo = 0.0, vn = 0.0, mo[D], mn[D];
-#pragma unroll
-    for (int a = 0; a < D; ++a) mo[a] = mn[a] = 0.0;
-    for (int q = own_ptr[c]; q < own_ptr[c + 1]; ++q) {
-      const int f = own[q];
-      double v, vc[D];
-      pyramid<D>(fc + D * (int64_t)f, S + D * (int64_t)f, 1.0, cac, v, vc);
-      vo += v;
-#pragma unroll
-      for (int a = 0; a < D; ++a) mo[a] += vc[a];
-    }
-    for (int q = nei_ptr[c]; q < nei_ptr[c + 1]; ++q) {
-      const int f = nei[q];
-      double v, vc[D];
-      pyramid<D>(fc + D * (int64_t)f, S + D * (int64_t)f, -1.0, cac, v, vc);
-      vn += v;
-#pragma unroll
-      for (int a = 0; a < D; ++a) mn[a] += vc[a];
-    }
-    const double V = vo + vn;
-    vol[c] = V;
-#pragma unroll
-    for (int a = 0; a < D; ++a) xc[D * (int64_t)c + a] = (mo[a] + mn[a]) / V;
-    if (!(V > 0.0)) ++local;
-  }
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    local += cell_volume<D>(c, own_ptr, own, nei_ptr, nei, fc, S, ca, vol, xc) ? 0 : 1;
   if (local) atomicAdd(nonpos, local);
 }
 
@@ -495,6 +499,79 @@ int b2s_ls_matrices_d(int32_t dim, int32_t nc, const int32_t* pi_ptr, const int3
     ls_matrices_k<3><<<grid_for(nc), kThreads, 0, st>>>(nc, pi_ptr, pi, ni_ptr, ni, pb_ptr, pb, d, wl, db, wlb, G, Ginv,
                                                         flag);
   B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+/* Host counterpart of b2s_face_geometry_d (host pointers): the number of faces whose node count
+ * the dimension does not allow, or B2S_ERR_ARG. */
+int b2s_host_face_geometry(int32_t dim, int32_t nf, const double* nodes, const int32_t* face_ptr,
+                           const int32_t* face_nodes, double* fc, double* S) {
+  if ((dim != 2 && dim != 3) || nf < 0 || (nf > 0 && (!nodes || !face_ptr || !face_nodes || !fc || !S)))
+    return B2S_ERR_ARG;
+  int bad = 0;
+  for (int64_t f = 0; f < nf; ++f) {
+    const bool ok = dim == 2 ? face_geometry<2>(f, nodes, face_ptr, face_nodes, fc, S)
+                             : face_geometry<3>(f, nodes, face_ptr, face_nodes, fc, S);
+    if (!ok) ++bad;
+  }
+  return bad;
+}
+
+/* Host counterpart of b2s_face_geometry_d + b2s_cell_geometry_d (the same per-face and per-cell
+ * code, run in loops): the geometry of flowtrace/mesh/unstructured.py:171-261 for host callers
+ * (tests without a device, reports). repair != 0 turns the area vectors away from their owners;
+ * counts[3]: faces with a node count the dimension does not allow, faces turned, cells of
+ * non-positive volume. Returns B2S_OK or B2S_ERR_ARG. */
+int b2s_host_geometry(int32_t dim, int32_t nc, int32_t nf, const double* nodes, const int32_t* face_ptr,
+                      const int32_t* face_nodes, const int32_t* owner, const int32_t* neighbour, int32_t repair,
+                      double* fc, double* S, double* xc, double* vol, int32_t* counts) {
+  if ((dim != 2 && dim != 3) || nc < 0 || nf < 0 || !counts ||
+      (nf > 0 && (!nodes || !face_ptr || !face_nodes || !owner || !neighbour || !fc || !S)) ||
+      (nc > 0 && (!xc || !vol)))
+    return B2S_ERR_ARG;
+  counts[0] = counts[1] = counts[2] = 0;
+  for (int64_t f = 0; f < nf; ++f)
+    if (owner[f] < 0 || owner[f] >= nc || neighbour[f] >= nc) return B2S_ERR_ARG;
+  // per-cell face lists in increasing face index (counting sort)
+  std::vector<int32_t> own_ptr(nc + 1, 0), nei_ptr(nc + 1, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    ++own_ptr[owner[f] + 1];
+    if (neighbour[f] >= 0) ++nei_ptr[neighbour[f] + 1];
+  }
+  for (int64_t c = 0; c < nc; ++c) {
+    own_ptr[c + 1] += own_ptr[c];
+    nei_ptr[c + 1] += nei_ptr[c];
+  }
+  std::vector<int32_t> own(own_ptr[nc]), nei(nei_ptr[nc]), po(own_ptr.begin(), own_ptr.end() - 1),
+      pn(nei_ptr.begin(), nei_ptr.end() - 1);
+  for (int64_t f = 0; f < nf; ++f) {
+    own[po[owner[f]]++] = (int32_t)f;
+    if (neighbour[f] >= 0) nei[pn[neighbour[f]]++] = (int32_t)f;
+  }
+  std::vector<double> ca((size_t)nc * dim);
+  const int32_t* op = own_ptr.data();
+  const int32_t* np_ = nei_ptr.data();
+  for (int64_t f = 0; f < nf; ++f) {
+    const bool ok = dim == 2 ? face_geometry<2>(f, nodes, face_ptr, face_nodes, fc, S)
+                             : face_geometry<3>(f, nodes, face_ptr, face_nodes, fc, S);
+    if (!ok) ++counts[0];
+  }
+  if (counts[0]) return B2S_OK;
+  for (int64_t c = 0; c < nc; ++c) {
+    if (dim == 2) centre_estimate<2>(c, op, own.data(), np_, nei.data(), fc, ca.data());
+    else centre_estimate<3>(c, op, own.data(), np_, nei.data(), fc, ca.data());
+  }
+  if (repair)
+    for (int64_t f = 0; f < nf; ++f) {
+      const bool t = dim == 2 ? orient<2>(f, owner, neighbour, fc, ca.data(), S)
+                              : orient<3>(f, owner, neighbour, fc, ca.data(), S);
+      if (t) ++counts[1];
+    }
+  for (int64_t c = 0; c < nc; ++c) {
+    const bool ok = dim == 2 ? cell_volume<2>(c, op, own.data(), np_, nei.data(), fc, S, ca.data(), vol, xc)
+                             : cell_volume<3>(c, op, own.data(), np_, nei.data(), fc, S, ca.data(), vol, xc);
+    if (!ok) ++counts[2];
+  }
   return B2S_OK;
 }
 

@@ -36,7 +36,7 @@ from typing import Dict, List, Tuple
 
 import numpy as np
 
-from .unstructured import BC_CODES, UnstructuredMesh, Zone, _face_centres_and_areas
+from .unstructured import BC_CODES, UnstructuredMesh, Zone, face_centres_and_areas
 
 _SPACE = b" \t\r\n\f\v"
 _DELIM = _SPACE + b"()"
@@ -370,7 +370,7 @@ def _parse(data: bytes, name: str) -> UnstructuredMesh:
                             owner=owner.astype(np.int64), neighbour=neighbour.astype(np.int64), face_zone=fzone,
                             n_cells=n_cells, cell_zone=cell_zone, zones=zones, name=name)
     if periodic:
-        fc, _ = _face_centres_and_areas(mesh)
+        fc, _ = face_centres_and_areas(mesh)
         for h, pairs in periodic:
             fa, fb = pairs[:, 0], pairs[:, 1]
             if fa.size == 0 or fa.max() >= mesh.n_faces or fb.max() >= mesh.n_faces:

@@ -145,91 +145,59 @@ class Geometry:
         return float(self.cell_volume.sum())
 
 
-_FACE_BLOCK = 1 << 19
+def _host_arrays(mesh: UnstructuredMesh):
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+    return (np.ascontiguousarray(mesh.nodes, dtype=np.float64), i32(mesh.face_ptr), i32(mesh.face_nodes))
 
 
-def _face_centres_and_areas(mesh: UnstructuredMesh):
-    """Face centres and area vectors (``flowtrace/mesh/unstructured.py:171-212``).
+def face_centres_and_areas(mesh: UnstructuredMesh):
+    """Face centres and area vectors (``flowtrace/mesh/unstructured.py:171-212``), by the library's
+    host loop over the same per-face code as the device set-up (``b2s_host_face_geometry``):
+    2-D, the segment midpoint and S = (n1 - n0) x z; 3-D, each face fanned into triangles about
+    its node mean, the centre the triangle centroids weighted by their areas projected on S."""
+    from .. import _lib
 
-    2-D: the segment midpoint and S = (n1 - n0) x z. 3-D: each k-node face is fanned into k
-    triangles about the node mean; S is the sum of the triangle area vectors and the centre
-    is the triangle-centroid mean weighted by the triangles' areas projected on S.
-    """
-    X = mesh.nodes
-    ptr, fn = mesh.face_ptr, mesh.face_nodes
+    X, fptr, fnodes = _host_arrays(mesh)
     nf = mesh.n_faces
-    dim = mesh.dim
-    if dim == 2:
-        if np.any(np.diff(ptr) != 2):
-            raise ValueError("2-D meshes must have 2-node faces")
-        a = X[fn[ptr[:-1]]]
-        b = X[fn[ptr[:-1] + 1]]
-        e = b - a
-        return 0.5 * (a + b), np.stack([e[:, 1], -e[:, 0]], axis=1)
-    fc = np.zeros((nf, 3))
-    S = np.zeros((nf, 3))
-    counts = np.diff(ptr)
-    for k in np.unique(counts):
-        faces_k = np.flatnonzero(counts == k)
-        for lo in range(0, faces_k.size, _FACE_BLOCK):
-            idx = faces_k[lo:lo + _FACE_BLOCK]
-            loop = fn[ptr[idx][:, None] + np.arange(k)[None, :]]
-            pts = X[loop]
-            mean = pts.mean(axis=1)
-            nxt = np.roll(pts, -1, axis=1)
-            tri = 0.5 * np.cross(pts - mean[:, None, :], nxt - mean[:, None, :])
-            Sk = tri.sum(axis=1)
-            unit = Sk / np.maximum(np.linalg.norm(Sk, axis=1, keepdims=True), 1e-300)
-            wt = np.einsum("mkd,md->mk", tri, unit)
-            cen = (mean[:, None, :] + pts + nxt) / 3.0
-            wsum = wt.sum(axis=1, keepdims=True)
-            fc[idx] = (wt[:, :, None] * cen).sum(axis=1) / np.where(np.abs(wsum) > 0, wsum, 1.0)
-            S[idx] = Sk
+    fc, S = np.empty((nf, mesh.dim)), np.empty((nf, mesh.dim))
+    bad = _lib.lib().b2s_host_face_geometry(mesh.dim, nf, X.ctypes.data, fptr.ctypes.data, fnodes.ctypes.data,
+                                            fc.ctypes.data, S.ctypes.data)
+    if bad < 0:
+        raise ValueError("invalid mesh arrays")
+    if bad:
+        raise ValueError("2-D meshes must have 2-node faces" if mesh.dim == 2 else
+                         "3-D faces must have 3 to 32 nodes")
     return fc, S
 
 
 def compute_geometry(mesh: UnstructuredMesh, repair: bool = True) -> Geometry:
-    """Cell volumes and centroids from a pyramid decomposition
-    (``flowtrace/mesh/unstructured.py:215-261``)."""
-    dim, nc = mesh.dim, mesh.n_cells
-    own, nei = mesh.owner, mesh.neighbour
-    inner = nei >= 0
-    fc, S = _face_centres_and_areas(mesh)
-    cnt = np.bincount(own, minlength=nc) + np.bincount(nei[inner], minlength=nc)
-    ca = np.zeros((nc, dim))
-    for a in range(dim):
-        ca[:, a] = np.bincount(own, fc[:, a], minlength=nc) + np.bincount(nei[inner], fc[inner, a], minlength=nc)
-    ca /= np.maximum(cnt, 1)[:, None]
-    flipped = 0
-    nf = own.size
-    if repair:
-        for lo in range(0, nf, _FACE_BLOCK):
-            sl = slice(lo, lo + _FACE_BLOCK)
-            o, n, it = own[sl], nei[sl], inner[sl]
-            ref = np.where(it[:, None], ca[np.where(it, n, 0)] - ca[o], fc[sl] - ca[o])
-            bad = np.einsum("fd,fd->f", S[sl], ref) < 0
-            flipped += int(bad.sum())
-            S[lo + np.flatnonzero(bad)] *= -1.0
-    vol = np.zeros(nc)
-    mom = np.zeros((nc, dim))
-    frac = 2.0 / 3.0 if dim == 2 else 0.75
-    for cells, sign, faces in ((own, 1.0, None), (nei[inner], -1.0, np.flatnonzero(inner))):
-        m = cells.size
-        v = np.empty(m)
-        vc = np.empty((dim, m))
-        for lo in range(0, m, _FACE_BLOCK):
-            sl = slice(lo, lo + _FACE_BLOCK)
-            f = sl if faces is None else faces[sl]
-            h = fc[f] - ca[cells[sl]]
-            v[sl] = np.einsum("fd,fd->f", S[f] * sign, h) / dim
-            vc[:, sl] = (v[sl][:, None] * (ca[cells[sl]] + frac * h)).T
-        vol += np.bincount(cells, v, minlength=nc)
-        for a in range(dim):
-            mom[:, a] += np.bincount(cells, vc[a], minlength=nc)
-    if np.any(vol <= 0):
-        raise ValueError(f"{int((vol <= 0).sum())} cells have non-positive volume")
-    return Geometry(face_centre=fc, face_area_vec=S, face_area=np.linalg.norm(S, axis=1),
-                    cell_centre=mom / vol[:, None], cell_volume=vol, flipped_faces=flipped)
+    """Face, cell and volume geometry (``flowtrace/mesh/unstructured.py:171-261``) by the library's
+    host loops over the per-face and per-cell code of the device set-up (``b2s_host_geometry``):
+    face centres and areas, approximate cell centres (the mean of the face centres), the
+    orientation repair (``repair``: every S turned to point away from its owner) and cell volumes
+    and centroids from the pyramids of the faces over the approximate centres, each cell's sums
+    taken over its owned and then its neighbour faces in face order, as the reference's
+    ``np.bincount`` sums."""
+    from .. import _lib
+
+    X, fptr, fnodes = _host_arrays(mesh)
+    nf, nc, dim = mesh.n_faces, mesh.n_cells, mesh.dim
+    own = np.ascontiguousarray(mesh.owner, dtype=np.int32)
+    nei = np.ascontiguousarray(mesh.neighbour, dtype=np.int32)
+    fc, S = np.empty((nf, dim)), np.empty((nf, dim))
+    xc, vol = np.empty((nc, dim)), np.empty(nc)
+    cnt = np.zeros(3, dtype=np.int32)
+    rc = _lib.lib().b2s_host_geometry(dim, nc, nf, X.ctypes.data, fptr.ctypes.data, fnodes.ctypes.data,
+                                      own.ctypes.data, nei.ctypes.data, int(bool(repair)), fc.ctypes.data,
+                                      S.ctypes.data, xc.ctypes.data, vol.ctypes.data, cnt.ctypes.data)
+    if rc != 0:
+        raise ValueError("invalid mesh arrays")
+    if cnt[0]:
+        raise ValueError("2-D meshes must have 2-node faces" if dim == 2 else "3-D faces must have 3 to 32 nodes")
+    if cnt[2]:
+        raise ValueError(f"{int(cnt[2])} cells have non-positive volume")
+    return Geometry(face_centre=fc, face_area_vec=S, face_area=np.linalg.norm(S, axis=1), cell_centre=xc,
+                    cell_volume=vol, flipped_faces=int(cnt[1]))
 
 
 # ----------------------------------------------------------------------------------------------

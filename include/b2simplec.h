@@ -142,6 +142,15 @@ B2S_API int b2s_fv_faces_d(int32_t dim, int32_t n_if, const int32_t* if_idx, con
                            const double* S, double* d, double* w, double* alpha, double* wl, double* Tv, double* dPf,
                            double* dNf, double* dxm, double* db, double* alpha_b, double* wlb, double* Sb_mag,
                            double* nb, double* db_t, double* yb, double* cos_min, b2s_stream_t s);
+/* Host counterpart of the two geometry calls above (the same per-face and per-cell code in host
+ * loops; every pointer a HOST pointer): fc, S [nf][dim], xc [nc][dim], vol [nc]; repair != 0
+ * turns area vectors away from their owners; counts[3]: faces of a node count the dimension does
+ * not allow (nothing else is computed then), faces turned, cells of non-positive volume. */
+B2S_API int b2s_host_face_geometry(int32_t dim, int32_t nf, const double* nodes, const int32_t* face_ptr,
+                                   const int32_t* face_nodes, double* fc, double* S);
+B2S_API int b2s_host_geometry(int32_t dim, int32_t nc, int32_t nf, const double* nodes, const int32_t* face_ptr,
+                              const int32_t* face_nodes, const int32_t* owner, const int32_t* neighbour,
+                              int32_t repair, double* fc, double* S, double* xc, double* vol, int32_t* counts);
 B2S_API int b2s_ls_matrices_d(int32_t dim, int32_t nc, const int32_t* pi_ptr, const int32_t* pi,
                               const int32_t* ni_ptr, const int32_t* ni, const int32_t* pb_ptr, const int32_t* pb,
                               const double* d, const double* wl, const double* db, const double* wlb, double* G,
