@@ -70,7 +70,7 @@ def make_workload(name):
 
         def inlet(solver):
             z = mesh.zone_by_name("inlet")
-            fc = solver.fv.host.xfb[solver.fv.host.bzone == z.id]
+            fc = solver.fv.boundary_centres_host()[solver.fv.bzone == z.id]
             u = 36.0 * fc[:, 1] * (1 - fc[:, 1]) * fc[:, 2] * (1 - fc[:, 2])
             solver.set_boundary_velocity("inlet", np.stack([u, 0 * u, 0 * u], axis=1))
             solver.initialize({})

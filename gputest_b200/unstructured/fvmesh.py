@@ -167,7 +167,7 @@ class FVMesh:
         self.h2d_bytes = 8 * sum(np.asarray(a).size for a in (h.w, h.alpha, h.wl, h.S, h.d, h.Tvec, h.dxm, h.dP_f,
                                                               h.dN_f, h.alpha_b, h.wlb, h.Sb_mag, h.Sb, h.db, h.nb,
                                                               h.db_t, h.vol, h.Ginv))
-        return {"dim": h.dim, "nc": h.nc, "P": h.P, "N": h.N, "Pb": h.Pb, "bzone": h.bzone,
+        return {"dim": h.dim, "nc": h.nc, "P": h.P, "N": h.N, "Pb": h.Pb, "bzone": h.bzone, "xfb": h.xfb,
                 "non_orthogonality_deg": h.non_orthogonality_deg,
                 "w": T(h.w), "alpha": T(h.alpha), "wl": T(h.wl), "S": T(h.S), "d": T(h.d), "Tv": T(h.Tvec),
                 "dxm": T(h.dxm), "dPf": T(h.dP_f), "dNf": T(h.dN_f), "alpha_b": T(h.alpha_b), "wlb": T(h.wlb),
@@ -258,7 +258,7 @@ class FVMesh:
                 "w": o["w"][:n_if], "alpha": o["alpha"][:n_if], "wl": o["wl"][:n_if], "S": Sif, "d": o["d"],
                 "Tv": o["Tv"], "dxm": o["dxm"], "dPf": o["dPf"], "dNf": o["dNf"], "alpha_b": o["alpha_b"][:n_bf],
                 "wlb": o["wlb"][:n_bf], "Sb_mag": o["Sb_mag"][:n_bf], "Sb": Sbf, "db": o["db"], "nbv": o["nbv"],
-                "dbt": o["dbt"], "vol": vol, "Ginv": Ginv, "xc": xc, "yb": o["yb"][:n_bf]}
+                "dbt": o["dbt"], "vol": vol, "Ginv": Ginv, "xc": xc, "yb": o["yb"][:n_bf], "xfb": fc[bf_t.long()]}
 
     def _layout(self, r, reorder, groups):
         """The device layout (module docstring) of reference-numbered quantities ``r``: the cell
@@ -367,6 +367,11 @@ class FVMesh:
         self.cmesh_ref = ctypes.byref(self.cmesh)
         self.row_terms_max = int(stats[0]) + 1 if nc else 1
         self.cell_faces_max = int(stats[1]) if nc else 1
+
+    def boundary_centres_host(self):
+        """Boundary-face centres, (nb, dim), reference order."""
+        x = self._ref["xfb"]
+        return x.detach().cpu().numpy() if hasattr(x, "detach") else np.asarray(x)
 
     def boundary_normals_host(self):
         """Unit outward normals of the boundary faces, (nb, dim), reference order."""

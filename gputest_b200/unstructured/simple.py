@@ -402,7 +402,7 @@ class SimpleSolver:
         z = self.mesh.zone_by_name(zone)
         if z is None:
             raise ValueError(f"unknown zone {zone!r}")
-        m = self.fv.host.bzone == z.id
+        m = self.fv.bzone == z.id
         if not np.all((self.bkind_h[m] == WALL) | (self.bkind_h[m] == INLET)):
             raise ValueError(f"zone {zone!r} is not a wall or an inlet")
         ub = self._ub_fixed_h.copy()
@@ -1005,7 +1005,7 @@ class SimpleSolver:
         Fb = self.Fb
         out = {}
         for z in self.mesh.boundary_zones():
-            m = self.fv.host.bzone == z.id
+            m = self.fv.bzone == z.id
             if m.any():
                 out[z.name] = float(Fb[m].sum())
         return out
