@@ -32,7 +32,7 @@ import numpy as np
 
 from .. import _lib
 from ..linalg.amg import AMGHierarchy
-from ..linalg.krylov import INFO_DTYPE, read_info
+from ..linalg.krylov import INFO_DTYPE
 from ..mesh.unstructured import UnstructuredMesh, union_groups, union_mesh
 from .case import UnstructuredCase
 from .mixed import MixedSimpleSolver
@@ -207,12 +207,17 @@ class BatchSimpleSolver(MixedSimpleSolver):
 
     def _snapshot_cases(self, cases):
         c = self._cur
+        self._snap_it[cases] = self.iteration
+        if len(cases) == self.ncase:  # every case: whole-array copies
+            self._snap_Up.copy_(self._Up[c])
+            self._snap_F.copy_(self._F[c])
+            self._snap_Fb.copy_(self._Fb[c])
+            return
         for g in cases:
             (a, b), (fa, fb), (ba, bb) = self._case_slices(g)
             self._snap_Up[:, a:b] = self._Up[c][:, a:b]
             self._snap_F[fa:fb] = self._F[c][fa:fb]
             self._snap_Fb[ba:bb] = self._Fb[c][ba:bb]
-            self._snap_it[g] = self.iteration
 
     def _restore_case(self, g):
         c = self._cur
@@ -365,7 +370,9 @@ class BatchSimpleSolver(MixedSimpleSolver):
         raw = self.report_g_host.numpy()
         ng = self.ncase
         scal = raw[: ng * self.NQ * 8].view(np.float64).reshape(ng, self.NQ).copy()
-        infos = read_info(raw[ng * self.NQ * 8:])
+        # the solve records as one structured array (one Python object per record would cost
+        # milliseconds per iteration for hundreds of cases)
+        infos = raw[ng * self.NQ * 8:].view(INFO_DTYPE).copy()
         return scal, infos
 
     def step(self) -> float:
@@ -399,10 +406,10 @@ class BatchSimpleSolver(MixedSimpleSolver):
         res["continuity"] = cont / np.maximum(self._res_max5_case, 1e-3 * flux)
         self._case_res = res
         rolled = self._case_guard(cont, flux)
-        mom = infos[: ng * dim]
-        self.last_linear = {"momentum_iters": np.array([i.iterations for i in mom]).reshape(ng, dim),
-                            "pressure_iters": np.array([i.iterations for i in infos[ng * dim: ng * (dim + 1)]]),
-                            "pressure_residual": np.array([i.residual for i in infos[ng * dim: ng * (dim + 1)]])}
+        it = infos["iterations"].astype(np.int64)
+        self.last_linear = {"momentum_iters": it[: ng * dim].reshape(ng, dim),
+                            "pressure_iters": it[ng * dim: ng * (dim + 1)],
+                            "pressure_residual": infos["residual"][ng * dim: ng * (dim + 1)].astype(np.float64)}
         worst = np.max(np.stack(list(res.values())), axis=0)
         done = (worst < c.tol) & (self.iteration > 5) & ~rolled
         newly = done & (self.case_converged_at < 0)
