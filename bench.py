@@ -16,7 +16,7 @@ max over ranks and ``value`` the aggregate. ``e2e`` is the same metric through t
 from host data: constructing ``SimpleSolver`` from the host mesh (its host->device copies),
 W + K steps (each reads its residual report back) and the final ``fields()`` read.
 
-``--impl reference`` times the reference's CPU path on this box's cores: the oracle driver
+``--impl reference`` times the reference's CPU path on the host's cores: the oracle driver
 with the reference's own C++/OpenMP kernels (built from its sources into ``oracle/_ref``) or,
 without that library, the NumPy oracle; rank 0 only.
 """
