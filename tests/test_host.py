@@ -306,3 +306,42 @@ def test_extract_cells_equals_the_reference_and_orients_the_interfaces():
         assert np.isclose(g.cell_volume.sum(), g0.cell_volume[keep].sum(), rtol=1e-13)
         iface = [z for z in sub.boundary_zones() if z.name.startswith("interface-")]
         assert len(iface) == 1 and iface[0].count > 0
+
+
+def test_host_geometry_errors_and_orientation_repair():
+    """The library's host geometry (``b2s_host_geometry``): a turned face is turned back and
+    counted, a face with a node count the dimension does not allow and a cell of non-positive
+    volume raise, as the reference's ``compute_geometry`` does."""
+    import copy
+
+    import pytest as _pytest
+
+    from gputest_b200.mesh.unstructured import face_centres_and_areas
+
+    m = cartesian_mesh_2d(6, 5, triangulate=True, warp=0.05)
+    g0 = compute_geometry(m)
+    # reverse the node order of three faces: their area vectors flip and the repair restores them
+    m2 = copy.deepcopy(m)
+    for f in (0, 7, 20):
+        a, b = m2.face_ptr[f], m2.face_ptr[f + 1]
+        m2.face_nodes[a:b] = m2.face_nodes[a:b][::-1].copy()
+    g2 = compute_geometry(m2)
+    assert g2.flipped_faces == g0.flipped_faces + 3
+    np.testing.assert_array_equal(g2.face_area_vec, g0.face_area_vec)
+    np.testing.assert_array_equal(g2.cell_volume, g0.cell_volume)
+    fc, S = face_centres_and_areas(m)
+    np.testing.assert_array_equal(fc, g0.face_centre)
+    # a 2-D mesh whose first face lists three nodes
+    m3 = copy.deepcopy(m)
+    m3.face_ptr = m3.face_ptr.copy()
+    m3.face_nodes = np.insert(m3.face_nodes, 2, m3.face_nodes[0])
+    m3.face_ptr[1:] += 1
+    with _pytest.raises(ValueError, match="2-node faces"):
+        compute_geometry(m3)
+    # without the repair, a turned boundary face gives a cell of non-positive volume
+    m4 = cartesian_mesh_2d(1, 1)
+    for f in range(m4.n_faces):
+        a, b = m4.face_ptr[f], m4.face_ptr[f + 1]
+        m4.face_nodes[a:b] = m4.face_nodes[a:b][::-1].copy()
+    with _pytest.raises(ValueError, match="non-positive volume"):
+        compute_geometry(m4, repair=False)
