@@ -73,58 +73,6 @@ __global__ void __launch_bounds__(kCoopThreads) power_coop_k(b2s_amg_level L, do
 // barrier per iteration costs more than the work).
 constexpr int kPowerBlockRows = 2048;
 
-// The same power iteration by one thread-block cluster (levels of at most kPowerClusterRows
-// rows): the blocks exchange their two partial sums through distributed shared memory, double
-// buffered so one cluster barrier per iteration suffices, and every block adds the partials in
-// rank order (deterministic, the same scalars in every block).
-constexpr int kPowerClusterRows = 65536;
-
-__global__ void __launch_bounds__(kCoopThreads) power_cluster_k(b2s_amg_level L, double* ya, double* yb) {
-  cg::cluster_group cl = cg::this_cluster();
-  __shared__ double red[(kCoopThreads / 32 + 1) * 2];
-  __shared__ double mine[2][2];  // [iteration parity][quantity]: this block's partials
-  const int rank = (int)cl.block_rank(), C = (int)cl.num_blocks();
-  const int gt = rank * blockDim.x + threadIdx.x, gs = C * blockDim.x;
-  double* ybuf[2] = {ya, yb};
-  double lam = 1.0, sc = 1.0;
-  for (int it = 0; it < 15; ++it) {
-    const double* xin = it == 0 ? L.x0 : ybuf[(it - 1) & 1];
-    double* yout = ybuf[it & 1];
-    double acc[2] = {0.0, 0.0};
-    for (int i = gt; i < L.n; i += gs) {
-      const double di = L.dinv[i];
-      double s = 0.0;
-      for (int j = L.rowptr[i]; j < L.rowptr[i + 1]; ++j) {
-        const int c = L.col[j];
-        const double xc = it == 0 ? xin[c] : xin[c] / sc;
-        s += (di * L.val[j]) * xc;
-      }
-      yout[i] = s;
-      acc[0] += s * s;
-      const double xi = it == 0 ? xin[i] : xin[i] / sc;
-      acc[1] += xi * xi;
-    }
-    double tot[2];
-    block_sum<2>(acc, red, tot);
-    if (threadIdx.x == 0) {
-      mine[it & 1][0] = tot[0];
-      mine[it & 1][1] = tot[1];
-    }
-    cl.sync();  // partials and y of this iteration visible to the whole cluster
-    double t0 = 0.0, t1 = 0.0;
-    for (int r = 0; r < C; ++r) {
-      const double* m = cl.map_shared_rank(&mine[it & 1][0], r);
-      t0 += m[0];
-      t1 += m[1];
-    }
-    const double ny = sqrt(t0), nx = sqrt(t1);
-    lam = ny / fmax(nx, 1e-300);
-    sc = fmax(ny, 1e-300);
-  }
-  cl.sync();  // no block leaves while another may still read its shared memory
-  if (rank == 0 && threadIdx.x == 0) *L.rho = lam;
-}
-
 // Batches: the power iteration of power_block_k per case (one block per case on its rows). A
 // case that this level does not coarsen (every row its own aggregate, next_ptr giving the same
 // row count) gets rho = infinity, so that its prolongation is the plain injection P = T and its
@@ -509,36 +457,6 @@ int64_t b2s_amg_workspace_bytes(const b2s_amg* h) {
 }  // extern "C"
 
 namespace {
-// One cluster of 16 blocks (8 where 16 is refused) for power_cluster_k; false when no cluster
-// launch is possible (the caller uses the cooperative kernel).
-bool launch_power_cluster(const b2s_amg_level& L, double* xa, double* xb, cudaStream_t st) {
-  static int allowed = -1;
-  if (allowed < 0)
-    allowed = cudaFuncSetAttribute(power_cluster_k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess
-                  ? 1
-                  : 0;
-  if (!allowed) cudaGetLastError();
-  b2s_amg_level Lc = L;
-  void* args[] = {&Lc, &xa, &xb};
-  for (int C : {16, 8}) {
-    if (C > 8 && !allowed) continue;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)C, 1, 1);
-    cfg.blockDim = dim3(kCoopThreads, 1, 1);
-    cfg.stream = st;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (cudaLaunchKernelExC(&cfg, (const void*)power_cluster_k, args) == cudaSuccess) return true;
-    cudaGetLastError();
-  }
-  return false;
-}
-
 // Numeric rebuild of one level from its matrix values: D^-1, rho, P, R, W = A P and the next
 // level's values A_c = R W on the pattern (crow, ccol).
 int rebuild_level(const b2s_amg_level& L, int ngroups, const int32_t* next_group_ptr, const int32_t* crow,
@@ -554,8 +472,6 @@ int rebuild_level(const b2s_amg_level& L, int ngroups, const int32_t* next_group
     power_groups_k<<<(unsigned)ngroups, kCoopThreads, 0, st>>>(L, next_group_ptr, xa, xb);
   } else if (L.n <= kPowerBlockRows) {
     power_block_k<<<1, kCoopThreads, 0, st>>>(L, xa, xb);
-  } else if (L.n <= kPowerClusterRows && launch_power_cluster(L, xa, xb, st)) {
-    // one cluster of blocks, cluster barriers
   } else {
     b2s_amg_level Lc = L;
     void* args[] = {&Lc, &xa, &xb, &part0, &part1};  // xa, xb: the two power-iteration buffers
