@@ -305,13 +305,17 @@ _START_VECTORS = {}
 
 def _start_vector(n, dev):
     """The reference's power-iteration start vector (``default_rng(0)``, ``amg.py:69-77``) of
-    length n, on the device (cached: a re-aggregated hierarchy reuses the sizes it had)."""
+    length n, on the device. A draw of n normals is the first n values of a longer draw from the
+    same seed, so one vector per device, as long as the longest level yet, serves every level
+    (re-aggregated hierarchies change their coarse sizes; the cache does not grow with them)."""
     import torch
 
-    key = (int(n), str(dev))
-    if key not in _START_VECTORS:
-        _START_VECTORS[key] = torch.as_tensor(np.random.default_rng(0).standard_normal(n), device=dev)
-    return _START_VECTORS[key]
+    key = str(dev)
+    v = _START_VECTORS.get(key)
+    if v is None or v.numel() < n:
+        v = torch.as_tensor(np.random.default_rng(0).standard_normal(max(int(n), 1)), device=dev)
+        _START_VECTORS[key] = v
+    return v[: int(n)]
 
 
 class AMGHierarchy:
