@@ -273,10 +273,15 @@ class FVMesh:
         self.non_orthogonality_deg = r["non_orthogonality_deg"]
         self.bzone = r["bzone"]
         self._ref = r
-        # ---- cell order (host): reverse Cuthill-McKee of the cell adjacency
+        L64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=dev)  # noqa: E731
+        P_t, N_t, Pb_t = L64(P), L64(N), L64(Pb)
+        ar = torch.arange(nc + 1, device=dev)
+        # ---- cell order: reverse Cuthill-McKee (SciPy, host) of the cell adjacency, whose sorted
+        # CSR is built from distinct keys on the device
         if reorder and nf:
-            adj = sp.csr_matrix((np.ones(2 * nf, dtype=np.int8), (np.concatenate([P, N]), np.concatenate([N, P]))),
-                                shape=(nc, nc))
+            akeys = torch.unique(torch.cat([P_t * nc + N_t, N_t * nc + P_t]), sorted=True)
+            adj = sp.csr_matrix((np.ones(akeys.numel(), dtype=np.int8), (akeys % nc).cpu().numpy(),
+                                 torch.searchsorted(akeys // nc, ar).cpu().numpy()), shape=(nc, nc))
             perm = np.asarray(reverse_cuthill_mckee(adj, symmetric_mode=True), dtype=np.int64)
         else:
             perm = np.arange(nc, dtype=np.int64)
@@ -286,10 +291,8 @@ class FVMesh:
         iperm = np.empty(nc, dtype=np.int64)
         iperm[perm] = np.arange(nc)
         self.perm, self.iperm = perm, iperm  # device -> reference, reference -> device
-        L64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=dev)  # noqa: E731
-        perm_t, iperm_t, P_t, N_t, Pb_t = L64(perm), L64(iperm), L64(P), L64(N), L64(Pb)
+        perm_t, iperm_t = L64(perm), L64(iperm)
         self.h2d_bytes += 8 * (2 * nc + 2 * nf + nb)
-        ar = torch.arange(nc + 1, device=dev)
         # ---- interior faces by (device owner, reference index); faces by neighbour
         Pn, Nn = iperm_t[P_t], iperm_t[N_t]
         forder = torch.sort(Pn, stable=True).indices
