@@ -337,9 +337,8 @@ class FVMesh:
         if self.duplicate_pairs:
             raise NotImplementedError("meshes with two faces joining the same pair of cells are not supported")
         self._ref_csr = (r_indptr, r_indices)
-        self.face_ref = forder.cpu().numpy()  # device face -> reference interior face
         self.bface_ref = border.cpu().numpy()  # device boundary face -> reference boundary face
-        self.slot_ref = src.cpu().numpy()
+        self._maps = {"face_ref": forder, "slot_ref": src}  # host copies made on first use
         # ---- device tensors
         i32 = lambda t: t.to(torch.int32).contiguous()  # noqa: E731
         soa = lambda t: t.t().contiguous()  # (n, k) -> [k][n]  # noqa: E731
@@ -370,6 +369,22 @@ class FVMesh:
         self.cmesh_ref = ctypes.byref(self.cmesh)
         self.row_terms_max = int(stats[0]) + 1 if nc else 1
         self.cell_faces_max = int(stats[1]) if nc else 1
+
+    @property
+    def face_ref(self):
+        """Device interior face -> reference interior face (host array)."""
+        m = self._maps["face_ref"]
+        if not isinstance(m, np.ndarray):
+            m = self._maps["face_ref"] = m.cpu().numpy()
+        return m
+
+    @property
+    def slot_ref(self):
+        """Device CSR slot -> reference CSR slot (host array)."""
+        m = self._maps["slot_ref"]
+        if not isinstance(m, np.ndarray):
+            m = self._maps["slot_ref"] = m.cpu().numpy()
+        return m
 
     def boundary_centres_host(self):
         """Boundary-face centres, (nb, dim), reference order."""
