@@ -123,6 +123,10 @@ _SIGS = {
     "b2s_amg_level_workspace_bytes": ([P], I64),
     "b2s_amg_level_rebuild_d": ([P, P, P, P, P, I64, P], ctypes.c_int),
     "b2s_amg_coarse_inverse_d": ([P, P, I64, P], ctypes.c_int),
+    "b2s_amg_p_pattern_d": ([I32, P, P, P, I32, P, P, I64, P, P, P, I64, P, P], ctypes.c_int),
+    "b2s_amg_w_pattern_d": ([I32, P, P, P, P, I32, P, P, P, P, I64, I64, P, P, P, P, P, P], ctypes.c_int),
+    "b2s_scan_workspace_bytes": ([I32], I64),
+    "b2s_scan_counts_d": ([I32, P, P, P, I64, P], ctypes.c_int),
     "b2s_row_residuals_d": ([I32, P, P, P, P, P, P, P, P, P, P], ctypes.c_int),
     "b2s_flux_balance_d": ([P, P, P, P, P, P], ctypes.c_int),
     "b2s_matrix_properties_workspace_bytes": ([], I64),

@@ -317,6 +317,163 @@ __global__ void aggregate_sizes_k(int n, const int32_t* __restrict__ agg, int32_
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) atomicAdd(cnt + agg[i], 1);
 }
 
+// ------------------------------------------------------------------ P and W patterns, per row
+// P = A T has, in row i, one entry per distinct aggregate among the columns of A's row i; W = A P
+// one per distinct column among the P rows of those columns. One thread builds one row in
+// local arrays (rows of at most kMaxRowP entries, at most kMaxRowW W candidates; a longer row
+// raises *overflow and the caller builds the level with sorted keys instead). The term lists
+// follow the order the row-owned rebuild kernels add terms in: P slot (i, J) lists the A
+// entries of row i with aggregate J in stored order; W slot (i, c) lists the pairs (A entry e of
+// row i, P entry f of row col[e]) with column c, e in stored order, then f.
+constexpr int kMaxRowP = 64;
+constexpr int kMaxRowW = 128;
+
+// Inserts v into the ascending distinct list u[0..m); returns the new length (cap: no insert
+// past it, *full set).
+__device__ __forceinline__ int insert_distinct(int32_t* u, int m, int cap, int32_t v, bool& full) {
+  int lo = 0, hi = m;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (u[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo < m && u[lo] == v) return m;
+  if (m >= cap) {
+    full = true;
+    return m;
+  }
+  for (int k = m; k > lo; --k) u[k] = u[k - 1];
+  u[lo] = v;
+  return m + 1;
+}
+
+__device__ __forceinline__ int find_distinct(const int32_t* u, int m, int32_t v) {
+  int lo = 0, hi = m;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (u[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// pass 0: pcnt[i] = distinct aggregates of row i. pass 1: p_idx, p_tptr (slot starts), p_tj.
+__global__ void p_pattern_k(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ cl,
+                            const int32_t* __restrict__ agg, int pass, int32_t* __restrict__ pcnt,
+                            const int32_t* __restrict__ p_ptr, int64_t p_cap, int32_t* __restrict__ p_idx,
+                            int32_t* __restrict__ p_tptr, int32_t* __restrict__ p_tj, int64_t nnz,
+                            int32_t* __restrict__ overflow) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int e0 = rp[i], e1 = rp[i + 1];
+    if (e1 - e0 > kMaxRowP) {
+      atomicExch(overflow, 1);
+      if (pass == 0) pcnt[i] = 0;
+      continue;
+    }
+    int32_t u[kMaxRowP];
+    int m = 0;
+    bool full = false;
+    for (int e = e0; e < e1; ++e) m = insert_distinct(u, m, kMaxRowP, agg[cl[e]], full);
+    if (pass == 0) {
+      pcnt[i] = m;
+      continue;
+    }
+    const int64_t base = p_ptr[i];
+    if (base + m > p_cap || p_ptr[i + 1] - base != m) {
+      atomicExch(overflow, 2);
+      continue;
+    }
+    int32_t cnt[kMaxRowP];
+    for (int k = 0; k < m; ++k) cnt[k] = 0;
+    for (int e = e0; e < e1; ++e) {
+      const int r = find_distinct(u, m, agg[cl[e]]);
+      if (r < m) ++cnt[r];
+    }
+    int acc = e0;
+    for (int k = 0; k < m; ++k) {  // slot starts, then the running positions
+      p_idx[base + k] = u[k];
+      p_tptr[base + k] = acc;
+      const int c = cnt[k];
+      cnt[k] = acc;
+      acc += c;
+    }
+    for (int e = e0; e < e1; ++e) {
+      const int r = find_distinct(u, m, agg[cl[e]]);
+      if (r >= m) continue;
+      const int pos = cnt[r]++;
+      if (pos >= 0 && pos < nnz) p_tj[pos] = e;
+    }
+    if (i == n - 1) p_tptr[base + m] = (int32_t)nnz;
+  }
+}
+
+// pass 0: wcnt[i] = distinct W columns, tcnt[i] = W terms of row i. pass 1: w_idx, w_tptr,
+// w_tj, w_te (row i's terms from t_ptr[i]).
+__global__ void w_pattern_k(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ cl,
+                            const int32_t* __restrict__ p_ptr, const int32_t* __restrict__ p_idx, int pass,
+                            int32_t* __restrict__ wcnt, int32_t* __restrict__ tcnt, const int32_t* __restrict__ w_ptr,
+                            const int32_t* __restrict__ t_ptr, int64_t w_cap, int64_t t_cap,
+                            int32_t* __restrict__ w_idx, int32_t* __restrict__ w_tptr, int32_t* __restrict__ w_tj,
+                            int32_t* __restrict__ w_te, int32_t* __restrict__ overflow) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int e0 = rp[i], e1 = rp[i + 1];
+    int terms = 0;
+    for (int e = e0; e < e1; ++e) terms += p_ptr[cl[e] + 1] - p_ptr[cl[e]];
+    if (terms > kMaxRowW) {
+      atomicExch(overflow, 1);
+      if (pass == 0) wcnt[i] = tcnt[i] = 0;
+      continue;
+    }
+    int32_t u[kMaxRowW];
+    int m = 0;
+    bool full = false;
+    for (int e = e0; e < e1; ++e) {
+      const int j = cl[e];
+      for (int f = p_ptr[j]; f < p_ptr[j + 1]; ++f) m = insert_distinct(u, m, kMaxRowW, p_idx[f], full);
+    }
+    if (pass == 0) {
+      wcnt[i] = m;
+      tcnt[i] = terms;
+      continue;
+    }
+    const int64_t base = w_ptr[i], tb = t_ptr[i];
+    if (base + m > w_cap || w_ptr[i + 1] - base != m || tb + terms > t_cap || t_ptr[i + 1] - tb != terms) {
+      atomicExch(overflow, 2);
+      continue;
+    }
+    int32_t cnt[kMaxRowW];
+    for (int k = 0; k < m; ++k) cnt[k] = 0;
+    for (int e = e0; e < e1; ++e) {
+      const int j = cl[e];
+      for (int f = p_ptr[j]; f < p_ptr[j + 1]; ++f) {
+        const int r = find_distinct(u, m, p_idx[f]);
+        if (r < m) ++cnt[r];
+      }
+    }
+    int64_t acc = tb;
+    for (int k = 0; k < m; ++k) {
+      w_idx[base + k] = u[k];
+      w_tptr[base + k] = (int32_t)acc;
+      const int c = cnt[k];
+      cnt[k] = (int32_t)(acc - tb);
+      acc += c;
+    }
+    for (int e = e0; e < e1; ++e) {
+      const int j = cl[e];
+      for (int f = p_ptr[j]; f < p_ptr[j + 1]; ++f) {
+        const int r = find_distinct(u, m, p_idx[f]);
+        if (r >= m) continue;
+        const int64_t pos = tb + cnt[r]++;
+        if (pos >= tb && pos < tb + terms) {
+          w_tj[pos] = e;
+          w_te[pos] = f;
+        }
+      }
+    }
+    if (i == n - 1) w_tptr[base + m] = (int32_t)(tb + terms);
+  }
+}
+
 }  // namespace b2s
 
 using namespace b2s;
@@ -426,6 +583,48 @@ int b2s_amg_aggregate_d(int32_t n, const int32_t* rowptr, const int32_t* col, co
   aggregate_sizes_k<<<gn, kThreads, 0, st>>>(n, agg, counts);
   B2S_LAUNCH_CHECK();
   return B2S_OK;
+}
+
+/* P and W patterns with their term lists, one thread per row (the order of the row-owned rebuild
+ * kernels; see p_pattern_k / w_pattern_k). Each builder has two passes: pass 0 writes per-row
+ * counts (pcnt; wcnt and tcnt), the caller scans them into p_ptr (w_ptr, t_ptr) and allocates;
+ * pass 1 fills. *overflow (device int, not cleared here): 1 where a row exceeds the per-thread
+ * capacity (64 A entries, 128 W terms), 2 where the offsets disagree with the counts. */
+int b2s_amg_p_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* agg, int32_t pass,
+                        int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx, int32_t* p_tptr,
+                        int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s) {
+  if (n < 1 || !rp || !cl || !agg || !overflow || (pass == 0 && !pcnt) ||
+      (pass == 1 && (!p_ptr || !p_idx || !p_tptr || !p_tj)) || (pass != 0 && pass != 1))
+    return B2S_ERR_ARG;
+  p_pattern_k<<<grid_for(n, 128), 128, 0, (cudaStream_t)s>>>(n, rp, cl, agg, pass, pcnt, p_ptr, p_cap, p_idx, p_tptr,
+                                                             p_tj, nnz, overflow);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+int b2s_amg_w_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* p_ptr, const int32_t* p_idx,
+                        int32_t pass, int32_t* wcnt, int32_t* tcnt, const int32_t* w_ptr, const int32_t* t_ptr,
+                        int64_t w_cap, int64_t t_cap, int32_t* w_idx, int32_t* w_tptr, int32_t* w_tj, int32_t* w_te,
+                        int32_t* overflow, b2s_stream_t s) {
+  if (n < 1 || !rp || !cl || !p_ptr || !p_idx || !overflow || (pass == 0 && (!wcnt || !tcnt)) ||
+      (pass == 1 && (!w_ptr || !t_ptr || !w_idx || !w_tptr || !w_tj || !w_te)) || (pass != 0 && pass != 1))
+    return B2S_ERR_ARG;
+  w_pattern_k<<<grid_for(n, 128), 128, 0, (cudaStream_t)s>>>(n, rp, cl, p_ptr, p_idx, pass, wcnt, tcnt, w_ptr, t_ptr,
+                                                             w_cap, t_cap, w_idx, w_tptr, w_tj, w_te, overflow);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+/* Exclusive scan of n int32 counts into out[0..n] (out[n] the total), for the pattern builders. */
+int64_t b2s_scan_workspace_bytes(int32_t n) {
+  if (n < 0) return -1;
+  return (int64_t)sizeof(int32_t) * (cdiv(n > 0 ? n : 1, kScanTile) + 8);
+}
+
+int b2s_scan_counts_d(int32_t n, const int32_t* counts, int32_t* out, void* work, int64_t work_bytes, b2s_stream_t s) {
+  if (n < 1 || !counts || !out || !work) return B2S_ERR_ARG;
+  if (work_bytes < b2s_scan_workspace_bytes(n)) return B2S_ERR_WORKSPACE;
+  return scan_flags(n, counts, out, (int32_t*)work, out + n, (cudaStream_t)s);
 }
 
 }  // extern "C"

@@ -194,41 +194,104 @@ def _rows_of(ptr, nnz):
     return torch.repeat_interleave(torch.arange(n, device=ptr.device), ptr[1:] - ptr[:-1], output_size=nnz)
 
 
-def product_patterns(rp, cl, agg, na, cap=TERM_CAP):
+def row_patterns(rp, cl, agg, stream=None):
+    """The P and W patterns and term lists by the per-row kernels (``b2s_amg_p_pattern_d``,
+    ``b2s_amg_w_pattern_d``; rp, cl, agg int32 device tensors), the same arrays as the key-based
+    construction of ``product_patterns``; None when a row exceeds the kernels' per-thread
+    capacity (the caller uses the key-based construction). Three host synchronisations."""
+    import torch
+
+    L = _lib.lib()
+    sp_ = _lib.stream_ptr(stream)
+    dev = cl.device
+    n, nnz = rp.numel() - 1, cl.numel()
+    e32 = lambda k: torch.empty(max(int(k), 1), dtype=torch.int32, device=dev)  # noqa: E731
+    ov = torch.zeros(1, dtype=torch.int32, device=dev)
+    ws = e32(L.b2s_scan_workspace_bytes(n) // 4 + 1)
+
+    def scan(counts):
+        out = e32(n + 1)
+        _lib.check(L.b2s_scan_counts_d(n, counts.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel() * 4, sp_),
+                   "b2s_scan_counts_d")
+        return out
+
+    pcnt = e32(n)
+    _lib.check(L.b2s_amg_p_pattern_d(n, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 0, pcnt.data_ptr(), None, 0,
+                                     None, None, None, nnz, ov.data_ptr(), sp_), "b2s_amg_p_pattern_d")
+    p_ptr = scan(pcnt)
+    h = torch.cat([ov, p_ptr[n:]]).cpu()
+    if int(h[0]):
+        return None
+    p_nnz = int(h[1])
+    p_idx, p_tptr, p_tj = e32(p_nnz), e32(p_nnz + 1), e32(nnz)
+    _lib.check(L.b2s_amg_p_pattern_d(n, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 1, None, p_ptr.data_ptr(),
+                                     p_nnz, p_idx.data_ptr(), p_tptr.data_ptr(), p_tj.data_ptr(), nnz, ov.data_ptr(),
+                                     sp_), "b2s_amg_p_pattern_d")
+    wcnt, tcnt = e32(n), e32(n)
+    _lib.check(L.b2s_amg_w_pattern_d(n, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 0,
+                                     wcnt.data_ptr(), tcnt.data_ptr(), None, None, 0, 0, None, None, None, None,
+                                     ov.data_ptr(), sp_), "b2s_amg_w_pattern_d")
+    w_ptr, t_ptr = scan(wcnt), scan(tcnt)
+    h = torch.cat([ov, w_ptr[n:], t_ptr[n:]]).cpu()
+    if int(h[0]) or int(h[2]) > TERM_CAP:
+        return None
+    w_nnz, w_terms = int(h[1]), int(h[2])
+    w_idx, w_tptr, w_tj, w_te = e32(w_nnz), e32(w_nnz + 1), e32(w_terms), e32(w_terms)
+    _lib.check(L.b2s_amg_w_pattern_d(n, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 1, None,
+                                     None, w_ptr.data_ptr(), t_ptr.data_ptr(), w_nnz, w_terms, w_idx.data_ptr(),
+                                     w_tptr.data_ptr(), w_tj.data_ptr(), w_te.data_ptr(), ov.data_ptr(), sp_),
+               "b2s_amg_w_pattern_d")
+    if int(ov.item()):
+        return None
+    return {"p_ptr": p_ptr, "p_idx": p_idx[:p_nnz], "p_tptr": p_tptr[:p_nnz + 1], "p_tj": p_tj[:nnz],
+            "w_ptr": w_ptr, "w_idx": w_idx[:w_nnz], "w_tptr": w_tptr[:w_nnz + 1], "w_tj": w_tj[:w_terms],
+            "w_te": w_te[:w_terms]}
+
+
+def product_patterns(rp, cl, agg, na, cap=TERM_CAP, pw=None):
     """Patterns of P = A T, W = A P, A_c = P^T W and R = P^T for the aggregates ``agg`` (``na`` of
     them) of the level whose CSR in stored order is (rp, cl) (int64 torch tensors on one device),
     with the term lists of ``term_lists``, computed from sorted distinct keys instead of SciPy
     products: every structure the device set-up needs, on the tensors' device (four host
-    synchronisations: the sizes of the products). Returns a dict of int64 tensors (patterns:
-    p_ptr/p_idx, w_ptr/w_idx, c_ptr/c_idx, r_rowptr/r_col/r_from_p) and int32 term lists (None
-    where a list would exceed ``cap`` terms)."""
+    synchronisations: the sizes of the products). ``pw``: the P and W parts already built by
+    ``row_patterns``. Returns a dict of int64 tensors (patterns: p_ptr/p_idx, w_ptr/w_idx,
+    c_ptr/c_idx, r_rowptr/r_col/r_from_p) and int32 term lists (None where a list would exceed
+    ``cap`` terms)."""
     import torch
 
     dev = rp.device
     n, nnz = rp.numel() - 1, cl.numel()
-    rows = _rows_of(rp, nnz)
     i32 = lambda t: t.to(torch.int32).contiguous()  # noqa: E731
     out = {}
-    # P: A entry j of row i -> (i, agg[col j])
-    kp = rows * na + agg[cl]
-    p_ptr, p_idx, p_keys = _unique_pattern(kp, n, na)
-    p_nnz = p_idx.numel()
-    out.update(p_ptr=p_ptr, p_idx=p_idx)
-    ptr, order = _grouped(torch.searchsorted(p_keys, kp), p_nnz)
-    out["p_tptr"], out["p_tj"] = i32(ptr), i32(order)
-    # W: (A entry j of row i, P entry e of row col j) -> (i, col e), generated j-major
-    lens = p_ptr[cl + 1] - p_ptr[cl]
-    w_terms = int(lens.sum())
-    jj, e = _expand_sized(p_ptr, cl, w_terms)
-    kw = rows[jj] * na + p_idx[e]
-    w_ptr, w_idx, w_keys = _unique_pattern(kw, n, na)
-    out.update(w_ptr=w_ptr, w_idx=w_idx)
-    if w_terms <= cap:
-        ptr, order = _grouped(torch.searchsorted(w_keys, kw), w_idx.numel())
-        out["w_tptr"], out["w_tj"], out["w_te"] = i32(ptr), i32(jj[order]), i32(e[order])
+    if pw is not None:
+        i64 = lambda t: t.to(torch.int64)  # noqa: E731
+        p_ptr, p_idx, w_ptr, w_idx = i64(pw["p_ptr"]), i64(pw["p_idx"]), i64(pw["w_ptr"]), i64(pw["w_idx"])
+        p_nnz = p_idx.numel()
+        out.update(p_ptr=p_ptr, p_idx=p_idx, w_ptr=w_ptr, w_idx=w_idx)
+        for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te"):
+            out[k] = pw[k].contiguous()
     else:
-        out["w_tptr"] = out["w_tj"] = out["w_te"] = None
-    del jj, e, kw
+        rows = _rows_of(rp, nnz)
+        # P: A entry j of row i -> (i, agg[col j])
+        kp = rows * na + agg[cl]
+        p_ptr, p_idx, p_keys = _unique_pattern(kp, n, na)
+        p_nnz = p_idx.numel()
+        out.update(p_ptr=p_ptr, p_idx=p_idx)
+        ptr, order = _grouped(torch.searchsorted(p_keys, kp), p_nnz)
+        out["p_tptr"], out["p_tj"] = i32(ptr), i32(order)
+        # W: (A entry j of row i, P entry e of row col j) -> (i, col e), generated j-major
+        lens = p_ptr[cl + 1] - p_ptr[cl]
+        w_terms = int(lens.sum())
+        jj, e = _expand_sized(p_ptr, cl, w_terms)
+        kw = rows[jj] * na + p_idx[e]
+        w_ptr, w_idx, w_keys = _unique_pattern(kw, n, na)
+        out.update(w_ptr=w_ptr, w_idx=w_idx)
+        if w_terms <= cap:
+            ptr, order = _grouped(torch.searchsorted(w_keys, kw), w_idx.numel())
+            out["w_tptr"], out["w_tj"], out["w_te"] = i32(ptr), i32(jj[order]), i32(e[order])
+        else:
+            out["w_tptr"] = out["w_tj"] = out["w_te"] = None
+        del jj, e, kw
     # R = P^T: P entries by (column, row)
     prow = _rows_of(p_ptr, p_nnz)
     r_from_p = torch.argsort(p_idx * n + prow)
@@ -326,6 +389,8 @@ class AMGHierarchy:
     ``diag_slot``; ``val`` is the device tensor of level-0 values that the solver rewrites
     before every rebuild.
     """
+
+    ROW_PATTERNS = True  # device set-up: P and W by the per-row kernels where rows fit them
 
     def __init__(self, A_host, perm, rowptr, col, diag_slot, val, slot_ref, singular=False, theta=0.08,
                  max_coarse=150, max_levels=20, sweeps=2, omega=0.8, groups=None, group_singular=None):
@@ -531,6 +596,7 @@ class AMGHierarchy:
         dev = val.device
         L = _lib.lib()
         sp_ = _lib.stream_ptr(stream)
+        self._row_patterns = cls.ROW_PATTERNS
         self.singular, self.sweeps, self.omega, self.theta = bool(singular), int(sweeps), float(omega), theta
         self._keep, self.sizes = [], []
         h = self.c = _lib.Amg()
@@ -584,7 +650,8 @@ class AMGHierarchy:
             na = int(ih[0])
             if na >= n * 0.9:
                 break
-            pat = product_patterns(lv_rp64, lv_cl64, agg.to(torch.int64), na)
+            pw = row_patterns(lv_rp, lv_cl, agg, stream) if self._row_patterns else None
+            pat = product_patterns(lv_rp64, lv_cl64, agg.to(torch.int64), na, pw=pw)
             Lv = h.levels[nlev]
             Lv.n, Lv.nnz, Lv.nc = n, lv_cl.numel(), na
             Lv.p_nnz, Lv.w_nnz = pat["p_idx"].numel(), pat["w_idx"].numel()

@@ -476,6 +476,25 @@ B2S_API int b2s_amg_level_rebuild_d(const b2s_amg_level* L, const int32_t* crow,
                                     void* work, int64_t work_bytes, b2s_stream_t s);
 B2S_API int b2s_amg_coarse_inverse_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s);
 
+/* The patterns of P = A T and W = A P of one level, with the term lists of the row-owned rebuild
+ * (b2s_amg_level), one thread per row: rp/cl the level's CSR in stored order, agg its aggregates.
+ * Two passes each: pass 0 writes per-row counts (pcnt; wcnt = W entries, tcnt = W terms), which
+ * the caller scans (b2s_scan_counts_d) into p_ptr (w_ptr, t_ptr) and allocates from; pass 1
+ * fills p_idx, p_tptr, p_tj (w_idx, w_tptr, w_tj, w_te), never past p_cap/nnz (w_cap/t_cap).
+ * *overflow (device int, not cleared): 1 where a row has more than 64 entries or 128 W terms,
+ * 2 where the offsets disagree with the counts; the caller then builds the level another way. */
+B2S_API int b2s_amg_p_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* agg, int32_t pass,
+                                int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx, int32_t* p_tptr,
+                                int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s);
+B2S_API int b2s_amg_w_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* p_ptr,
+                                const int32_t* p_idx, int32_t pass, int32_t* wcnt, int32_t* tcnt, const int32_t* w_ptr,
+                                const int32_t* t_ptr, int64_t w_cap, int64_t t_cap, int32_t* w_idx, int32_t* w_tptr,
+                                int32_t* w_tj, int32_t* w_te, int32_t* overflow, b2s_stream_t s);
+/* Exclusive scan of n int32 counts into out[0..n], out[n] the total. */
+B2S_API int64_t b2s_scan_workspace_bytes(int32_t n);
+B2S_API int b2s_scan_counts_d(int32_t n, const int32_t* counts, int32_t* out, void* work, int64_t work_bytes,
+                              b2s_stream_t s);
+
 /* ----------------------------------------------------------------------------------------- */
 /* Mixed precision. No counterpart in the reference (its path is FP64 throughout): the linear    */
 /* systems are stored and solved in float, while the nonlinear residuals, the continuity and     */
