@@ -185,31 +185,39 @@ def test_partial_reaggregation_equals_a_full_device_set_up():
     assert checked >= 2
 
 
-@pytest.mark.parametrize("kind,n,seed", [("grid", 2500, 11), ("random", 3000, 12), ("random", 400, 13)])
+@pytest.mark.parametrize("kind,n,seed", [("grid", 2500, 11), ("grid", 10000, 14), ("random", 3000, 12)])
 def test_row_pattern_kernels_equal_the_key_based_patterns(kind, n, seed):
     """``row_patterns`` (one thread per row) against the sorted-key construction of
-    ``product_patterns`` on the same level and aggregates: every pattern and term list equal;
-    a level whose rows exceed the kernels' capacity is handed back (None)."""
+    ``product_patterns`` on the same level and aggregates: every pattern and term list equal
+    where every row fits the kernels (at most 64 entries and 128 W terms), the level handed back
+    (None) where one does not (the random graph: up to 177 W terms in a row)."""
+    import scipy.sparse as sp
     import torch
 
     from gputest_b200.linalg import amg
     from tests.test_amg_device_setup import _graph
 
     A = _graph(seed, n, kind)
+    n = A.shape[0]
     rng = np.random.default_rng(seed)
     rp, cl, val, diag, _ = _device_csr(A, rng)
     S = amg.strength(A, 0.08)
     agg_h, na = amg.aggregate(S)
+    T = sp.csr_matrix((np.ones(n), (np.arange(n), agg_h)), shape=(n, na))
+    Pp = amg._pattern(amg._pattern(A) @ T)
+    plen = np.diff(Pp.indptr)
+    terms = max(int(plen[A.indices[A.indptr[i]:A.indptr[i + 1]]].sum()) for i in range(n))
+    fits = terms <= 128 and int(np.diff(A.indptr).max()) <= 64
     agg = torch.as_tensor(agg_h, dtype=torch.int32, device="cuda")
     pw = amg.row_patterns(rp, cl, agg)
-    assert pw is not None
-    ref = amg.product_patterns(rp.long(), cl.long(), agg.long(), na)
-    for k in ("p_ptr", "p_idx", "w_ptr", "w_idx"):
-        assert torch.equal(pw[k].long(), ref[k]), k
-    for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te"):
-        assert torch.equal(pw[k], ref[k]), k
+    assert (pw is not None) == fits
+    if fits:
+        ref = amg.product_patterns(rp.long(), cl.long(), agg.long(), na)
+        for k in ("p_ptr", "p_idx", "w_ptr", "w_idx"):
+            assert torch.equal(pw[k].long(), ref[k]), k
+        for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te"):
+            assert torch.equal(pw[k], ref[k]), k
     # a row of 70 entries is over the P kernel's 64: the level is handed back
-    dense = torch.zeros_like(agg)
     rp2 = torch.tensor([0, 70], dtype=torch.int32, device="cuda")
-    cl2 = torch.arange(70, dtype=torch.int32, device="cuda") % 1
-    assert amg.row_patterns(rp2, cl2, dense[:1]) is None
+    cl2 = torch.zeros(70, dtype=torch.int32, device="cuda")
+    assert amg.row_patterns(rp2, cl2, torch.zeros(1, dtype=torch.int32, device="cuda")) is None
