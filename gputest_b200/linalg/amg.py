@@ -390,7 +390,7 @@ class AMGHierarchy:
     before every rebuild.
     """
 
-    ROW_PATTERNS = False  # True: P and W by the per-row kernels where rows fit them
+    ROW_PATTERNS = True  # device set-up: P and W by the per-row kernels where rows fit them
 
     def __init__(self, A_host, perm, rowptr, col, diag_slot, val, slot_ref, singular=False, theta=0.08,
                  max_coarse=150, max_levels=20, sweeps=2, omega=0.8, groups=None, group_singular=None):
