@@ -4,8 +4,9 @@ The set-up is the reference's (``flowtrace/linalg/amg.py:80-117``): strength of 
 the greedy three-pass aggregation, P = (I - 4/(3 rho) D^-1 A) T, W = A P and A_c = P^T W,
 level by level. ``AMGHierarchy.on_device`` does it on the device: strength flags and the
 aggregation in CUDA (``b2s_amg_strength_d``, ``b2s_amg_aggregate_d``, which reproduces the
-sequential greedy exactly), the patterns and term lists of the products from sorted distinct
-keys (``product_patterns``), and each level's numeric rebuild, whose Galerkin product gives the
+sequential greedy exactly), the patterns and term lists of the products (P and W one row per
+thread, ``row_patterns``; R and A_c, and rows too long for those kernels, from sorted distinct
+keys, ``product_patterns``), and each level's numeric rebuild, whose Galerkin product gives the
 next level's values. ``AMGHierarchy(...)`` is the same set-up on the host (SciPy, the C++ helper
 ``b2s_host_aggregate``); batches of independent cases use it. Afterwards every numeric quantity
 is rebuilt on the device by ``rebuild()`` (``b2s_amg_rebuild_d``): D^-1, the spectral radius by
