@@ -202,14 +202,15 @@ __global__ void flow_bvals_k(b2s_mesh m, b2s_bc bc, const double* __restrict__ U
 
 // ------------------------------------------------------------------------------ momentum
 // 2-D: at most 64 registers, so four 256-thread blocks fit per SM and a 131k-cell mesh runs in
-// one wave (80 registers gave 1.16 waves; measured 0.045 -> 0.033 ms); 3-D keeps the 128
-// registers it uses without a bound (two blocks per SM: a tighter bound's spills cost what the
-// occupancy gains).
+// one wave (80 registers gave 1.16 waves; measured 0.045 -> 0.033 ms); 3-D at most 80 registers,
+// three blocks per SM (measured against 128 registers and two blocks: 2.12 -> 1.90 ms on a
+// 4.2M-cell duct, 0.262 -> 0.227 ms on the 524k duct, despite 180 bytes of spills; 64 registers
+// and four blocks spilled twice as much and gained nothing).
 // TURB: per-face viscosities mu_f [nf] / mu_b [nb] and a per-cell source tsrc [DIM][nc] from the
 // turbulence model (mu + mu_t, the wall-function viscosity on walls, the transpose stress;
 // simple.py:545-548); the laminar instantiation is the scalar-viscosity kernel unchanged.
 template <int DIM, bool TURB>
-__global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Up,
+__global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3) momentum_assemble_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Up,
                                     const double* __restrict__ gUp, const double* __restrict__ gp,
                                     const double* __restrict__ bUp, const double* __restrict__ F,
                                     const double* __restrict__ Fb, const double* __restrict__ por,
@@ -534,9 +535,10 @@ __device__ __forceinline__ void offdiag_apply(const b2s_mesh& m, int c, double g
 }
 
 // 2-D: at most 64 registers, so four 256-thread blocks fit per SM and a 131k-cell mesh runs in
-// one wave (80 registers gave 1.16 waves; measured 0.045 -> 0.033 ms); 3-D keeps the 128
-// registers it uses without a bound (two blocks per SM: a tighter bound's spills cost what the
-// occupancy gains).
+// one wave (80 registers gave 1.16 waves; measured 0.045 -> 0.033 ms); 3-D at most 80 registers,
+// three blocks per SM (measured against 128 registers and two blocks: 2.12 -> 1.90 ms on a
+// 4.2M-cell duct, 0.262 -> 0.227 ms on the 524k duct, despite 180 bytes of spills; 64 registers
+// and four blocks spilled twice as much and gained nothing).
 // TURB: per-face viscosities and the transpose-stress source, as momentum_assemble_k<DIM, true>.
 template <int DIM, bool TURB>
 __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2) momentum_assemble_mixed_k(b2s_mesh m, b2s_bc bc, b2s_flow_params prm, const double* __restrict__ Up,
