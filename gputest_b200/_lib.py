@@ -125,6 +125,9 @@ _SIGS = {
     "b2s_amg_coarse_inverse_d": ([P, P, I64, P], ctypes.c_int),
     "b2s_amg_p_pattern_d": ([I32, P, P, P, I32, P, P, I64, P, P, P, I64, P, P], ctypes.c_int),
     "b2s_amg_w_pattern_d": ([I32, P, P, P, P, I32, P, P, P, P, I64, I64, P, P, P, P, P, P], ctypes.c_int),
+    "b2s_amg_r_workspace_bytes": ([I32], I64),
+    "b2s_amg_r_pattern_d": ([I32, I32, P, P, I64, P, P, P, P, I64, P, P], ctypes.c_int),
+    "b2s_amg_c_pattern_d": ([I32, P, P, P, P, I32, P, P, P, P, I64, I64, P, P, P, P, P, P, P], ctypes.c_int),
     "b2s_scan_workspace_bytes": ([I32], I64),
     "b2s_scan_counts_d": ([I32, P, P, P, I64, P], ctypes.c_int),
     "b2s_row_residuals_d": ([I32, P, P, P, P, P, P, P, P, P, P], ctypes.c_int),

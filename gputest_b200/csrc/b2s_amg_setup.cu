@@ -474,6 +474,135 @@ __global__ void w_pattern_k(int n, const int32_t* __restrict__ rp, const int32_t
   }
 }
 
+// ------------------------------------------------------------------ R = P^T and A_c = R W, per row
+// R row I lists the fine rows i whose P row holds aggregate I, ascending, with the P entry of
+// each (r_from_p). A_c row I has one entry per distinct column among the W rows of R row I's
+// fine rows; its term list holds, per column, the pairs (R entry q, W entry s) in the order the
+// row-owned Galerkin kernel adds them: q ascending, then s. Rows of at most kMaxRowR R entries
+// and kMaxRowC distinct A_c columns; a longer row raises *overflow and the caller builds the
+// level with sorted keys instead.
+constexpr int kMaxRowR = 256;
+constexpr int kMaxRowC = 128;
+
+__global__ void r_count_k(int64_t p_nnz, const int32_t* __restrict__ p_idx, int na, int32_t* __restrict__ rcnt) {
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < p_nnz; f += (int64_t)gridDim.x * blockDim.x) {
+    const int c = p_idx[f];
+    if (c >= 0 && c < na) atomicAdd(rcnt + c, 1);
+  }
+}
+
+// Places every fine row i at a free position of each R row its P row names (the order inside an
+// R row is fixed afterwards by r_sort_k); cursor holds the R row starts on entry.
+__global__ void r_fill_k(int n, const int32_t* __restrict__ p_ptr, const int32_t* __restrict__ p_idx, int na,
+                         int32_t* __restrict__ cursor, int64_t p_nnz, int32_t* __restrict__ r_col) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int f = p_ptr[i]; f < p_ptr[i + 1]; ++f) {
+      const int c = p_idx[f];
+      if (c < 0 || c >= na) continue;
+      const int pos = atomicAdd(cursor + c, 1);
+      if (pos >= 0 && pos < p_nnz) r_col[pos] = i;
+    }
+  }
+}
+
+// Sorts each R row's fine rows ascending (distinct: a P row names an aggregate once) and finds
+// the P entry of each by a binary search of the fine row's ascending P columns.
+__global__ void r_sort_k(int na, const int32_t* __restrict__ r_rowptr, const int32_t* __restrict__ p_ptr,
+                         const int32_t* __restrict__ p_idx, int32_t* __restrict__ r_col, int32_t* __restrict__ r_from_p,
+                         int32_t* __restrict__ overflow) {
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < na; I += gridDim.x * blockDim.x) {
+    const int q0 = r_rowptr[I], len = r_rowptr[I + 1] - q0;
+    if (len > kMaxRowR) {
+      atomicExch(overflow, 1);
+      continue;
+    }
+    int32_t v[kMaxRowR];
+    for (int k = 0; k < len; ++k) {
+      const int32_t x = r_col[q0 + k];
+      int j = k;
+      while (j > 0 && v[j - 1] > x) {
+        v[j] = v[j - 1];
+        --j;
+      }
+      v[j] = x;
+    }
+    for (int k = 0; k < len; ++k) {
+      const int i = v[k], f0 = p_ptr[i];
+      r_col[q0 + k] = i;
+      r_from_p[q0 + k] = f0 + find_distinct(p_idx + f0, p_ptr[i + 1] - f0, I);
+    }
+  }
+}
+
+// pass 0: ccnt[I] = distinct A_c columns, tcnt[I] = A_c terms of row I. pass 1: c_idx, c_diag
+// (the slot of column I in row I, or where it would sit), c_tptr, c_te, c_ts (row I's terms from
+// t_ptr[I]).
+__global__ void c_pattern_k(int na, const int32_t* __restrict__ r_rowptr, const int32_t* __restrict__ r_col,
+                            const int32_t* __restrict__ w_ptr, const int32_t* __restrict__ w_idx, int pass,
+                            int32_t* __restrict__ ccnt, int32_t* __restrict__ tcnt, const int32_t* __restrict__ c_ptr,
+                            const int32_t* __restrict__ t_ptr, int64_t c_cap, int64_t t_cap,
+                            int32_t* __restrict__ c_idx, int32_t* __restrict__ c_diag, int32_t* __restrict__ c_tptr,
+                            int32_t* __restrict__ c_te, int32_t* __restrict__ c_ts, int32_t* __restrict__ overflow) {
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < na; I += gridDim.x * blockDim.x) {
+    const int q0 = r_rowptr[I], q1 = r_rowptr[I + 1];
+    int32_t u[kMaxRowC];
+    int m = 0;
+    int64_t terms = 0;
+    bool full = false;
+    for (int q = q0; q < q1 && !full; ++q) {
+      const int i = r_col[q];
+      for (int s = w_ptr[i]; s < w_ptr[i + 1]; ++s) m = insert_distinct(u, m, kMaxRowC, w_idx[s], full);
+      terms += w_ptr[i + 1] - w_ptr[i];
+    }
+    if (full || terms > INT32_MAX) {
+      atomicExch(overflow, 1);
+      if (pass == 0) ccnt[I] = tcnt[I] = 0;
+      continue;
+    }
+    if (pass == 0) {
+      ccnt[I] = m;
+      tcnt[I] = (int32_t)terms;
+      continue;
+    }
+    const int64_t base = c_ptr[I], tb = t_ptr[I];
+    if (base + m > c_cap || c_ptr[I + 1] - base != m || tb + terms > t_cap || t_ptr[I + 1] - tb != terms) {
+      atomicExch(overflow, 2);
+      continue;
+    }
+    int32_t cnt[kMaxRowC];
+    for (int k = 0; k < m; ++k) cnt[k] = 0;
+    for (int q = q0; q < q1; ++q) {
+      const int i = r_col[q];
+      for (int s = w_ptr[i]; s < w_ptr[i + 1]; ++s) {
+        const int r = find_distinct(u, m, w_idx[s]);
+        if (r < m) ++cnt[r];
+      }
+    }
+    int64_t acc = tb;
+    for (int k = 0; k < m; ++k) {
+      c_idx[base + k] = u[k];
+      c_tptr[base + k] = (int32_t)acc;
+      const int c = cnt[k];
+      cnt[k] = (int32_t)(acc - tb);
+      acc += c;
+    }
+    c_diag[I] = (int32_t)(base + find_distinct(u, m, I));
+    for (int q = q0; q < q1; ++q) {
+      const int i = r_col[q];
+      for (int s = w_ptr[i]; s < w_ptr[i + 1]; ++s) {
+        const int r = find_distinct(u, m, w_idx[s]);
+        if (r >= m) continue;
+        const int64_t pos = tb + cnt[r]++;
+        if (pos >= tb && pos < tb + terms) {
+          c_te[pos] = q;
+          c_ts[pos] = s;
+        }
+      }
+    }
+    if (I == na - 1) c_tptr[base + m] = (int32_t)(tb + terms);
+  }
+}
+
 }  // namespace b2s
 
 using namespace b2s;
@@ -611,6 +740,60 @@ int b2s_amg_w_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const i
     return B2S_ERR_ARG;
   w_pattern_k<<<grid_for(n, 128), 128, 0, (cudaStream_t)s>>>(n, rp, cl, p_ptr, p_idx, pass, wcnt, tcnt, w_ptr, t_ptr,
                                                              w_cap, t_cap, w_idx, w_tptr, w_tj, w_te, overflow);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+/* R = P^T of a level with n fine rows and na aggregates, from P's pattern (p_ptr [n + 1], p_idx
+ * [p_nnz], each row's columns ascending): r_rowptr [na + 1], r_col [p_nnz] (fine rows,
+ * ascending in each R row) and r_from_p [p_nnz] (the P entry of each R entry). Needs no host
+ * synchronisation (R has p_nnz entries). *overflow (device int, not cleared here): 1 where an R
+ * row holds more than 256 entries (that row is left unsorted). */
+int64_t b2s_amg_r_workspace_bytes(int32_t na) {
+  if (na < 0) return -1;
+  const int64_t m = na > 0 ? na : 1;
+  return (int64_t)sizeof(int32_t) * (m + cdiv(m, kScanTile) + 8);
+}
+
+int b2s_amg_r_pattern_d(int32_t n, int32_t na, const int32_t* p_ptr, const int32_t* p_idx, int64_t p_nnz,
+                        int32_t* r_rowptr, int32_t* r_col, int32_t* r_from_p, void* work, int64_t work_bytes,
+                        int32_t* overflow, b2s_stream_t s) {
+  if (n < 1 || na < 1 || p_nnz < 0 || p_nnz > INT32_MAX || !p_ptr || !p_idx || !r_rowptr || !r_col || !r_from_p ||
+      !work || !overflow)
+    return B2S_ERR_ARG;
+  if (work_bytes < b2s_amg_r_workspace_bytes(na)) return B2S_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)s;
+  int32_t* cnt = (int32_t*)work;  // counts, then the running positions
+  int32_t* tsum = cnt + na;
+  if (cudaMemsetAsync(cnt, 0, (size_t)na * sizeof(int32_t), st) != cudaSuccess) return B2S_ERR_LAUNCH;
+  if (p_nnz > 0) r_count_k<<<grid_for(p_nnz), kThreads, 0, st>>>(p_nnz, p_idx, na, cnt);
+  B2S_LAUNCH_CHECK();
+  int rc;
+  if ((rc = scan_flags(na, cnt, r_rowptr, tsum, r_rowptr + na, st)) != B2S_OK) return rc;
+  if (cudaMemcpyAsync(cnt, r_rowptr, (size_t)na * sizeof(int32_t), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return B2S_ERR_LAUNCH;
+  r_fill_k<<<grid_for(n), kThreads, 0, st>>>(n, p_ptr, p_idx, na, cnt, p_nnz, r_col);
+  r_sort_k<<<grid_for(na, 128), 128, 0, st>>>(na, r_rowptr, p_ptr, p_idx, r_col, r_from_p, overflow);
+  B2S_LAUNCH_CHECK();
+  return B2S_OK;
+}
+
+/* Pattern and term lists of A_c = R W, one thread per coarse row (the order of the row-owned
+ * Galerkin kernel; see c_pattern_k), in two passes like the P and W builders: pass 0 writes
+ * ccnt and tcnt, the caller scans them into c_ptr and t_ptr and allocates; pass 1 writes c_idx,
+ * c_diag [na], c_tptr [c_nnz + 1], c_te and c_ts. *overflow: 1 where a row has more than 128
+ * distinct columns, 2 where the offsets disagree with the counts. */
+int b2s_amg_c_pattern_d(int32_t na, const int32_t* r_rowptr, const int32_t* r_col, const int32_t* w_ptr,
+                        const int32_t* w_idx, int32_t pass, int32_t* ccnt, int32_t* tcnt, const int32_t* c_ptr,
+                        const int32_t* t_ptr, int64_t c_cap, int64_t t_cap, int32_t* c_idx, int32_t* c_diag,
+                        int32_t* c_tptr, int32_t* c_te, int32_t* c_ts, int32_t* overflow, b2s_stream_t s) {
+  if (na < 1 || !r_rowptr || !r_col || !w_ptr || !w_idx || !overflow || (pass == 0 && (!ccnt || !tcnt)) ||
+      (pass == 1 && (!c_ptr || !t_ptr || !c_idx || !c_diag || !c_tptr || !c_te || !c_ts)) ||
+      (pass != 0 && pass != 1))
+    return B2S_ERR_ARG;
+  c_pattern_k<<<grid_for(na, 128), 128, 0, (cudaStream_t)s>>>(na, r_rowptr, r_col, w_ptr, w_idx, pass, ccnt, tcnt,
+                                                              c_ptr, t_ptr, c_cap, t_cap, c_idx, c_diag, c_tptr,
+                                                              c_te, c_ts, overflow);
   B2S_LAUNCH_CHECK();
   return B2S_OK;
 }

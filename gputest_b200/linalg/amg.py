@@ -4,9 +4,9 @@ The set-up is the reference's (``flowtrace/linalg/amg.py:80-117``): strength of 
 the greedy three-pass aggregation, P = (I - 4/(3 rho) D^-1 A) T, W = A P and A_c = P^T W,
 level by level. ``AMGHierarchy.on_device`` does it on the device: strength flags and the
 aggregation in CUDA (``b2s_amg_strength_d``, ``b2s_amg_aggregate_d``, which reproduces the
-sequential greedy exactly), the patterns and term lists of the products (P and W one row per
-thread, ``row_patterns``; R and A_c, and rows too long for those kernels, from sorted distinct
-keys, ``product_patterns``), and each level's numeric rebuild, whose Galerkin product gives the
+sequential greedy exactly), the patterns and term lists of the products (P, W, R and A_c one
+row per thread, ``row_products``; rows too long for those kernels from sorted distinct keys,
+``product_patterns``), and each level's numeric rebuild, whose Galerkin product gives the
 next level's values. ``AMGHierarchy(...)`` is the same set-up on the host (SciPy, the C++ helper
 ``b2s_host_aggregate``); batches of independent cases use it. Afterwards every numeric quantity
 is rebuilt on the device by ``rebuild()`` (``b2s_amg_rebuild_d``): D^-1, the spectral radius by
@@ -195,11 +195,18 @@ def _rows_of(ptr, nnz):
     return torch.repeat_interleave(torch.arange(n, device=ptr.device), ptr[1:] - ptr[:-1], output_size=nnz)
 
 
-def row_patterns(rp, cl, agg, stream=None):
-    """The P and W patterns and term lists by the per-row kernels (``b2s_amg_p_pattern_d``,
-    ``b2s_amg_w_pattern_d``; rp, cl, agg int32 device tensors), the same arrays as the key-based
-    construction of ``product_patterns``; None when a row exceeds the kernels' per-thread
-    capacity (the caller uses the key-based construction). Three host synchronisations."""
+def row_products(rp, cl, agg, na, stream=None):
+    """Every pattern and term list of a level's products by the per-row kernels: P and W
+    (``b2s_amg_p_pattern_d``, ``b2s_amg_w_pattern_d``), R = P^T (``b2s_amg_r_pattern_d``) and
+    A_c = R W (``b2s_amg_c_pattern_d``); rp, cl, agg int32 device tensors, na aggregates. The
+    keys of ``product_patterns`` as int32 tensors, with ``c_diag`` (the slot of each coarse
+    row's diagonal) in place of ``c_keys``, ``conflicts`` (the next level's aggregation work-space
+    bound: A_c's entries plus its squared row lengths) and ``check``, a device int that is
+    nonzero if A_c's fill pass found its offsets inconsistent (read at the caller's next
+    synchronisation). Two host synchronisations. Where a row exceeds the P or W kernel (64
+    entries, 128 W terms) the result is None; where it exceeds the R or A_c kernel (256 R
+    entries, 128 distinct A_c columns), or a term list ``TERM_CAP``, it holds P and W only, with
+    ``complete`` False (``product_patterns`` adds R and A_c from sorted keys)."""
     import torch
 
     L = _lib.lib()
@@ -207,46 +214,71 @@ def row_patterns(rp, cl, agg, stream=None):
     dev = cl.device
     n, nnz = rp.numel() - 1, cl.numel()
     e32 = lambda k: torch.empty(max(int(k), 1), dtype=torch.int32, device=dev)  # noqa: E731
-    ov = torch.zeros(1, dtype=torch.int32, device=dev)
-    ws = e32(L.b2s_scan_workspace_bytes(n) // 4 + 1)
+    ov = torch.zeros(1, dtype=torch.int32, device=dev)  # P and W kernels
+    ovc = torch.zeros(1, dtype=torch.int32, device=dev)  # R and A_c kernels
+    ws = e32(L.b2s_scan_workspace_bytes(max(n, na)) // 4 + 1)
 
-    def scan(counts):
-        out = e32(n + 1)
-        _lib.check(L.b2s_scan_counts_d(n, counts.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel() * 4, sp_),
+    def scan(counts, m):
+        out = e32(m + 1)
+        _lib.check(L.b2s_scan_counts_d(m, counts.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel() * 4, sp_),
                    "b2s_scan_counts_d")
         return out
 
+    # P: counts, offsets, then the fill into room for nnz entries (a P row has at most as many
+    # entries as the A row), so the sizes are read once, together with W's
     pcnt = e32(n)
     _lib.check(L.b2s_amg_p_pattern_d(n, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 0, pcnt.data_ptr(), None, 0,
                                      None, None, None, nnz, ov.data_ptr(), sp_), "b2s_amg_p_pattern_d")
-    p_ptr = scan(pcnt)
-    h = torch.cat([ov, p_ptr[n:]]).cpu()
-    if int(h[0]):
-        return None
-    p_nnz = int(h[1])
-    p_idx, p_tptr, p_tj = e32(p_nnz), e32(p_nnz + 1), e32(nnz)
+    p_ptr = scan(pcnt, n)
+    p_idx, p_tptr, p_tj = e32(nnz), e32(nnz + 1), e32(nnz)
     _lib.check(L.b2s_amg_p_pattern_d(n, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 1, None, p_ptr.data_ptr(),
-                                     p_nnz, p_idx.data_ptr(), p_tptr.data_ptr(), p_tj.data_ptr(), nnz, ov.data_ptr(),
+                                     nnz, p_idx.data_ptr(), p_tptr.data_ptr(), p_tj.data_ptr(), nnz, ov.data_ptr(),
                                      sp_), "b2s_amg_p_pattern_d")
     wcnt, tcnt = e32(n), e32(n)
     _lib.check(L.b2s_amg_w_pattern_d(n, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 0,
                                      wcnt.data_ptr(), tcnt.data_ptr(), None, None, 0, 0, None, None, None, None,
                                      ov.data_ptr(), sp_), "b2s_amg_w_pattern_d")
-    w_ptr, t_ptr = scan(wcnt), scan(tcnt)
-    h = torch.cat([ov, w_ptr[n:], t_ptr[n:]]).cpu()
-    if int(h[0]) or int(h[2]) > TERM_CAP:
+    w_ptr, t_ptr = scan(wcnt, n), scan(tcnt, n)
+    h = torch.cat([ov, p_ptr[n:], w_ptr[n:], t_ptr[n:]]).cpu()
+    if int(h[0]) or int(h[3]) > TERM_CAP:
         return None
-    w_nnz, w_terms = int(h[1]), int(h[2])
+    p_nnz, w_nnz, w_terms = int(h[1]), int(h[2]), int(h[3])
     w_idx, w_tptr, w_tj, w_te = e32(w_nnz), e32(w_nnz + 1), e32(w_terms), e32(w_terms)
     _lib.check(L.b2s_amg_w_pattern_d(n, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 1, None,
                                      None, w_ptr.data_ptr(), t_ptr.data_ptr(), w_nnz, w_terms, w_idx.data_ptr(),
                                      w_tptr.data_ptr(), w_tj.data_ptr(), w_te.data_ptr(), ov.data_ptr(), sp_),
                "b2s_amg_w_pattern_d")
-    if int(ov.item()):
-        return None
-    return {"p_ptr": p_ptr, "p_idx": p_idx[:p_nnz], "p_tptr": p_tptr[:p_nnz + 1], "p_tj": p_tj[:nnz],
-            "w_ptr": w_ptr, "w_idx": w_idx[:w_nnz], "w_tptr": w_tptr[:w_nnz + 1], "w_tj": w_tj[:w_terms],
-            "w_te": w_te[:w_terms]}
+    out = {"p_ptr": p_ptr, "p_idx": p_idx[:p_nnz], "p_tptr": p_tptr[:p_nnz + 1], "p_tj": p_tj[:nnz],
+           "w_ptr": w_ptr, "w_idx": w_idx[:w_nnz], "w_tptr": w_tptr[:w_nnz + 1], "w_tj": w_tj[:w_terms],
+           "w_te": w_te[:w_terms], "complete": False}
+    # R = P^T (no sizes to read), then A_c's counts
+    r_rowptr, r_col, r_from_p = e32(na + 1), e32(p_nnz), e32(p_nnz)
+    rw = e32(L.b2s_amg_r_workspace_bytes(na) // 4 + 1)
+    _lib.check(L.b2s_amg_r_pattern_d(n, na, p_ptr.data_ptr(), p_idx.data_ptr(), p_nnz, r_rowptr.data_ptr(),
+                                     r_col.data_ptr(), r_from_p.data_ptr(), rw.data_ptr(), rw.numel() * 4,
+                                     ovc.data_ptr(), sp_), "b2s_amg_r_pattern_d")
+    ccnt, ctc = e32(na), e32(na)
+    _lib.check(L.b2s_amg_c_pattern_d(na, r_rowptr.data_ptr(), r_col.data_ptr(), w_ptr.data_ptr(), w_idx.data_ptr(), 0,
+                                     ccnt.data_ptr(), ctc.data_ptr(), None, None, 0, 0, None, None, None, None, None,
+                                     ovc.data_ptr(), sp_), "b2s_amg_c_pattern_d")
+    c_ptr, ct_ptr = scan(ccnt, na), scan(ctc, na)
+    sq = ccnt[:na].to(torch.int64)
+    h = torch.cat([ov.to(torch.int64), ovc.to(torch.int64), c_ptr[na:].to(torch.int64),
+                   ct_ptr[na:].to(torch.int64), (sq * sq).sum().view(1)]).cpu()
+    if int(h[0]):
+        raise RuntimeError("AMG set-up: the W pattern kernel's offsets disagree with its counts")
+    if int(h[1]) or int(h[3]) > TERM_CAP:
+        return out  # a row too long for the R or A_c kernel
+    c_nnz, c_terms = int(h[2]), int(h[3])
+    c_idx, c_diag, c_tptr, c_te, c_ts = e32(c_nnz), e32(na), e32(c_nnz + 1), e32(c_terms), e32(c_terms)
+    _lib.check(L.b2s_amg_c_pattern_d(na, r_rowptr.data_ptr(), r_col.data_ptr(), w_ptr.data_ptr(), w_idx.data_ptr(), 1,
+                                     None, None, c_ptr.data_ptr(), ct_ptr.data_ptr(), c_nnz, c_terms, c_idx.data_ptr(),
+                                     c_diag.data_ptr(), c_tptr.data_ptr(), c_te.data_ptr(), c_ts.data_ptr(),
+                                     ovc.data_ptr(), sp_), "b2s_amg_c_pattern_d")
+    out.update(r_rowptr=r_rowptr, r_col=r_col[:p_nnz], r_from_p=r_from_p[:p_nnz], c_ptr=c_ptr, c_idx=c_idx[:c_nnz],
+               c_diag=c_diag[:na], c_tptr=c_tptr[:c_nnz + 1], c_te=c_te[:c_terms], c_ts=c_ts[:c_terms],
+               conflicts=c_nnz + int(h[4]), check=ovc, complete=True)
+    return out
 
 
 def product_patterns(rp, cl, agg, na, cap=TERM_CAP, pw=None):
@@ -339,17 +371,20 @@ def device_transpose_slots(rowptr, col, sorted_cols, stream=None):
     return tslot, missing
 
 
-def device_aggregate(rowptr, col, strong, tslot, prio, rank_node, stream=None):
+def device_aggregate(rowptr, col, strong, tslot, prio, rank_node, stream=None, capacity=None):
     """The reference's greedy aggregation on the device (``b2s_amg_aggregate_d``), nodes visited
     in the order ``prio``: (agg int32 [n], counts int32 [n], info int32 [4]) on the device;
-    info[0] is the number of aggregates, info[1] an error code."""
+    info[0] is the number of aggregates, info[1] an error code. ``capacity``: the conflict lists'
+    room, nnz plus the sum of squared row lengths (computed here, with a host synchronisation,
+    when not given)."""
     import torch
 
     n = rowptr.numel() - 1
     dev = col.device
     L = _lib.lib()
-    rl = (rowptr[1:] - rowptr[:-1]).to(torch.int64)
-    capacity = int(col.numel() + int((rl * rl).sum()))  # bounds every node's conflict list
+    if capacity is None:
+        rl = (rowptr[1:] - rowptr[:-1]).to(torch.int64)
+        capacity = int(col.numel() + int((rl * rl).sum()))  # bounds every node's conflict list
     wb = L.b2s_amg_aggregate_workspace_bytes(n, capacity)
     if wb < 0:
         raise RuntimeError("invalid aggregation size")
@@ -362,6 +397,12 @@ def device_aggregate(rowptr, col, strong, tslot, prio, rank_node, stream=None):
                                      info.data_ptr(), work.data_ptr(), work.numel() * 4, _lib.stream_ptr(stream)),
                "b2s_amg_aggregate_d")
     return agg, counts, info
+
+
+def _pattern_checks(flags):
+    """Raise where an A_c fill pass (``row_products``) found its offsets inconsistent."""
+    if flags.numel() and bool((flags != 0).any()):
+        raise RuntimeError("AMG set-up: the A_c pattern kernel's offsets disagree with its counts")
 
 
 _START_VECTORS = {}
@@ -391,7 +432,7 @@ class AMGHierarchy:
     before every rebuild.
     """
 
-    ROW_PATTERNS = True  # device set-up: P and W by the per-row kernels where rows fit them
+    ROW_PATTERNS = True  # device set-up: the products' patterns by the per-row kernels where rows fit them
 
     def __init__(self, A_host, perm, rowptr, col, diag_slot, val, slot_ref, singular=False, theta=0.08,
                  max_coarse=150, max_levels=20, sweeps=2, omega=0.8, groups=None, group_singular=None):
@@ -617,10 +658,7 @@ class AMGHierarchy:
                 self.sizes.append(prev.sizes[l])
             nxt = prev._keep[2 * start - 1]
             lv_rp, lv_cl, lv_val, lv_diag = nxt["rowptr"], nxt["col"], nxt["val"], nxt["diag"]
-            lv_rp64 = nxt.get("rowptr64", None)
-            lv_rp64 = lv_rp.to(torch.int64) if lv_rp64 is None else lv_rp64
-            lv_cl64 = nxt.get("col64", None)
-            lv_cl64 = lv_cl.to(torch.int64) if lv_cl64 is None else lv_cl64
+            lv_rp64, lv_cl64 = nxt.get("rowptr64", lv_rp), nxt.get("col64", lv_cl)
             n = prev.sizes[start]
             prio = rank_node = torch.arange(n, dtype=torch.int32, device=dev)
             x0_src = _start_vector(n, dev)
@@ -634,16 +672,20 @@ class AMGHierarchy:
             rank_node = torch.empty(n0, dtype=torch.int32, device=dev)
             rank_node[perm_t] = torch.arange(n0, dtype=torch.int32, device=dev)
             lv_rp, lv_cl, lv_val, lv_diag = rowptr, col, self.val0, diag_slot
-            lv_rp64, lv_cl64 = rowptr.to(torch.int64), col.to(torch.int64)
+            lv_rp64, lv_cl64 = rowptr, col  # widened where the sorted-key construction needs them
             x0_src = _start_vector(n0, dev)[perm_t]
             sorted_cols = False  # level 0's columns are in the reference's order, not the device's
             n = n0
         nlev = start
+        conflicts, checks = None, []
         while n > max_coarse and nlev < max_levels - 1:
             strong = device_strength(lv_rp, lv_cl, lv_val, lv_diag, theta, stream)
             tslot, missing = device_transpose_slots(lv_rp, lv_cl, sorted_cols, stream)
-            agg, counts, info = device_aggregate(lv_rp, lv_cl, strong, tslot, prio, rank_node, stream)
-            ih = torch.cat([info, missing]).cpu()  # the level's read-back: aggregates and errors
+            agg, counts, info = device_aggregate(lv_rp, lv_cl, strong, tslot, prio, rank_node, stream, conflicts)
+            # the level's read-back: aggregates and errors, and the previous level's A_c check
+            ih = torch.cat([info, missing] + checks).cpu()
+            _pattern_checks(ih[5:])
+            checks = []
             if int(ih[4]) != 0:
                 raise RuntimeError("AMG set-up: the level's pattern is not structurally symmetric")
             if int(ih[1]) != 0:
@@ -651,8 +693,13 @@ class AMGHierarchy:
             na = int(ih[0])
             if na >= n * 0.9:
                 break
-            pw = row_patterns(lv_rp, lv_cl, agg, stream) if self._row_patterns else None
-            pat = product_patterns(lv_rp64, lv_cl64, agg.to(torch.int64), na, pw=pw)
+            pat = row_products(lv_rp, lv_cl, agg, na, stream) if self._row_patterns else None
+            if pat is None or not pat["complete"]:
+                pat = product_patterns(lv_rp64.to(torch.int64), lv_cl64.to(torch.int64), agg.to(torch.int64), na,
+                                       pw=pat)
+            else:
+                checks.append(pat["check"])
+            conflicts = pat.get("conflicts")
             Lv = h.levels[nlev]
             Lv.n, Lv.nnz, Lv.nc = n, lv_cl.numel(), na
             Lv.p_nnz, Lv.w_nnz = pat["p_idx"].numel(), pat["w_idx"].numel()
@@ -686,7 +733,7 @@ class AMGHierarchy:
             _lib.check(L.b2s_amg_level_rebuild_d(ctypes.byref(Lv), c_rp.data_ptr(), c_cl.data_ptr(), c_val.data_ptr(),
                                                  work.data_ptr(), work.numel() * 8, sp_), "b2s_amg_level_rebuild_d")
             ar = torch.arange(na, device=dev)
-            lv_diag = i32(torch.searchsorted(pat["c_keys"], ar * na + ar))
+            lv_diag = pat["c_diag"] if "c_diag" in pat else i32(torch.searchsorted(pat["c_keys"], ar * na + ar))
             lv_rp, lv_cl, lv_val = c_rp, c_cl, c_val
             lv_rp64, lv_cl64 = pat["c_ptr"], pat["c_idx"]
             self._keep.append({"rowptr": lv_rp, "col": lv_cl, "val": lv_val, "diag": lv_diag, "work": work,
@@ -696,6 +743,8 @@ class AMGHierarchy:
             sorted_cols = True
             n = na
             nlev += 1
+        if checks:
+            _pattern_checks(torch.cat(checks).cpu())
         h.nlevels = nlev
         self.n_levels = nlev + 1
         self.coarse_n = n

@@ -490,6 +490,23 @@ B2S_API int b2s_amg_w_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl,
                                 const int32_t* p_idx, int32_t pass, int32_t* wcnt, int32_t* tcnt, const int32_t* w_ptr,
                                 const int32_t* t_ptr, int64_t w_cap, int64_t t_cap, int32_t* w_idx, int32_t* w_tptr,
                                 int32_t* w_tj, int32_t* w_te, int32_t* overflow, b2s_stream_t s);
+/* R = P^T (the transposes of amg.py:102,115): r_rowptr [na + 1], r_col [p_nnz] (fine rows,
+ * ascending in each row) and r_from_p [p_nnz] (the P entry of each R entry), from P's pattern
+ * (each row's columns ascending), with no host synchronisation; work space from
+ * b2s_amg_r_workspace_bytes(na). *overflow: 1 where an R row has more than 256 entries. */
+B2S_API int64_t b2s_amg_r_workspace_bytes(int32_t na);
+B2S_API int b2s_amg_r_pattern_d(int32_t n, int32_t na, const int32_t* p_ptr, const int32_t* p_idx, int64_t p_nnz,
+                                int32_t* r_rowptr, int32_t* r_col, int32_t* r_from_p, void* work, int64_t work_bytes,
+                                int32_t* overflow, b2s_stream_t s);
+/* The pattern of A_c = R W (the Galerkin product P^T A P, amg.py:102) with its term lists, one
+ * thread per coarse row, in the two passes of the P and W builders: pass 0 writes ccnt (A_c
+ * entries) and tcnt (terms) per row; pass 1 fills c_idx, c_diag [na] (the slot of each row's
+ * diagonal), c_tptr [c_nnz + 1], c_te (R entries) and c_ts (W entries). *overflow: 1 where a row
+ * has more than 128 distinct columns, 2 where the offsets disagree with the counts. */
+B2S_API int b2s_amg_c_pattern_d(int32_t na, const int32_t* r_rowptr, const int32_t* r_col, const int32_t* w_ptr,
+                                const int32_t* w_idx, int32_t pass, int32_t* ccnt, int32_t* tcnt, const int32_t* c_ptr,
+                                const int32_t* t_ptr, int64_t c_cap, int64_t t_cap, int32_t* c_idx, int32_t* c_diag,
+                                int32_t* c_tptr, int32_t* c_te, int32_t* c_ts, int32_t* overflow, b2s_stream_t s);
 /* Exclusive scan of n int32 counts into out[0..n], out[n] the total. */
 B2S_API int64_t b2s_scan_workspace_bytes(int32_t n);
 B2S_API int b2s_scan_counts_d(int32_t n, const int32_t* counts, int32_t* out, void* work, int64_t work_bytes,

@@ -186,11 +186,12 @@ def test_partial_reaggregation_equals_a_full_device_set_up():
 
 
 @pytest.mark.parametrize("kind,n,seed", [("grid", 2500, 11), ("grid", 10000, 14), ("random", 3000, 12)])
-def test_row_pattern_kernels_equal_the_key_based_patterns(kind, n, seed):
-    """``row_patterns`` (one thread per row) against the sorted-key construction of
-    ``product_patterns`` on the same level and aggregates: every pattern and term list equal
-    where every row fits the kernels (at most 64 entries and 128 W terms), the level handed back
-    (None) where one does not (the random graph: up to 177 W terms in a row)."""
+def test_row_product_kernels_equal_the_key_based_patterns(kind, n, seed):
+    """``row_products`` (one thread per row: P, W, R = P^T and A_c) against the sorted-key
+    construction of ``product_patterns`` on the same level and aggregates: every pattern and term
+    list equal where every row fits the kernels (at most 64 entries and 128 W terms), the level
+    handed back (None) where one does not (the random graph: up to 177 W terms in a row); the
+    diagonal slots and the next level's conflict bound from the same pattern."""
     import scipy.sparse as sp
     import torch
 
@@ -209,15 +210,49 @@ def test_row_pattern_kernels_equal_the_key_based_patterns(kind, n, seed):
     terms = max(int(plen[A.indices[A.indptr[i]:A.indptr[i + 1]]].sum()) for i in range(n))
     fits = terms <= 128 and int(np.diff(A.indptr).max()) <= 64
     agg = torch.as_tensor(agg_h, dtype=torch.int32, device="cuda")
-    pw = amg.row_patterns(rp, cl, agg)
+    pw = amg.row_products(rp, cl, agg, na)
     assert (pw is not None) == fits
     if fits:
+        assert pw["complete"] and int(pw["check"].item()) == 0
         ref = amg.product_patterns(rp.long(), cl.long(), agg.long(), na)
-        for k in ("p_ptr", "p_idx", "w_ptr", "w_idx"):
+        for k in ("p_ptr", "p_idx", "w_ptr", "w_idx", "r_rowptr", "r_col", "r_from_p", "c_ptr", "c_idx"):
             assert torch.equal(pw[k].long(), ref[k]), k
-        for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te"):
+        for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te", "c_ts"):
             assert torch.equal(pw[k], ref[k]), k
+        ar = torch.arange(na, device="cuda")
+        assert torch.equal(pw["c_diag"].long(), torch.searchsorted(ref["c_keys"], ar * na + ar))
+        cl_len = (ref["c_ptr"][1:] - ref["c_ptr"][:-1])
+        assert pw["conflicts"] == ref["c_idx"].numel() + int((cl_len * cl_len).sum())
     # a row of 70 entries is over the P kernel's 64: the level is handed back
     rp2 = torch.tensor([0, 70], dtype=torch.int32, device="cuda")
     cl2 = torch.zeros(70, dtype=torch.int32, device="cuda")
-    assert amg.row_patterns(rp2, cl2, torch.zeros(1, dtype=torch.int32, device="cuda")) is None
+    assert amg.row_products(rp2, cl2, torch.zeros(1, dtype=torch.int32, device="cuda"), 1) is None
+
+
+@pytest.mark.parametrize("m,why", [(300, "R row"), (256, "A_c row")])
+def test_row_products_hand_r_and_a_c_back_where_a_row_does_not_fit(m, why):
+    """A path of m nodes whose even nodes form aggregate 0 and whose odd nodes are singletons: P
+    and W fit the kernels, but R's row 0 holds every node (over 256 entries for m = 300) or A_c's
+    row 0 every aggregate (129 distinct columns for m = 256, over 128). P and W come back with
+    ``complete`` False, and ``product_patterns`` completes them to the key-based level."""
+    import scipy.sparse as sp
+    import torch
+
+    from gputest_b200.linalg import amg
+
+    i = np.arange(m - 1)
+    A = sp.csr_matrix((np.ones(2 * (m - 1)), (np.r_[i, i + 1], np.r_[i + 1, i])), shape=(m, m)) + sp.eye(m)
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    agg_h = np.where(np.arange(m) % 2 == 0, 0, (np.arange(m) + 1) // 2)
+    na = int(agg_h.max()) + 1
+    rp, cl, _, _, _ = _device_csr(A, np.random.default_rng(m))
+    agg = torch.as_tensor(agg_h, dtype=torch.int32, device="cuda")
+    pw = amg.row_products(rp, cl, agg, na)
+    assert pw is not None and not pw["complete"], why
+    got = amg.product_patterns(rp.long(), cl.long(), agg.long(), na, pw=pw)
+    ref = amg.product_patterns(rp.long(), cl.long(), agg.long(), na)
+    for k in ("p_ptr", "p_idx", "w_ptr", "w_idx", "r_rowptr", "r_col", "r_from_p", "c_ptr", "c_idx", "c_keys"):
+        assert torch.equal(got[k].long(), ref[k]), k
+    for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te", "c_ts"):
+        assert torch.equal(got[k], ref[k]), k
