@@ -320,8 +320,9 @@ __global__ void aggregate_sizes_k(int n, const int32_t* __restrict__ agg, int32_
 // ------------------------------------------------------------------ P and W patterns, per row
 // P = A T has, in row i, one entry per distinct aggregate among the columns of A's row i; W = A P
 // one per distinct column among the P rows of those columns. One thread builds one row in
-// local arrays (rows of at most kMaxRowP entries, at most kMaxRowW W candidates; a longer row
-// raises *overflow and the caller builds the level with sorted keys instead). The term lists
+// local arrays (at most kMaxRowP distinct P columns and kMaxRowW distinct W columns a row, any
+// number of A entries and W terms; a row with more raises *overflow and the caller builds the
+// level with sorted keys instead). The term lists
 // follow the order the row-owned rebuild kernels add terms in: P slot (i, J) lists the A
 // entries of row i with aggregate J in stored order; W slot (i, c) lists the pairs (A entry e of
 // row i, P entry f of row col[e]) with column c, e in stored order, then f.
@@ -365,15 +366,15 @@ __global__ void p_pattern_k(int n, const int32_t* __restrict__ rp, const int32_t
                             int32_t* __restrict__ overflow) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int e0 = rp[i], e1 = rp[i + 1];
-    if (e1 - e0 > kMaxRowP) {
+    int32_t u[kMaxRowP];
+    int m = 0;
+    bool full = false;
+    for (int e = e0; e < e1 && !full; ++e) m = insert_distinct(u, m, kMaxRowP, agg[cl[e]], full);
+    if (full) {
       atomicExch(overflow, 1);
       if (pass == 0) pcnt[i] = 0;
       continue;
     }
-    int32_t u[kMaxRowP];
-    int m = 0;
-    bool full = false;
-    for (int e = e0; e < e1; ++e) m = insert_distinct(u, m, kMaxRowP, agg[cl[e]], full);
     if (pass == 0) {
       pcnt[i] = m;
       continue;
@@ -417,23 +418,23 @@ __global__ void w_pattern_k(int n, const int32_t* __restrict__ rp, const int32_t
                             int32_t* __restrict__ w_te, int32_t* __restrict__ overflow) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int e0 = rp[i], e1 = rp[i + 1];
-    int terms = 0;
-    for (int e = e0; e < e1; ++e) terms += p_ptr[cl[e] + 1] - p_ptr[cl[e]];
-    if (terms > kMaxRowW) {
+    int32_t u[kMaxRowW];
+    int m = 0;
+    int64_t terms = 0;
+    bool full = false;
+    for (int e = e0; e < e1 && !full; ++e) {
+      const int j = cl[e];
+      for (int f = p_ptr[j]; f < p_ptr[j + 1]; ++f) m = insert_distinct(u, m, kMaxRowW, p_idx[f], full);
+      terms += p_ptr[j + 1] - p_ptr[j];
+    }
+    if (full || terms > INT32_MAX) {
       atomicExch(overflow, 1);
       if (pass == 0) wcnt[i] = tcnt[i] = 0;
       continue;
     }
-    int32_t u[kMaxRowW];
-    int m = 0;
-    bool full = false;
-    for (int e = e0; e < e1; ++e) {
-      const int j = cl[e];
-      for (int f = p_ptr[j]; f < p_ptr[j + 1]; ++f) m = insert_distinct(u, m, kMaxRowW, p_idx[f], full);
-    }
     if (pass == 0) {
       wcnt[i] = m;
-      tcnt[i] = terms;
+      tcnt[i] = (int32_t)terms;
       continue;
     }
     const int64_t base = w_ptr[i], tb = t_ptr[i];
@@ -718,7 +719,8 @@ int b2s_amg_aggregate_d(int32_t n, const int32_t* rowptr, const int32_t* col, co
  * kernels; see p_pattern_k / w_pattern_k). Each builder has two passes: pass 0 writes per-row
  * counts (pcnt; wcnt and tcnt), the caller scans them into p_ptr (w_ptr, t_ptr) and allocates;
  * pass 1 fills. *overflow (device int, not cleared here): 1 where a row exceeds the per-thread
- * capacity (64 A entries, 128 W terms), 2 where the offsets disagree with the counts. */
+ * capacity (64 distinct P columns, 128 distinct W columns), 2 where the offsets disagree with the
+ * counts. */
 int b2s_amg_p_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* agg, int32_t pass,
                         int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx, int32_t* p_tptr,
                         int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s) {

@@ -204,7 +204,7 @@ def row_products(rp, cl, agg, na, stream=None):
     bound: A_c's entries plus its squared row lengths) and ``check``, a device int that is
     nonzero if A_c's fill pass found its offsets inconsistent (read at the caller's next
     synchronisation). Two host synchronisations. Where a row exceeds the P or W kernel (64
-    entries, 128 W terms) the result is None; where it exceeds the R or A_c kernel (256 R
+    distinct P columns, 128 distinct W columns) the result is None; where it exceeds the R or A_c kernel (256 R
     entries, 128 distinct A_c columns), or a term list ``TERM_CAP``, it holds P and W only, with
     ``complete`` False (``product_patterns`` adds R and A_c from sorted keys)."""
     import torch
@@ -433,6 +433,11 @@ class AMGHierarchy:
     """
 
     ROW_PATTERNS = True  # device set-up: the products' patterns by the per-row kernels where rows fit them
+    # Levels with fewer rows take the sorted keys: one thread per row walks a dense coarse row's
+    # terms one after another (measured on the 131k cavity's hierarchy: 1.0 ms by the kernels
+    # against about 4 ms by the keys at 32,768 rows; 2.5 against 2 ms at 4,400, 4.3 against
+    # 1.7 ms at 507).
+    ROW_KERNEL_MIN_ROWS = 8192
 
     def __init__(self, A_host, perm, rowptr, col, diag_slot, val, slot_ref, singular=False, theta=0.08,
                  max_coarse=150, max_levels=20, sweeps=2, omega=0.8, groups=None, group_singular=None):
@@ -693,7 +698,8 @@ class AMGHierarchy:
             na = int(ih[0])
             if na >= n * 0.9:
                 break
-            pat = row_products(lv_rp, lv_cl, agg, na, stream) if self._row_patterns else None
+            kernels = self._row_patterns and n >= cls.ROW_KERNEL_MIN_ROWS
+            pat = row_products(lv_rp, lv_cl, agg, na, stream) if kernels else None
             if pat is None or not pat["complete"]:
                 pat = product_patterns(lv_rp64.to(torch.int64), lv_cl64.to(torch.int64), agg.to(torch.int64), na,
                                        pw=pat)

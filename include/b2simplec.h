@@ -481,8 +481,9 @@ B2S_API int b2s_amg_coarse_inverse_d(const b2s_amg* h, void* work, int64_t work_
  * Two passes each: pass 0 writes per-row counts (pcnt; wcnt = W entries, tcnt = W terms), which
  * the caller scans (b2s_scan_counts_d) into p_ptr (w_ptr, t_ptr) and allocates from; pass 1
  * fills p_idx, p_tptr, p_tj (w_idx, w_tptr, w_tj, w_te), never past p_cap/nnz (w_cap/t_cap).
- * *overflow (device int, not cleared): 1 where a row has more than 64 entries or 128 W terms,
- * 2 where the offsets disagree with the counts; the caller then builds the level another way. */
+ * *overflow (device int, not cleared): 1 where a row has more than 64 distinct P columns or 128
+ * distinct W columns, 2 where the offsets disagree with the counts; the caller then builds the
+ * level another way. */
 B2S_API int b2s_amg_p_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* agg, int32_t pass,
                                 int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx, int32_t* p_tptr,
                                 int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s);

@@ -88,12 +88,18 @@ def _meshes():
 
 @pytest.mark.parametrize("which", [0, 1])
 @pytest.mark.parametrize("theta", [0.08, 0.0])
-def test_device_hierarchy_equals_the_host_hierarchy(which, theta):
+@pytest.mark.parametrize("all_kernels", [False, True])
+def test_device_hierarchy_equals_the_host_hierarchy(which, theta, all_kernels, monkeypatch):
     """Both set-ups from the same pressure-correction matrix: the same levels, aggregates,
-    patterns and strong flags, and the same V-cycle bit for bit."""
+    patterns and strong flags, and the same V-cycle bit for bit; with the products' patterns by
+    the per-row kernels on every level that fits them, or on the large levels only (the
+    default)."""
     import torch
 
     from gputest_b200.linalg.amg import AMGHierarchy
+
+    if all_kernels:
+        monkeypatch.setattr(AMGHierarchy, "ROW_KERNEL_MIN_ROWS", 0)
 
     s = _pressure_system(_meshes()[which])
     fv = s.fv
@@ -189,9 +195,11 @@ def test_partial_reaggregation_equals_a_full_device_set_up():
 def test_row_product_kernels_equal_the_key_based_patterns(kind, n, seed):
     """``row_products`` (one thread per row: P, W, R = P^T and A_c) against the sorted-key
     construction of ``product_patterns`` on the same level and aggregates: every pattern and term
-    list equal where every row fits the kernels (at most 64 entries and 128 W terms), the level
-    handed back (None) where one does not (the random graph: up to 177 W terms in a row); the
-    diagonal slots and the next level's conflict bound from the same pattern."""
+    list equal where every row fits the kernels (at most 64 distinct P columns, 128 distinct W
+    columns, 256 R entries and 128 distinct A_c columns), the diagonal slots and the next level's
+    conflict bound from the same pattern; P and W alone where an A_c row does not fit (the random
+    graph), completed by the sorted keys; the level handed back (None) where a P row does not
+    fit."""
     import scipy.sparse as sp
     import torch
 
@@ -206,27 +214,34 @@ def test_row_product_kernels_equal_the_key_based_patterns(kind, n, seed):
     agg_h, na = amg.aggregate(S)
     T = sp.csr_matrix((np.ones(n), (np.arange(n), agg_h)), shape=(n, na))
     Pp = amg._pattern(amg._pattern(A) @ T)
-    plen = np.diff(Pp.indptr)
-    terms = max(int(plen[A.indices[A.indptr[i]:A.indptr[i + 1]]].sum()) for i in range(n))
-    fits = terms <= 128 and int(np.diff(A.indptr).max()) <= 64
+    Wp = amg._pattern(amg._pattern(A) @ Pp)
+    Cp = amg._pattern(Pp.T @ Wp)
+    pw_fits = int(np.diff(Pp.indptr).max()) <= 64 and int(np.diff(Wp.indptr).max()) <= 128
+    rc_fits = int(np.bincount(Pp.indices, minlength=na).max()) <= 256 and int(np.diff(Cp.indptr).max()) <= 128
+    assert pw_fits and rc_fits == (kind == "grid")  # the random graph's A_c rows: up to 550 columns
     agg = torch.as_tensor(agg_h, dtype=torch.int32, device="cuda")
     pw = amg.row_products(rp, cl, agg, na)
-    assert (pw is not None) == fits
-    if fits:
-        assert pw["complete"] and int(pw["check"].item()) == 0
-        ref = amg.product_patterns(rp.long(), cl.long(), agg.long(), na)
-        for k in ("p_ptr", "p_idx", "w_ptr", "w_idx", "r_rowptr", "r_col", "r_from_p", "c_ptr", "c_idx"):
-            assert torch.equal(pw[k].long(), ref[k]), k
-        for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te", "c_ts"):
-            assert torch.equal(pw[k], ref[k]), k
+    assert pw is not None and pw["complete"] == rc_fits
+    ref = amg.product_patterns(rp.long(), cl.long(), agg.long(), na)
+    got = pw if rc_fits else amg.product_patterns(rp.long(), cl.long(), agg.long(), na, pw=pw)
+    for k in ("p_ptr", "p_idx", "w_ptr", "w_idx", "r_rowptr", "r_col", "r_from_p", "c_ptr", "c_idx"):
+        assert torch.equal(got[k].long(), ref[k]), k
+    for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te", "c_ts"):
+        assert torch.equal(got[k], ref[k]), k
+    if rc_fits:
+        assert int(pw["check"].item()) == 0
         ar = torch.arange(na, device="cuda")
         assert torch.equal(pw["c_diag"].long(), torch.searchsorted(ref["c_keys"], ar * na + ar))
-        cl_len = (ref["c_ptr"][1:] - ref["c_ptr"][:-1])
+        cl_len = ref["c_ptr"][1:] - ref["c_ptr"][:-1]
         assert pw["conflicts"] == ref["c_idx"].numel() + int((cl_len * cl_len).sum())
-    # a row of 70 entries is over the P kernel's 64: the level is handed back
-    rp2 = torch.tensor([0, 70], dtype=torch.int32, device="cuda")
-    cl2 = torch.zeros(70, dtype=torch.int32, device="cuda")
-    assert amg.row_products(rp2, cl2, torch.zeros(1, dtype=torch.int32, device="cuda"), 1) is None
+    # a star of 70 nodes, each its own aggregate: the centre's P row has 70 distinct columns,
+    # over the P kernel's 64, and the level is handed back
+    star = sp.csr_matrix((np.ones(138), (np.r_[np.zeros(69, int), np.arange(1, 70)],
+                                         np.r_[np.arange(1, 70), np.zeros(69, int)])), shape=(70, 70)) + sp.eye(70)
+    star = sp.csr_matrix(star)
+    star.sort_indices()
+    rp2, cl2, _, _, _ = _device_csr(star, rng)
+    assert amg.row_products(rp2, cl2, torch.arange(70, dtype=torch.int32, device="cuda"), 70) is None
 
 
 @pytest.mark.parametrize("m,why", [(300, "R row"), (256, "A_c row")])
