@@ -13,7 +13,7 @@ from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "csrc", "libb2simplec.so")
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 B2S_OK = 0
 _ERRORS = {-1: "invalid argument", -2: "kernel launch failed", -3: "work space too small", -4: "no usable CUDA device",
@@ -123,8 +123,9 @@ _SIGS = {
     "b2s_amg_level_workspace_bytes": ([P], I64),
     "b2s_amg_level_rebuild_d": ([P, P, P, P, P, I64, P], ctypes.c_int),
     "b2s_amg_coarse_inverse_d": ([P, P, I64, P], ctypes.c_int),
-    "b2s_amg_p_pattern_d": ([I32, P, P, P, I32, P, P, I64, P, P, P, I64, P, P], ctypes.c_int),
-    "b2s_amg_w_pattern_d": ([I32, P, P, P, P, I32, P, P, P, P, I64, I64, P, P, P, P, P, P], ctypes.c_int),
+    "b2s_amg_p_pattern_d": ([I32, I32, P, P, P, I32, P, P, I64, P, P, P, I64, P, P], ctypes.c_int),
+    "b2s_amg_w_pattern_d": ([I32, I32, P, P, P, P, I32, P, P, P, P, I64, I64, P, P, P, P, P, P], ctypes.c_int),
+    "b2s_amg_pattern_warp_cols": ([I32], ctypes.c_int),
     "b2s_amg_r_workspace_bytes": ([I32], I64),
     "b2s_amg_r_pattern_d": ([I32, I32, P, P, I64, P, P, P, P, I64, P, P], ctypes.c_int),
     "b2s_amg_c_pattern_d": ([I32, P, P, P, P, I32, P, P, P, P, I64, I64, P, P, P, P, P, P, P], ctypes.c_int),

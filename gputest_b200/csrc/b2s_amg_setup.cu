@@ -604,6 +604,189 @@ __global__ void c_pattern_k(int na, const int32_t* __restrict__ r_rowptr, const 
   }
 }
 
+// ------------------------------------------------------------------ the same patterns, one warp per row
+// For levels of at most kWarpRowCols columns (the coarse levels, whose rows are dense and whose
+// terms one thread would walk one after another): a warp builds one row with a counter per
+// column in shared memory. The row's terms are a two-level walk - outer entries o of the row,
+// then the inner range of each - each term landing on a column. The warp counts the terms per
+// column (lanes take outer entries in turn), turns the counts into the sorted distinct columns
+// and their slot starts by one sweep over the columns, then places the terms 32 at a time in
+// the walk's order: a lane finds its outer entry by a binary search over the 32 outer entries'
+// running term counts, lanes landing on the same column take consecutive positions in lane
+// order (__match_any_sync), so every slot lists its terms in the walk's order - the order of
+// the thread-per-row kernels above, bit for bit.
+constexpr int kWarpRowCols = 2048;
+constexpr int kPatternWarps = 4;
+int g_warp_cols = kWarpRowCols;  // levels of at most this many columns are built one warp per row
+
+struct PTerms {  // P = A T: the A entries e of row i, each one term on column agg[col[e]]
+  const int32_t* rp;
+  const int32_t* cl;
+  const int32_t* agg;
+  __device__ int o0(int r) const { return rp[r]; }
+  __device__ int o1(int r) const { return rp[r + 1]; }
+  __device__ int i0(int o) const { return o; }
+  __device__ int i1(int o) const { return o + 1; }
+  __device__ int col(int x) const { return agg[cl[x]]; }
+};
+struct WTerms {  // W = A P: A entry e of row i, then P entry f of row col[e], on column p_idx[f]
+  const int32_t* rp;
+  const int32_t* cl;
+  const int32_t* p_ptr;
+  const int32_t* p_idx;
+  __device__ int o0(int r) const { return rp[r]; }
+  __device__ int o1(int r) const { return rp[r + 1]; }
+  __device__ int i0(int o) const { return p_ptr[cl[o]]; }
+  __device__ int i1(int o) const { return p_ptr[cl[o] + 1]; }
+  __device__ int col(int x) const { return p_idx[x]; }
+};
+struct CTerms {  // A_c = R W: R entry q of row I, then W entry s of row r_col[q], on column w_idx[s]
+  const int32_t* r_rowptr;
+  const int32_t* r_col;
+  const int32_t* w_ptr;
+  const int32_t* w_idx;
+  __device__ int o0(int r) const { return r_rowptr[r]; }
+  __device__ int o1(int r) const { return r_rowptr[r + 1]; }
+  __device__ int i0(int o) const { return w_ptr[r_col[o]]; }
+  __device__ int i1(int o) const { return w_ptr[r_col[o] + 1]; }
+  __device__ int col(int x) const { return w_idx[x]; }
+};
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  return v;
+}
+
+// pass 0: cnt_out[r] = distinct columns, tcnt[r] (if not null) = terms of row r. pass 1: idx (the distinct
+// columns, ascending, from c_ptr[r]), tptr (each slot's first term, from t_ptr[r]; tptr[c_nnz]
+// written by the last row), pay_o/pay_i (each term's outer and inner entry; pay_i may be null),
+// diag (if not null: the slot of column r, or where it would sit). Terms whose columns fall
+// outside [0, ncols) are not counted and raise *overflow (1); offsets that disagree with the
+// counts raise 2.
+template <class T>
+__global__ void __launch_bounds__(kPatternWarps * 32)
+    warp_pattern_k(T t, int nrows, int ncols, int pass, int32_t* __restrict__ cnt_out, int32_t* __restrict__ tcnt,
+                   const int32_t* __restrict__ c_ptr, const int32_t* __restrict__ t_ptr, int64_t c_cap, int64_t t_cap,
+                   int32_t* __restrict__ idx, int32_t* __restrict__ tptr, int32_t* __restrict__ pay_o,
+                   int32_t* __restrict__ pay_i, int32_t* __restrict__ diag, int32_t* __restrict__ overflow) {
+  __shared__ int32_t cnt_all[kPatternWarps][kWarpRowCols];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  int32_t* cnt = cnt_all[warp];
+  for (int c = lane; c < ncols; c += 32) cnt[c] = 0;
+  __syncwarp();
+  for (int r = blockIdx.x * kPatternWarps + warp; r < nrows; r += gridDim.x * kPatternWarps) {
+    const int o0 = t.o0(r), o1 = t.o1(r);
+    int fresh = 0, bad = 0;
+    int64_t my_terms = 0;
+    for (int o = o0 + lane; o < o1; o += 32) {
+      const int x1 = t.i1(o);
+      for (int x = t.i0(o); x < x1; ++x) {
+        const int c = t.col(x);
+        if (c < 0 || c >= ncols) {
+          bad = 1;
+          continue;
+        }
+        if (atomicAdd(cnt + c, 1) == 0) ++fresh;
+      }
+      my_terms += x1 - t.i0(o);
+    }
+    int m = fresh;
+    int64_t terms = my_terms;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+      m += __shfl_xor_sync(0xffffffffu, m, s);
+      terms += __shfl_xor_sync(0xffffffffu, terms, s);
+    }
+    const bool fail = __any_sync(0xffffffffu, bad) || terms > INT32_MAX;
+    __syncwarp();
+    if (fail) {
+      if (lane == 0) {
+        atomicExch(overflow, 1);
+        if (pass == 0) {
+          cnt_out[r] = 0;
+          if (tcnt != nullptr) tcnt[r] = 0;
+        }
+      }
+    } else if (pass == 0) {
+      if (lane == 0) {
+        cnt_out[r] = m;
+        if (tcnt != nullptr) tcnt[r] = (int32_t)terms;
+      }
+    } else {
+      const int64_t base = c_ptr[r], tb = t_ptr[r];
+      const bool ok = base + m <= c_cap && c_ptr[r + 1] - base == m && tb + terms <= t_cap &&
+                      t_ptr[r + 1] - tb == terms;
+      if (!ok) {
+        if (lane == 0) atomicExch(overflow, 2);
+      } else {
+        // distinct columns and slot starts; each counter becomes its slot's next position
+        int run_m = 0;
+        int64_t run_t = tb;
+        for (int c0 = 0; c0 < ncols; c0 += 32) {
+          const int c = c0 + lane;
+          const int v = c < ncols ? cnt[c] : 0;
+          const unsigned hit = __ballot_sync(0xffffffffu, v > 0);
+          const int incl = warp_incl_scan(v, lane);
+          if (v > 0) {
+            const int rank = run_m + __popc(hit & below);
+            idx[base + rank] = c;
+            tptr[base + rank] = (int32_t)(run_t + incl - v);
+            cnt[c] = (int32_t)(run_t + incl - v);
+          }
+          if (diag != nullptr && lane == 0 && r >= c0 && r < c0 + 32)
+            diag[r] = (int32_t)(base + run_m + __popc(hit & ((1u << (r - c0)) - 1u)));
+          run_m += __popc(hit);
+          run_t += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (diag != nullptr && lane == 0 && r >= ncols) diag[r] = (int32_t)(base + m);
+        if (r == nrows - 1 && lane == 0) tptr[base + m] = (int32_t)(tb + terms);
+        __syncwarp();
+        // the terms in the walk's order, 32 at a time
+        for (int ob = o0; ob < o1; ob += 32) {
+          const int o = ob + lane;
+          const int x0 = o < o1 ? t.i0(o) : 0;
+          const int len = o < o1 ? t.i1(o) - x0 : 0;
+          const int incl = warp_incl_scan(len, lane);
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          for (int tt0 = 0; tt0 < total; tt0 += 32) {
+            const int tt = tt0 + lane;
+            int lo = 0, hi = 31;  // the first outer entry whose running count exceeds tt
+#pragma unroll
+            for (int step = 0; step < 5; ++step) {
+              const int mid = (lo + hi) >> 1;
+              if (__shfl_sync(0xffffffffu, incl, mid) > tt) hi = mid;
+              else lo = mid + 1;
+            }
+            const int start = __shfl_sync(0xffffffffu, incl - len, lo);
+            const int xk = __shfl_sync(0xffffffffu, x0, lo);
+            const bool act = tt < total;
+            const int x = xk + (tt - start);
+            const int c = act ? t.col(x) : -1 - lane;
+            const unsigned peers = __match_any_sync(0xffffffffu, c);
+            const int rank = __popc(peers & below);
+            const int pos = act ? cnt[c] + rank : 0;
+            __syncwarp();
+            if (act && rank == 0) cnt[c] += __popc(peers);
+            __syncwarp();
+            if (act && pos >= tb && pos < tb + terms) {
+              pay_o[pos] = ob + lo;
+              if (pay_i != nullptr) pay_i[pos] = x;
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+    for (int c = lane; c < ncols; c += 32) cnt[c] = 0;
+    __syncwarp();
+  }
+}
+
 }  // namespace b2s
 
 using namespace b2s;
@@ -715,33 +898,48 @@ int b2s_amg_aggregate_d(int32_t n, const int32_t* rowptr, const int32_t* col, co
   return B2S_OK;
 }
 
-/* P and W patterns with their term lists, one thread per row (the order of the row-owned rebuild
- * kernels; see p_pattern_k / w_pattern_k). Each builder has two passes: pass 0 writes per-row
- * counts (pcnt; wcnt and tcnt), the caller scans them into p_ptr (w_ptr, t_ptr) and allocates;
- * pass 1 fills. *overflow (device int, not cleared here): 1 where a row exceeds the per-thread
- * capacity (64 distinct P columns, 128 distinct W columns), 2 where the offsets disagree with the
- * counts. */
-int b2s_amg_p_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* agg, int32_t pass,
-                        int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx, int32_t* p_tptr,
-                        int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s) {
-  if (n < 1 || !rp || !cl || !agg || !overflow || (pass == 0 && !pcnt) ||
+/* P and W patterns with their term lists (the order of the row-owned rebuild kernels; see
+ * p_pattern_k / w_pattern_k): one warp per row where P and W have at most g_warp_cols columns
+ * (ncols: the level's aggregates), else one thread per row. Each builder has two passes: pass 0
+ * writes per-row counts (pcnt; wcnt and tcnt), the caller scans them into p_ptr (w_ptr, t_ptr)
+ * and allocates; pass 1 fills. *overflow (device int, not cleared here): 1 where a row exceeds
+ * the per-thread capacity (64 distinct P columns, 128 distinct W columns), 2 where the offsets
+ * disagree with the counts. */
+int b2s_amg_p_pattern_d(int32_t n, int32_t ncols, const int32_t* rp, const int32_t* cl, const int32_t* agg,
+                        int32_t pass, int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx,
+                        int32_t* p_tptr, int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s) {
+  if (n < 1 || ncols < 1 || !rp || !cl || !agg || !overflow || (pass == 0 && !pcnt) ||
       (pass == 1 && (!p_ptr || !p_idx || !p_tptr || !p_tj)) || (pass != 0 && pass != 1))
     return B2S_ERR_ARG;
-  p_pattern_k<<<grid_for(n, 128), 128, 0, (cudaStream_t)s>>>(n, rp, cl, agg, pass, pcnt, p_ptr, p_cap, p_idx, p_tptr,
-                                                             p_tj, nnz, overflow);
+  cudaStream_t st = (cudaStream_t)s;
+  if (ncols <= g_warp_cols) {
+    warp_pattern_k<PTerms><<<grid_for((int64_t)n * 32, kPatternWarps * 32), kPatternWarps * 32, 0, st>>>(
+        PTerms{rp, cl, agg}, n, ncols, pass, pcnt, nullptr, p_ptr, rp, p_cap, nnz, p_idx, p_tptr, p_tj, nullptr,
+        nullptr, overflow);
+  } else {
+    p_pattern_k<<<grid_for(n, 128), 128, 0, st>>>(n, rp, cl, agg, pass, pcnt, p_ptr, p_cap, p_idx, p_tptr, p_tj, nnz,
+                                                  overflow);
+  }
   B2S_LAUNCH_CHECK();
   return B2S_OK;
 }
 
-int b2s_amg_w_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* p_ptr, const int32_t* p_idx,
-                        int32_t pass, int32_t* wcnt, int32_t* tcnt, const int32_t* w_ptr, const int32_t* t_ptr,
-                        int64_t w_cap, int64_t t_cap, int32_t* w_idx, int32_t* w_tptr, int32_t* w_tj, int32_t* w_te,
-                        int32_t* overflow, b2s_stream_t s) {
-  if (n < 1 || !rp || !cl || !p_ptr || !p_idx || !overflow || (pass == 0 && (!wcnt || !tcnt)) ||
+int b2s_amg_w_pattern_d(int32_t n, int32_t ncols, const int32_t* rp, const int32_t* cl, const int32_t* p_ptr,
+                        const int32_t* p_idx, int32_t pass, int32_t* wcnt, int32_t* tcnt, const int32_t* w_ptr,
+                        const int32_t* t_ptr, int64_t w_cap, int64_t t_cap, int32_t* w_idx, int32_t* w_tptr,
+                        int32_t* w_tj, int32_t* w_te, int32_t* overflow, b2s_stream_t s) {
+  if (n < 1 || ncols < 1 || !rp || !cl || !p_ptr || !p_idx || !overflow || (pass == 0 && (!wcnt || !tcnt)) ||
       (pass == 1 && (!w_ptr || !t_ptr || !w_idx || !w_tptr || !w_tj || !w_te)) || (pass != 0 && pass != 1))
     return B2S_ERR_ARG;
-  w_pattern_k<<<grid_for(n, 128), 128, 0, (cudaStream_t)s>>>(n, rp, cl, p_ptr, p_idx, pass, wcnt, tcnt, w_ptr, t_ptr,
-                                                             w_cap, t_cap, w_idx, w_tptr, w_tj, w_te, overflow);
+  cudaStream_t st = (cudaStream_t)s;
+  if (ncols <= g_warp_cols) {
+    warp_pattern_k<WTerms><<<grid_for((int64_t)n * 32, kPatternWarps * 32), kPatternWarps * 32, 0, st>>>(
+        WTerms{rp, cl, p_ptr, p_idx}, n, ncols, pass, wcnt, tcnt, w_ptr, t_ptr, w_cap, t_cap, w_idx, w_tptr, w_tj,
+        w_te, nullptr, overflow);
+  } else {
+    w_pattern_k<<<grid_for(n, 128), 128, 0, st>>>(n, rp, cl, p_ptr, p_idx, pass, wcnt, tcnt, w_ptr, t_ptr, w_cap,
+                                                  t_cap, w_idx, w_tptr, w_tj, w_te, overflow);
+  }
   B2S_LAUNCH_CHECK();
   return B2S_OK;
 }
@@ -780,11 +978,12 @@ int b2s_amg_r_pattern_d(int32_t n, int32_t na, const int32_t* p_ptr, const int32
   return B2S_OK;
 }
 
-/* Pattern and term lists of A_c = R W, one thread per coarse row (the order of the row-owned
- * Galerkin kernel; see c_pattern_k), in two passes like the P and W builders: pass 0 writes
- * ccnt and tcnt, the caller scans them into c_ptr and t_ptr and allocates; pass 1 writes c_idx,
- * c_diag [na], c_tptr [c_nnz + 1], c_te and c_ts. *overflow: 1 where a row has more than 128
- * distinct columns, 2 where the offsets disagree with the counts. */
+/* Pattern and term lists of A_c = R W (the order of the row-owned Galerkin kernel; see
+ * c_pattern_k), one warp per coarse row where na <= g_warp_cols, else one thread per row, in
+ * two passes like the P and W builders: pass 0 writes ccnt and tcnt, the caller scans them into
+ * c_ptr and t_ptr and allocates; pass 1 writes c_idx, c_diag [na], c_tptr [c_nnz + 1], c_te and
+ * c_ts. *overflow: 1 where a row has more than 128 distinct columns (one thread per row), 2 where
+ * the offsets disagree with the counts. */
 int b2s_amg_c_pattern_d(int32_t na, const int32_t* r_rowptr, const int32_t* r_col, const int32_t* w_ptr,
                         const int32_t* w_idx, int32_t pass, int32_t* ccnt, int32_t* tcnt, const int32_t* c_ptr,
                         const int32_t* t_ptr, int64_t c_cap, int64_t t_cap, int32_t* c_idx, int32_t* c_diag,
@@ -793,11 +992,26 @@ int b2s_amg_c_pattern_d(int32_t na, const int32_t* r_rowptr, const int32_t* r_co
       (pass == 1 && (!c_ptr || !t_ptr || !c_idx || !c_diag || !c_tptr || !c_te || !c_ts)) ||
       (pass != 0 && pass != 1))
     return B2S_ERR_ARG;
-  c_pattern_k<<<grid_for(na, 128), 128, 0, (cudaStream_t)s>>>(na, r_rowptr, r_col, w_ptr, w_idx, pass, ccnt, tcnt,
-                                                              c_ptr, t_ptr, c_cap, t_cap, c_idx, c_diag, c_tptr,
-                                                              c_te, c_ts, overflow);
+  cudaStream_t st = (cudaStream_t)s;
+  if (na <= g_warp_cols) {
+    warp_pattern_k<CTerms><<<grid_for((int64_t)na * 32, kPatternWarps * 32), kPatternWarps * 32, 0, st>>>(
+        CTerms{r_rowptr, r_col, w_ptr, w_idx}, na, na, pass, ccnt, tcnt, c_ptr, t_ptr, c_cap, t_cap, c_idx, c_tptr,
+        c_te, c_ts, c_diag, overflow);
+  } else {
+    c_pattern_k<<<grid_for(na, 128), 128, 0, st>>>(na, r_rowptr, r_col, w_ptr, w_idx, pass, ccnt, tcnt, c_ptr, t_ptr,
+                                                   c_cap, t_cap, c_idx, c_diag, c_tptr, c_te, c_ts, overflow);
+  }
   B2S_LAUNCH_CHECK();
   return B2S_OK;
+}
+
+/* The largest column count whose pattern builders run one warp per row (default and maximum
+ * kWarpRowCols; 0: one thread per row always); ncols < 0 only queries. Returns the previous
+ * value. Process-wide and not synchronised: set it before the builders run. */
+int b2s_amg_pattern_warp_cols(int32_t ncols) {
+  const int prev = g_warp_cols;
+  if (ncols >= 0) g_warp_cols = ncols < kWarpRowCols ? ncols : kWarpRowCols;
+  return prev;
 }
 
 /* Exclusive scan of n int32 counts into out[0..n] (out[n] the total), for the pattern builders. */

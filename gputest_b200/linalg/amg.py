@@ -203,10 +203,12 @@ def row_products(rp, cl, agg, na, stream=None):
     row's diagonal) in place of ``c_keys``, ``conflicts`` (the next level's aggregation work-space
     bound: A_c's entries plus its squared row lengths) and ``check``, a device int that is
     nonzero if A_c's fill pass found its offsets inconsistent (read at the caller's next
-    synchronisation). Two host synchronisations. Where a row exceeds the P or W kernel (64
-    distinct P columns, 128 distinct W columns) the result is None; where it exceeds the R or A_c kernel (256 R
-    entries, 128 distinct A_c columns), or a term list ``TERM_CAP``, it holds P and W only, with
-    ``complete`` False (``product_patterns`` adds R and A_c from sorted keys)."""
+    synchronisation). Two host synchronisations. Levels of at most ``b2s_amg_pattern_warp_cols``
+    (2048) aggregates are built one warp per row, larger ones one thread per row. Where a row
+    exceeds a thread's capacity (64 distinct P columns, 128 distinct W columns) the result is
+    None; where an R row has over 256 entries, an A_c row built by one thread over 128 distinct
+    columns, or a term list over ``TERM_CAP`` terms, it holds P and W only, with ``complete``
+    False (``product_patterns`` adds R and A_c from sorted keys)."""
     import torch
 
     L = _lib.lib()
@@ -227,15 +229,15 @@ def row_products(rp, cl, agg, na, stream=None):
     # P: counts, offsets, then the fill into room for nnz entries (a P row has at most as many
     # entries as the A row), so the sizes are read once, together with W's
     pcnt = e32(n)
-    _lib.check(L.b2s_amg_p_pattern_d(n, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 0, pcnt.data_ptr(), None, 0,
-                                     None, None, None, nnz, ov.data_ptr(), sp_), "b2s_amg_p_pattern_d")
+    _lib.check(L.b2s_amg_p_pattern_d(n, na, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 0, pcnt.data_ptr(), None,
+                                     0, None, None, None, nnz, ov.data_ptr(), sp_), "b2s_amg_p_pattern_d")
     p_ptr = scan(pcnt, n)
     p_idx, p_tptr, p_tj = e32(nnz), e32(nnz + 1), e32(nnz)
-    _lib.check(L.b2s_amg_p_pattern_d(n, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 1, None, p_ptr.data_ptr(),
+    _lib.check(L.b2s_amg_p_pattern_d(n, na, rp.data_ptr(), cl.data_ptr(), agg.data_ptr(), 1, None, p_ptr.data_ptr(),
                                      nnz, p_idx.data_ptr(), p_tptr.data_ptr(), p_tj.data_ptr(), nnz, ov.data_ptr(),
                                      sp_), "b2s_amg_p_pattern_d")
     wcnt, tcnt = e32(n), e32(n)
-    _lib.check(L.b2s_amg_w_pattern_d(n, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 0,
+    _lib.check(L.b2s_amg_w_pattern_d(n, na, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 0,
                                      wcnt.data_ptr(), tcnt.data_ptr(), None, None, 0, 0, None, None, None, None,
                                      ov.data_ptr(), sp_), "b2s_amg_w_pattern_d")
     w_ptr, t_ptr = scan(wcnt, n), scan(tcnt, n)
@@ -244,8 +246,8 @@ def row_products(rp, cl, agg, na, stream=None):
         return None
     p_nnz, w_nnz, w_terms = int(h[1]), int(h[2]), int(h[3])
     w_idx, w_tptr, w_tj, w_te = e32(w_nnz), e32(w_nnz + 1), e32(w_terms), e32(w_terms)
-    _lib.check(L.b2s_amg_w_pattern_d(n, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 1, None,
-                                     None, w_ptr.data_ptr(), t_ptr.data_ptr(), w_nnz, w_terms, w_idx.data_ptr(),
+    _lib.check(L.b2s_amg_w_pattern_d(n, na, rp.data_ptr(), cl.data_ptr(), p_ptr.data_ptr(), p_idx.data_ptr(), 1,
+                                     None, None, w_ptr.data_ptr(), t_ptr.data_ptr(), w_nnz, w_terms, w_idx.data_ptr(),
                                      w_tptr.data_ptr(), w_tj.data_ptr(), w_te.data_ptr(), ov.data_ptr(), sp_),
                "b2s_amg_w_pattern_d")
     out = {"p_ptr": p_ptr, "p_idx": p_idx[:p_nnz], "p_tptr": p_tptr[:p_nnz + 1], "p_tj": p_tj[:nnz],
@@ -433,11 +435,6 @@ class AMGHierarchy:
     """
 
     ROW_PATTERNS = True  # device set-up: the products' patterns by the per-row kernels where rows fit them
-    # Levels with fewer rows take the sorted keys: one thread per row walks a dense coarse row's
-    # terms one after another (measured on the 131k cavity's hierarchy: 1.0 ms by the kernels
-    # against about 4 ms by the keys at 32,768 rows; 2.5 against 2 ms at 4,400, 4.3 against
-    # 1.7 ms at 507).
-    ROW_KERNEL_MIN_ROWS = 8192
 
     def __init__(self, A_host, perm, rowptr, col, diag_slot, val, slot_ref, singular=False, theta=0.08,
                  max_coarse=150, max_levels=20, sweeps=2, omega=0.8, groups=None, group_singular=None):
@@ -698,8 +695,7 @@ class AMGHierarchy:
             na = int(ih[0])
             if na >= n * 0.9:
                 break
-            kernels = self._row_patterns and n >= cls.ROW_KERNEL_MIN_ROWS
-            pat = row_products(lv_rp, lv_cl, agg, na, stream) if kernels else None
+            pat = row_products(lv_rp, lv_cl, agg, na, stream) if self._row_patterns else None
             if pat is None or not pat["complete"]:
                 pat = product_patterns(lv_rp64.to(torch.int64), lv_cl64.to(torch.int64), agg.to(torch.int64), na,
                                        pw=pat)

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define B2S_ABI_VERSION 4
+#define B2S_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define B2S_API __attribute__((visibility("default")))
@@ -477,17 +477,19 @@ B2S_API int b2s_amg_level_rebuild_d(const b2s_amg_level* L, const int32_t* crow,
 B2S_API int b2s_amg_coarse_inverse_d(const b2s_amg* h, void* work, int64_t work_bytes, b2s_stream_t s);
 
 /* The patterns of P = A T and W = A P of one level, with the term lists of the row-owned rebuild
- * (b2s_amg_level), one thread per row: rp/cl the level's CSR in stored order, agg its aggregates.
+ * (b2s_amg_level): rp/cl the level's CSR in stored order, agg its aggregates, ncols their number
+ * (one warp per row, with a counter per column in shared memory, when ncols is at most
+ * b2s_amg_pattern_warp_cols - 2048 by default; else one thread per row).
  * Two passes each: pass 0 writes per-row counts (pcnt; wcnt = W entries, tcnt = W terms), which
  * the caller scans (b2s_scan_counts_d) into p_ptr (w_ptr, t_ptr) and allocates from; pass 1
  * fills p_idx, p_tptr, p_tj (w_idx, w_tptr, w_tj, w_te), never past p_cap/nnz (w_cap/t_cap).
  * *overflow (device int, not cleared): 1 where a row has more than 64 distinct P columns or 128
- * distinct W columns, 2 where the offsets disagree with the counts; the caller then builds the
- * level another way. */
-B2S_API int b2s_amg_p_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* agg, int32_t pass,
-                                int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx, int32_t* p_tptr,
-                                int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s);
-B2S_API int b2s_amg_w_pattern_d(int32_t n, const int32_t* rp, const int32_t* cl, const int32_t* p_ptr,
+ * distinct W columns (one thread per row), 2 where the offsets disagree with the counts; the
+ * caller then builds the level another way. */
+B2S_API int b2s_amg_p_pattern_d(int32_t n, int32_t ncols, const int32_t* rp, const int32_t* cl, const int32_t* agg,
+                                int32_t pass, int32_t* pcnt, const int32_t* p_ptr, int64_t p_cap, int32_t* p_idx,
+                                int32_t* p_tptr, int32_t* p_tj, int64_t nnz, int32_t* overflow, b2s_stream_t s);
+B2S_API int b2s_amg_w_pattern_d(int32_t n, int32_t ncols, const int32_t* rp, const int32_t* cl, const int32_t* p_ptr,
                                 const int32_t* p_idx, int32_t pass, int32_t* wcnt, int32_t* tcnt, const int32_t* w_ptr,
                                 const int32_t* t_ptr, int64_t w_cap, int64_t t_cap, int32_t* w_idx, int32_t* w_tptr,
                                 int32_t* w_tj, int32_t* w_te, int32_t* overflow, b2s_stream_t s);
@@ -499,15 +501,20 @@ B2S_API int64_t b2s_amg_r_workspace_bytes(int32_t na);
 B2S_API int b2s_amg_r_pattern_d(int32_t n, int32_t na, const int32_t* p_ptr, const int32_t* p_idx, int64_t p_nnz,
                                 int32_t* r_rowptr, int32_t* r_col, int32_t* r_from_p, void* work, int64_t work_bytes,
                                 int32_t* overflow, b2s_stream_t s);
-/* The pattern of A_c = R W (the Galerkin product P^T A P, amg.py:102) with its term lists, one
- * thread per coarse row, in the two passes of the P and W builders: pass 0 writes ccnt (A_c
+/* The pattern of A_c = R W (the Galerkin product P^T A P, amg.py:102) with its term lists (one
+ * warp per coarse row as for P and W, else one thread), in the two passes of the P and W builders: pass 0 writes ccnt (A_c
  * entries) and tcnt (terms) per row; pass 1 fills c_idx, c_diag [na] (the slot of each row's
  * diagonal), c_tptr [c_nnz + 1], c_te (R entries) and c_ts (W entries). *overflow: 1 where a row
- * has more than 128 distinct columns, 2 where the offsets disagree with the counts. */
+ * has more than 128 distinct columns (one thread per row), 2 where the offsets disagree with the
+ * counts. */
 B2S_API int b2s_amg_c_pattern_d(int32_t na, const int32_t* r_rowptr, const int32_t* r_col, const int32_t* w_ptr,
                                 const int32_t* w_idx, int32_t pass, int32_t* ccnt, int32_t* tcnt, const int32_t* c_ptr,
                                 const int32_t* t_ptr, int64_t c_cap, int64_t t_cap, int32_t* c_idx, int32_t* c_diag,
                                 int32_t* c_tptr, int32_t* c_te, int32_t* c_ts, int32_t* overflow, b2s_stream_t s);
+/* The largest column count (aggregates) whose P, W and A_c builders run one warp per row:
+ * default and maximum 2048, 0 for one thread per row always; ncols < 0 only queries. Returns the
+ * previous value. Process-wide and not synchronised: set it before the builders run. */
+B2S_API int b2s_amg_pattern_warp_cols(int32_t ncols);
 /* Exclusive scan of n int32 counts into out[0..n], out[n] the total. */
 B2S_API int64_t b2s_scan_workspace_bytes(int32_t n);
 B2S_API int b2s_scan_counts_d(int32_t n, const int32_t* counts, int32_t* out, void* work, int64_t work_bytes,

@@ -17,6 +17,18 @@ def _cuda():
         pytest.skip("no CUDA device")
 
 
+@pytest.fixture(params=[2048, 0], ids=["warp-rows", "thread-rows"])
+def warp_cols(request):
+    """The pattern builders' warp-per-row threshold for one test (2048: the default, coarse levels
+    one warp per row; 0: one thread per row on every level), restored afterwards."""
+    from gputest_b200 import _lib
+
+    L = _lib.lib()
+    prev = L.b2s_amg_pattern_warp_cols(request.param)
+    yield request.param
+    L.b2s_amg_pattern_warp_cols(prev)
+
+
 def _device_csr(A, rng):
     """A's rows on the device with each row's entries shuffled (the device code may not rely on
     sorted columns), plus the diagonal slots."""
@@ -88,18 +100,14 @@ def _meshes():
 
 @pytest.mark.parametrize("which", [0, 1])
 @pytest.mark.parametrize("theta", [0.08, 0.0])
-@pytest.mark.parametrize("all_kernels", [False, True])
-def test_device_hierarchy_equals_the_host_hierarchy(which, theta, all_kernels, monkeypatch):
+def test_device_hierarchy_equals_the_host_hierarchy(which, theta, warp_cols):
     """Both set-ups from the same pressure-correction matrix: the same levels, aggregates,
-    patterns and strong flags, and the same V-cycle bit for bit; with the products' patterns by
-    the per-row kernels on every level that fits them, or on the large levels only (the
-    default)."""
+    patterns and strong flags, and the same V-cycle bit for bit; with the products' patterns
+    built one warp per row on the levels of at most 2048 aggregates, or one thread per row on
+    every level."""
     import torch
 
     from gputest_b200.linalg.amg import AMGHierarchy
-
-    if all_kernels:
-        monkeypatch.setattr(AMGHierarchy, "ROW_KERNEL_MIN_ROWS", 0)
 
     s = _pressure_system(_meshes()[which])
     fv = s.fv
@@ -192,14 +200,15 @@ def test_partial_reaggregation_equals_a_full_device_set_up():
 
 
 @pytest.mark.parametrize("kind,n,seed", [("grid", 2500, 11), ("grid", 10000, 14), ("random", 3000, 12)])
-def test_row_product_kernels_equal_the_key_based_patterns(kind, n, seed):
-    """``row_products`` (one thread per row: P, W, R = P^T and A_c) against the sorted-key
-    construction of ``product_patterns`` on the same level and aggregates: every pattern and term
-    list equal where every row fits the kernels (at most 64 distinct P columns, 128 distinct W
-    columns, 256 R entries and 128 distinct A_c columns), the diagonal slots and the next level's
-    conflict bound from the same pattern; P and W alone where an A_c row does not fit (the random
-    graph), completed by the sorted keys; the level handed back (None) where a P row does not
-    fit."""
+def test_row_product_kernels_equal_the_key_based_patterns(kind, n, seed, warp_cols):
+    """``row_products`` (P, W, R = P^T and A_c by the per-row kernels) against the sorted-key
+    construction of ``product_patterns`` on the same level and aggregates, one warp per row and
+    one thread per row: every pattern and term list equal, the diagonal slots and the next
+    level's conflict bound from the same pattern. One thread per row handles at most 64 distinct
+    P columns, 128 distinct W columns and 128 distinct A_c columns a row (a warp has no such
+    limit); where an A_c row does not fit (the random graph: up to 550 columns) P and W come back
+    alone and the sorted keys complete them; where a P row does not fit the level is handed back
+    (None)."""
     import scipy.sparse as sp
     import torch
 
@@ -216,9 +225,12 @@ def test_row_product_kernels_equal_the_key_based_patterns(kind, n, seed):
     Pp = amg._pattern(amg._pattern(A) @ T)
     Wp = amg._pattern(amg._pattern(A) @ Pp)
     Cp = amg._pattern(Pp.T @ Wp)
-    pw_fits = int(np.diff(Pp.indptr).max()) <= 64 and int(np.diff(Wp.indptr).max()) <= 128
-    rc_fits = int(np.bincount(Pp.indices, minlength=na).max()) <= 256 and int(np.diff(Cp.indptr).max()) <= 128
-    assert pw_fits and rc_fits == (kind == "grid")  # the random graph's A_c rows: up to 550 columns
+    by_warp = na <= warp_cols
+    assert na <= 2048
+    pw_fits = by_warp or (int(np.diff(Pp.indptr).max()) <= 64 and int(np.diff(Wp.indptr).max()) <= 128)
+    rc_fits = int(np.bincount(Pp.indices, minlength=na).max()) <= 256 and (
+        by_warp or int(np.diff(Cp.indptr).max()) <= 128)
+    assert pw_fits and rc_fits == (by_warp or kind == "grid")
     agg = torch.as_tensor(agg_h, dtype=torch.int32, device="cuda")
     pw = amg.row_products(rp, cl, agg, na)
     assert pw is not None and pw["complete"] == rc_fits
@@ -235,21 +247,29 @@ def test_row_product_kernels_equal_the_key_based_patterns(kind, n, seed):
         cl_len = ref["c_ptr"][1:] - ref["c_ptr"][:-1]
         assert pw["conflicts"] == ref["c_idx"].numel() + int((cl_len * cl_len).sum())
     # a star of 70 nodes, each its own aggregate: the centre's P row has 70 distinct columns,
-    # over the P kernel's 64, and the level is handed back
+    # over one thread's 64 (the level is handed back), within a warp's reach
     star = sp.csr_matrix((np.ones(138), (np.r_[np.zeros(69, int), np.arange(1, 70)],
                                          np.r_[np.arange(1, 70), np.zeros(69, int)])), shape=(70, 70)) + sp.eye(70)
     star = sp.csr_matrix(star)
     star.sort_indices()
     rp2, cl2, _, _, _ = _device_csr(star, rng)
-    assert amg.row_products(rp2, cl2, torch.arange(70, dtype=torch.int32, device="cuda"), 70) is None
+    agg2 = torch.arange(70, dtype=torch.int32, device="cuda")
+    got = amg.row_products(rp2, cl2, agg2, 70)
+    if by_warp:
+        ref = amg.product_patterns(rp2.long(), cl2.long(), agg2.long(), 70)
+        assert got["complete"] and all(torch.equal(got[k].long(), ref[k].long()) for k in ("p_idx", "w_idx", "c_idx", "c_ts"))
+    else:
+        assert got is None
 
 
-@pytest.mark.parametrize("m,why", [(300, "R row"), (256, "A_c row")])
-def test_row_products_hand_r_and_a_c_back_where_a_row_does_not_fit(m, why):
-    """A path of m nodes whose even nodes form aggregate 0 and whose odd nodes are singletons: P
-    and W fit the kernels, but R's row 0 holds every node (over 256 entries for m = 300) or A_c's
-    row 0 every aggregate (129 distinct columns for m = 256, over 128). P and W come back with
-    ``complete`` False, and ``product_patterns`` completes them to the key-based level."""
+@pytest.mark.parametrize("m", [300, 256])
+def test_row_products_hand_r_and_a_c_back_where_a_row_does_not_fit(m, warp_cols):
+    """A path of m nodes whose even nodes form aggregate 0 and whose odd nodes are singletons:
+    P and W fit every kernel, but R's row 0 holds every node (over 256 entries for m = 300), or
+    A_c's row 0 every aggregate of the path (129 distinct columns for m = 256: over one thread's
+    128, within a warp's reach). Where a row does not fit, P and W come back with ``complete``
+    False and ``product_patterns`` completes them; either way the level equals the key-based
+    one."""
     import scipy.sparse as sp
     import torch
 
@@ -264,10 +284,10 @@ def test_row_products_hand_r_and_a_c_back_where_a_row_does_not_fit(m, why):
     rp, cl, _, _, _ = _device_csr(A, np.random.default_rng(m))
     agg = torch.as_tensor(agg_h, dtype=torch.int32, device="cuda")
     pw = amg.row_products(rp, cl, agg, na)
-    assert pw is not None and not pw["complete"], why
-    got = amg.product_patterns(rp.long(), cl.long(), agg.long(), na, pw=pw)
+    assert pw is not None and pw["complete"] == (m == 256 and warp_cols > 0)
+    got = pw if pw["complete"] else amg.product_patterns(rp.long(), cl.long(), agg.long(), na, pw=pw)
     ref = amg.product_patterns(rp.long(), cl.long(), agg.long(), na)
-    for k in ("p_ptr", "p_idx", "w_ptr", "w_idx", "r_rowptr", "r_col", "r_from_p", "c_ptr", "c_idx", "c_keys"):
+    for k in ("p_ptr", "p_idx", "w_ptr", "w_idx", "r_rowptr", "r_col", "r_from_p", "c_ptr", "c_idx"):
         assert torch.equal(got[k].long(), ref[k]), k
     for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te", "c_tptr", "c_te", "c_ts"):
         assert torch.equal(got[k], ref[k]), k
