@@ -144,15 +144,26 @@ __global__ void conflict_lists_k(AggGraph g, const int32_t* __restrict__ off, co
 // root, kRoot once all are decided "not a root"; -1 when the poll budget ran out or another
 // thread reported an error. A poll reads the list from the first entry found undecided on (the
 // ones before it are decided "not a root" and stay so); the list is read-only (cached), the
-// decisions are relaxed loads at device scope, issued together.
+// decisions are relaxed loads at device scope, kPollBatch of them issued before any is tested
+// (straight-line loads, the last entry repeated past the list's end), so a poll costs a few
+// load latencies rather than one per entry.
+constexpr int kPollBatch = 8;
+
 __device__ int decide_node(const int32_t* __restrict__ lists, int k0, int k1, const int32_t* status, int64_t limit,
                            int64_t& polls, const int32_t* err) {
   for (;;) {
     int first = -1;
-    for (int k = k0; k < k1; ++k) {
-      const int32_t s = ld_relaxed(status + __ldg(lists + k));
-      if (s == kRoot) return kNotRoot;
-      if (s == kUndecided && first < 0) first = k;
+    for (int k = k0; k < k1; k += kPollBatch) {
+      int32_t s[kPollBatch];
+#pragma unroll
+      for (int j = 0; j < kPollBatch; ++j) s[j] = ld_relaxed(status + __ldg(lists + min(k + j, k1 - 1)));
+      bool root = false;
+#pragma unroll
+      for (int j = 0; j < kPollBatch; ++j) {
+        root = root || s[j] == kRoot;
+        if (first < 0 && k + j < k1 && s[j] == kUndecided) first = k + j;
+      }
+      if (root) return kNotRoot;
     }
     if (first < 0) return kRoot;
     if (++polls > limit) return -1;
