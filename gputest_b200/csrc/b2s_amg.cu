@@ -2,9 +2,9 @@
 //
 // The reference builds its hierarchy on the host every 10 outer iterations
 // (flowtrace/linalg/amg.py:80-117, flowtrace/unstructured/simple.py:624-628). Here the
-// aggregates and the sparsity patterns of P, W = A P and A_c = P^T A P are fixed once (the
-// greedy aggregation below runs on the host at set-up), and every numeric quantity is rebuilt
-// on the device from the current matrix values:
+// aggregates and the sparsity patterns of P, W = A P and A_c = P^T A P come from a set-up (the
+// device set-up of b2s_amg_setup.cu, or the host one with b2s_host_aggregate below), and every
+// numeric quantity is rebuilt on the device from the current matrix values:
 //   D^-1, the spectral radius of D^-1 A (15 power iterations from a fixed start vector, as
 //   amg.py:69-77), P = T - 4/(3 rho) D^-1 A T (amg.py:95-101), R = P^T, A_c = R (A P), and the
 //   inverse of the coarsest matrix (shifted by 1e-10 mean|diag| when singular, amg.py:106-112).

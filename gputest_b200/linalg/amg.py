@@ -289,7 +289,8 @@ def product_patterns(rp, cl, agg, na, cap=TERM_CAP, pw=None):
     with the term lists of ``term_lists``, computed from sorted distinct keys instead of SciPy
     products: every structure the device set-up needs, on the tensors' device (four host
     synchronisations: the sizes of the products). ``pw``: the P and W parts already built by
-    ``row_patterns``. Returns a dict of int64 tensors (patterns: p_ptr/p_idx, w_ptr/w_idx,
+    ``row_products`` (which hands a level back with P and W alone where an R or A_c row does
+    not fit its kernels). Returns a dict of int64 tensors (patterns: p_ptr/p_idx, w_ptr/w_idx,
     c_ptr/c_idx, r_rowptr/r_col/r_from_p) and int32 term lists (None where a list would exceed
     ``cap`` terms)."""
     import torch
