@@ -181,3 +181,51 @@ def test_product_patterns_equal_the_scipy_patterns_and_term_lists():
     np.testing.assert_array_equal(got["r_from_p"].numpy(), order)
     for k, v in ref.items():
         np.testing.assert_array_equal(got[k].numpy(), v.numpy(), err_msg=k)
+
+
+def _shuffled_level(seed, n):
+    """A grid level in "device" order (rows renumbered, each row's entries shuffled) with its
+    greedy aggregates: (rp, cl, agg, na) as int64 torch tensors on the CPU and na."""
+    import torch
+
+    A = _graph(seed, n, "grid")
+    n = A.shape[0]
+    agg, na = amg.aggregate(amg.strength(A, 0.08))
+    rng = np.random.default_rng(seed + 1)
+    perm = rng.permutation(n)
+    iperm = np.empty(n, dtype=np.int64)
+    iperm[perm] = np.arange(n)
+    rl = np.diff(A.indptr)
+    rp = np.concatenate([[0], np.cumsum(rl[perm])])
+    src = np.concatenate([A.indptr[perm[i]] + rng.permutation(rl[perm[i]]) for i in range(n)])
+    t = lambda a: torch.as_tensor(np.asarray(a, dtype=np.int64))  # noqa: E731
+    return t(rp), t(iperm[A.indices[src]]), t(agg[perm]), na
+
+
+def test_product_patterns_complete_a_level_handed_back_with_p_and_w_only():
+    """Where an R or A_c row does not fit the per-row kernels, ``row_products`` hands the level
+    back with P and W alone (int32 patterns, ``complete`` False); ``product_patterns`` adds R and
+    A_c from sorted keys, and the level equals the key-based construction of all four."""
+    import torch
+
+    rp, cl, agg, na = _shuffled_level(11, 1600)
+    full = amg.product_patterns(rp, cl, agg, na)
+    pw = {k: full[k].to(torch.int32) for k in ("p_ptr", "p_idx", "w_ptr", "w_idx")}
+    pw.update({k: full[k] for k in ("p_tptr", "p_tj", "w_tptr", "w_tj", "w_te")}, complete=False)
+    got = amg.product_patterns(rp, cl, agg, na, pw=pw)
+    assert set(got) == set(full)
+    for k, v in full.items():
+        assert (got[k] is None) == (v is None), k
+        if v is not None:
+            assert torch.equal(got[k].long(), v.long()), k
+
+
+def test_pattern_checks_raise_on_an_inconsistent_fill():
+    """The A_c fill passes' consistency flags, read at the set-up's next synchronisation: zero
+    flags (or none) pass, any nonzero flag raises."""
+    import torch
+
+    amg._pattern_checks(torch.zeros(0, dtype=torch.int32))
+    amg._pattern_checks(torch.zeros(3, dtype=torch.int32))
+    with pytest.raises(RuntimeError, match="A_c pattern kernel"):
+        amg._pattern_checks(torch.tensor([0, 2, 0], dtype=torch.int32))
