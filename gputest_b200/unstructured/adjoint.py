@@ -364,8 +364,12 @@ class DeviceAdjoint:
     # ---------------------------------------------------------------- GMRES
     def solve(self, rhs, tol=1e-11, restart=60, maxiter=2000, history=None):
         """lambda with (dR/dx)^T lambda = rhs: flexible restarted GMRES (the preconditioner
-        contains inner Krylov solves; modified Gram-Schmidt, Givens rotations). Returns (lambda,
-        iterations, relative residual); ``history`` (a list) receives the residual per cycle."""
+        contains inner Krylov solves; Givens rotations). Each new basis vector is orthogonalised
+        by classical Gram-Schmidt applied twice - two products with the stacked basis and one
+        read-back of the Hessenberg column per iteration, instead of a dot product and a
+        read-back per basis vector - which is as accurate as modified Gram-Schmidt. Returns
+        (lambda, iterations, relative residual); ``history`` (a list) receives the residual per
+        cycle."""
         import torch
 
         x = torch.zeros_like(rhs)
@@ -373,6 +377,7 @@ class DeviceAdjoint:
         if bnorm == 0.0:
             return x, 0, 0.0
         its, rel = 0, 1.0
+        V = torch.empty((restart + 1, rhs.numel()), dtype=rhs.dtype, device=rhs.device)
         while its < maxiter:
             r = rhs - self.vjp(x)
             beta = float(torch.linalg.vector_norm(r))
@@ -381,7 +386,7 @@ class DeviceAdjoint:
                 history.append((its, rel))
             if rel < tol:
                 break
-            V = [r / beta]
+            V[0] = r / beta
             Z = []
             H = np.zeros((restart + 1, restart))
             cs, sn = np.zeros(restart), np.zeros(restart)
@@ -392,11 +397,14 @@ class DeviceAdjoint:
                 z = self.precondition(V[k])
                 Z.append(z)
                 w = self.vjp(z)
-                for i in range(k + 1):
-                    H[i, k] = float(torch.dot(w, V[i]))
-                    w = w - H[i, k] * V[i]
-                H[k + 1, k] = float(torch.linalg.vector_norm(w))
-                V.append(w / H[k + 1, k] if H[k + 1, k] > 0 else w)
+                Vk = V[: k + 1]
+                h = Vk @ w
+                w = w - Vk.T @ h
+                h2 = Vk @ w
+                w = w - Vk.T @ h2
+                hw = torch.cat([h + h2, torch.linalg.vector_norm(w).view(1)]).cpu().numpy()
+                H[: k + 2, k] = hw
+                V[k + 1] = w / hw[k + 1] if hw[k + 1] > 0 else w
                 for i in range(k):
                     a, b = H[i, k], H[i + 1, k]
                     H[i, k], H[i + 1, k] = cs[i] * a + sn[i] * b, -sn[i] * a + cs[i] * b
@@ -410,8 +418,7 @@ class DeviceAdjoint:
                 if rel < tol or its >= maxiter:
                     break
             y = np.linalg.solve(np.triu(H[:k_used, :k_used]), e[:k_used])
-            for i in range(k_used):
-                x = x + float(y[i]) * Z[i]
+            x = x + torch.stack(Z).T @ torch.as_tensor(y, dtype=rhs.dtype, device=rhs.device)
         r = rhs - self.vjp(x)
         return x, its, float(torch.linalg.vector_norm(r)) / bnorm
 
