@@ -259,7 +259,8 @@ class DeviceAdjoint:
         # the right-preconditioned GMRES stalled on fine grids (a CPU emulation of this solve on
         # the 256x64 correlated-porosity channel: relative residual 0.999 after 1200 iterations,
         # even with exact inner solves; 787 iterations to 1e-10 with the relaxed one, whose
-        # Jacobi-BiCGSTAB also needs 4 iterations a solve instead of 108).
+        # Jacobi-BiCGSTAB also needs 4 iterations a solve instead of 108; on the 512x128 channel
+        # the relaxed one stalls too, at 0.98).
         t = fv.t
         val = s.val_A.clone()
         dslot = t["slot_diag"].long()
