@@ -1,5 +1,5 @@
-"""The adjoint's flexible restarted GMRES (``DeviceAdjoint.solve``: modified Gram-Schmidt, Givens
-rotations, right preconditioning by a sweep that may change between calls) on the CPU, with the
+"""The adjoint's flexible restarted GMRES (``DeviceAdjoint.solve``: classical Gram-Schmidt applied
+twice, Givens rotations, right preconditioning by a sweep that may change between calls) on the CPU, with the
 operator and the preconditioner given as plain functions in place of the CUDA VJP and the
 transposed SIMPLE sweep."""
 
